@@ -1,0 +1,395 @@
+// Optic-lobe rate step for sm_100a: CSR SpMV/SpMM y = W_rr @ dr fused with the rate update
+// (flyverse/optic.py:_substep, optic.py:525-551; neural.cu:62-88), the held-input products
+// (optic.py:579-580, 599-602) and the reference-compatible elementwise / CSR launchers.
+//
+// Layout: state [m][batch] (unit-major, fly-minor). One warp owns one CSR row for all flies: a
+// chunk of 32 (col, w) entries is loaded coalesced, then broadcast by shuffle; each lane gathers
+// FPL consecutive flies of x[col][*] (a 4-, 8- or 16-byte vector when FPL is 1, 2 or 4), and
+// 32/F lane groups split the entries when the batch is narrower than a warp. The gathered vector
+// (dr, 0.36 MB per fly) stays L2-resident; the CSR streams from HBM once per substep for all flies.
+// Substeps ping-pong dr between two buffers, so one grid barrier per substep suffices.
+#include "common.cuh"
+
+namespace flyb {
+
+struct OpticK {
+  int m, batch, nsteps;
+  const int* __restrict__ ptr; const int* __restrict__ col; const float* __restrict__ w;
+  float* __restrict__ v; float* __restrict__ adapt;
+  float* buf0; float* buf1;
+  const float* __restrict__ pr; const float* __restrict__ spk;
+  const float* __restrict__ a; const float* __restrict__ b;
+  float gr, ga, aad;
+  float* v_hist; float* inp_hist;
+  int* status; int* sync;
+};
+
+template <int FPL> struct VecT;
+template <> struct VecT<1> { using T = float; };
+template <> struct VecT<2> { using T = float2; };
+template <> struct VecT<4> { using T = float4; };
+
+template <int FPL>
+__device__ __forceinline__ void load_x(const float* __restrict__ p, float (&x)[FPL]) {
+  if constexpr (FPL == 1) {
+    x[0] = __ldg(p);
+  } else if constexpr (FPL == 2) {
+    const float2 q = __ldg(reinterpret_cast<const float2*>(p)); x[0] = q.x; x[1] = q.y;
+  } else if constexpr (FPL == 4) {
+    const float4 q = __ldg(reinterpret_cast<const float4*>(p)); x[0] = q.x; x[1] = q.y; x[2] = q.z; x[3] = q.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < FPL; q += 4) {
+      const float4 r = __ldg(reinterpret_cast<const float4*>(p + q));
+      x[q] = r.x; x[q + 1] = r.y; x[q + 2] = r.z; x[q + 3] = r.w;
+    }
+  }
+}
+
+// acc[q] = sum over the row of w * x[col][f*FPL + q] for this lane's flies; full-warp result on
+// lanes of group 0 (lane < F). `vec` means batch == F * FPL exactly (aligned vector loads).
+template <int F, int FPL>
+__device__ __forceinline__ void row_product(const int* __restrict__ ptr, const int* __restrict__ col,
+                                            const float* __restrict__ w, const float* __restrict__ x, int batch,
+                                            int row, float (&acc)[FPL]) {
+  constexpr int G = 32 / F;
+  const int lane = threadIdx.x & 31, g = lane / F, f = lane % F;
+  const int fb = f * FPL;
+  const bool full = batch == F * FPL;
+#pragma unroll
+  for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+  const int e0 = __ldg(&ptr[row]), e1 = __ldg(&ptr[row + 1]);
+  for (int base = e0; base < e1; base += 32) {
+    const int e = base + lane;
+    int cj = 0;
+    float cw = 0.0f;
+    if (e < e1) { cj = __ldg(&col[e]); cw = __ldg(&w[e]); }
+    const int cnt = min(32, e1 - base);
+    for (int idx = 0; idx < cnt; idx += G) {
+      const int src = idx + g;
+      const int j = __shfl_sync(0xffffffffu, cj, src & 31);
+      const float wv = __shfl_sync(0xffffffffu, cw, src & 31);
+      if (src < cnt) {
+        const float* xp = x + (size_t)j * batch + fb;
+        if (full) {
+          float xv[FPL];
+          load_x<FPL>(xp, xv);
+#pragma unroll
+          for (int q = 0; q < FPL; ++q) { const float p = wv * xv[q]; acc[q] = acc[q] + p; }
+        } else {
+#pragma unroll
+          for (int q = 0; q < FPL; ++q)
+            if (fb + q < batch) { const float p = wv * __ldg(xp + q); acc[q] = acc[q] + p; }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = F; o < 32; o <<= 1)
+#pragma unroll
+    for (int q = 0; q < FPL; ++q) acc[q] = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], o);
+}
+
+// The fused rate update of one (unit, fly), reference order (neural.cu:68-79, optic.py:528-551).
+__device__ __forceinline__ void optic_update(const OpticK& k, int s, size_t t, int i, float y,
+                                             const float* __restrict__ dr_in, float* __restrict__ dr_out) {
+  const float old = dr_in[t];
+  float inp = k.gr * y;
+  inp = inp + k.pr[t];
+  const float ad = k.ga * k.adapt[t];
+  inp = inp - ad;
+  inp = inp + k.spk[t];
+  float vv = k.v[t];
+  const size_t sz = (size_t)k.m * k.batch;
+  if (k.v_hist) k.v_hist[(size_t)s * sz + t] = vv;
+  if (k.inp_hist) k.inp_hist[(size_t)s * sz + t] = inp;
+  float dv = vv - inp;
+  dv = dv * k.a[i];
+  vv = inp + dv;
+  k.v[t] = vv;
+  float da = k.adapt[t] - old;
+  da = da * k.aad;
+  k.adapt[t] = old + da;
+  const float bb = k.b[i];
+  const float r = clip01(vv + bb);
+  dr_out[t] = r - bb;
+}
+
+template <int F, int FPL>
+__device__ __forceinline__ void optic_rows(const OpticK& k, int s, const float* dr_in, float* dr_out,
+                                           long long warp0, long long nwarps) {
+  const int lane = threadIdx.x & 31;
+  for (long long row = warp0; row < k.m; row += nwarps) {
+    float acc[FPL];
+    row_product<F, FPL>(k.ptr, k.col, k.w, dr_in, k.batch, (int)row, acc);
+    if (lane < F) {
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) {
+        const int bb = lane * FPL + q;
+        if (bb < k.batch) optic_update(k, s, (size_t)row * k.batch + bb, (int)row, acc[q], dr_in, dr_out);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void init_dr(const OpticK& k, float* dr, long long tid, long long nthreads) {
+  const long long sz = (long long)k.m * k.batch;
+  for (long long t = tid; t < sz; t += nthreads) {
+    const int i = (int)(t / k.batch);
+    const float bb = k.b[i];
+    dr[t] = clip01(k.v[t] + bb) - bb;
+  }
+}
+
+__global__ void optic_init_kernel(OpticK k) {
+  init_dr(k, k.buf0, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+}
+
+template <int F, int FPL>
+__global__ void __launch_bounds__(256) optic_step_kernel(OpticK k, int s) {
+  const float* in = (s & 1) ? k.buf1 : k.buf0;
+  float* out = (s & 1) ? k.buf0 : k.buf1;
+  optic_rows<F, FPL>(k, s, in, out, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
+                     ((long long)gridDim.x * blockDim.x) >> 5);
+}
+
+template <int F, int FPL>
+__global__ void __launch_bounds__(256) optic_persistent_kernel(OpticK k) {
+  int generation = 0;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nth = (long long)gridDim.x * blockDim.x;
+  init_dr(k, k.buf0, tid, nth);
+  if (!grid_barrier(k.sync, k.status, generation, -1)) return;
+  for (int s = 0; s < k.nsteps; ++s) {
+    const float* in = (s & 1) ? k.buf1 : k.buf0;
+    float* out = (s & 1) ? k.buf0 : k.buf1;
+    optic_rows<F, FPL>(k, s, in, out, tid >> 5, nth >> 5);
+    if (s + 1 < k.nsteps && !grid_barrier(k.sync, k.status, generation, s)) return;
+  }
+}
+
+template <int F, int FPL>
+static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st) {
+  const long long sz = (long long)k.m * k.batch;
+  if (launch == FLYB_LAUNCH_STEP) {
+    optic_init_kernel<<<(unsigned)((sz + 255) / 256), 256, 0, st>>>(k);
+    FLYB_CHECK_LAUNCH();
+    const unsigned blocks = (unsigned)((k.m + 7) / 8);   // one warp per row, 8 warps per block
+    for (int s = 0; s < k.nsteps; ++s) {
+      optic_step_kernel<F, FPL><<<blocks, 256, 0, st>>>(k, s);
+      FLYB_CHECK_LAUNCH();
+    }
+    return 0;
+  }
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, optic_persistent_kernel<F, FPL>, 256, 0);
+  long long grid = (long long)sms * per_sm;
+  const long long need = (k.m + 7) / 8;
+  if (grid > need) grid = need;
+  if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
+  if (grid < 1) return FLYB_ECOOP;
+  cudaError_t e = cudaMemsetAsync(k.sync, 0, 2 * sizeof(int), st);
+  if (e != cudaSuccess) return (int)e;
+  OpticK kk = k;
+  void* args[] = {&kk};
+  e = cudaLaunchCooperativeKernel((void*)optic_persistent_kernel<F, FPL>, dim3((unsigned)grid), dim3(256), args, 0, st);
+  return (int)e;
+}
+
+// Picks (F, FPL) from the batch: F lanes across flies, FPL consecutive flies per lane.
+#define FLYB_BATCH_DISPATCH(B, CALL)                                   \
+  do {                                                                 \
+    if ((B) == 1) { constexpr int F = 1, FPL = 1; return CALL; }       \
+    if ((B) <= 2) { constexpr int F = 2, FPL = 1; return CALL; }       \
+    if ((B) <= 4) { constexpr int F = 4, FPL = 1; return CALL; }       \
+    if ((B) <= 8) { constexpr int F = 8, FPL = 1; return CALL; }       \
+    if ((B) <= 16) { constexpr int F = 16, FPL = 1; return CALL; }     \
+    if ((B) <= 32) { constexpr int F = 32, FPL = 1; return CALL; }     \
+    if ((B) <= 64) { constexpr int F = 32, FPL = 2; return CALL; }     \
+    if ((B) <= 128) { constexpr int F = 32, FPL = 4; return CALL; }    \
+    if ((B) <= 256) { constexpr int F = 32, FPL = 8; return CALL; }    \
+    return FLYB_ETOOBIG;                                               \
+  } while (0)
+
+// ------------------------------------------------------------------ held-input products
+struct SpmmK {
+  int rows, batch, accumulate;
+  const int* __restrict__ ptr; const int* __restrict__ col; const float* __restrict__ w;
+  const float* __restrict__ x; const int* __restrict__ x_index;
+  float x_div, x_lo, x_hi;
+  float* y; const int* __restrict__ y_index;
+  float alpha, y_lo, y_hi;
+};
+
+template <int F, int FPL>
+__global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
+  constexpr int G = 32 / F;
+  const int lane = threadIdx.x & 31, g = lane / F, f = lane % F, fb = f * FPL;
+  const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= k.rows) return;
+  float acc[FPL];
+#pragma unroll
+  for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+  const int e0 = k.ptr[row], e1 = k.ptr[row + 1];
+  for (int base = e0; base < e1; base += 32) {
+    const int e = base + lane;
+    int cj = 0;
+    float cw = 0.0f;
+    if (e < e1) { cj = k.col[e]; cw = k.w[e]; if (k.x_index) cj = k.x_index[cj]; }
+    const int cnt = min(32, e1 - base);
+    for (int idx = 0; idx < cnt; idx += G) {
+      const int src = idx + g;
+      const int j = __shfl_sync(0xffffffffu, cj, src & 31);
+      const float wv = __shfl_sync(0xffffffffu, cw, src & 31);
+      if (src < cnt) {
+#pragma unroll
+        for (int q = 0; q < FPL; ++q) {
+          if (fb + q < k.batch) {
+            float xv = k.x[(size_t)j * k.batch + fb + q] / k.x_div;
+            xv = xv < k.x_lo ? k.x_lo : (xv > k.x_hi ? k.x_hi : xv);
+            const float p = wv * xv;
+            acc[q] = acc[q] + p;
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int o = F; o < 32; o <<= 1)
+#pragma unroll
+    for (int q = 0; q < FPL; ++q) acc[q] = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], o);
+  if (lane < F) {
+    const long long yi = k.y_index ? k.y_index[row] : row;
+#pragma unroll
+    for (int q = 0; q < FPL; ++q) {
+      const int bb = fb + q;
+      if (bb < k.batch) {
+        float r = k.alpha * acc[q];
+        r = r < k.y_lo ? k.y_lo : (r > k.y_hi ? k.y_hi : r);
+        float* yp = k.y + (size_t)yi * k.batch + bb;
+        *yp = k.accumulate ? *yp + r : r;
+      }
+    }
+  }
+}
+
+template <int F, int FPL>
+static int run_spmm(const SpmmK& k, cudaStream_t st) {
+  const unsigned blocks = (unsigned)((k.rows + 7) / 8);
+  if (blocks) spmm_kernel<F, FPL><<<blocks, 256, 0, st>>>(k);
+  return (int)cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ reference-compatible launchers
+__global__ void ref_optic_dr_kernel(const float* v, const float* b, float* dr, int n, long long total) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < total) { const float base = b[t % n]; dr[t] = clip01(v[t] + base) - base; }
+}
+
+struct RefOptic { float *v, *adapt, *dr, *y, *pr, *spk, *a, *b; };
+
+__global__ void ref_optic_kernel(RefOptic s, int n, long long total, float gr, float ga, float aad) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= total) return;
+  const int i = (int)(t % n);
+  const float old = s.dr[t];
+  float inp = gr * s.y[t];
+  inp = inp + s.pr[t];
+  const float ad = ga * s.adapt[t];
+  inp = inp - ad;
+  inp = inp + s.spk[t];
+  float dv = s.v[t] - inp;
+  dv = dv * s.a[i];
+  const float v = inp + dv;
+  s.v[t] = v;
+  float da = s.adapt[t] - old;
+  da = da * aad;
+  s.adapt[t] = old + da;
+  s.dr[t] = clip01(v + s.b[i]) - s.b[i];
+}
+
+// Warp per (fly, row) with a fixed shuffle tree, batch-major (neural.cu:90-104).
+template <typename W>
+__global__ void ref_csr_kernel(const int* __restrict__ ptr, const int* __restrict__ idx, const W* __restrict__ w,
+                               const float* __restrict__ x, float* out, int rows, int cols, int batch) {
+  const int lane = threadIdx.x & 31;
+  const long long gid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (gid >= (long long)rows * batch) return;
+  const int b = (int)(gid / rows), row = (int)(gid - (long long)b * rows);
+  float sum = 0.0f;
+  for (int e = ptr[row] + lane; e < ptr[row + 1]; e += 32) {
+    float xv = x[(size_t)b * cols + idx[e]];
+    if (sizeof(W) == 2) xv = __half2float(__float2half_rn(xv));
+    const float p = (float)w[e] * xv;
+    sum = sum + p;
+  }
+#pragma unroll
+  for (int k = 16; k; k >>= 1) sum = sum + __shfl_down_sync(0xffffffffu, sum, k);
+  if (lane == 0) out[gid] = sum;
+}
+
+int optic_blocks_per_sm() {
+  int b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, optic_persistent_kernel<1, 1>, 256, 0);
+  return b;
+}
+
+}  // namespace flyb
+
+using namespace flyb;
+
+FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
+  if (!a || a->m <= 0 || a->batch <= 0 || a->nsteps < 0 || !a->ptr || !a->col || !a->w || !a->v || !a->adapt ||
+      !a->dr || !a->dr_tmp || !a->pr || !a->spk || !a->a || !a->b)
+    return FLYB_EINVAL;
+  if ((long long)a->m * a->batch >= (1ll << 31)) return FLYB_ETOOBIG;
+  if (a->launch == FLYB_LAUNCH_PERSISTENT && (!a->sync || !a->status)) return FLYB_EINVAL;
+  if (a->nsteps == 0) return 0;
+  OpticK k{a->m, a->batch, a->nsteps, a->ptr, a->col, a->w, a->v, a->adapt, a->dr, a->dr_tmp, a->pr, a->spk,
+           a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
+           (a->flags & 1) ? a->inp_hist : nullptr, a->status, a->sync};
+  cudaStream_t st = (cudaStream_t)stream;
+  FLYB_BATCH_DISPATCH(a->batch, (run_optic<F, FPL>(k, a->launch, a->grid, st)));
+}
+
+FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
+  if (!a || a->rows < 0 || a->batch <= 0 || !a->ptr || !a->col || !a->w || !a->x || !a->y || a->x_div == 0.0f)
+    return FLYB_EINVAL;
+  if (a->rows == 0) return 0;
+  SpmmK k{a->rows, a->batch, a->accumulate, a->ptr, a->col, a->w, a->x, a->x_index, a->x_div, a->x_lo, a->x_hi,
+          a->y, a->y_index, a->alpha, a->y_lo, a->y_hi};
+  cudaStream_t st = (cudaStream_t)stream;
+  FLYB_BATCH_DISPATCH(a->batch, (run_spmm<F, FPL>(k, st)));
+}
+
+FLYB_API int launch_optic_dr(void** p, int n, int batch, void* stream) {
+  const long long total = (long long)n * batch;
+  if (total > 0)
+    ref_optic_dr_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>((float*)p[0], (float*)p[1],
+                                                                                            (float*)p[2], n, total);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int launch_optic(void** p, int n, int batch, float gr, float ga, float aad, void* stream) {
+  RefOptic s{(float*)p[0], (float*)p[1], (float*)p[2], (float*)p[3], (float*)p[4], (float*)p[5], (float*)p[6], (float*)p[7]};
+  const long long total = (long long)n * batch;
+  if (total > 0)
+    ref_optic_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(s, n, total, gr, ga, aad);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int launch_csr(void** p, int rows, int cols, int batch, int half, void* stream) {
+  const long long warps = (long long)rows * batch;
+  const unsigned blocks = (unsigned)((warps + 7) / 8);
+  if (blocks) {
+    if (half)
+      ref_csr_kernel<__half><<<blocks, 256, 0, (cudaStream_t)stream>>>((int*)p[0], (int*)p[1], (__half*)p[2], (float*)p[3],
+                                                                       (float*)p[4], rows, cols, batch);
+    else
+      ref_csr_kernel<float><<<blocks, 256, 0, (cudaStream_t)stream>>>((int*)p[0], (int*)p[1], (float*)p[2], (float*)p[3],
+                                                                      (float*)p[4], rows, cols, batch);
+  }
+  return (int)cudaGetLastError();
+}

@@ -1,0 +1,129 @@
+// Readouts either side of the brain step: motor group means (flyverse/motor.py:232-270 through
+// neural.cu:133-144) and the photoreceptor stage of the optic frame (flyverse/optic.py:496-517);
+// plus the library's version / ABI / occupancy queries.
+#include "common.cuh"
+
+namespace flyb {
+
+// Fixed-order double accumulation per (fly, group), batch-major rates (neural.cu:133-140).
+__global__ void ref_means_kernel(const int* __restrict__ ptr, const int* __restrict__ idx, const float* __restrict__ rates,
+                                 double* out, int n, int groups, int batch, int stride) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)groups * batch) return;
+  const int b = (int)(t / groups), k = (int)(t - (long long)b * groups);
+  double sum = 0.0;
+  for (int j = ptr[k]; j < ptr[k + 1]; ++j) sum += (double)rates[(size_t)b * n + idx[j]];
+  const int count = ptr[k + 1] - ptr[k];
+  out[(size_t)b * stride + k] = count ? sum / count : 0.0;
+}
+
+struct PhotoK {
+  int n_pr, n_col, batch;
+  const float* __restrict__ rad; const int* __restrict__ pr_column; const float* __restrict__ sens;
+  const int* __restrict__ avg_ptr; const int* __restrict__ avg_idx; const float* __restrict__ avg_w;
+  const int* __restrict__ pr_cell; const unsigned char* __restrict__ has;
+  float* I_lp; float* I_mean; float* contrast; unsigned char* fresh;
+  float a_lp, c_lp, a_ad, c_ad, eps, clip_hi;
+  float* a_pr;
+};
+
+// One thread per (fly, column x family cell): photoreceptor intensities of the cell's members,
+// their mean, the low-pass / adaptation update and the clipped contrast (optic.py:503-513).
+__global__ void photo_cell_kernel(PhotoK k) {
+  const int cells = k.n_col * 5;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)cells * k.batch) return;
+  const int b = (int)(t / cells), c = (int)(t - (long long)b * cells);
+  const float* rb = k.rad + (size_t)b * k.n_col * 4;
+  float I = 0.0f;
+  for (int e = k.avg_ptr[c]; e < k.avg_ptr[c + 1]; ++e) {
+    const int p = k.avg_idx[e];
+    const float* r = rb + (size_t)k.pr_column[p] * 4;
+    const float* s = k.sens + (size_t)p * 4;
+    float ip = r[0] * s[0];
+    float q = r[1] * s[1]; ip = ip + q;
+    q = r[2] * s[2]; ip = ip + q;
+    q = r[3] * s[3]; ip = ip + q;
+    const float term = k.avg_w[e] * ip;
+    I = I + term;
+  }
+  const size_t o = (size_t)b * cells + c;
+  float lp = k.I_lp[o], mean = k.I_mean[o];
+  if (k.fresh[b]) { lp = I; mean = I; }
+  float x = k.a_lp * lp, y = k.c_lp * I;
+  lp = x + y;
+  x = k.a_ad * mean; y = k.c_ad * lp;
+  mean = x + y;
+  k.I_lp[o] = lp;
+  k.I_mean[o] = mean;
+  float num = lp - mean, den = mean + k.eps;
+  float con = num / den;
+  con = con < -1.0f ? -1.0f : (con > k.clip_hi ? k.clip_hi : con);
+  k.contrast[o] = k.has[c] ? con : 0.0f;
+}
+
+// Gather of the contrast of each photoreceptor's cell, fly-minor; clears the fresh flags.
+__global__ void photo_gather_kernel(PhotoK k) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)k.n_pr * k.batch) return;
+  const int p = (int)(t / k.batch), b = (int)(t - (long long)p * k.batch);
+  k.a_pr[t] = k.contrast[(size_t)b * k.n_col * 5 + k.pr_cell[p]];
+  if (p == 0) k.fresh[b] = 0;
+}
+
+int lif_blocks_per_sm(int block);
+int optic_blocks_per_sm();
+int adjoint_blocks_per_sm();
+
+}  // namespace flyb
+
+using namespace flyb;
+
+FLYB_API int launch_means(void** p, int n, int groups, int batch, int stride, void* stream) {
+  const long long total = (long long)groups * batch;
+  if (total > 0)
+    ref_means_kernel<<<(unsigned)((total + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        (int*)p[0], (int*)p[1], (float*)p[2], (double*)p[3], n, groups, batch, stride);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_photoreceptor(const flyb_photo_args* a, void* stream) {
+  if (!a || a->n_pr < 0 || a->n_col <= 0 || a->batch <= 0 || !a->rad || !a->pr_column || !a->sens || !a->avg_ptr ||
+      !a->avg_idx || !a->avg_w || !a->pr_cell || !a->has || !a->I_lp || !a->I_mean || !a->contrast || !a->fresh ||
+      !a->a_pr)
+    return FLYB_EINVAL;
+  PhotoK k{a->n_pr, a->n_col, a->batch, a->rad, a->pr_column, a->sens, a->avg_ptr, a->avg_idx, a->avg_w, a->pr_cell,
+           a->has, a->I_lp, a->I_mean, a->contrast, a->fresh, a->a_lp, a->c_lp, a->a_ad, a->c_ad, a->eps, a->clip_hi,
+           a->a_pr};
+  cudaStream_t st = (cudaStream_t)stream;
+  const long long cells = (long long)a->n_col * 5 * a->batch;
+  photo_cell_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(k);
+  FLYB_CHECK_LAUNCH();
+  const long long prs = (long long)a->n_pr * a->batch;
+  if (prs > 0) photo_gather_kernel<<<(unsigned)((prs + 255) / 256), 256, 0, st>>>(k);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (sm_count) cudaDeviceGetAttribute(sm_count, cudaDevAttrMultiProcessorCount, dev);
+  int b = 0;
+  if (kind == 0) b = lif_blocks_per_sm(block ? block : 256);
+  else if (kind == 1) b = optic_blocks_per_sm();
+  else if (kind == 2) b = adjoint_blocks_per_sm();
+  else return FLYB_EINVAL;
+  if (blocks_per_sm) *blocks_per_sm = b;
+  return (int)cudaGetLastError();
+}
+
+FLYB_API const char* flyb_version(void) { return "flyb200 0.1.0 (sm_100a)"; }
+
+FLYB_API int flyb_abi_sizes(int* sizes, int n) {
+  const int s[5] = {(int)sizeof(flyb_lif_args), (int)sizeof(flyb_optic_args), (int)sizeof(flyb_spmm_args),
+                    (int)sizeof(flyb_adjoint_args), (int)sizeof(flyb_photo_args)};
+  int k = 0;
+  for (; k < n && k < 5; ++k) sizes[k] = s[k];
+  return k;
+}

@@ -1,0 +1,152 @@
+"""ctypes mirror of include/flyb200.h and the loader of the in-tree CUDA library.
+
+The library is a plain C ABI (`extern "C"`, raw device pointers, the caller's stream), bound the
+same way the reference binds its kernels (flyverse/cuda.py:37-91): a ctypes CDLL whose functions
+take pointers and return an int status. There is no fallback: if the library is missing or no
+CUDA device is visible, every native call raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import threading
+from pathlib import Path
+
+LIB_NAME = "libflyb200.so"
+_HERE = Path(__file__).resolve().parent
+_LOCK = threading.Lock()
+_LIB = None
+
+# ------------------------------------------------------------------ constants (flyb200.h)
+OK, EINVAL, EBARRIER, ECOOP, ETOOBIG = 0, 1001, 1002, 1003, 1004
+LIF_POISSON, LIF_STD, LIF_COUNTS, LIF_ADAPT = 1, 2, 4, 8
+LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES = 16, 32, 64
+RING_COUNT, RING_FIXED = 0, 1
+LAUNCH_STEP, LAUNCH_PERSISTENT = 0, 1
+LAUNCHES_BY_NAME = {"step": LAUNCH_STEP, "persistent": LAUNCH_PERSISTENT}
+(P_V_REST, P_V_RESET, P_V_TH, P_A_M, P_A_S, P_DT, P_T_REF, P_ADAPT_JUMP, P_A_AD, P_A_STD, P_A_R,
+ P_RATE_GAIN, P_W_SYN, LIF_NPARAM) = range(14)
+LIF_SYNC_WORDS = 64
+OPTIC_HISTORY = 1
+
+_VP = ct.c_void_p
+_I = ct.c_int
+
+
+class LifArgs(ct.Structure):
+    _fields_ = [("n", _I), ("batch", _I), ("n_delay", _I), ("ring_slots", _I), ("ring_mode", _I),
+                ("ring_pos", _I), ("flags", _I), ("nsteps", _I), ("launch", _I), ("block", _I),
+                ("grid", _I), ("raster_slots", _I), ("raster_pos", _I), ("fly0", _I),
+                ("step0", ct.c_longlong), ("seed", ct.c_ulonglong),
+                ("out_ptr", _VP), ("out_edge", _VP),
+                ("v", _VP), ("g", _VP), ("refrac", _VP), ("adapt", _VP), ("res", _VP),
+                ("rate", _VP), ("counts", _VP), ("spikes", _VP), ("drive", _VP), ("poisson_p", _VP),
+                ("active", _VP), ("std_u", _VP), ("params", _VP), ("ring", _VP), ("uniforms", _VP),
+                ("fly_steps", _VP), ("clock", _VP), ("raster", _VP), ("events", _VP), ("status", _VP),
+                ("sync", _VP)]
+
+
+class OpticArgs(ct.Structure):
+    _fields_ = [("m", _I), ("batch", _I), ("nsteps", _I), ("launch", _I), ("block", _I), ("grid", _I),
+                ("lanes_per_row", _I), ("flags", _I),
+                ("ptr", _VP), ("col", _VP), ("w", _VP), ("v", _VP), ("adapt", _VP), ("dr", _VP),
+                ("dr_tmp", _VP), ("pr", _VP), ("spk", _VP), ("a", _VP), ("b", _VP),
+                ("gr", ct.c_float), ("ga", ct.c_float), ("aad", ct.c_float), ("pad0", _I),
+                ("v_hist", _VP), ("inp_hist", _VP), ("status", _VP), ("sync", _VP)]
+
+
+class SpmmArgs(ct.Structure):
+    _fields_ = [("rows", _I), ("cols", _I), ("batch", _I), ("accumulate", _I),
+                ("ptr", _VP), ("col", _VP), ("w", _VP),
+                ("x", _VP), ("x_index", _VP), ("x_rows", _I),
+                ("x_div", ct.c_float), ("x_lo", ct.c_float), ("x_hi", ct.c_float),
+                ("y", _VP), ("y_index", _VP), ("y_rows", _I),
+                ("alpha", ct.c_float), ("y_lo", ct.c_float), ("y_hi", ct.c_float),
+                ("lanes_per_row", _I)]
+
+
+class AdjointArgs(ct.Structure):
+    _fields_ = [("m", _I), ("batch", _I), ("nsteps", _I), ("launch", _I), ("block", _I), ("grid", _I),
+                ("pad0", _I), ("pad1", _I),
+                ("t_ptr", _VP), ("t_col", _VP), ("t_w", _VP), ("t_perm", _VP),
+                ("v_hist", _VP), ("inp_hist", _VP), ("a", _VP), ("b", _VP),
+                ("gr", ct.c_float), ("ga", ct.c_float), ("aad", ct.c_float), ("pad2", _I),
+                ("lam_v", _VP), ("lam_a", _VP), ("lam_tmp", _VP), ("mu", _VP),
+                ("g_edge", _VP), ("g_a", _VP), ("status", _VP), ("sync", _VP)]
+
+
+class PhotoArgs(ct.Structure):
+    _fields_ = [("n_pr", _I), ("n_col", _I), ("batch", _I), ("pad0", _I),
+                ("rad", _VP), ("pr_column", _VP), ("sens", _VP),
+                ("avg_ptr", _VP), ("avg_idx", _VP), ("avg_w", _VP), ("pr_cell", _VP), ("has", _VP),
+                ("I_lp", _VP), ("I_mean", _VP), ("contrast", _VP), ("fresh", _VP),
+                ("a_lp", ct.c_float), ("c_lp", ct.c_float), ("a_ad", ct.c_float), ("c_ad", ct.c_float),
+                ("eps", ct.c_float), ("clip_hi", ct.c_float),
+                ("a_pr", _VP)]
+
+
+STRUCTS = (LifArgs, OpticArgs, SpmmArgs, AdjointArgs, PhotoArgs)
+
+# Every symbol include/flyb200.h declares, with its ctypes signature.
+_P = ct.POINTER(ct.c_void_p)
+SIGNATURES = {
+    "launch_lif": [_P, _I, _I, _I, _VP],
+    "launch_optic_dr": [_P, _I, _I, _VP],
+    "launch_optic": [_P, _I, _I, ct.c_float, ct.c_float, ct.c_float, _VP],
+    "launch_csr": [_P, _I, _I, _I, _I, _VP],
+    "launch_events": [_P, _I, _I, _I, _I, _VP],
+    "launch_means": [_P, _I, _I, _I, _I, _VP],
+    "flyb_lif_run": [ct.POINTER(LifArgs), _VP],
+    "flyb_ring_deposit": [_I, _I, _I, _VP, _VP, _VP, _VP, _VP],
+    "flyb_optic_run": [ct.POINTER(OpticArgs), _VP],
+    "flyb_spmm": [ct.POINTER(SpmmArgs), _VP],
+    "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
+    "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
+    "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
+    "flyb_version": [],
+    "flyb_abi_sizes": [ct.POINTER(_I), _I],
+}
+RESTYPES = {"flyb_version": ct.c_char_p}
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("FLYB200_LIB", _HERE / LIB_NAME))
+
+
+def bind(lib: ct.CDLL) -> ct.CDLL:
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = RESTYPES.get(name, _I)
+    return lib
+
+
+def lib() -> ct.CDLL:
+    """The loaded native library; raises if it was not built (no fallback exists)."""
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            path = library_path()
+            if not path.exists():
+                raise RuntimeError(f"flyb200 native library not found at {path}; run "
+                                   "`python -m flyb200.build` (or __graft_entry__.build()) first")
+            _LIB = bind(ct.CDLL(str(path)))
+            check_abi(_LIB)
+        return _LIB
+
+
+def check_abi(library: ct.CDLL) -> None:
+    sizes = (ct.c_int * len(STRUCTS))()
+    n = library.flyb_abi_sizes(sizes, len(STRUCTS))
+    for k, S in enumerate(STRUCTS[:n]):
+        if sizes[k] != ct.sizeof(S):
+            raise RuntimeError(f"ABI mismatch: {S.__name__} is {ct.sizeof(S)} bytes here, {sizes[k]} in the library")
+
+
+def ptr(t) -> int | None:
+    """Device (or host) address of a tensor / array, None for None."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data

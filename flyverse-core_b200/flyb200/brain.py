@@ -1,0 +1,444 @@
+"""Batched Shiu-style LIF brain on the B200 native step: the drop-in for flyverse/brain.py.
+
+`Brain(c, params, device, seed, batch, ...)` keeps the reference constructor (brain.py:373-376),
+`step(n)` / `run_ms` / `set_drive` / `set_poisson` / `freeze` / `reset(rows)` / `prune` /
+`set_weights` and the public (B, N) state tensors (v, g, refrac, drive, poisson_p, rate, spikes,
+spike_counts, adapt, res). Differences that follow from the design:
+
+  * every step runs the fused native kernel (include/flyb200.h: flyb_lif_run); there is no Torch
+    or CPU path, and a missing library or a non-CUDA device raises;
+  * state is stored neuron-major, fly-minor ([N][B]); the public attributes are (B, N) views of that
+    storage, so in-place edits (`brain.v[:, 3] = -40`) reach the kernel and assignment copies in;
+  * the delay is an exact ring of pending synaptic input (`ring`, [R][N][B]) rather than a float
+    spike buffer: int32 synapse counts when W is w_syn x integer counts (the model of the
+    benchmark graphs), Q32.32 millivolts otherwise. `spike_buf` is rebuilt on demand from a
+    1-bit spike history, and `load_spike_buf` converts a reference checkpoint's buffer;
+  * Poisson draws come from Philox4x32-10 keyed by (seed, step, neuron, fly); `step(n, uniforms=)`
+    takes external uniforms instead (parity runs feed the reference generator's draws).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from . import _abi
+from .weights import DEFAULT_ADAPT_BY_TYPE, DEFAULT_STD_U_BY_TYPE, integer_counts, lif_weights, per_type
+
+
+@dataclass
+class LIFParams:
+    """The reference's LIF parameters (brain.py:29-158), same names and defaults."""
+    v_rest: float = -52.0
+    v_reset: float = -52.0
+    v_th: float = -45.0
+    tau_m: float = 20.0
+    tau_syn: float = 5.0
+    t_ref: float = 2.2
+    delay: float = 1.8
+    w_syn: float = 0.275
+    dt: float = 0.5
+    rate_tau: float = 100.0
+    adapt_jump: float = 1.5
+    adapt_tau: float = 200.0
+    adapt_by_type: dict | None = None
+    std_u: float = 0.0
+    std_tau: float = 300.0
+    std_u_by_type: dict = None
+    input_norm_alpha: float = 1.0
+    input_norm_ref: float = 5000.0
+    same_type_gain: float = 0.1
+    conn_cap: float = 60.0
+    path_gain: list = None
+    type_path_gain: list = None
+    event_driven: bool | None = None
+    weight_dtype: str = "float32"
+    dt_by_module: dict | None = None
+    prune_frozen: bool = True
+    receptor_model: str | None = "sign"
+    receptor_net_rule: str = "abs"
+    receptor_nt_class_fallback: bool = False
+    receptor_table: str | None = None
+    receptor_gain: dict | None = None
+    slow_tau_ms: float = 200.0
+    slow_gain: float = 0.02
+    slow_gain_by_class: dict | None = None
+    slow_tau_by_class: dict | None = None
+    slow_mode: str = "additive"
+    slow_gain_clip: tuple = (0.0, 4.0)
+    w_syn_by_nt: dict | None = None
+    surrogate_grad: bool = False
+
+
+_STATE = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
+LAUNCHES = {"step": _abi.LAUNCH_STEP, "persistent": _abi.LAUNCH_PERSISTENT}
+
+
+def lif_coefficients(p: LIFParams, std_on: bool) -> np.ndarray:
+    """The float32 coefficient vector of the native step (the reference's `_cuda_P`, brain.py:493-520,
+    plus tau_syn's decay and w_syn), with the exponentials taken in double as the reference does."""
+    a_r = math.exp(-p.dt / p.rate_tau)
+    P = np.zeros(_abi.LIF_NPARAM, np.float32)
+    P[_abi.P_V_REST], P[_abi.P_V_RESET], P[_abi.P_V_TH] = p.v_rest, p.v_reset, p.v_th
+    P[_abi.P_A_M], P[_abi.P_A_S] = math.exp(-p.dt / p.tau_m), math.exp(-p.dt / p.tau_syn)
+    P[_abi.P_DT], P[_abi.P_T_REF] = p.dt, p.t_ref
+    P[_abi.P_ADAPT_JUMP] = p.adapt_jump
+    P[_abi.P_A_AD] = math.exp(-p.dt / p.adapt_tau) if p.adapt_jump > 0 else 0.0
+    P[_abi.P_A_STD] = math.exp(-p.dt / p.std_tau) if std_on else 1.0
+    P[_abi.P_A_R], P[_abi.P_RATE_GAIN] = a_r, (1 - a_r) * 1000.0 / p.dt
+    P[_abi.P_W_SYN] = p.w_syn
+    return P
+
+
+def out_edges(W, w_syn: float, prefer: str = "auto", std_on: bool = False):
+    """Pre-major (CSC) outgoing synapses of W[post, pre] for the native step.
+
+    Returns (out_ptr int32 [N+1], out_edge int32 [nnz][2], ring mode): {post, signed count} on the
+    int32 count ring when every weight is w_syn x an integer count and depression is off (unless
+    prefer='fixed'), else {post, float32 bits of w} on the Q32.32 ring."""
+    Wc = sp.csc_matrix(W, dtype=np.float32)
+    Wc.sum_duplicates()
+    Wc.sort_indices()
+    if max(*Wc.shape, Wc.nnz) >= 2**31:
+        raise ValueError("the native step needs 32-bit dimensions and indices")
+    counts = None if (std_on or prefer == "fixed") else integer_counts(Wc, w_syn)
+    if prefer == "count" and counts is None:
+        raise ValueError("ring='count' needs weights that are w_syn x integer synapse counts and no depression")
+    mode = _abi.RING_COUNT if counts is not None else _abi.RING_FIXED
+    second = counts if counts is not None else Wc.data.astype(np.float32).view(np.int32)
+    edges = np.ascontiguousarray(np.stack([Wc.indices.astype(np.int32), second.astype(np.int32)], axis=1))
+    return Wc.indptr.astype(np.int32), edges, mode
+
+
+def _unsupported(p: LIFParams, metal_kernels, cuda_kernels, cuda_sparse) -> None:
+    if metal_kernels:
+        raise ValueError("flyb200 runs on B200 CUDA kernels only; the Metal backend is not provided")
+    if cuda_kernels is False:
+        raise ValueError("flyb200 has no Torch path: cuda_kernels=False is not available")
+    if cuda_sparse not in ("torch", "warp"):
+        raise ValueError("cuda_sparse must be torch or warp")
+    if p.surrogate_grad:
+        raise NotImplementedError("surrogate_grad (Torch autograd through the LIF) is not part of the native step; "
+                                  "the spiking path is left undifferentiated")
+    if p.dt_by_module:
+        raise NotImplementedError("per-module clocks (dt_by_module) are not in the native LIF step")
+    if p.receptor_model == "full":
+        raise NotImplementedError("the slow receptor term (receptor_model='full') is not in the native LIF step")
+    if (DEFAULT_ADAPT_BY_TYPE if p.adapt_by_type is None else p.adapt_by_type):
+        raise NotImplementedError("per-type adaptation (adapt_by_type) is not in the native LIF step")
+    if p.weight_dtype not in ("float32", "float16"):
+        raise ValueError("weight_dtype must be float32 or float16")
+    if p.event_driven is False:
+        pass   # the native step is event driven for every activity level; the flag is accepted for compatibility
+
+
+class Brain:
+    def __init__(self, c, params: LIFParams | None = None, device=None, seed: int = 0, batch: int = 1,
+                 metal_kernels=None, cuda_kernels=None, cuda_sparse: str = "torch", cuda_compact: bool = True,
+                 receptor=None, *, launch: str = "persistent", ring: str = "auto", block: int = 256,
+                 ring_slots: int | None = None):
+        p = params or LIFParams()
+        _unsupported(p, metal_kernels, cuda_kernels, cuda_sparse)
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise ValueError("flyb200.Brain runs on a CUDA device only; there is no CPU path")
+        if int(batch) < 1 or not math.isfinite(p.dt) or p.dt <= 0:
+            raise ValueError("batch must be positive and dt must be positive and finite")
+        if launch not in LAUNCHES:
+            raise ValueError(f"launch must be one of {sorted(LAUNCHES)}")
+        if ring not in ("auto", "count", "fixed"):
+            raise ValueError("ring must be 'auto', 'count' or 'fixed'")
+        self._lib = _abi.lib()
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.c, self.p, self.n, self.B = c, p, c.n, int(batch)
+        self.seed, self.launch, self.block, self.ring_pref = int(seed), launch, int(block), ring
+        self.cuda, self.metal, self.event_driven = True, False, True
+        self.cuda_sparse, self.cuda_compact = cuda_sparse, bool(cuda_compact)
+        self.receptor = receptor
+        W, self.input_scale = lif_weights(c, p, receptor)
+        if p.weight_dtype == "float16":
+            W.data = W.data.astype(np.float16).astype(np.float32)
+        N, B, dev = self.n, self.B, self.device
+        self.n_delay = max(1, int(round(p.delay / p.dt)))
+        self.R = int(ring_slots) if ring_slots else self.n_delay + 1
+        if self.R < self.n_delay + 1:
+            raise ValueError("ring_slots must exceed the delay in steps")
+        std_map = DEFAULT_STD_U_BY_TYPE if p.std_u_by_type is None else p.std_u_by_type
+        u = per_type(c, std_map, p.std_u)
+        self._std_on = bool((u > 0).any())
+        self.std_u_vec = torch.from_numpy(u).to(dev)
+        self._a_m = math.exp(-p.dt / p.tau_m)
+        self._a_s = math.exp(-p.dt / p.tau_syn)
+        self._a_r = math.exp(-p.dt / p.rate_tau)
+        self._a_ad = math.exp(-p.dt / p.adapt_tau) if p.adapt_jump > 0 else 0.0
+        self._a_std = math.exp(-p.dt / p.std_tau) if self._std_on else 1.0
+        self._P = lif_coefficients(p, self._std_on)
+        # state: [N][B] storage, (B, N) public views
+        self._st = {k: torch.zeros(N, B, device=dev) for k in _STATE}
+        self._st["v"].fill_(p.v_rest)
+        self._st["res"].fill_(1.0)
+        self.active = torch.ones(N, device=dev)
+        self.g_slow = torch.zeros(B, N, device=dev)
+        self.g_slow_cls = torch.zeros(0, B, N, device=dev)
+        self.gen = torch.Generator(device=dev).manual_seed(seed)
+        self.words = (N * B + 31) // 32
+        self._hist = torch.zeros(self.n_delay, self.words, dtype=torch.int32, device=dev)   # 1-bit spike history
+        self._clock = torch.zeros(3, dtype=torch.int64, device=dev)        # {step, ring_pos, hist_pos}
+        self._status = torch.zeros(4, dtype=torch.int32, device=dev)
+        self._sync = torch.zeros(_abi.LIF_SYNC_WORDS, dtype=torch.int32, device=dev)
+        self._events = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.ring = None
+        self.record_activity = False
+        self._poisson_on = False
+        self.t, self.step_count, self.buf_pos = 0.0, 0, 0
+        self._rate_np, self._rate_np_key = None, None
+        self._weights_version = 0
+        self._W_cpu = W
+        self.set_weights(W)
+
+    # ------------------------------------------------------------------ public state views
+    def __getattr__(self, name):
+        st = self.__dict__.get("_st")
+        if st is not None and name in st:
+            return st[name].t()
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        st = self.__dict__.get("_st")
+        if st is not None and name in st:
+            st[name].t().copy_(torch.as_tensor(value, dtype=torch.float32, device=self.device))
+            return
+        object.__setattr__(self, name, value)
+
+    # ------------------------------------------------------------------ weights
+    def set_weights(self, W) -> None:
+        """Install W[post, pre] in mV per transmitted spike (brain.py:525-545); pending deliveries
+        are rebuilt with the new weights from the spike history, as the reference's buffer would."""
+        indptr, edges, mode = out_edges(W, self.p.w_syn, self.ring_pref, self._std_on)
+        had_ring = self.ring is not None
+        spike_buf = None
+        if had_ring and self.step_count and not self._std_on:
+            spike_buf = self.spike_buf
+        self._W_cpu = sp.csr_matrix(W, dtype=np.float32)
+        self._weights_version += 1
+        self.ring_mode = mode
+        self.nnz = int(edges.shape[0])
+        self._out_ptr = torch.from_numpy(indptr).to(self.device)
+        self._out_edge = torch.from_numpy(edges).to(self.device)
+        dtype = torch.int32 if mode == _abi.RING_COUNT else torch.int64
+        self.ring = torch.zeros(self.R, self.n, self.B, dtype=dtype, device=self.device)
+        self._make_args()
+        if had_ring and spike_buf is not None:
+            self.load_spike_buf(spike_buf)
+
+    def prune(self, idx) -> None:
+        """Drop every synapse from and onto neurons `idx` (brain.py:602-616)."""
+        keep = np.ones(self.n, np.float32)
+        keep[np.asarray(idx)] = 0.0
+        W = (sp.diags(keep) @ self._W_cpu @ sp.diags(keep)).tocsr()
+        W.eliminate_zeros()
+        self.set_weights(W)
+
+    # ------------------------------------------------------------------ native call
+    def _make_args(self) -> None:
+        st, a = self._st, _abi.LifArgs()
+        a.n, a.batch, a.n_delay, a.ring_slots, a.ring_mode = self.n, self.B, self.n_delay, self.R, self.ring_mode
+        a.launch, a.block = LAUNCHES[self.launch], self.block
+        a.raster_slots = self.n_delay
+        a.seed = self.seed & 0xFFFFFFFFFFFFFFFF
+        a.out_ptr, a.out_edge = self._out_ptr.data_ptr(), self._out_edge.data_ptr()
+        for name, field_ in (("v", "v"), ("g", "g"), ("refrac", "refrac"), ("adapt", "adapt"), ("res", "res"),
+                             ("rate", "rate"), ("spike_counts", "counts"), ("spikes", "spikes"), ("drive", "drive"),
+                             ("poisson_p", "poisson_p")):
+            setattr(a, field_, st[name].data_ptr())
+        a.active, a.std_u = self.active.data_ptr(), self.std_u_vec.data_ptr()
+        a.params = self._P.ctypes.data
+        a.ring, a.clock, a.raster = self.ring.data_ptr(), self._clock.data_ptr(), self._hist.data_ptr()
+        a.events, a.status, a.sync = self._events.data_ptr(), self._status.data_ptr(), self._sync.data_ptr()
+        self._args = a
+
+    def _flags(self, external: bool) -> int:
+        f = 0
+        if self._poisson_on:
+            f |= _abi.LIF_POISSON
+        if self._std_on:
+            f |= _abi.LIF_STD
+        if self.record_activity:
+            f |= _abi.LIF_COUNTS
+        if self.p.adapt_jump > 0:
+            f |= _abi.LIF_ADAPT
+        if self.cuda_compact:
+            f |= _abi.LIF_SKIP_FROZEN
+        if external:
+            f |= _abi.LIF_EXT_UNIFORM
+        return f
+
+    def step(self, n_steps: int = 1, *, uniforms: torch.Tensor | None = None) -> None:
+        """Advance n_steps of dt. `uniforms` (n_steps, B, N): external Poisson draws."""
+        n_steps = int(n_steps)
+        if n_steps <= 0:
+            return
+        a = self._args
+        ext = None
+        if uniforms is not None:
+            if tuple(uniforms.shape) != (n_steps, self.B, self.n):
+                raise ValueError(f"uniforms must have shape ({n_steps}, {self.B}, {self.n})")
+            ext = uniforms.to(self.device, torch.float32).transpose(1, 2).contiguous()
+        a.flags = self._flags(ext is not None)
+        a.nsteps = n_steps
+        a.uniforms = ext.data_ptr() if ext is not None else None
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        with torch.cuda.device(self.device):
+            rc = self._lib.flyb_lif_run(ct.byref(a), stream)
+        if rc:
+            raise RuntimeError(f"flyb_lif_run: error {rc}")
+        self.buf_pos = (self.buf_pos + n_steps) % self.R
+        self.t += n_steps * self.p.dt
+        self.step_count += n_steps
+
+    def run_ms(self, ms: float) -> None:
+        self.step(int(round(ms / self.p.dt)))
+
+    def check(self) -> None:
+        """Raise if a kernel recorded an error (bounded barrier wait ran out); host sync."""
+        s = self._status.cpu().tolist()
+        if s[0]:
+            raise RuntimeError(f"flyb200 LIF kernel status {s[0]} (where {s[1]}, step {s[2]})")
+
+    # ------------------------------------------------------------------ inputs
+    def _idx(self, idx) -> torch.Tensor:
+        return torch.as_tensor(idx, device=self.device, dtype=torch.long)
+
+    def set_drive(self, idx, mv) -> None:
+        """Injected current (mV) of neurons `idx`: scalar, (len(idx),) or (B, len(idx))."""
+        self.drive[:, self._idx(idx)] = torch.as_tensor(mv, dtype=torch.float32, device=self.device)
+
+    def set_poisson(self, idx, rate_hz) -> None:
+        """Poisson forcing at rate_hz on neurons `idx` (brain.py:707-713)."""
+        r = torch.as_tensor(rate_hz, dtype=torch.float32, device=self.device)
+        self.poisson_p[:, self._idx(idx)] = r * (self.p.dt / 1000.0)
+        self._poisson_on = bool((r > 0).any()) or bool(self._st["poisson_p"].count_nonzero() > 0)
+
+    def freeze(self, idx) -> None:
+        self.active[self._idx(idx)] = 0.0
+
+    def reset(self, rows=None) -> None:
+        """Reset brains `rows` (all if None) to rest, their pending input included."""
+        sel = slice(None) if rows is None else torch.as_tensor(np.asarray(rows), device=self.device, dtype=torch.long)
+        st = self._st
+        st["v"][:, sel] = self.p.v_rest
+        for k in ("g", "refrac", "drive", "poisson_p", "rate", "spikes", "adapt", "spike_counts"):
+            st[k][:, sel] = 0.0
+        st["res"][:, sel] = 1.0
+        self.g_slow[sel] = 0.0
+        self.ring[:, :, sel] = 0
+        if rows is None:
+            self._hist.zero_()
+        else:
+            self._clear_hist_rows(np.asarray(rows))
+        self._rate_np_key = None
+
+    def _clear_hist_rows(self, rows: np.ndarray) -> None:
+        flat = (np.arange(self.n)[:, None] * self.B + rows[None, :]).ravel()
+        mask = np.zeros(self.words * 32, bool)
+        mask[flat] = True
+        keep = ~np.packbits(mask, bitorder="little").view(np.uint32)
+        self._hist &= torch.from_numpy(keep.view(np.int32)).to(self.device)
+
+    # ------------------------------------------------------------------ spike buffer interchange
+    @property
+    def spike_buf(self) -> torch.Tensor:
+        """(D, B, N) transmitted spikes in the reference's buffer order (brain.py:486, 858-865):
+        slot (buf + k) % D holds the spikes delivered k steps from now. Depression makes the
+        transmitted amount fractional, which the 1-bit history does not keep."""
+        if self._std_on:
+            raise NotImplementedError("spike_buf export needs the transmitted amounts; depression is on")
+        D, N, B = self.n_delay, self.n, self.B
+        words = self._hist.cpu().numpy().view(np.uint32)
+        bits = np.unpackbits(words.view(np.uint8), bitorder="little").reshape(D, -1)[:, : N * B]
+        hist = bits.reshape(D, N, B).transpose(0, 2, 1).astype(np.float32)     # hist slot -> (B, N)
+        pos = int(self._clock[2].item()) % D           # next history slot = oldest entry = due now
+        out = np.empty((D, B, N), np.float32)
+        for k in range(D):
+            out[(self.step_count + k) % D] = hist[(pos + k) % D]
+        return torch.from_numpy(out).to(self.device)
+
+    def load_spike_buf(self, spike_buf, buf_pos: int | None = None) -> None:
+        """Rebuild the pending-input ring from a (D, B, N) spike buffer (a reference checkpoint's
+        `spike_buf` with its `buf_pos`): slot (buf_pos + k) % D is delivered k steps from now."""
+        sb = torch.as_tensor(spike_buf, dtype=torch.float32, device=self.device)
+        D = self.n_delay
+        if tuple(sb.shape) != (D, self.B, self.n):
+            raise ValueError(f"spike_buf must have shape ({D}, {self.B}, {self.n})")
+        buf_pos = self.step_count % D if buf_pos is None else int(buf_pos)
+        if self.ring_mode == _abi.RING_COUNT and not bool(((sb == 0) | (sb == 1)).all()):
+            raise ValueError("a count ring needs 0/1 spikes; rebuild the brain with ring='fixed'")
+        self.ring.zero_()
+        rpos = int(self._clock[1].item()) % self.R
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        hist = np.zeros((D, self.words), np.uint32)
+        hpos = int(self._clock[2].item()) % D
+        for k in range(D):
+            x = sb[(buf_pos + k) % D].t().contiguous()
+            slot = self.ring[(rpos + k) % self.R]
+            rc = self._lib.flyb_ring_deposit(self.n, self.B, self.ring_mode, self._out_ptr.data_ptr(),
+                                             self._out_edge.data_ptr(), x.data_ptr(), slot.data_ptr(), stream)
+            if rc:
+                raise RuntimeError(f"flyb_ring_deposit: error {rc}")
+            bits = np.packbits((x.cpu().numpy().ravel() != 0), bitorder="little")
+            bits = np.concatenate([bits, np.zeros(self.words * 4 - bits.size, np.uint8)])
+            hist[(hpos + k) % D] = bits.view(np.uint32)
+        self._hist.copy_(torch.from_numpy(hist.view(np.int32)))
+
+    # ------------------------------------------------------------------ checkpoint
+    def state_dict(self) -> dict:
+        out = {k: getattr(self, k).detach().cpu().clone() for k in _STATE}
+        out.update(ring=self.ring.cpu().clone(), hist=self._hist.cpu().clone(), clock=self._clock.cpu().clone(),
+                   scalars=dict(t=self.t, step_count=self.step_count, buf_pos=self.buf_pos, _poisson_on=self._poisson_on))
+        return out
+
+    def load_state_dict(self, state: dict) -> None:
+        for k in _STATE:
+            getattr(self, k).copy_(state[k].to(self.device))
+        if state["ring"].dtype != self.ring.dtype or state["ring"].shape != self.ring.shape:
+            raise ValueError("checkpoint ring does not match this brain's ring")
+        self.ring.copy_(state["ring"].to(self.device))
+        self._hist.copy_(state["hist"].to(self.device))
+        self._clock.copy_(state["clock"].to(self.device))
+        for k, v in state["scalars"].items():
+            setattr(self, k, v)
+        self._rate_np_key = None
+
+    # ------------------------------------------------------------------ readouts (brain.py:963-992)
+    def rate_np(self) -> np.ndarray:
+        key = (self.step_count, self.t)
+        if self._rate_np_key != key:
+            self._rate_np = self.rate[0].detach().cpu().numpy()
+            self._rate_np_key = key
+        return self._rate_np
+
+    def rates(self, idx) -> np.ndarray:
+        if self.B == 1:
+            return self.rate_np()[np.asarray(idx)]
+        return self.rate[:, self._idx(idx)].detach().cpu().numpy()
+
+    def mean_rate(self, idx):
+        if len(idx) == 0:
+            return 0.0 if self.B == 1 else np.zeros(self.B)
+        if self.B == 1:
+            return float(self.rate_np()[np.asarray(idx)].mean())
+        return self.rate[:, self._idx(idx)].mean(dim=1).detach().cpu().numpy()
+
+    def total_spikes(self):
+        s = self.spikes.sum(dim=1)
+        return float(s[0]) if self.B == 1 else s.cpu().numpy()
+
+    @property
+    def synaptic_events(self) -> int:
+        """Edges delivered since construction (sum over spikes of the out-degree); host sync."""
+        return int(self._events.item())

@@ -1,0 +1,445 @@
+"""Graded rate-model optic lobe on the B200 native substep: the drop-in for flyverse/optic.py.
+
+`OpticLobe(c, retina, params, device, batch, ...)` keeps the reference constructor
+(optic.py:169-172), `step_frame(col_radiance, spk_rate_hz, frame_ms) -> drive (B, N)`,
+`photoreceptor_activity`, `rates`, `relax`, `reset(rows)` and the state tensors of
+FlyBrain.OPTIC_TENSORS (fly.py:39). The matrices are built by the reference's rules
+(optic.py:238-348: per-target L1 / L2 normalisation, pair gains matched with re.match,
+per-type time constants and operating points) and run on:
+
+  flyb_photoreceptor  the photoreceptor stage (optic.py:496-517)
+  flyb_spmm           the held inputs gain_in * W_rp a_pr and gain_fb * W_rs s (optic.py:579-580),
+                      s = clamp(rate / 100, 0, 3) gathered straight from the brain's rate storage,
+                      and the drive gain_out * W_sr dr clipped to +-drive_clip (optic.py:599-602)
+  flyb_optic_run      the fused substeps: W_rr SpMV/SpMM + rate update (optic.py:525-551)
+
+State is stored unit-major, fly-minor ([n][B]); the (B, n) attributes are views of it. The
+opt-in per-stream hooks and the slow receptor term are Torch-only in the reference and are not
+provided here (they raise).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import math
+import re
+from dataclasses import dataclass
+
+import numpy as np
+import scipy.sparse as sp
+import torch
+
+from . import _abi
+from .connectome import PHOTORECEPTOR_TYPES
+
+FAMILY_OF_TYPE = {"R1-R6": 0, "R7p": 1, "R7y": 2, "R7d": 1, "R7_unclear": 2, "R8p": 3, "R8y": 4,
+                  "R8d": 1, "R8_unclear": 4, "R7R8_unclear": 2}
+# Model constants of the reference's optic lobe (optic.py:126-146), needed for identical weights.
+DEFAULT_TAU_BY_TYPE = {"Mi4": 150.0, "Mi9": 150.0, "CT1": 150.0, "Tm9": 150.0, "L3": 40.0, "Mi1": 8.0, "Tm3": 8.0,
+                       "Tm1": 8.0, "Tm2": 8.0, "Tm4": 8.0, "L1": 6.0, "L2": 6.0, "T4a": 10.0, "T4b": 10.0, "T4c": 10.0,
+                       "T4d": 10.0, "T5a": 10.0, "T5b": 10.0, "T5c": 10.0, "T5d": 10.0}
+T4T5 = ["T4a", "T4b", "T4c", "T4d", "T5a", "T5b", "T5c", "T5d"]
+DEFAULT_BASELINE_BY_TYPE = {t: 0.0 for t in T4T5}
+DEFAULT_PAIR_GAIN = [(r"^(Mi4|Mi9|CT1|C3)$", r"^T4[abcd]$", 5.0), (r"^(Tm4|Tm9|CT1|TmY15)$", r"^T5[abcd]$", 5.0),
+                     (r"^LPi(34|43)$", r"^LPLC2$", 4.0), (r"^T[45][abcd]$", r".*", 2.0)]
+
+
+@dataclass
+class OpticParams:
+    """The reference's optic-lobe parameters (optic.py:47-123), same names and defaults."""
+    tau_ms: float = 10.0
+    dt_ms: float = 1.0
+    baseline: float = 0.5
+    gain_rr: float = 1.0
+    gain_in: float = 3.0
+    norm: str = "l2"
+    gain_fb: float = 0.5
+    adapt_tau_ms: float = 400.0
+    adapt_gain: float = 1.0
+    tau_by_type: dict = None
+    baseline_by_type: dict = None
+    pair_gain: list = None
+    gain_out_mv: float = 100.0
+    out_norm: str = "l1"
+    drive_clip_mv: float = 35.0
+    tau_lp_ms: float = 10.0
+    tau_adapt_ms: float = 300.0
+    contrast_clip: float = 2.0
+    eps: float = 0.02
+    stream_rectify: list = None
+    stream_adapt: list = None
+    spatial_suppress: list = None
+    fb_hold: list = None
+
+
+# ------------------------------------------------------------------ device CSR and the products
+class DeviceCSR:
+    """A scipy CSR copied to the device as int32 row pointers / columns and float32 values."""
+
+    def __init__(self, M: sp.spmatrix, device):
+        M = sp.csr_matrix(M, dtype=np.float32)
+        M.sum_duplicates()
+        M.sort_indices()
+        if max(*M.shape, M.nnz) >= 2**31:
+            raise ValueError("the native products need 32-bit dimensions and indices")
+        self.shape, self.nnz = M.shape, int(M.nnz)
+        self.ptr = torch.from_numpy(M.indptr.astype(np.int32)).to(device)
+        self.col = torch.from_numpy(M.indices.astype(np.int32)).to(device)
+        self.w = torch.from_numpy(M.data.astype(np.float32)).to(device)
+
+    def transpose(self, device):
+        """(CSR of M^T, perm) with perm[e'] = index in M's CSR order of transposed entry e'."""
+        rows = np.repeat(np.arange(self.shape[0], dtype=np.int64), np.diff(self.ptr.cpu().numpy()))
+        cols = self.col.cpu().numpy().astype(np.int64)
+        order = np.lexsort((rows, cols))
+        T = sp.csr_matrix((self.w.cpu().numpy()[order], (cols[order], rows[order])), shape=self.shape[::-1])
+        t = DeviceCSR.__new__(DeviceCSR)
+        t.shape, t.nnz = T.shape, int(T.nnz)
+        t.ptr = torch.from_numpy(np.concatenate([[0], np.cumsum(np.bincount(cols, minlength=self.shape[1]))]).astype(np.int32)).to(device)
+        t.col = torch.from_numpy(rows[order].astype(np.int32)).to(device)
+        t.w = torch.from_numpy(self.w.cpu().numpy()[order]).to(device)
+        return t, torch.from_numpy(order.astype(np.int32)).to(device)
+
+
+def spmm(M: DeviceCSR, x: torch.Tensor, y: torch.Tensor, *, x_index=None, x_div=1.0, x_lo=-math.inf,
+         x_hi=math.inf, y_index=None, alpha=1.0, y_lo=-math.inf, y_hi=math.inf, accumulate=False) -> None:
+    """y[ymap(i)][b] (+)= clamp(alpha * sum_e w_e * clamp(x[xmap(col_e)][b] / x_div, x_lo, x_hi), y_lo, y_hi).
+
+    x, y: contiguous fly-minor storage [rows][B] on the device (include/flyb200.h: flyb_spmm)."""
+    B = x.shape[1]
+    if x.dtype != torch.float32 or y.dtype != torch.float32 or not x.is_contiguous() or not y.is_contiguous():
+        raise ValueError("spmm needs contiguous float32 [rows][batch] tensors")
+    if y.shape[1] != B:
+        raise ValueError("x and y batch widths differ")
+    a = _abi.SpmmArgs(rows=M.shape[0], cols=M.shape[1], batch=B, accumulate=int(accumulate), ptr=M.ptr.data_ptr(),
+                      col=M.col.data_ptr(), w=M.w.data_ptr(), x=x.data_ptr(),
+                      x_index=None if x_index is None else x_index.data_ptr(), x_rows=x.shape[0], x_div=x_div,
+                      x_lo=x_lo, x_hi=x_hi, y=y.data_ptr(), y_index=None if y_index is None else y_index.data_ptr(),
+                      y_rows=y.shape[0], alpha=alpha, y_lo=y_lo, y_hi=y_hi)
+    rc = _abi.lib().flyb_spmm(ct.byref(a), torch.cuda.current_stream(x.device).cuda_stream)
+    if rc:
+        raise RuntimeError(f"flyb_spmm: error {rc}")
+
+
+class OpticCore:
+    """The rate-unit recurrence on the device: W_rr, per-unit a / b, state [M][B], held inputs."""
+
+    def __init__(self, W_rr: sp.spmatrix, a: np.ndarray, b: np.ndarray, *, batch: int, device, gain_rr: float,
+                 adapt_gain: float, aad: float, launch: str = "persistent"):
+        self.device, self.B = torch.device(device), int(batch)
+        if self.device.type != "cuda":
+            raise ValueError("the optic lobe runs on a CUDA device only; there is no CPU path")
+        self._lib = _abi.lib()
+        self.W = DeviceCSR(W_rr, self.device)
+        self.m = self.W.shape[0]
+        self.a = torch.from_numpy(np.asarray(a, np.float32)).to(self.device)
+        self.b = torch.from_numpy(np.asarray(b, np.float32)).to(self.device)
+        self.gain_rr, self.adapt_gain, self.aad = float(gain_rr), float(adapt_gain), float(aad)
+        self.launch = launch
+        M, B, dev = self.m, self.B, self.device
+        self.v_s = torch.zeros(M, B, device=dev)
+        self.adapt_s = torch.zeros(M, B, device=dev)
+        self.pr_in = torch.zeros(M, B, device=dev)
+        self.spk_in = torch.zeros(M, B, device=dev)
+        self._dr = torch.zeros(M, B, device=dev)
+        self._dr_tmp = torch.zeros(M, B, device=dev)
+        self._status = torch.zeros(4, dtype=torch.int32, device=dev)
+        self._sync = torch.zeros(64, dtype=torch.int32, device=dev)
+        self._WT = None
+
+    def substeps(self, nsteps: int, v_hist: torch.Tensor | None = None, inp_hist: torch.Tensor | None = None) -> None:
+        if nsteps <= 0:
+            return
+        a = _abi.OpticArgs(m=self.m, batch=self.B, nsteps=int(nsteps), launch=_abi.LAUNCHES_BY_NAME[self.launch],
+                           ptr=self.W.ptr.data_ptr(), col=self.W.col.data_ptr(), w=self.W.w.data_ptr(),
+                           v=self.v_s.data_ptr(), adapt=self.adapt_s.data_ptr(), dr=self._dr.data_ptr(),
+                           dr_tmp=self._dr_tmp.data_ptr(), pr=self.pr_in.data_ptr(), spk=self.spk_in.data_ptr(),
+                           a=self.a.data_ptr(), b=self.b.data_ptr(), gr=self.gain_rr, ga=self.adapt_gain, aad=self.aad,
+                           flags=_abi.OPTIC_HISTORY if v_hist is not None else 0,
+                           v_hist=None if v_hist is None else v_hist.data_ptr(),
+                           inp_hist=None if inp_hist is None else inp_hist.data_ptr(),
+                           status=self._status.data_ptr(), sync=self._sync.data_ptr())
+        with torch.cuda.device(self.device):
+            rc = self._lib.flyb_optic_run(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError(f"flyb_optic_run: error {rc}")
+
+    def dr(self) -> torch.Tensor:
+        """clip(v + b, 0, 1) - b, [M][B]."""
+        return (self.v_s + self.b[:, None]).clamp(0.0, 1.0) - self.b[:, None]
+
+    def check(self) -> None:
+        s = self._status.cpu().tolist()
+        if s[0]:
+            raise RuntimeError(f"flyb200 optic kernel status {s[0]} (where {s[1]}, step {s[2]})")
+
+
+# ------------------------------------------------------------------ the reference-API lobe
+def _mask(regex: str, labels: np.ndarray) -> np.ndarray:
+    rx = re.compile(regex)
+    cache = {t: bool(rx.match(t)) for t in np.unique(labels)}
+    return np.fromiter((cache[t] for t in labels), bool, len(labels))
+
+
+def _full_mask(regex: str, labels: np.ndarray) -> np.ndarray:
+    rx = re.compile(str(regex))
+    cache = {t: bool(rx.fullmatch(t)) for t in np.unique(labels)}
+    return np.fromiter((cache[t] for t in labels), bool, len(labels))
+
+
+@dataclass
+class LobeMatrices:
+    """Everything the optic lobe derives from the connectome once (host side, scipy)."""
+    rate_idx: np.ndarray
+    pr_idx: np.ndarray
+    spk_idx: np.ndarray
+    M_rr: sp.csr_matrix
+    M_rp: sp.csr_matrix
+    M_rs: sp.csr_matrix
+    M_sr: sp.csr_matrix
+    a: np.ndarray
+    b: np.ndarray
+    aad: float
+    pr_family: np.ndarray
+    has: np.ndarray
+    avg: sp.csr_matrix
+    pr_cell: np.ndarray
+    pr_column: np.ndarray
+    sens: np.ndarray
+
+
+def lobe_matrices(c, retina, p: OpticParams, receptor=None, receptor_gain=None) -> LobeMatrices:
+    """The reference's optic-lobe construction (optic.py:229-348): unit selection, normalised and
+    gain-shaped blocks, per-type constants and the photoreceptor averaging matrix."""
+    nrn = c.neurons
+    types = nrn.type.fillna("").to_numpy()
+    is_pr = nrn.type.isin(PHOTORECEPTOR_TYPES).to_numpy()
+    rate_idx = np.flatnonzero((nrn.superclass == "ol_intrinsic").to_numpy() & ~is_pr)
+    pr_idx = np.asarray(retina.pr_index)
+    is_rate = np.zeros(c.n, bool)
+    is_rate[rate_idx] = True
+    spk_idx = np.flatnonzero(~is_rate & ~is_pr)
+    W = c.W.tocsr()
+    if receptor is not None:
+        if len(receptor.fast_sign) != W.nnz:
+            raise ValueError("receptor signs are not aligned with this connectome's W")
+        W = W.copy()
+        W.data = np.abs(W.data) * receptor.fast_factor(receptor_gain)
+    tot = c.neurons.in_syn.to_numpy()
+    Wn = (sp.diags(1.0 / np.maximum(tot, 1.0)) @ W).tocsr()
+    if p.norm == "l2":
+        Wn_ol = (sp.diags(1.0 / np.maximum(c.neurons.in_syn_l2.to_numpy(), 1.0)) @ W).tocsr()
+    else:
+        Wn_ol = Wn
+    pair_gain = DEFAULT_PAIR_GAIN if p.pair_gain is None else p.pair_gain
+
+    def gains(M, pre_types, post_types):
+        if not pair_gain:
+            return M
+        M = M.tocoo()
+        for pre_re, post_re, f in pair_gain:
+            sel = _mask(pre_re, pre_types)[M.col] & _mask(post_re, post_types)[M.row]
+            M.data[sel] *= f
+        return M.tocsr()
+
+    rt, st = types[rate_idx], types[spk_idx]
+    M_rr = gains(Wn_ol[rate_idx][:, rate_idx], rt, rt)
+    M_rs = Wn_ol[rate_idx][:, spk_idx].tocsr()
+    M_sr = gains((Wn_ol if p.out_norm == "l2" else Wn)[spk_idx][:, rate_idx], rt, st)
+    if p.fb_hold:
+        C = M_rs.tocsr()
+        rows = np.repeat(np.arange(C.shape[0]), np.diff(C.indptr))
+        keep = np.ones(C.nnz, bool)
+        for pre_re, post_re in p.fb_hold:
+            keep &= ~(_full_mask(pre_re, st)[C.indices] & _full_mask(post_re, rt)[rows])
+        indptr = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=C.shape[0]))])
+        M_rs = sp.csr_matrix((C.data[keep], C.indices[keep], indptr), shape=C.shape)
+    M_rp = Wn_ol[rate_idx][:, pr_idx].tocsr()
+    tau_map = DEFAULT_TAU_BY_TYPE if p.tau_by_type is None else p.tau_by_type
+    tau = np.array([tau_map.get(t, p.tau_ms) for t in rt], dtype=np.float32)
+    a = np.exp(-p.dt_ms / tau)
+    bl_map = DEFAULT_BASELINE_BY_TYPE if p.baseline_by_type is None else p.baseline_by_type
+    b = np.array([bl_map.get(t, p.baseline) for t in rt], dtype=np.float32)
+    pr_family = np.array([FAMILY_OF_TYPE[t] for t in types[pr_idx]], dtype=np.int64)
+    n_col = retina.n_columns
+    has = np.zeros((n_col, 5), bool)
+    np.add.at(has, (retina.pr_column, pr_family), True)
+    cnt = np.zeros((n_col, 5), np.float32)
+    np.add.at(cnt, (retina.pr_column, pr_family), 1.0)
+    rows = np.asarray(retina.pr_column) * 5 + pr_family
+    avg = sp.csr_matrix((1.0 / cnt[retina.pr_column, pr_family], (rows, np.arange(len(pr_idx)))),
+                        shape=(n_col * 5, len(pr_idx)))
+    return LobeMatrices(rate_idx, pr_idx, spk_idx, M_rr, M_rp, M_rs, M_sr, a.astype(np.float32), b,
+                        float(np.exp(-p.dt_ms / p.adapt_tau_ms)), pr_family, has, avg, rows,
+                        np.asarray(retina.pr_column, np.int64), np.asarray(retina.pr_sens, np.float32).reshape(-1, 4))
+
+
+class OpticLobe:
+    def __init__(self, c, retina, params: OpticParams | None = None, device=None, batch: int = 1,
+                 metal_kernels=None, cuda_kernels=None, cuda_sparse: str = "torch", receptor=None,
+                 receptor_gain=None, slow=None, surrogate_grad: bool = False, *, launch: str = "persistent"):
+        c.require("optic_columns")
+        self.c, self.r, self.p = c, retina, params or OpticParams()
+        p = self.p
+        if metal_kernels:
+            raise ValueError("flyb200 runs on B200 CUDA kernels only; the Metal backend is not provided")
+        if cuda_kernels is False:
+            raise ValueError("flyb200 has no Torch path: cuda_kernels=False is not available")
+        if surrogate_grad:
+            raise NotImplementedError("use flyb200.adjoint (hand-written optic adjoint) for gradients")
+        if p.stream_rectify or p.stream_adapt or p.spatial_suppress:
+            raise NotImplementedError("the per-stream hooks are Torch-only in the reference and not provided")
+        if slow is not None and receptor is not None and getattr(slow, "gain", None):
+            raise NotImplementedError("the slow receptor term is Torch-only in the reference and not provided")
+        if not np.isfinite(p.dt_ms) or p.dt_ms <= 0:
+            raise ValueError("optic dt_ms must be positive and finite")
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise ValueError("flyb200.OpticLobe runs on a CUDA device only; there is no CPU path")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.B = int(batch)
+        self.receptor, self.slow, self.surrogate_grad = receptor, None, False
+        self._pending_ms = 0.0
+        L = lobe_matrices(c, retina, p, receptor, receptor_gain)
+        self.L = L
+        self.rate_idx, self.pr_idx, self.spk_idx = L.rate_idx, L.pr_idx, L.spk_idx
+        self.n_rate, self.n_pr, self.n_spk = len(self.rate_idx), len(self.pr_idx), len(self.spk_idx)
+        self.M_rr, self.M_rp, self.M_rs, self.M_sr = L.M_rr, L.M_rp, L.M_rs, L.M_sr
+        M_rr, M_rp, M_rs, M_sr, a, b = L.M_rr, L.M_rp, L.M_rs, L.M_sr, L.a, L.b
+        self._a_ad = L.aad
+        self.core = OpticCore(M_rr, a, b, batch=self.B, device=self.device, gain_rr=p.gain_rr,
+                              adapt_gain=p.adapt_gain, aad=self._a_ad, launch=launch)
+        dev = self.device
+        self.W_rp, self.W_rs, self.W_sr = DeviceCSR(M_rp, dev), DeviceCSR(M_rs, dev), DeviceCSR(M_sr, dev)
+        self.rate_idx_t = torch.as_tensor(self.rate_idx, device=dev)
+        self.spk_idx_t = torch.as_tensor(self.spk_idx, device=dev)
+        self._spk_idx32 = self.spk_idx_t.to(torch.int32)
+        self._a, self.b_vec = self.core.a, self.core.b
+        self.pr_family, self.has = L.pr_family, L.has
+        n_col = retina.n_columns
+        self.avg = DeviceCSR(L.avg, dev)
+        self.sens = torch.from_numpy(np.ascontiguousarray(retina.pr_sens, np.float32)).to(dev)
+        self.pr_column_t = torch.as_tensor(np.asarray(retina.pr_column, np.int32), device=dev)
+        self.pr_cell_t = torch.as_tensor(L.pr_cell.astype(np.int32), device=dev)
+        self.has_t = torch.from_numpy(self.has.reshape(-1).astype(np.uint8)).to(dev)
+        B = self.B
+        self.I_lp = torch.zeros(B, n_col * 5, device=dev)
+        self.I_mean = torch.zeros(B, n_col * 5, device=dev)
+        self.contrast = torch.zeros(B, n_col * 5, device=dev)
+        self._fresh_u8 = torch.ones(B, dtype=torch.uint8, device=dev)
+        self._a_pr = torch.zeros(self.n_pr, B, device=dev)
+        self._delta = torch.zeros(self.n_rate, B, device=dev)
+        self._drive = torch.zeros(c.n, B, device=dev)
+        self.g_slow_cls = torch.zeros(0, B, self.n_rate, device=dev)
+        self.g_slow = torch.zeros(B, self.n_rate, device=dev)
+        self._slow_in_s = torch.zeros(0, B, self.n_rate, device=dev)
+        self.stream_adapt_state = torch.zeros(0, B, self.n_rate, device=dev)
+        self.r0 = None
+        self.last = {}
+        self.diagnostics = False
+
+    # public (B, n) views of the fly-minor storage
+    @property
+    def v(self):
+        return self.core.v_s.t()
+
+    @v.setter
+    def v(self, value):
+        self.core.v_s.t().copy_(value)
+
+    @property
+    def adapt(self):
+        return self.core.adapt_s.t()
+
+    @adapt.setter
+    def adapt(self, value):
+        self.core.adapt_s.t().copy_(value)
+
+    @property
+    def delta_rate(self):
+        return self._delta.t()
+
+    @property
+    def _fresh(self):
+        return self._fresh_u8.view(torch.bool)
+
+    # ------------------------------------------------------------------ photoreceptors
+    @torch.no_grad()
+    def photoreceptor_activity(self, col_radiance, dt_ms: float, *, intensity=None) -> torch.Tensor:
+        """(B, n_col, 4) radiance -> (B, n_pr) contrast activity (a view of [n_pr][B] storage)."""
+        if intensity is not None:
+            raise NotImplementedError("an intensity override is an extension-module input, not provided here")
+        p = self.p
+        rad = torch.as_tensor(col_radiance, dtype=torch.float32, device=self.device)
+        if rad.dim() == 2:
+            rad = rad[None]
+        rad = rad.expand(self.B, -1, -1).contiguous()
+        a_lp = float(np.exp(-dt_ms / p.tau_lp_ms))
+        a_ad = float(np.exp(-dt_ms / p.tau_adapt_ms))
+        args = _abi.PhotoArgs(n_pr=self.n_pr, n_col=self.r.n_columns, batch=self.B, rad=rad.data_ptr(),
+                              pr_column=self.pr_column_t.data_ptr(), sens=self.sens.data_ptr(),
+                              avg_ptr=self.avg.ptr.data_ptr(), avg_idx=self.avg.col.data_ptr(), avg_w=self.avg.w.data_ptr(),
+                              pr_cell=self.pr_cell_t.data_ptr(), has=self.has_t.data_ptr(), I_lp=self.I_lp.data_ptr(),
+                              I_mean=self.I_mean.data_ptr(), contrast=self.contrast.data_ptr(),
+                              fresh=self._fresh_u8.data_ptr(), a_lp=a_lp, c_lp=1 - a_lp, a_ad=a_ad, c_ad=1 - a_ad,
+                              eps=p.eps, clip_hi=p.contrast_clip, a_pr=self._a_pr.data_ptr())
+        rc = _abi.lib().flyb_photoreceptor(ct.byref(args), torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError(f"flyb_photoreceptor: error {rc}")
+        return self._a_pr.t()
+
+    # ------------------------------------------------------------------ rate dynamics
+    def rates(self) -> torch.Tensor:
+        return (self.v + self.b_vec[None]).clamp(0.0, 1.0)
+
+    def relax(self, ms: float = 0.0) -> None:
+        self.core.v_s.zero_()
+        self.r0 = self.b_vec[None].clone()
+
+    @staticmethod
+    def _fly_minor(x: torch.Tensor) -> torch.Tensor:
+        """[n][B] contiguous storage behind a (B, n) tensor (no copy for a Brain's state view)."""
+        t = x.t()
+        return t if t.is_contiguous() else t.contiguous()
+
+    @torch.no_grad()
+    def step_frame(self, col_radiance, spk_rate_hz, frame_ms: float, *, intensity=None,
+                   out: torch.Tensor | None = None) -> torch.Tensor:
+        """Advance one frame; returns the drive (B, N) in mV (optic.py:563-604).
+
+        `out` ([N][B] float32 storage, e.g. a Brain's drive storage) receives the drive in place."""
+        if self.r0 is None:
+            self.relax()
+        p = self.p
+        a_pr = self.photoreceptor_activity(col_radiance, frame_ms, intensity=intensity)
+        if spk_rate_hz.dim() == 1:
+            spk_rate_hz = spk_rate_hz[None]
+        rates_s = self._fly_minor(spk_rate_hz.to(self.device, torch.float32).expand(self.B, -1))
+        total = self._pending_ms + frame_ms
+        steps = int(np.floor((total + 1e-9) / p.dt_ms))
+        self._pending_ms = max(0.0, total - steps * p.dt_ms)
+        if steps:
+            spmm(self.W_rp, self._fly_minor(a_pr), self.core.pr_in, alpha=p.gain_in)
+            spmm(self.W_rs, rates_s, self.core.spk_in, x_index=self._spk_idx32, x_div=100.0, x_lo=0.0, x_hi=3.0,
+                 alpha=p.gain_fb)
+            self.core.substeps(steps)
+        torch.sub(self.rates(), self.r0, out=self.delta_rate)
+        drive = out if out is not None else self._drive
+        drive.zero_()
+        spmm(self.W_sr, self._delta, drive, y_index=self._spk_idx32, alpha=p.gain_out_mv, y_lo=-p.drive_clip_mv,
+             y_hi=p.drive_clip_mv)
+        self.last["dr"] = self.delta_rate
+        return drive.t() if out is not None else drive.t().clone()
+
+    def reset(self, rows=None) -> None:
+        if rows is None:
+            self._fresh_u8.fill_(1)
+            self.core.v_s.zero_()
+            self.core.adapt_s.zero_()
+            self._pending_ms = 0.0
+        else:
+            sel = torch.as_tensor(np.asarray(rows), device=self.device, dtype=torch.long)
+            self._fresh_u8[sel] = 1
+            self.core.v_s[:, sel] = 0.0
+            self.core.adapt_s[:, sel] = 0.0
+

@@ -1,0 +1,246 @@
+/*
+ * flyb200 -- C ABI of the B200-native brain-step engine.
+ *
+ * Every entry point takes plain pointers and sizes, launches on the caller's CUDA stream
+ * (`stream` is a cudaStream_t passed as void*), allocates nothing, and returns 0 or a
+ * cudaError_t / FLYB_E* code. Device buffers are owned by the caller (in the Python host
+ * layer: torch tensors). All kernels are compiled for sm_100a only.
+ *
+ * Two groups of entry points:
+ *
+ *  1. Reference-compatible launchers. Same names, argument order, pointer order and
+ *     semantics as the ctypes-bound functions of flyverse/kernels/neural.cu, so the
+ *     reference's loader (flyverse/cuda.py:37-79) can bind this library unchanged.
+ *
+ *  2. The native path: a fused, event-driven LIF step over an exact integer delay ring,
+ *     the fused optic-lobe SpMV/SpMM substep, the held-input products, the optic adjoint,
+ *     and the readout / photoreceptor stages. State is laid out neuron-major, fly-minor:
+ *     element (neuron i, fly b) of a (B, N) state lives at [i * batch + b].
+ */
+#ifndef FLYB200_H
+#define FLYB200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define FLYB_OK              0
+#define FLYB_EINVAL          1001   /* bad size, null pointer or inconsistent arguments */
+#define FLYB_EBARRIER        1002   /* a bounded grid-barrier wait gave up (see status word) */
+#define FLYB_ECOOP           1003   /* persistent launch does not fit co-resident on the device */
+#define FLYB_ETOOBIG         1004   /* request exceeds a stated maximum */
+
+/* ================================================================== 1. reference-compatible
+ * Pointer arrays and flags exactly as flyverse/cuda.py builds them.                        */
+
+/* Fused LIF update, one step, batch-major (B, N) float32 state.
+ * Replaces flyverse/kernels/neural.cu:54 `launch_lif` (pointer order cuda.py:103-107:
+ * v, g, drive, adapt, refrac, active, prob, rnd, res, std_u, spikes, out, rate, counts, P, phase;
+ * flags 1 Poisson, 2 STD, 4 counts, 8 adapt, 16 per-phase coefficients (8, N), 32 skip frozen). */
+int launch_lif(void** p, int n, int batch, int flags, void* stream);
+
+/* dr = clip01(v + b) - b.  Replaces neural.cu:80 `launch_optic_dr` (p: v, b, dr). */
+int launch_optic_dr(void** p, int n, int batch, void* stream);
+
+/* Optic substep update.  Replaces neural.cu:84 `launch_optic`
+ * (p: v, adapt, dr, y, pr, spk, a, b; cuda.py:123-128). */
+int launch_optic(void** p, int n, int batch, float gr, float ga, float aad, void* stream);
+
+/* out(batch, rows) = x(batch, cols) @ CSR^T, fp32 or fp16 weights.
+ * Replaces neural.cu:105 `launch_csr` (p: ptr, idx, w, x, out; cuda.py:151-152). */
+int launch_csr(void** p, int rows, int cols, int batch, int half, void* stream);
+
+/* g(batch, n) += x(batch, n) scattered over CSC columns (float atomics, as the reference).
+ * Replaces neural.cu:124 `launch_events` (p: ptr, idx, w, x, g, pre_ids; cuda.py:167-168). */
+int launch_events(void** p, int n, int batch, int half, int count, void* stream);
+
+/* out[b*stride + k] = mean of rates[b, idx[ptr[k]:ptr[k+1]]] in fixed-order double.
+ * Replaces neural.cu:141 `launch_means` (p: ptr, idx, rates, out; cuda.py:180). */
+int launch_means(void** p, int n, int groups, int batch, int stride, void* stream);
+
+/* ================================================================== 2. native path */
+
+/* LIF flags */
+#define FLYB_LIF_POISSON      1    /* Poisson forcing from poisson_p                          */
+#define FLYB_LIF_STD          2    /* short-term depression (transmit spike * res)            */
+#define FLYB_LIF_COUNTS       4    /* spike_counts += spikes                                  */
+#define FLYB_LIF_ADAPT        8    /* adaptation current                                      */
+#define FLYB_LIF_EXT_UNIFORM  16   /* Poisson uniforms from `uniforms` instead of Philox      */
+#define FLYB_LIF_SKIP_FROZEN  32   /* frozen cells at rest are left untouched                 */
+#define FLYB_LIF_EPISODES     64   /* per-fly remaining-step counters gate the update         */
+
+/* Delay-ring element types */
+#define FLYB_RING_COUNT  0   /* int32 signed synapse counts; g += w_syn * count (exact sum)     */
+#define FLYB_RING_FIXED  1   /* int64 Q32.32 millivolts; each edge rounds w*x once (exact sum)  */
+
+/* Launch modes */
+#define FLYB_LAUNCH_STEP       0   /* one kernel launch per step (the "plain" kernel)        */
+#define FLYB_LAUNCH_PERSISTENT 1   /* one cooperative launch for all steps, grid barrier/step */
+
+/* LIF coefficient vector P[FLYB_LIF_NPARAM] (float32) */
+enum {
+  FLYB_P_V_REST = 0, FLYB_P_V_RESET, FLYB_P_V_TH, FLYB_P_A_M, FLYB_P_A_S, FLYB_P_DT,
+  FLYB_P_T_REF, FLYB_P_ADAPT_JUMP, FLYB_P_A_AD, FLYB_P_A_STD, FLYB_P_A_R, FLYB_P_RATE_GAIN,
+  FLYB_P_W_SYN, FLYB_LIF_NPARAM
+};
+
+/* Words of caller scratch a persistent LIF launch needs (grid-barrier counters). */
+#define FLYB_LIF_SYNC_WORDS 64
+
+typedef struct flyb_lif_args {
+  int n;                 /* neurons                                                  */
+  int batch;             /* flies                                                    */
+  int n_delay;           /* D: a spike of step t is delivered at step t + D          */
+  int ring_slots;        /* R >= D + 1 ring slots                                    */
+  int ring_mode;         /* FLYB_RING_COUNT or FLYB_RING_FIXED                       */
+  int ring_pos;          /* slot read by the first step                              */
+  int flags;             /* FLYB_LIF_*                                               */
+  int nsteps;            /* steps to run                                             */
+  int launch;            /* FLYB_LAUNCH_*                                            */
+  int block;             /* threads per block (multiple of 32; 0 = default 256)       */
+  int grid;              /* persistent grid size cap (0 = all co-resident blocks)    */
+  int raster_slots;      /* 0: raster is [nsteps][words]; else a ring of that many slots */
+  int raster_pos;        /* ring slot written by the first step (raster_slots > 0)   */
+  int fly0;              /* global index of local fly 0 (Philox key when flies are sharded) */
+  long long step0;       /* global step index of the first step (Philox counter)     */
+  unsigned long long seed;
+  /* outgoing synapses, pre-major (CSC of W[post, pre]) */
+  const int* out_ptr;    /* [n + 1]                                                  */
+  const int* out_edge;   /* [nnz][2]: {post, count} (COUNT) or {post, float bits of w} (FIXED) */
+  /* state, [n][batch] float32 */
+  float* v; float* g; float* refrac; float* adapt; float* res;
+  float* rate; float* counts; float* spikes;
+  const float* drive; const float* poisson_p;
+  const float* active;   /* [n] 1 = spiking, 0 = frozen                              */
+  const float* std_u;    /* [n] depression use fraction                              */
+  const float* params;   /* [FLYB_LIF_NPARAM] host memory                            */
+  void* ring;            /* [R][n][batch] int32 (COUNT) or int64 (FIXED)             */
+  const float* uniforms; /* [nsteps][n][batch] when FLYB_LIF_EXT_UNIFORM             */
+  int* fly_steps;        /* [batch] remaining steps per fly when FLYB_LIF_EPISODES: fly b
+                            is live for local steps k < fly_steps[b]; after the run each
+                            entry is lowered by the steps taken (never below 0)      */
+  long long* clock;      /* optional device [3]: {step, ring_pos, raster_pos}. When set it
+                            replaces step0 / ring_pos / raster_pos and the launch advances
+                            it by nsteps, so a captured CUDA graph replays correctly */
+  unsigned* raster;      /* optional spike bits, words of ceil(n*batch/32), bit i*batch+b:
+                            [nsteps][words], or [raster_slots][words] used as a ring   */
+  unsigned long long* events; /* optional [1]: += synaptic events (edges delivered)    */
+  int* status;           /* [4] device words: [0] error code, [1] where, [2] step    */
+  int* sync;             /* [FLYB_LIF_SYNC_WORDS] zeroed device scratch (persistent) */
+} flyb_lif_args;
+
+int flyb_lif_run(const flyb_lif_args* a, void* stream);
+
+/* Deposit transmitted spikes x[n][batch] into ring slot `slot` (checkpoint import of a
+ * reference spike buffer). COUNT rings need x in {0, 1}. */
+int flyb_ring_deposit(int n, int batch, int ring_mode, const int* out_ptr, const int* out_edge,
+                      const float* x, void* ring_slot, void* stream);
+
+/* Optic lobe: `nsteps` fused substeps of y = W_rr @ dr and the rate update, state [m][batch]. */
+typedef struct flyb_optic_args {
+  int m;                 /* rate units                                               */
+  int batch;
+  int nsteps;
+  int launch;            /* FLYB_LAUNCH_*                                            */
+  int block;             /* threads per block (0 = default)                          */
+  int grid;              /* persistent grid cap (0 = occupancy)                      */
+  int lanes_per_row;     /* 0 = auto; else lanes cooperating on one row (1..32)      */
+  int flags;             /* bit0: store per-substep history (adjoint recompute)      */
+  const int* ptr; const int* col; const float* w;    /* W_rr CSR, rows = post           */
+  float* v; float* adapt;                             /* [m][batch]                      */
+  float* dr; float* dr_tmp;                           /* [m][batch] ping-pong scratch    */
+  const float* pr; const float* spk;                  /* held inputs [m][batch]          */
+  const float* a; const float* b;                     /* [m] exp(-dt/tau), operating point */
+  float gr, ga, aad;
+  int pad0;
+  float* v_hist;         /* optional [nsteps][m][batch]: v before each substep       */
+  float* inp_hist;       /* optional [nsteps][m][batch]: input of each substep       */
+  int* status; int* sync;
+} flyb_optic_args;
+
+int flyb_optic_run(const flyb_optic_args* a, void* stream);
+
+/* y[rows][batch] (+)= clamp(alpha * (M @ x'), lo, hi) with
+ * x'[j][b] = clamp(x[xmap(j)][b] / x_div, x_lo, x_hi) (xmap = identity when x_index is null;
+ * a correctly rounded division, as torch's `rate / 100.0` at flyverse/optic.py:572)
+ * and the result row i written at y[ymap(i)]. accumulate != 0 adds into y.
+ * x and y use the stated fly-minor layout with `x_rows` / `y_rows` leading rows. */
+typedef struct flyb_spmm_args {
+  int rows, cols, batch;
+  int accumulate;
+  const int* ptr; const int* col; const float* w;
+  const float* x; const int* x_index; int x_rows;
+  float x_div, x_lo, x_hi;
+  float* y; const int* y_index; int y_rows;
+  float alpha, y_lo, y_hi;
+  int lanes_per_row;
+} flyb_spmm_args;
+
+int flyb_spmm(const flyb_spmm_args* a, void* stream);
+
+/* Optic adjoint over one checkpoint segment, run backwards from step nsteps-1 to 0.
+ * Given the stored v_t and inp_t of the segment and the incoming adjoints lam_v / lam_a
+ * (of v and adapt after the segment), it leaves the adjoints at the segment start in
+ * lam_v / lam_a and accumulates
+ *   g_edge[e] += sum_t sum_b mu[t][i][b] * dr[t][j][b]      (e = (i <- j) in W_rr CSR order)
+ *   g_a[i]    += sum_t sum_b lam_v[t+1][i][b] * (v[t][i][b] - inp[t][i][b])
+ * where mu = (1 - a) * lam_v. W^T is given as CSR of the transpose with `t_perm` mapping each
+ * transposed entry to its CSR entry index. */
+typedef struct flyb_adjoint_args {
+  int m, batch, nsteps;
+  int launch;
+  int block, grid;
+  int pad0, pad1;
+  const int* t_ptr; const int* t_col; const float* t_w; const int* t_perm;  /* W_rr^T CSR */
+  const float* v_hist; const float* inp_hist;        /* [nsteps][m][batch] from forward */
+  const float* a; const float* b;
+  float gr, ga, aad;
+  int pad2;
+  float* lam_v; float* lam_a;                          /* [m][batch] in/out              */
+  float* lam_tmp;                                      /* [m][batch] scratch             */
+  float* mu;                                           /* [m][batch] scratch             */
+  float* g_edge;                                       /* [nnz] per-edge accumulator     */
+  float* g_a;                                          /* [m] d/d a_i accumulator        */
+  int* status; int* sync;
+} flyb_adjoint_args;
+
+int flyb_optic_adjoint(const flyb_adjoint_args* a, void* stream);
+
+/* Photoreceptor stage (flyverse/optic.py:496-517), fly-minor:
+ * rad [batch][n_col][4] -> I_pr -> column x family mean -> low-pass / adaptation -> contrast,
+ * writes a_pr [n_pr][batch]. `fresh` [batch] bytes are consumed (cleared). */
+typedef struct flyb_photo_args {
+  int n_pr, n_col, batch;
+  int pad0;
+  const float* rad;        /* [batch][n_col][4]                  */
+  const int* pr_column;    /* [n_pr]                             */
+  const float* sens;       /* [n_pr][4]                          */
+  const int* avg_ptr; const int* avg_idx; const float* avg_w;  /* (n_col*5) x n_pr CSR */
+  const int* pr_cell;      /* [n_pr] -> column*5 + family        */
+  const unsigned char* has;/* [n_col*5]                          */
+  float* I_lp; float* I_mean; float* contrast;   /* [batch][n_col*5] (reference layout) */
+  unsigned char* fresh;    /* [batch]                            */
+  float a_lp, c_lp;        /* low-pass coefficient exp(-dt/tau_lp) and 1 - it (rounded from double) */
+  float a_ad, c_ad;        /* adaptation coefficient and 1 - it  */
+  float eps, clip_hi;
+  float* a_pr;             /* [n_pr][batch] output                */
+} flyb_photo_args;
+
+int flyb_photoreceptor(const flyb_photo_args* a, void* stream);
+
+/* Device facts for grid sizing: SM count and co-resident blocks per SM for the persistent
+ * kernels at `block` threads. kind: 0 LIF, 1 optic, 2 adjoint. */
+int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm);
+
+/* Library version string. */
+const char* flyb_version(void);
+
+/* sizeof of the argument structs, in header order (lif, optic, spmm, adjoint, photo), so a
+ * binding can check its mirror of this header. Returns the number of sizes written. */
+int flyb_abi_sizes(int* sizes, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLYB200_H */

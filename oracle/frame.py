@@ -1,0 +1,66 @@
+"""ORACLE (test infrastructure): one optic frame on the CPU, the order of flyverse/optic.py:563-604.
+
+photoreceptor stage (optic.py:496-517) in numpy FP32, held inputs and drive through
+oracle.spmm, substeps through oracle.optic_run. State is fly-minor [n][B] like the device.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import optic_run, spmm
+
+
+def photoreceptor(L, st: dict, rad: np.ndarray, dt_ms: float, p) -> np.ndarray:
+    """rad (B, n_col, 4) -> a_pr [n_pr][B]; updates st['I_lp'], st['I_mean'], st['contrast'] (B, n_col*5)."""
+    f32 = np.float32
+    sens = L.sens.astype(f32)
+    r = rad[:, L.pr_column, :].astype(f32)                                  # (B, n_pr, 4)
+    ip = r[..., 0] * sens[:, 0]
+    for k in (1, 2, 3):
+        ip = ip + r[..., k] * sens[:, k]
+    avg = L.avg.tocsr()
+    I = np.zeros((rad.shape[0], avg.shape[0]), f32)
+    for c in range(avg.shape[0]):
+        acc = np.zeros(rad.shape[0], f32)
+        for e in range(avg.indptr[c], avg.indptr[c + 1]):
+            acc = acc + f32(avg.data[e]) * ip[:, avg.indices[e]]
+        I[:, c] = acc
+    fresh = st["fresh"][:, None]
+    lp = np.where(fresh, I, st["I_lp"])
+    mean = np.where(fresh, I, st["I_mean"])
+    st["fresh"][:] = False
+    a_lp, a_ad = float(np.exp(-dt_ms / p.tau_lp_ms)), float(np.exp(-dt_ms / p.tau_adapt_ms))
+    lp = f32(a_lp) * lp + f32(1 - a_lp) * I
+    mean = f32(a_ad) * mean + f32(1 - a_ad) * lp
+    con = np.clip((lp - mean) / (mean + f32(p.eps)), -1.0, p.contrast_clip).astype(f32)
+    con = np.where(L.has.reshape(-1)[None], con, f32(0))
+    st["I_lp"], st["I_mean"], st["contrast"] = lp.astype(f32), mean.astype(f32), con
+    return np.ascontiguousarray(con[:, L.pr_cell].T)                           # [n_pr][B]
+
+
+def frame(L, st: dict, rad: np.ndarray, spk_rate: np.ndarray, frame_ms: float, p) -> np.ndarray:
+    """Advance one frame in place; returns the drive (B, N) in mV. spk_rate: (B, N) Hz."""
+    B = rad.shape[0]
+    a_pr = photoreceptor(L, st, rad, frame_ms, p)
+    total = st["pending"] + frame_ms
+    steps = int(np.floor((total + 1e-9) / p.dt_ms))
+    st["pending"] = max(0.0, total - steps * p.dt_ms)
+    rates = np.ascontiguousarray(spk_rate.T.astype(np.float32))                # [N][B]
+    if steps:
+        M = L.M_rp.tocsr()
+        pr = spmm(M.indptr, M.indices, M.data, a_pr, B, rows=M.shape[0], alpha=p.gain_in)
+        M = L.M_rs.tocsr()
+        spk = spmm(M.indptr, M.indices, M.data, rates, B, rows=M.shape[0], x_index=L.spk_idx, x_div=100.0,
+                   x_lo=0.0, x_hi=3.0, alpha=p.gain_fb)
+        M = L.M_rr.tocsr()
+        optic_run(st["v"], st["adapt"], M.indptr, M.indices, M.data, pr, spk, L.a, L.b, p.gain_rr, p.adapt_gain,
+                  L.aad, steps)
+    b = L.b[:, None].astype(np.float32)
+    delta = (np.clip(st["v"] + b, 0.0, 1.0) - b).astype(np.float32)
+    st["delta"] = delta
+    M = L.M_sr.tocsr()
+    n = spk_rate.shape[1]
+    drive = np.zeros((n, B), np.float32)
+    spmm(M.indptr, M.indices, M.data, delta, B, rows=M.shape[0], y=drive, y_index=L.spk_idx, alpha=p.gain_out_mv,
+         y_lo=-p.drive_clip_mv, y_hi=p.drive_clip_mv)
+    return drive.T

@@ -1,0 +1,199 @@
+"""Regenerate the golden fixtures of tests/golden/ from the reference's own CPU implementation.
+
+    python tests/golden/make_golden.py [--reference /root/reference]
+
+Runs in the build container only (the reference is not on the GPU machines): it imports
+flyverse from the reference checkout and records what its CPU path produces on inputs both sides
+can rebuild. Every random input is a torch CPU generator draw or a seeded numpy draw that the tests
+regenerate; the fixtures store the reference's outputs and hashes of the inputs.
+
+  lif_c1.npz      flyverse.brain.Brain (CPU, event-driven) on the 2,000-neuron benchmark graph,
+                  three drive regimes x 1,000 steps: spike rasters (packed), final v / g / rate /
+                  counts. Uniforms: torch.rand((1, N)) per step from Generator().manual_seed(regime).
+  lif_19cell.npz  the same Brain with the default model constants (receptor_model=None) on the
+                  19-cell graph of tests/test_bit_identity.py::graph(), batch 2, depression and
+                  adaptation on: the shaped weights, rasters and final state.
+  optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
+                  of tests/test_optic_hooks.py::hex_graph(), batch 2, three frames.
+  optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
+                  synthetic 3,000-unit lobe from flyb200.synthetic.optic_config3, 60 substeps.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import sys
+from pathlib import Path
+
+os.environ.setdefault("CUDA_VISIBLE_DEVICES", "-1")
+
+import numpy as np
+import pandas as pd
+import scipy.sparse as sp
+import torch
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parents[1]
+sys.path.insert(0, str(ROOT / "flyverse-core_b200"))
+
+from flyb200 import synthetic  # noqa: E402
+
+REGIMES = {"poisson": 0.0, "drive65": 6.5, "drive72": 7.2}
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def uniforms(seed: int, steps: int, shape) -> np.ndarray:
+    gen = torch.Generator().manual_seed(seed)
+    return np.stack([torch.rand(shape, generator=gen).numpy() for _ in range(steps)])
+
+
+def lif_c1(ref) -> dict:
+    cn, brain = ref["connectome"], ref["brain"]
+    cfg = synthetic.lif_config1(seed=0)
+    c = cfg.c
+    out = {"W_sha": np.array(sha(c.W.data) + sha(c.W.indices) + sha(c.W.indptr))}
+    for k, (name, drive) in enumerate(REGIMES.items()):
+        rc = cn.Connectome(c.neurons[["bodyId", "type", "superclass", "nt"]].copy(), c.W.copy(),
+                           pd.Series(np.arange(c.n), index=c.neurons.bodyId.to_numpy()))
+        b = brain.Brain(rc, brain.LIFParams(**cfg.params, event_driven=True), device="cpu", seed=0)
+        b.set_poisson(cfg.poisson_idx, cfg.poisson_hz)
+        b.record_activity = True
+        if drive:
+            b.set_drive(np.arange(c.n), np.float32(drive))
+        U = uniforms(k, cfg.steps, (1, c.n))
+        b.gen.manual_seed(k)
+        ras = np.zeros((cfg.steps, c.n), bool)
+        for s in range(cfg.steps):
+            b.step(1)
+            ras[s] = b.spikes[0].numpy() > 0
+        out[f"{name}_raster"] = np.packbits(ras, axis=1, bitorder="little")
+        out[f"{name}_uniform_sha"] = np.array(sha(U))
+        for key in ("v", "g", "rate", "spike_counts"):
+            out[f"{name}_{key}"] = getattr(b, key)[0].numpy().copy()
+        out[f"{name}_drive"] = np.float32(drive)
+        out[f"{name}_seed"] = np.int64(k)
+        print(f"lif_c1 {name}: {int(ras.sum())} spikes")
+    return out
+
+
+def _table(n: pd.DataFrame) -> dict:
+    return {f"nrn_{col}": n[col].fillna("").astype(str).to_numpy().astype("U") for col in ("type", "superclass", "nt", "class")} | \
+        {"nrn_bodyId": n.bodyId.to_numpy().astype(np.int64)}
+
+
+def lif_19cell(ref) -> dict:
+    brain = ref["brain"]
+    tb = ref["test_bit_identity"]
+    c = tb.graph()
+    B, steps, seed = 2, 400, 7
+    p = brain.LIFParams(receptor_model=None, event_driven=True)
+    b = brain.Brain(c, p, device="cpu", seed=seed, batch=B)
+    frozen = np.flatnonzero((c.neurons.superclass == "ol_intrinsic").to_numpy())
+    b.freeze(frozen)
+    b.prune(frozen)
+    b.record_activity = True
+    orn = c.select(type="ORN_DM1")
+    jo = c.select(type="~^JO-")
+    b.set_poisson(orn, torch.tensor([[120.0], [40.0]]))
+    b.set_poisson(jo, torch.tensor([[90.0, 10.0], [0.0, 150.0]]))
+    b.set_drive(c.select(type="DNp01"), torch.tensor([[12.0], [0.0]]))
+    gen = torch.Generator().manual_seed(seed)
+    U = np.stack([torch.rand((B, c.n), generator=gen).numpy() for _ in range(steps)])
+    ras = np.zeros((steps, B, c.n), bool)
+    for s in range(steps):
+        b.step(1)
+        ras[s] = b.spikes.numpy() > 0
+    W = b._W_cpu.tocsr()
+    out = _table(c.neurons) | {"W_data": c.W.data, "W_indices": c.W.indices, "W_indptr": c.W.indptr,
+                               "shaped_data": W.data, "shaped_indices": W.indices, "shaped_indptr": W.indptr,
+                               "frozen": frozen, "orn": orn, "jo": jo, "dnp01": c.select(type="DNp01"),
+                               "raster": ras, "uniform_sha": np.array(sha(U)), "seed": np.int64(seed),
+                               "steps": np.int64(steps), "batch": np.int64(B)}
+    for key in ("v", "g", "refrac", "adapt", "res", "rate", "spike_counts", "spikes"):
+        out[f"final_{key}"] = getattr(b, key).numpy().copy()
+    print(f"lif_19cell: {int(ras.sum())} spikes, {W.nnz} shaped entries")
+    return out
+
+
+def optic_hex(ref) -> dict:
+    optic, rt = ref["optic"], ref["retina"]
+    th = ref["test_optic_hooks"]
+    c = th.hex_graph()
+    r = rt.build_retina(c)
+    B = 2
+    ol = optic.OpticLobe(c, r, optic.OpticParams(), device="cpu", batch=B)
+    ol.relax()
+    gen = torch.Generator().manual_seed(3)
+    out = _table(c.neurons) | {"W_data": c.W.data, "W_indices": c.W.indices, "W_indptr": c.W.indptr,
+                               "hex1": c.neurons.hex1.to_numpy(np.float64), "hex2": c.neurons.hex2.to_numpy(np.float64),
+                               "hex_side": c.neurons.hex_side.fillna("").astype(str).to_numpy().astype("U"),
+                               "pr_index": r.pr_index, "pr_column": r.pr_column, "pr_sens": r.pr_sens,
+                               "n_columns": np.int64(r.n_columns), "rate_idx": ol.rate_idx, "spk_idx": ol.spk_idx}
+    for f in range(3):
+        rad = torch.rand(B, r.n_columns, 4, generator=gen)
+        spk = torch.rand(B, c.n, generator=gen) * 80.0
+        drive = ol.step_frame(rad, spk, 10.0)
+        out[f"frame{f}_rad"], out[f"frame{f}_spk"] = rad.numpy(), spk.numpy()
+        for key in ("v", "adapt", "delta_rate", "contrast", "I_lp", "I_mean"):
+            out[f"frame{f}_{key}"] = getattr(ol, key).numpy().copy()
+        out[f"frame{f}_drive"] = drive.numpy().copy()
+    print("optic_hex: 3 frames")
+    return out
+
+
+def optic_synth(ref) -> dict:
+    """The reference's substep expressions on a synthetic lobe, called on the reference class."""
+    optic = ref["optic"]
+    cfg = synthetic.optic_config3(seed=1, m=3000, nnz=200_000, n_pr=300, n_types=60, n_spk=500)
+    W = cfg.W_rr()
+    B, steps = 2, 60
+    rng = np.random.default_rng(5)
+    v0 = (rng.standard_normal((B, cfg.m)) * 0.2).astype(np.float32)
+    ad0 = (rng.standard_normal((B, cfg.m)) * 0.05).astype(np.float32)
+    pr = (rng.standard_normal((B, cfg.m)) * 0.3).astype(np.float32)
+    spk = (rng.standard_normal((B, cfg.m)) * 0.1).astype(np.float32)
+    lobe = object.__new__(optic.OpticLobe)
+    lobe.p = optic.OpticParams(adapt_tau_ms=cfg.adapt_tau_ms, dt_ms=cfg.dt_ms)
+    lobe.slow, lobe._hooks = None, False
+    lobe.W_rr = torch.sparse_csr_tensor(torch.from_numpy(W.indptr.astype(np.int64)), torch.from_numpy(W.indices.astype(np.int64)),
+                                        torch.from_numpy(W.data), size=W.shape)
+    lobe._a = torch.from_numpy(cfg.a)
+    lobe.b_vec = torch.from_numpy(cfg.b)
+    lobe._a_ad = cfg.aad
+    lobe.v, lobe.adapt = torch.from_numpy(v0.copy()), torch.from_numpy(ad0.copy())
+    vs = []
+    for _ in range(steps):
+        optic.OpticLobe._substep(lobe, torch.from_numpy(pr), torch.from_numpy(spk))
+        vs.append(lobe.v.numpy().copy())
+    print("optic_synth: 60 substeps")
+    snap = np.array([0, 9, 19, 29, 39, 49, 59])
+    return {"seed": np.int64(1), "m": np.int64(cfg.m), "nnz": np.int64(200_000), "n_pr": np.int64(300),
+            "n_types": np.int64(60), "n_spk": np.int64(500), "W_sha": np.array(sha(W.data) + sha(W.indices)),
+            "v0": v0, "adapt0": ad0, "pr": pr, "spk": spk, "snap": snap, "v": np.stack(vs)[snap],
+            "adapt": lobe.adapt.numpy().copy(), "aad": np.float64(cfg.aad)}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default="/root/reference")
+    args = ap.parse_args()
+    sys.path.insert(1, args.reference)
+    sys.path.insert(2, str(Path(args.reference) / "tests"))
+    import importlib
+    ref = {k: importlib.import_module(m) for k, m in (("connectome", "flyverse.connectome"), ("brain", "flyverse.brain"),
+                                                      ("optic", "flyverse.optic"), ("retina", "flyverse.retina"),
+                                                      ("test_bit_identity", "test_bit_identity"),
+                                                      ("test_optic_hooks", "test_optic_hooks"))}
+    torch.set_num_threads(1)
+    np.savez_compressed(HERE / "lif_c1.npz", **lif_c1(ref))
+    np.savez_compressed(HERE / "lif_19cell.npz", **lif_19cell(ref))
+    np.savez_compressed(HERE / "optic_hex.npz", **optic_hex(ref))
+    np.savez_compressed(HERE / "optic_synth.npz", **optic_synth(ref))
+
+
+if __name__ == "__main__":
+    main()

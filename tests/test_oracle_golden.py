@@ -1,0 +1,163 @@
+"""The oracle pinned to the reference: its outputs against fixtures the reference's own CPU code
+produced (tests/golden/make_golden.py), and Philox against published known-answer vectors."""
+import numpy as np
+import pytest
+
+import oracle
+from oracle import frame as oframe
+from flyb200 import _abi, synthetic
+from flyb200.brain import LIFParams, lif_coefficients, out_edges
+from flyb200.optic import OpticParams, lobe_matrices
+from flyb200.retina import Retina
+from flyb200.weights import lif_weights, per_type, DEFAULT_STD_U_BY_TYPE
+from helpers import connectome_from_fixture, golden, sha, torch_uniforms, unpack
+
+
+def test_philox_known_answer_vectors():
+    # Random123 philox4x32-10 KAT vectors (counter, key) -> output
+    assert list(oracle.philox(0, [0, 0, 0, 0])) == [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]
+    assert list(oracle.philox(0xFFFFFFFFFFFFFFFF, [0xFFFFFFFF] * 4)) == [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]
+    assert list(oracle.philox(0x299F31D0A4093822, [0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344])) == \
+        [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
+
+
+def _c1_run(regime_seed, drive, ring="auto"):
+    cfg = synthetic.lif_config1(seed=0)
+    p = LIFParams(**cfg.params)
+    W, _ = lif_weights(cfg.c, p)
+    ptr, edges, mode = out_edges(W, p.w_syn, ring)
+    st = oracle.LifState(cfg.c.n, 1, 19, mode, p.v_rest)
+    st.poisson_p[cfg.poisson_idx, 0] = np.float32(cfg.poisson_hz) * np.float32(p.dt / 1000.0)
+    st.drive[:] = np.float32(drive)
+    U = torch_uniforms(regime_seed, cfg.steps, (1, cfg.c.n))
+    flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS
+    r, ev = oracle.lif_run(st, ptr, edges, lif_coefficients(p, False), n_delay=18, flags=flags, nsteps=cfg.steps,
+                           uniforms=U.transpose(0, 2, 1), raster=True)
+    return cfg, st, unpack(r, cfg.c.n), U, mode
+
+
+@pytest.mark.parametrize("regime", ["poisson", "drive65", "drive72"])
+def test_lif_config1_count_ring_matches_reference(regime):
+    z = golden("lif_c1")
+    cfg = synthetic.lif_config1(seed=0)
+    assert sha(cfg.c.W.data) + sha(cfg.c.W.indices) + sha(cfg.c.W.indptr) == str(z["W_sha"])
+    cfg, st, ras, U, mode = _c1_run(int(z[f"{regime}_seed"]), float(z[f"{regime}_drive"]))
+    assert mode == _abi.RING_COUNT
+    assert sha(U) == str(z[f"{regime}_uniform_sha"])
+    ref = np.unpackbits(z[f"{regime}_raster"], axis=1, bitorder="little")[:, : cfg.c.n].astype(bool)
+    assert ras.sum() > 0
+    np.testing.assert_array_equal(ras, ref)                       # bit-exact spike rasters
+    np.testing.assert_array_equal(st.counts[:, 0], z[f"{regime}_spike_counts"])
+    # the integer ring sums counts exactly; the reference sums float products in event order
+    np.testing.assert_allclose(st.v[:, 0], z[f"{regime}_v"], rtol=0, atol=2e-5)
+    np.testing.assert_allclose(st.g[:, 0], z[f"{regime}_g"], rtol=0, atol=2e-5)
+    np.testing.assert_allclose(st.rate[:, 0], z[f"{regime}_rate"], rtol=1e-6, atol=1e-3)
+
+
+def test_lif_config1_fixed_ring_matches_reference():
+    z = golden("lif_c1")
+    cfg, st, ras, _, mode = _c1_run(int(z["drive65_seed"]), float(z["drive65_drive"]), ring="fixed")
+    assert mode == _abi.RING_FIXED
+    ref = np.unpackbits(z["drive65_raster"], axis=1, bitorder="little")[:, : cfg.c.n].astype(bool)
+    np.testing.assert_array_equal(ras, ref)
+    np.testing.assert_allclose(st.v[:, 0], z["drive65_v"], rtol=0, atol=2e-5)
+
+
+def _nineteen():
+    z = golden("lif_19cell")
+    c = connectome_from_fixture(z)
+    p = LIFParams(receptor_model=None)
+    return z, c, p
+
+
+def test_lif_19cell_weights_identical_to_reference():
+    z, c, p = _nineteen()
+    W, _ = lif_weights(c, p)
+    keep = np.ones(c.n, np.float32)
+    keep[z["frozen"]] = 0
+    import scipy.sparse as sp
+    W = (sp.diags(keep) @ W @ sp.diags(keep)).tocsr()
+    W.eliminate_zeros()
+    np.testing.assert_array_equal(W.indptr, z["shaped_indptr"])
+    np.testing.assert_array_equal(W.indices, z["shaped_indices"])
+    np.testing.assert_array_equal(W.data, z["shaped_data"])        # float32 bit for bit
+
+
+def test_lif_19cell_rasters_match_reference():
+    """Default model constants: fan-in scale, cap, gains, adaptation, depression on ORNs -> Q32.32 ring."""
+    z, c, p = _nineteen()
+    import scipy.sparse as sp
+    W = sp.csr_matrix((z["shaped_data"], z["shaped_indices"], z["shaped_indptr"]), shape=(c.n, c.n))
+    u = per_type(c, DEFAULT_STD_U_BY_TYPE, p.std_u)
+    ptr, edges, mode = out_edges(W, p.w_syn, "auto", std_on=True)
+    assert mode == _abi.RING_FIXED
+    B, T, n = int(z["batch"]), int(z["steps"]), c.n
+    st = oracle.LifState(n, B, 5, mode, p.v_rest)        # dt 0.5: D = round(1.8 / 0.5) = 4
+    st.active[z["frozen"]] = 0
+    st.std_u[:] = u
+    dtp = np.float32(p.dt / 1000.0)
+    st.poisson_p[z["orn"], 0], st.poisson_p[z["orn"], 1] = np.float32(120.0) * dtp, np.float32(40.0) * dtp
+    st.poisson_p[z["jo"], 0] = np.array([90.0, 10.0], np.float32) * dtp
+    st.poisson_p[z["jo"], 1] = np.array([0.0, 150.0], np.float32) * dtp
+    st.drive[z["dnp01"], 0] = 12.0
+    U = torch_uniforms(int(z["seed"]), T, (B, n))
+    assert sha(U) == str(z["uniform_sha"])
+    flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD | _abi.LIF_SKIP_FROZEN
+    r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True), n_delay=4, flags=flags, nsteps=T,
+                          uniforms=U.transpose(0, 2, 1), raster=True)
+    ras = unpack(r, n * B).reshape(T, n, B).transpose(0, 2, 1)
+    assert ras.sum() > 20
+    np.testing.assert_array_equal(ras, z["raster"])
+    for key, mine in (("v", st.v), ("g", st.g), ("refrac", st.refrac), ("adapt", st.adapt), ("res", st.res),
+                      ("rate", st.rate), ("spike_counts", st.counts)):
+        np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
+
+
+def test_optic_substeps_match_reference_substep():
+    """FP32 oracle vs the reference's own _substep on a synthetic lobe (1e-5 relative)."""
+    z = golden("optic_synth")
+    cfg = synthetic.optic_config3(seed=int(z["seed"]), m=int(z["m"]), nnz=int(z["nnz"]), n_pr=int(z["n_pr"]),
+                                  n_types=int(z["n_types"]), n_spk=int(z["n_spk"]))
+    W = cfg.W_rr()
+    assert sha(W.data) + sha(W.indices) == str(z["W_sha"])
+    v, ad = np.ascontiguousarray(z["v0"].T), np.ascontiguousarray(z["adapt0"].T)
+    pr, spk = np.ascontiguousarray(z["pr"].T), np.ascontiguousarray(z["spk"].T)
+    done = 0
+    v64, ad64 = v.astype(np.float64), ad.astype(np.float64)
+    for k, s in enumerate(z["snap"]):
+        oracle.optic_run(v, ad, W.indptr, W.indices, W.data, pr, spk, cfg.a, cfg.b, 1.0, 1.0, float(z["aad"]), s + 1 - done)
+        oracle.optic_run_f64(v64, ad64, W.indptr, W.indices, W.data, pr, spk, cfg.a, cfg.b, 1.0, 1.0, float(z["aad"]),
+                             s + 1 - done)
+        done = s + 1
+        ref = z["v"][k].T
+        np.testing.assert_allclose(v, ref, rtol=1e-5, atol=1e-6)
+        assert np.abs(v64 - ref).max() < 1e-4                       # FP32 reference vs FP64 restatement
+    np.testing.assert_allclose(ad, z["adapt"].T, rtol=1e-5, atol=1e-6)
+
+
+def hex_lobe():
+    z = golden("optic_hex")
+    c = connectome_from_fixture(z, extra=())
+    c.neurons["hex1"], c.neurons["hex2"], c.neurons["hex_side"] = z["hex1"], z["hex2"], z["hex_side"]
+    r = Retina(pr_index=z["pr_index"], pr_column=z["pr_column"], pr_sens=z["pr_sens"],
+               col_side=np.array(["L"] * int(z["n_columns"])), col_hex=np.zeros((int(z["n_columns"]), 2)))
+    return z, c, r
+
+
+def test_optic_hex_frames_match_reference():
+    z, c, r = hex_lobe()
+    p = OpticParams()
+    L = lobe_matrices(c, r, p)
+    np.testing.assert_array_equal(L.rate_idx, z["rate_idx"])
+    np.testing.assert_array_equal(L.spk_idx, z["spk_idx"])
+    B = 2
+    st = {"v": np.zeros((len(L.rate_idx), B), np.float32), "adapt": np.zeros((len(L.rate_idx), B), np.float32),
+          "I_lp": np.zeros((B, r.n_columns * 5), np.float32), "I_mean": np.zeros((B, r.n_columns * 5), np.float32),
+          "fresh": np.ones(B, bool), "pending": 0.0}
+    for f in range(3):
+        drive = oframe.frame(L, st, z[f"frame{f}_rad"], z[f"frame{f}_spk"], 10.0, p)
+        np.testing.assert_allclose(st["contrast"], z[f"frame{f}_contrast"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["v"].T, z[f"frame{f}_v"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["adapt"].T, z[f"frame{f}_adapt"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["delta"].T, z[f"frame{f}_delta_rate"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(drive, z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
