@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Headline benchmark: neuron-steps/s of the whole-fly brain step at 167,106 neurons.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl flyb200|reference]
+
+Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthetic.whole_fly_config5,
+167,106 neurons = 89,390 graded optic units + 71,618 LIF + 6,098 Poisson-driven sensory cells,
+25.6 M edges (~124 M synapses), dt 0.1 ms, optic <-> LIF coupling every step, a drifting grating on
+5,895 photoreceptors. One step advances all 167,106 neurons of every fly once (flyb200.whole).
+
+  value          neuron-steps/s of B=64 flies per GPU (whole job over N GPUs, weak scaling),
+                 steps replayed from a CUDA graph; state > L2, so no flush is needed
+  batch1         the plain single-instance kernels (B=1, one launch per kernel per step), L2 flushed
+                 between timed steps, for the "vs plain" ratio
+  adjoint        optic-lobe adjoint over 200 substeps (89,390 units, 6 M nnz, checkpoint 20) over
+                 the forward pass time
+  e2e            the same B=64 step through the public API with, every step, the radiance copied in
+                 from pinned host memory and the motor readout copied out
+  roofline       the LIF step kernel: algorithmic bytes / CUDA-event time against measured HBM copy
+  cpu_baseline   the C oracle port (oracle/) on this host's cores, a bounded sample of the workload
+`--impl reference` times that CPU port alone on the same config and prints the same line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT, ROOT / "flyverse-core_b200"):
+    if str(_p) not in sys.path:
+        sys.path.insert(0, str(_p))
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "neuron-steps/s at 167k neurons (batch 1 & 64, vs plain); adjoint/forward cost"
+BATCH = 64
+L2_BYTES = 126 * 2**20
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.proc = index, None
+        self.path = Path(tempfile.mkstemp(prefix="flyb_clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self) -> dict:
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()] if self.path.exists() else []
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ helpers
+def flush_l2(buf: torch.Tensor) -> None:
+    buf.add_(1.0)
+
+
+def events_time(fn, reps: int, flush=None) -> float:
+    """Mean device ms of fn() over reps, each bracketed by CUDA events on the current stream."""
+    total = 0.0
+    for _ in range(reps):
+        if flush is not None:
+            flush()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        e.synchronize()
+        total += s.elapsed_time(e)
+    return total / reps
+
+
+def build_engine(cfg, batch, device, launch, fly0=0):
+    from flyb200.whole import WholeFly
+    eng = WholeFly(cfg, batch, device=device, seed=1, launch=launch)
+    eng.lif._args.fly0 = fly0
+    o = cfg.optic
+    rad = torch.from_numpy(o.grating(0.0, batch, seed=fly0)).to(device)
+    a_pr = photoreceptor_contrast(cfg, rad)
+    eng.set_photoreceptors(a_pr)
+    return eng
+
+
+def photoreceptor_contrast(cfg, rad: torch.Tensor) -> torch.Tensor:
+    """Held photoreceptor activity [n_pr][B] of a radiance frame (B, n_col, 4): channel-weighted
+    intensity, contrast against the frame mean (the stage's steady state)."""
+    o = cfg.optic
+    sens = torch.from_numpy(o.sens).to(rad.device)
+    col = torch.from_numpy(o.pr_column.astype(np.int64)).to(rad.device)
+    ip = (rad[:, col, :] * sens[None]).sum(-1)                            # (B, n_pr)
+    con = ((ip - ip.mean(1, keepdim=True)) / (ip.mean(1, keepdim=True) + 0.02)).clamp(-1.0, 2.0)
+    return con.t().contiguous()
+
+
+def capture(eng, steps: int):
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            eng.step(steps)
+    torch.cuda.current_stream().wait_stream(s)
+    return g
+
+
+# ------------------------------------------------------------------ measurements
+def measure_batched(cfg, device, steps, warmup, fly0):
+    eng = build_engine(cfg, BATCH, device, "step", fly0)
+    eng.step(max(3, warmup))
+    chunk = max(1, min(25, steps))
+    g = capture(eng, chunk)
+    reps = max(1, math.ceil(steps / chunk))
+    g.replay()
+    torch.cuda.synchronize()
+    return eng, g, chunk, reps
+
+
+def time_graph(g, reps) -> float:
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s.record()
+    for _ in range(reps):
+        g.replay()
+    e.record()
+    e.synchronize()
+    return s.elapsed_time(e)
+
+
+def kernel_roofline(eng, reps=20) -> dict:
+    """The LIF step and the optic substep timed alone with CUDA events (B=64)."""
+    lif_ms = events_time(lambda: eng.lif.step(1), reps)
+    opt_ms = events_time(lambda: eng.optic.substeps(1), reps)
+    lif_b, opt_b = eng.lif_bytes_per_step(), eng.optic_bytes_per_step()
+    return {"lif_ms": lif_ms, "optic_ms": opt_ms, "lif_bytes": lif_b, "optic_bytes": opt_b}
+
+
+def measure_plain(cfg, device, steps, warmup):
+    eng = build_engine(cfg, 1, device, "step")
+    eng.step(max(3, warmup))
+    torch.cuda.synchronize()
+    buf = torch.zeros(int(2 * L2_BYTES // 4), device=device)
+    n = min(steps, 50)
+    ms = events_time(lambda: eng.step(1), n, flush=lambda: flush_l2(buf))
+    del buf
+    return eng, ms
+
+
+def measure_adjoint(device) -> dict:
+    from flyb200 import synthetic
+    from flyb200.adjoint import OpticAdjoint
+    cfg = synthetic.optic_config3(seed=3)
+    rng = np.random.default_rng(0)
+    m, T = cfg.m, 200
+    pr = torch.from_numpy((rng.standard_normal((m, 1)) * 0.2).astype(np.float32)).to(device)
+    spk = torch.zeros(m, 1, device=device)
+    eng = OpticAdjoint(cfg.W0, cfg.pair_id, len(cfg.gain0), cfg.type_of, cfg.n_types, cfg.b, pr, spk,
+                       dt_ms=cfg.dt_ms, batch=1, checkpoint=20, device=device)
+    eng.set_params(torch.from_numpy(cfg.gain0), torch.from_numpy(cfg.tau_of_type))
+    v0 = torch.from_numpy((rng.standard_normal((m, 1)) * 0.2).astype(np.float32)).to(device)
+    a0 = torch.zeros(m, 1, device=device)
+    w = torch.zeros(m, 1, device=device)
+    w[:50], w[50:100] = 1 / 50, -1 / 50
+    eng.forward(v0, a0, T)
+    eng.backward(w)
+    fwd = events_time(lambda: eng.forward(v0, a0, T), 3)
+    bwd = events_time(lambda: eng.backward(w), 3)
+    eng.check()
+    return {"forward_ms": fwd, "backward_ms": bwd, "ratio": bwd / fwd, "units": m, "nnz": int(cfg.W0.nnz), "steps": T,
+            "checkpoint": 20}
+
+
+def measure_e2e(cfg, eng, device, steps) -> dict:
+    """Public-API loop: pinned radiance in, photoreceptor activity + one step, motor readout out."""
+    from flyb200 import cuda as fcuda
+    o, B = cfg.optic, eng.B
+    rad_host = torch.from_numpy(o.grating(0.0, B, seed=0)).pin_memory()
+    rad_dev = torch.empty_like(rad_host, device=device)
+    groups = np.array_split(np.asarray(cfg.vpn_idx[:900]), 90)
+    ptr = torch.tensor(np.r_[0, np.cumsum([len(g) for g in groups])], dtype=torch.int32, device=device)
+    idx = torch.tensor(np.concatenate(groups), dtype=torch.int32, device=device)
+    out_host = torch.empty(B, 90, dtype=torch.float64).pin_memory()
+    rate = eng.lif.rate                               # (B, N) view; the readout reads it batch-major
+    rate_bm = torch.empty(B, cfg.n_spiking, device=device)
+    n = min(steps, 100)
+
+    def one():
+        rad_dev.copy_(rad_host, non_blocking=True)
+        eng.set_photoreceptors(photoreceptor_contrast(cfg, rad_dev))
+        eng.step(1)
+        rate_bm.copy_(rate)
+        out_host.copy_(fcuda.group_means(ptr, idx, rate_bm), non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(3):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(n):
+        one()
+    dt = time.perf_counter() - t0
+    return {"value": eng.n_neurons * B * n / dt, "unit": "neuron-steps/s",
+            "h2d_bytes_per_step": int(rad_host.numel() * 4), "d2h_bytes_per_step": int(out_host.numel() * 8),
+            "steps": n}
+
+
+def cpu_port_rate(cfg, batch: int, steps: int, threads: int) -> dict:
+    """The oracle whole-fly step on host cores: neuron-steps/s over a bounded sample."""
+    import oracle
+    from flyb200 import _abi
+    from flyb200.brain import LIFParams, lif_coefficients, out_edges
+    from flyb200.weights import lif_weights
+    p = LIFParams(**cfg.lif.params)
+    W, _ = lif_weights(cfg.lif.c, p)
+    ptr, edges, mode = out_edges(W, p.w_syn)
+    n = cfg.n_spiking
+    st = oracle.LifState(n, batch, 19, mode, p.v_rest)
+    st.poisson_p[cfg.sensory_idx, :] = np.float32(cfg.lif.poisson_hz) * np.float32(p.dt / 1000.0)
+    o = cfg.optic
+    Wr = o.W_rr()
+    tau = o.tau_of_type[o.type_of].astype(np.float32)
+    a = np.exp(-0.1 / tau).astype(np.float32)
+    aad = float(np.exp(-0.1 / o.adapt_tau_ms))
+    m = o.m
+    v = np.zeros((m, batch), np.float32)
+    ad = np.zeros((m, batch), np.float32)
+    rng = np.random.default_rng(0)
+    pr = (rng.standard_normal((m, batch)) * 0.1).astype(np.float32)
+    Wrs, Wsr = o.W_rs.tocsr(), o.W_sr.tocsr()
+    P = lif_coefficients(p, False)
+    flags = _abi.LIF_POISSON | _abi.LIF_COUNTS
+
+    def step():
+        spk = oracle.spmm(Wrs.indptr, Wrs.indices, Wrs.data, st.rate, batch, rows=m, x_div=100.0, x_lo=0.0, x_hi=3.0,
+                          alpha=o.gain_fb)
+        oracle.optic_run(v, ad, Wr.indptr, Wr.indices, Wr.data, pr, spk, a, o.b, o.gain_rr, o.adapt_gain, aad, 1,
+                         threads=threads)
+        dr = (np.clip(v + o.b[:, None], 0, 1) - o.b[:, None]).astype(np.float32)
+        oracle.spmm(Wsr.indptr, Wsr.indices, Wsr.data, dr, batch, rows=n, y=st.drive, alpha=o.gain_out_mv,
+                    y_lo=-o.drive_clip_mv, y_hi=o.drive_clip_mv)
+        oracle.lif_run(st, ptr, edges, P, n_delay=18, flags=flags, nsteps=1, seed=1, threads=threads)
+
+    step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    dt = time.perf_counter() - t0
+    return {"value": (m + n) * batch * steps / dt, "unit": "neuron-steps/s", "cores": threads,
+            "kind": "port", "sample": f"{steps} whole-fly steps x {batch} flies ({m + n:,} neurons) on the C oracle"}
+
+
+# ------------------------------------------------------------------ arms
+def reference_arm(args) -> None:
+    """The CPU port of the path (the C oracle; the reference itself is Python/torch and is not
+    installed on the GPU machines), timed on every host thread, same metric and config."""
+    from flyb200 import synthetic
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = synthetic.whole_fly_config5(seed=0)
+    threads = os.cpu_count() or 1
+    batch = 8
+    r = cpu_port_rate(cfg, batch, max(1, min(args.steps, 6)), threads)
+    line = {"metric": METRIC, "value": r["value"], "unit": "neuron-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "whole fly 167,106 neurons / 25.6M edges, dt 0.1 ms", "batch": batch},
+            "impl": "reference", "cpu_baseline": r,
+            "e2e": {"value": r["value"], "unit": "neuron-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="flyb200", choices=["flyb200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=device)
+    from flyb200 import synthetic
+    from flyb200 import build as fbuild
+    fbuild.build()
+    cfg = synthetic.whole_fly_config5(seed=0)
+    N = cfg.n_rate + cfg.n_spiking
+    eng, g, chunk, reps = measure_batched(cfg, device, args.steps, args.warmup, fly0=rank * BATCH)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = eng.lif.synaptic_events
+    with Clocks(local) as clk:
+        ms = time_graph(g, reps)
+    clocks = clk.summary()
+    timed_steps = chunk * reps
+    events_per_step = (eng.lif.synaptic_events - ev0) / timed_steps
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        del g                      # no collective is captured; release the graph before the group
+        dist.destroy_process_group()
+    value = N * BATCH * world * timed_steps / (ms / 1000.0)
+    eng.lif.check()
+    if rank != 0:
+        return
+    roof = kernel_roofline(eng)
+    peaks = load_peaks()
+    lif_gbs = roof["lif_bytes"] / (roof["lif_ms"] / 1000.0) / 1e9
+    opt_gbs = roof["optic_bytes"] / (roof["optic_ms"] / 1000.0) / 1e9
+    dom = "lif" if roof["lif_ms"] >= roof["optic_ms"] else "optic"
+    achieved = lif_gbs if dom == "lif" else opt_gbs
+    plain_eng, plain_ms = measure_plain(cfg, device, args.steps, args.warmup)
+    batch1 = N / (plain_ms / 1000.0)
+    adj = measure_adjoint(device)
+    e2e = measure_e2e(cfg, eng, device, args.steps)
+    traffic = None
+    tp = ROOT / "profiles" / "traffic.json"
+    if tp.exists():
+        traffic = json.loads(tp.read_text()).get(dom)
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cpu_port_rate(cfg, 8, 3, os.cpu_count() or 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": "neuron-steps/s", "n_gpus": world, "steps": timed_steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms / timed_steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded whole_fly_config5)",
+        "config": {"workload": "whole fly 167,106 neurons (89,390 optic + 71,618 LIF + 6,098 sensory), 25.6M edges, "
+                               "dt 0.1 ms, optic<->LIF coupling every step", "batch_per_gpu": BATCH,
+                   "flies_total": BATCH * world, "l2": "state of 64 flies > 126 MB L2; no flush needed",
+                   "parallelism": f"fly shards x{world}, no per-step collective"},
+        "batch1": {"value": batch1, "ms_per_step": plain_ms, "l2": "flushed between timed steps",
+                   "launches": "one launch per kernel per step"},
+        "batched_over_plain": value / world / batch1,
+        "adjoint": adj,
+        "synaptic_events_per_s": events_per_step * world * timed_steps / (ms / 1000.0),
+        "roofline": {"bound": "hbm", "kernel": f"{dom} step (B=64)", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "peak_source": peaks["source"], "lif_gbs": lif_gbs, "optic_gbs": opt_gbs,
+                     "lif_ms": roof["lif_ms"], "optic_ms": roof["optic_ms"], "lif_bytes": roof["lif_bytes"],
+                     "optic_bytes": roof["optic_bytes"]},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": eng.launches_per_step * timed_steps,
+        "clocks": clocks,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -36,6 +36,23 @@ __device__ __forceinline__ void st_release(int* p, int v) {
 // co-resident ends with an error status instead of hanging.
 constexpr long long kSpinLimit = 1ll << 24;   // polls with a 64-256 ns backoff: seconds at most
 
+// Polls *p until it differs from `value`, at most `limit` times (or until status is set).
+// Returns false, with FLYB_EBARRIER recorded at `where`, when the limit ran out.
+__device__ __forceinline__ bool bounded_wait_ne(const int* p, int value, int* status, long long limit, int where,
+                                                int step) {
+  long long it = 0;
+  unsigned ns = 64;
+  while (ld_acquire(p) == value) {
+    if (++it > limit || ld_acquire(status) != 0) {
+      set_error(status, FLYB_EBARRIER, where, step);
+      return false;
+    }
+    __nanosleep(ns);
+    if (ns < 256) ns <<= 1;
+  }
+  return true;
+}
+
 __device__ __forceinline__ bool grid_barrier(int* sync, int* status, int& generation, int step) {
   __syncthreads();
   __shared__ int ok;
@@ -49,18 +66,8 @@ __device__ __forceinline__ bool grid_barrier(int* sync, int* status, int& genera
       sync[0] = 0;
       __threadfence();
       st_release(&sync[1], gen + 1);
-    } else {
-      long long it = 0;
-      unsigned ns = 64;
-      while (ld_acquire(&sync[1]) == gen) {
-        if (++it > kSpinLimit || ld_acquire(status) != 0) {
-          set_error(status, FLYB_EBARRIER, 1, step);
-          ok = 0;
-          break;
-        }
-        __nanosleep(ns);
-        if (ns < 256) ns <<= 1;
-      }
+    } else if (!bounded_wait_ne(&sync[1], gen, status, kSpinLimit, 1, step)) {
+      ok = 0;
     }
     __threadfence();
   }

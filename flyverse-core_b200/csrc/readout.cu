@@ -71,6 +71,11 @@ __global__ void photo_gather_kernel(PhotoK k) {
   if (p == 0) k.fresh[b] = 0;
 }
 
+// One thread waits on a flag that nothing sets; the bounded wait gives up and records the error.
+__global__ void selftest_wait_kernel(const int* flag, int* status, long long spins) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) bounded_wait_ne(flag, 0, status, spins, 2, -1);
+}
+
 int lif_blocks_per_sm(int block);
 int optic_blocks_per_sm();
 int adjoint_blocks_per_sm();
@@ -115,6 +120,12 @@ FLYB_API int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_
   else if (kind == 2) b = adjoint_blocks_per_sm();
   else return FLYB_EINVAL;
   if (blocks_per_sm) *blocks_per_sm = b;
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_selftest_wait(const int* flag, int* status, long long spins, void* stream) {
+  if (!flag || !status || spins < 0) return FLYB_EINVAL;
+  selftest_wait_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(flag, status, spins);
   return (int)cudaGetLastError();
 }
 

@@ -103,6 +103,7 @@ SIGNATURES = {
     "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
     "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
+    "flyb_selftest_wait": [_VP, _VP, ct.c_longlong, _VP],
     "flyb_version": [],
     "flyb_abi_sizes": [ct.POINTER(_I), _I],
 }

@@ -260,3 +260,47 @@ def optic_config3(seed: int = 0, m: int = 89_390, nnz: int | None = 6_000_000, n
                        W0=W0, pair_id=pair_id.astype(np.int32), pairs=pairs, gain0=gain0, W_rp=W_rp.astype(np.float32),
                        W_rs=W_rs, W_sr=W_sr, n_pr=n_pr, n_col=n_col, pr_column=pr_column, pr_family=pr_family,
                        sens=sens, col_xy=col_xy)
+
+
+# ------------------------------------------------------------------ whole fly
+@dataclass
+class WholeFlyConfig:
+    """167,106 neurons = n_rate graded optic units + n_lif spiking + n_sensory Poisson-driven spiking.
+
+    Edge budget (total `edges`, default 25.6 M, counts geometric(0.2) so ~128 M synapses):
+      rate <- rate  W_rr  `optic_nnz` (optic_config3's rule)
+      spiking <- spiking  the rest after the three coupling blocks, lognormal(4.9, 1.2) out-degree
+                          over all spiking cells (sensory included), scaled to the remainder
+      spiking <- rate  W_sr  visual projection drive: 5 % of spiking cells, 50 rate inputs each ... scaled
+      rate <- spiking  W_rs  feedback: 2 % of rate units, 20 spiking inputs each
+      rate <- photoreceptor  W_rp  lamina (first 10 % of rate units), 6 photoreceptors of its column
+    The photoreceptors are the optic lobe's input stage (driven by the grating), not counted in N.
+    """
+    lif: LifConfig
+    optic: OpticConfig
+    sensory_idx: np.ndarray        # spiking-population rows of the Poisson-driven sensory cells
+    vpn_idx: np.ndarray            # spiking-population rows driven by the optic lobe (W_sr rows)
+    n_rate: int
+    n_spiking: int
+    edges: int
+
+
+def whole_fly_config5(seed: int = 0, n_rate: int = 89_390, n_lif: int = 71_618, n_sensory: int = 6_098,
+                      edges: int = 25_600_000, optic_nnz: int = 6_000_000, n_pr: int = 5_895) -> WholeFlyConfig:
+    rng = np.random.default_rng(seed)
+    n_spk = n_lif + n_sensory
+    optic = optic_config3(seed=seed + 1, m=n_rate, nnz=optic_nnz, n_pr=n_pr, n_spk=n_spk)
+    coupling = optic.W_rp.nnz + optic.W_rs.nnz + optic.W_sr.nnz
+    lif_edges = edges - optic_nnz - coupling
+    deg = np.minimum(np.round(rng.lognormal(4.9, 1.2, n_spk)).astype(np.int64), n_spk)
+    deg = scale_degrees(deg, lif_edges, n_spk)
+    pre, post = distinct_targets(rng, deg, n_spk)
+    W = _lif_graph(rng, n_spk, pre, post, 0.2, 0.6)
+    sensory = np.arange(n_lif, n_spk)                          # the last block of the spiking population
+    types = np.where(np.arange(n_spk) >= n_lif, "SENSORY", "LIF")
+    table = neuron_table(n_spk, type_names=types)
+    lif = LifConfig(f"whole fly, {n_rate + n_spk:,} neurons / {edges:,} edges", from_arrays(table, W), sensory,
+                    100.0, 2000)
+    vpn = np.unique(optic.W_sr.tocoo().row)
+    return WholeFlyConfig(lif=lif, optic=optic, sensory_idx=sensory, vpn_idx=vpn, n_rate=n_rate, n_spiking=n_spk,
+                          edges=int(W.nnz + optic.W0.nnz + coupling))

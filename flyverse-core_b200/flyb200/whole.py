@@ -1,0 +1,85 @@
+"""The whole-fly brain step: spiking LIF population and graded optic lobe, coupled every step.
+
+One step of dt advances every neuron once, in the order of the reference's frame
+(flyverse/fly.py:477-498 -> optic.py:563-604 -> brain.py:819-870) with the optic <-> LIF coupling
+refreshed every step instead of every 10 ms frame:
+
+  1. spk_in = gain_fb * W_rs clamp(rate / 100, 0, 3)     (flyb_spmm, gathers the LIF rate storage)
+  2. one optic substep: W_rr SpMV/SpMM + rate update      (flyb_optic_run)
+  3. drive[vpn] = clip(gain_out * W_sr dr, +-35 mV)       (flyb_spmm into the LIF drive storage)
+  4. one fused LIF step over the spiking population       (flyb_lif_run)
+and, every `frame_steps` steps, the photoreceptor stage and pr_in = gain_in * W_rp a_pr. All
+buffers are allocated at construction, so `capture(k)` records k steps into one CUDA graph.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import _abi
+from .brain import Brain, LIFParams
+from .optic import DeviceCSR, OpticCore, spmm
+from .synthetic import WholeFlyConfig
+
+
+class WholeFly:
+    def __init__(self, cfg: WholeFlyConfig, batch: int, *, device="cuda", seed: int = 0, dt_ms: float = 0.1,
+                 launch: str = "step", poisson_hz=None, record_activity: bool = True):
+        self.cfg, self.B = cfg, int(batch)
+        self.device = torch.device(device)
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        o = cfg.optic
+        self.dt_ms = dt_ms
+        params = dict(cfg.lif.params)
+        params["dt"] = dt_ms
+        self.lif = Brain(cfg.lif.c, LIFParams(**params), device=self.device, seed=seed, batch=self.B, launch=launch)
+        self.lif.record_activity = record_activity
+        hz = cfg.lif.poisson_hz if poisson_hz is None else poisson_hz
+        self.lif.set_poisson(cfg.sensory_idx, torch.as_tensor(hz, dtype=torch.float32))
+        tau = o.tau_of_type[o.type_of].astype(np.float32)
+        a = np.exp(-dt_ms / tau).astype(np.float32)
+        aad = float(np.exp(-dt_ms / o.adapt_tau_ms))
+        self.optic = OpticCore(o.W_rr(), a, o.b, batch=self.B, device=self.device, gain_rr=o.gain_rr,
+                               adapt_gain=o.adapt_gain, aad=aad, launch="step")
+        dev = self.device
+        self.W_rs, self.W_sr, self.W_rp = DeviceCSR(o.W_rs, dev), DeviceCSR(o.W_sr, dev), DeviceCSR(o.W_rp, dev)
+        self.a_pr = torch.zeros(o.n_pr, self.B, device=dev)
+        self.launches_per_step = 4 + (1 if launch == "step" else 0) + 1   # spmm, optic init + substep, spmm, lif (+advance)
+        self.steps_taken = 0
+
+    @property
+    def n_neurons(self) -> int:
+        return self.cfg.n_rate + self.cfg.n_spiking
+
+    def set_photoreceptors(self, a_pr: torch.Tensor) -> None:
+        """Photoreceptor activity [n_pr][B] -> held pr_in = gain_in * W_rp a_pr (a frame's input)."""
+        self.a_pr.copy_(a_pr)
+        spmm(self.W_rp, self.a_pr, self.optic.pr_in, alpha=self.cfg.optic.gain_in)
+
+    def step(self, n: int = 1) -> None:
+        o = self.cfg.optic
+        lif_rate = self.lif._st["rate"]
+        drive = self.lif._st["drive"]
+        for _ in range(int(n)):
+            spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb)
+            self.optic.substeps(1)
+            spmm(self.W_sr, self.optic._dr_tmp, drive, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
+                 y_hi=o.drive_clip_mv)
+            self.lif.step(1)
+        self.steps_taken += int(n)
+
+    # ------------------------------------------------------------------ algorithmic bytes (roofline)
+    def lif_bytes_per_step(self) -> int:
+        """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate, counts
+        read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active."""
+        per = 4 * (5 * 2 + 4 + 1)
+        return self.cfg.n_spiking * (self.B * per + 4)
+
+    def optic_bytes_per_step(self) -> int:
+        """CSR once (idx + w) + row pointers, per unit-fly v, adapt r+w, pr, spk, dr in / out."""
+        o = self.cfg.optic
+        nnz = int(o.W0.nnz)
+        return nnz * 8 + (o.m + 1) * 4 + o.m * self.B * 4 * 8 + o.m * 8

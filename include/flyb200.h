@@ -233,6 +233,12 @@ int flyb_photoreceptor(const flyb_photo_args* a, void* stream);
  * kernels at `block` threads. kind: 0 LIF, 1 optic, 2 adjoint. */
 int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm);
 
+/* Failure-detection self test: one thread polls `flag` (device int, never set by anyone) through the
+ * same bounded wait the grid barriers use, gives up after `spins` polls and records FLYB_EBARRIER in
+ * status[0] (where = 2). Lets a host check that a wait that cannot complete ends with an error
+ * status instead of a hang. No counterpart in the reference. */
+int flyb_selftest_wait(const int* flag, int* status, long long spins, void* stream);
+
 /* Library version string. */
 const char* flyb_version(void);
 

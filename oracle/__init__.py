@@ -107,7 +107,7 @@ class LifState:
 
 
 def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0,
-            uniforms=None, fly_steps=None, raster=False, threads=0):
+            uniforms=None, fly_steps=None, raster=False, threads=0, fly0=0):
     """Advance `state` in place by `nsteps`; returns (raster bits [nsteps][words] or None, events).
     With `fly_steps` (EPISODES), fly b is live for its first fly_steps[b] steps; the array is then
     reduced by the steps taken, as the host layer does after a launch."""
@@ -121,7 +121,7 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
     uni = None if uniforms is None else _f32(uniforms)
     fs = None if fly_steps is None else np.ascontiguousarray(fly_steps, np.int32)
     a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
-                     ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, step0=state.step, seed=seed,
+                     ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, step0=state.step, seed=seed, fly0=fly0,
                      out_ptr=_p(out_ptr), out_edge=_p(out_edge), v=_p(state.v), g=_p(state.g),
                      refrac=_p(state.refrac), adapt=_p(state.adapt), res=_p(state.res), rate=_p(state.rate),
                      counts=_p(state.counts), spikes=_p(state.spikes), drive=_p(state.drive),

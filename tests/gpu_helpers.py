@@ -1,0 +1,58 @@
+"""Run the native LIF entry point on a host-side oracle.LifState, through the C ABI (GPU tests)."""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import torch
+
+from flyb200 import _abi
+
+LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "drive", "poisson_p")
+
+
+def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
+                   fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
+                   device="cuda"):
+    """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
+    dev = torch.device(device)
+    n, B = state.n, state.batch
+    words = (n * B + 31) // 32
+    d = {k: torch.from_numpy(getattr(state, k)).to(dev) for k in LIF_ARRAYS}
+    active = torch.from_numpy(state.active).to(dev)
+    std_u = torch.from_numpy(state.std_u).to(dev)
+    ring = torch.from_numpy(state.ring).to(dev)
+    ptr = torch.from_numpy(np.ascontiguousarray(out_ptr, np.int32)).to(dev)
+    edge = torch.from_numpy(np.ascontiguousarray(out_edge, np.int32)).to(dev)
+    uni = None if uniforms is None else torch.from_numpy(np.ascontiguousarray(uniforms, np.float32)).to(dev)
+    fs = None if fly_steps is None else torch.from_numpy(np.ascontiguousarray(fly_steps, np.int32)).to(dev)
+    r = torch.zeros(nsteps, words, dtype=torch.int32, device=dev) if raster else None
+    events = torch.zeros(1, dtype=torch.int64, device=dev)
+    status = torch.zeros(4, dtype=torch.int32, device=dev)
+    sync = torch.zeros(_abi.LIF_SYNC_WORDS, dtype=torch.int32, device=dev)
+    P = np.ascontiguousarray(params, np.float32)
+    a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
+                     ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, launch=launch, block=block, grid=grid,
+                     fly0=fly0, step0=state.step, seed=seed, out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
+                     v=d["v"].data_ptr(), g=d["g"].data_ptr(), refrac=d["refrac"].data_ptr(),
+                     adapt=d["adapt"].data_ptr(), res=d["res"].data_ptr(), rate=d["rate"].data_ptr(),
+                     counts=d["counts"].data_ptr(), spikes=d["spikes"].data_ptr(), drive=d["drive"].data_ptr(),
+                     poisson_p=d["poisson_p"].data_ptr(), active=active.data_ptr(), std_u=std_u.data_ptr(),
+                     params=P.ctypes.data, ring=ring.data_ptr(), uniforms=None if uni is None else uni.data_ptr(),
+                     fly_steps=None if fs is None else fs.data_ptr(), raster=None if r is None else r.data_ptr(),
+                     events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr())
+    rc = _abi.lib().flyb_lif_run(ct.byref(a), torch.cuda.current_stream(dev).cuda_stream)
+    if rc:
+        raise RuntimeError(f"flyb_lif_run: error {rc}")
+    torch.cuda.synchronize(dev)
+    st = status.cpu().numpy()
+    if st[0]:
+        raise RuntimeError(f"kernel status {st.tolist()}")
+    for k in LIF_ARRAYS:
+        getattr(state, k)[...] = d[k].cpu().numpy()
+    state.ring[...] = ring.cpu().numpy()
+    state.ring_pos = (state.ring_pos + nsteps) % state.ring_slots
+    state.step += nsteps
+    if fly_steps is not None:
+        fly_steps[...] = fs.cpu().numpy()
+    return (r.cpu().numpy().view(np.uint32) if raster else None), int(events.item())
