@@ -415,7 +415,7 @@ using namespace flyb;
 
 FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   if (!a || a->n <= 0 || a->batch <= 0 || a->n_delay < 1 || a->ring_slots < a->n_delay + 1 || a->nsteps < 0 ||
-      !a->out_ptr || !a->out_edge || !a->v || !a->g || !a->refrac || !a->adapt || !a->res || !a->rate ||
+      !a->out_ptr || !a->v || !a->g || !a->refrac || !a->adapt || !a->res || !a->rate ||
       !a->counts || !a->spikes || !a->drive || !a->poisson_p || !a->active || !a->params || !a->ring ||
       (a->ring_mode != FLYB_RING_COUNT && a->ring_mode != FLYB_RING_FIXED))
     return FLYB_EINVAL;

@@ -341,7 +341,7 @@ int optic_blocks_per_sm() {
 using namespace flyb;
 
 FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
-  if (!a || a->m <= 0 || a->batch <= 0 || a->nsteps < 0 || !a->ptr || !a->col || !a->w || !a->v || !a->adapt ||
+  if (!a || a->m <= 0 || a->batch <= 0 || a->nsteps < 0 || !a->ptr || !a->v || !a->adapt ||
       !a->dr || !a->dr_tmp || !a->pr || !a->spk || !a->a || !a->b)
     return FLYB_EINVAL;
   if ((long long)a->m * a->batch >= (1ll << 31)) return FLYB_ETOOBIG;
@@ -355,7 +355,7 @@ FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
 }
 
 FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
-  if (!a || a->rows < 0 || a->batch <= 0 || !a->ptr || !a->col || !a->w || !a->x || !a->y || a->x_div == 0.0f)
+  if (!a || a->rows < 0 || a->batch <= 0 || !a->ptr || !a->x || !a->y || a->x_div == 0.0f)
     return FLYB_EINVAL;
   if (a->rows == 0) return 0;
   SpmmK k{a->rows, a->batch, a->accumulate, a->ptr, a->col, a->w, a->x, a->x_index, a->x_div, a->x_lo, a->x_hi,

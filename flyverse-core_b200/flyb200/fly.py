@@ -1,0 +1,249 @@
+"""The frame loop around the brain step: the drop-in for the brain-step part of flyverse/fly.py.
+
+`FlyBrain` holds a batched `Brain` and, when the connectome has an eye, an `OpticLobe`, and
+advances them frame by frame exactly as flyverse/fly.py:448-610 does: fractional milliseconds carry
+over, the optic frame runs once per frame on the held radiance and writes the LIF drive, pulses
+from `stimulate` end on a LIF step boundary, and with `cuda_graphs=True` each distinct frame shape
+(steps, ring position, Poisson on, radiance present, optic remainder) is captured once and replayed.
+Captured frames advance the device step clock themselves, so replays draw fresh Poisson numbers.
+Senses, motor programs and the body of the reference are outside the brain step; inputs arrive as
+Poisson rates (`set_input`, `stimulate`) and radiance (`vision`), outputs as group means (`motor`).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import asdict
+
+import numpy as np
+import torch
+
+from . import cuda as fcuda
+from .brain import Brain, LIFParams
+from .connectome import PHOTORECEPTOR_TYPES
+from .optic import OpticLobe, OpticParams
+from .retina import build_retina
+
+
+class FlyBrain:
+    BRAIN_TENSORS = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
+    OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate")
+
+    def __init__(self, c, *, batch: int = 1, device=None, seed: int = 0, lif_params: LIFParams | None = None,
+                 optic_params: OpticParams | None = None, cuda_graphs: bool = False, retina=None,
+                 launch: str = "persistent", receptor=None):
+        if c.n == 0:
+            raise ValueError("FlyBrain needs at least one neuron")
+        self.c = c
+        lp = lif_params or LIFParams()
+        self.brain = Brain(c, lp, device=device, seed=seed, batch=batch, launch=launch, receptor=receptor)
+        self.B, self.device = self.brain.B, self.brain.device
+        self.brain.record_activity = True
+        self.cuda_graphs = bool(cuda_graphs)
+        self._graphs = {}
+        self.retina = self.optic = None
+        has_eye = "hex1" in c.neurons and bool(c.neurons.type.isin(PHOTORECEPTOR_TYPES).any()) and \
+            bool((c.neurons.superclass == "ol_intrinsic").any())
+        if retina is not None or has_eye:
+            self.retina = retina if retina is not None else build_retina(c)
+            if self.retina.n_columns:
+                self.optic = OpticLobe(c, self.retina, optic_params, device=self.device, batch=self.B,
+                                       receptor=receptor, launch=launch)
+                self.optic.relax()
+                self.brain.freeze(self.optic.rate_idx)
+                if lp.prune_frozen:
+                    self.brain.prune(self.optic.rate_idx)
+        self._radiance = None
+        self._pending_ms = 0.0
+        self._base_poisson = torch.zeros_like(self.brain.poisson_p)
+        self._inputs_on = {}
+        self._pulses = []
+        self._activity_ms = np.zeros(self.B)
+
+    @property
+    def t(self) -> float:
+        return self.brain.t
+
+    # ------------------------------------------------------------------ inputs
+    def vision(self, radiance) -> None:
+        """(columns, 4) or (B, columns, 4) radiance [UV, B, G, R], held until the next call."""
+        if self.optic is None:
+            raise ValueError("vision is absent from this connectome subset")
+        value = torch.as_tensor(radiance, dtype=torch.float32, device=self.device)
+        if value.ndim == 2:
+            value = value[None].expand(self.B, -1, -1)
+        if value.shape != (self.B, self.retina.n_columns, 4):
+            raise ValueError(f"radiance must have shape ({self.B}, {self.retina.n_columns}, 4) or ({self.retina.n_columns}, 4)")
+        if not bool(torch.isfinite(value).all() & (value >= 0).all()):
+            raise ValueError("radiance must be finite and nonnegative")
+        if self._radiance is None:
+            self._radiance = value.clone()
+        else:
+            self._radiance.copy_(value)
+
+    def set_input(self, name: str, idx, hz) -> None:
+        """A held sensory Poisson input (the reference's `_input`, fly.py:312-324)."""
+        ti = self.brain._idx(idx)
+        prob = torch.as_tensor(np.asarray(hz, dtype=np.float32), device=self.device) * (self.brain.p.dt / 1000)
+        self.brain.poisson_p[:, ti] = prob
+        self._base_poisson[:, ti] = prob
+        self._inputs_on[name] = bool(np.any(np.asarray(hz) > 0))
+        if self._pulses:
+            self._refresh_poisson()
+        else:
+            self.brain._poisson_on = any(self._inputs_on.values())
+
+    def stimulate(self, selection, hz, ms) -> None:
+        """A Poisson pulse combined with the held inputs by maximum, ending on a LIF boundary."""
+        if not math.isfinite(ms) or ms <= 0:
+            raise ValueError("pulse duration must be positive and finite")
+        idx = self.c.indices(selection)
+        value = np.broadcast_to(np.asarray(hz, dtype=np.float32), (self.B, len(idx))).copy()
+        if not np.isfinite(value).all() or np.any((value < 0) | (value * self.brain.p.dt > 1000)):
+            raise ValueError("pulse rates must be finite and between 0 and 1000/dt Hz")
+        duration = math.ceil(ms / self.brain.p.dt) * self.brain.p.dt
+        self._pulses.append((idx.copy(), value, self.t + duration))
+        self._refresh_poisson()
+
+    def _refresh_poisson(self) -> None:
+        self.brain.poisson_p.copy_(self._base_poisson)
+        self._pulses = [p for p in self._pulses if p[2] > self.t + 1e-9]
+        for idx, hz, _ in self._pulses:
+            ti = self.brain._idx(idx)
+            prob = torch.as_tensor(hz, device=self.device) * (self.brain.p.dt / 1000)
+            self.brain.poisson_p[:, ti] = torch.maximum(self.brain.poisson_p[:, ti], prob)
+        self.brain._poisson_on = any(self._inputs_on.values()) or any(np.any(p[1] > 0) for p in self._pulses)
+
+    # ------------------------------------------------------------------ stepping (fly.py:398-610)
+    def step(self, ms: float = 10.0) -> float:
+        """Advance a frame; fractional LIF steps carry over. Returns the simulated ms."""
+        if not math.isfinite(ms) or ms < 0:
+            raise ValueError("ms must be finite and nonnegative")
+        total = self._pending_ms + ms
+        steps = int(math.floor((total + 1e-9) / self.brain.p.dt))
+        elapsed = steps * self.brain.p.dt
+        self._pending_ms = max(0.0, total - elapsed)
+        if not steps:
+            return 0.0
+        if self.cuda_graphs and not any(p[2] < self.t + elapsed - 1e-9 for p in self._pulses):
+            self._graph_frame(steps)
+            if self._pulses:
+                self._refresh_poisson()
+            self._activity_ms += elapsed
+            return elapsed
+        self._vision_frame(elapsed)
+        remaining = steps
+        while remaining:
+            count = remaining
+            if self._pulses:
+                until = min(p[2] for p in self._pulses) - self.t
+                count = min(count, max(1, int(round(until / self.brain.p.dt))))
+            self.brain.step(count)
+            remaining -= count
+            if self._pulses:
+                self._refresh_poisson()
+        self._activity_ms += elapsed
+        return elapsed
+
+    def _vision_frame(self, elapsed: float) -> None:
+        if self.optic is not None and self._radiance is not None:
+            self.optic.step_frame(self._radiance, self.brain.rate, elapsed, out=self.brain._st["drive"])
+
+    def _frame(self, steps: int) -> None:
+        self._vision_frame(steps * self.brain.p.dt)
+        self.brain.step(steps)
+
+    def _graph_frame(self, steps: int) -> None:
+        b, o = self.brain, self.optic
+        if getattr(self, "_graph_weights_version", None) != b._weights_version:
+            self._graphs.clear()
+            self._graph_weights_version = b._weights_version
+        pending = o._pending_ms if o is not None else 0.0
+        key = (steps, b.buf_pos, b._poisson_on, b.record_activity, self._radiance is not None, round(pending, 9))
+        if key not in self._graphs:
+            if len(self._graphs) >= 8:
+                self._frame(steps)
+                return
+            stream = torch.cuda.Stream(device=self.device)
+            stream.wait_stream(torch.cuda.current_stream(self.device))
+            graph = torch.cuda.CUDAGraph()
+            scalars = b.t, b.step_count, b.buf_pos
+            with torch.cuda.stream(stream):
+                with torch.cuda.graph(graph, stream=stream):
+                    self._frame(steps)            # recorded, not run: the device clock is untouched
+            torch.cuda.current_stream(self.device).wait_stream(stream)
+            b.t, b.step_count, b.buf_pos = scalars
+            if o is not None:
+                o._pending_ms = pending
+            self._graphs[key] = graph
+        self._graphs[key].replay()
+        b.t += steps * b.p.dt
+        b.step_count += steps
+        b.buf_pos = (b.buf_pos + steps) % b.R
+        if o is not None and self._radiance is not None:
+            total = pending + steps * b.p.dt
+            o._pending_ms = max(0.0, total - int(math.floor((total + 1e-9) / o.p.dt_ms)) * o.p.dt_ms)
+
+    # ------------------------------------------------------------------ outputs
+    def motor(self, groups: dict) -> dict:
+        """{name: (B,) mean rate in Hz} of named neuron groups, one GPU reduction and one copy
+        (the native motor readout, flyverse/motor.py:232-270)."""
+        names = list(groups)
+        idx = [np.asarray(groups[k], np.int64) for k in names]
+        ptr = torch.tensor(np.r_[0, np.cumsum([len(i) for i in idx])], dtype=torch.int32, device=self.device)
+        flat = torch.tensor(np.concatenate(idx) if idx else np.zeros(0, np.int64), dtype=torch.int32, device=self.device)
+        means = fcuda.group_means(ptr, flat, self.brain.rate.contiguous()).cpu().numpy()
+        return {k: means[:, n] for n, k in enumerate(names)}
+
+    def reset(self, rows=None) -> None:
+        self.brain.reset(rows)
+        if self.optic is not None:
+            self.optic.reset(rows)
+        sel = slice(None) if rows is None else self.brain._idx(rows)
+        self._base_poisson[sel] = 0
+        if rows is None:
+            self._pulses.clear()
+            self._inputs_on.clear()
+            self._pending_ms = 0.0
+            self._activity_ms[:] = 0.0
+            self._graphs.clear()
+            self._radiance = None
+            self.brain.t, self.brain.step_count, self.brain.buf_pos = 0.0, 0, 0
+            self.brain._clock.zero_()
+        else:
+            self._activity_ms[np.asarray(rows)] = 0.0
+            for _, hz, _ in self._pulses:
+                hz[np.asarray(rows)] = 0
+        self._refresh_poisson()
+
+    def state_dict(self) -> dict:
+        o = self.optic
+        return {"version": 1, "body_ids": self.c.neurons.bodyId.to_numpy().copy(),
+                "lif_params": asdict(self.brain.p), "optic_params": asdict(o.p) if o is not None else None,
+                "brain": self.brain.state_dict(),
+                "optic": {k: getattr(o, k).detach().cpu().clone() for k in self.OPTIC_TENSORS} if o is not None else None,
+                "optic_fresh": o._fresh_u8.cpu().clone() if o is not None else None,
+                "optic_pending_ms": o._pending_ms if o is not None else 0.0,
+                "radiance": self._radiance.detach().cpu().clone() if self._radiance is not None else None,
+                "base_poisson": self._base_poisson.cpu().clone(), "inputs_on": dict(self._inputs_on),
+                "pulses": [(i.copy(), h.copy(), e) for i, h, e in self._pulses], "pending_ms": self._pending_ms,
+                "activity_ms": self._activity_ms.copy()}
+
+    def load_state_dict(self, state: dict) -> None:
+        if state["version"] != 1 or not np.array_equal(state["body_ids"], self.c.neurons.bodyId.to_numpy()):
+            raise ValueError("state version/connectome does not match")
+        if state["lif_params"] != asdict(self.brain.p):
+            raise ValueError("state simulation parameters do not match")
+        self._graphs.clear()
+        self.brain.load_state_dict(state["brain"])
+        o = self.optic
+        if o is not None:
+            for k in self.OPTIC_TENSORS:
+                getattr(o, k).copy_(state["optic"][k].to(self.device))
+            o._fresh_u8.copy_(state["optic_fresh"].to(self.device))
+            o._pending_ms = state["optic_pending_ms"]
+            o.r0 = o.b_vec[None].clone()
+        self._radiance = state["radiance"].to(self.device).clone() if state["radiance"] is not None else None
+        self._base_poisson.copy_(state["base_poisson"].to(self.device))
+        self._inputs_on = dict(state["inputs_on"])
+        self._pulses = [(i.copy(), h.copy(), e) for i, h, e in state["pulses"]]
+        self._pending_ms, self._activity_ms = state["pending_ms"], state["activity_ms"].copy()

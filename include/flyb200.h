@@ -4,7 +4,8 @@
  * Every entry point takes plain pointers and sizes, launches on the caller's CUDA stream
  * (`stream` is a cudaStream_t passed as void*), allocates nothing, and returns 0 or a
  * cudaError_t / FLYB_E* code. Device buffers are owned by the caller (in the Python host
- * layer: torch tensors). All kernels are compiled for sm_100a only.
+ * layer: torch tensors). All kernels are compiled for sm_100a only. Column / weight / edge
+ * arrays of a sparse matrix may be null when the matrix has no entries.
  *
  * Two groups of entry points:
  *
