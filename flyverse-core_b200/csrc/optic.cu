@@ -8,6 +8,8 @@
 // 32/F lane groups split the entries when the batch is narrower than a warp. The gathered vector
 // (dr, 0.36 MB per fly) stays L2-resident; the CSR streams from HBM once per substep for all flies.
 // Substeps ping-pong dr between two buffers, so one grid barrier per substep suffices.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace flyb {
@@ -350,6 +352,51 @@ FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
   OpticK k{a->m, a->batch, a->nsteps, a->ptr, a->col, a->w, a->v, a->adapt, a->dr, a->dr_tmp, a->pr, a->spk,
            a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
            (a->flags & 1) ? a->inp_hist : nullptr, a->status, a->sync};
+  cudaStream_t st = (cudaStream_t)stream;
+  FLYB_BATCH_DISPATCH(a->batch, (run_optic<F, FPL>(k, a->launch, a->grid, st)));
+}
+
+// ------------------------------------------------------------------ allocation-free variant
+// Scratch of flyb_optic_run_noalloc: the two dr ping-pong buffers (FLYB_OPTIC_NOALLOC_MAX floats
+// each) and the grid-barrier words, in one file-scope device array. Every GPU that loads this
+// library holds it (8 MiB + 256 B) until the process exits.
+static __device__ __align__(256) float g_optic_scratch[2 * FLYB_OPTIC_NOALLOC_MAX + 64];
+
+// Device address of g_optic_scratch per device ordinal. Host code must not hand the symbol itself
+// to a kernel (on the host it is a stand-in, not a device address): the address is looked up once
+// per device, with that device current, by cudaGetSymbolAddress.
+static std::mutex g_scratch_mu;
+static float* g_scratch_addr[256];
+
+static int optic_noalloc_scratch(float** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return (int)e;
+  if (dev < 0 || dev >= 256) return FLYB_EINVAL;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_optic_scratch);
+    if (e != cudaSuccess || !p) return e != cudaSuccess ? (int)e : FLYB_EINVAL;
+    g_scratch_addr[dev] = (float*)p;
+  }
+  *out = g_scratch_addr[dev];
+  return 0;
+}
+
+FLYB_API int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream) {
+  if (!a || a->m <= 0 || a->batch <= 0 || a->nsteps < 0 || !a->ptr || !a->v || !a->adapt || !a->pr || !a->spk ||
+      !a->a || !a->b)
+    return FLYB_EINVAL;
+  if ((long long)a->m * a->batch > FLYB_OPTIC_NOALLOC_MAX) return FLYB_ETOOBIG;
+  if (a->launch == FLYB_LAUNCH_PERSISTENT && !a->status) return FLYB_EINVAL;
+  float* scratch = nullptr;
+  const int rc = optic_noalloc_scratch(&scratch);
+  if (rc) return rc;
+  if (a->nsteps == 0) return 0;
+  OpticK k{a->m, a->batch, a->nsteps, a->ptr, a->col, a->w, a->v, a->adapt, scratch, scratch + FLYB_OPTIC_NOALLOC_MAX,
+           a->pr, a->spk, a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
+           (a->flags & 1) ? a->inp_hist : nullptr, a->status, (int*)(scratch + 2 * FLYB_OPTIC_NOALLOC_MAX)};
   cudaStream_t st = (cudaStream_t)stream;
   FLYB_BATCH_DISPATCH(a->batch, (run_optic<F, FPL>(k, a->launch, a->grid, st)));
 }

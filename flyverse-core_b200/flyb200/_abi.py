@@ -99,6 +99,7 @@ SIGNATURES = {
     "flyb_lif_run": [ct.POINTER(LifArgs), _VP],
     "flyb_ring_deposit": [_I, _I, _I, _VP, _VP, _VP, _VP, _VP],
     "flyb_optic_run": [ct.POINTER(OpticArgs), _VP],
+    "flyb_optic_run_noalloc": [ct.POINTER(OpticArgs), _VP],
     "flyb_spmm": [ct.POINTER(SpmmArgs), _VP],
     "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],

@@ -162,6 +162,21 @@ typedef struct flyb_optic_args {
 
 int flyb_optic_run(const flyb_optic_args* a, void* stream);
 
+/* Allocation-free variant of flyb_optic_run; no counterpart in the reference. For callers that
+ * cannot allocate device memory: a host that owns every device buffer and forbids allocation in its
+ * step callback, code running under a fixed memory budget, or a CUDA-graph recorder that must not
+ * see allocations. The dr ping-pong buffers and the barrier words (`dr`, `dr_tmp`, `sync` of the
+ * argument struct, which are ignored here) live in a file-scope device array of the library, sized
+ * for m * batch <= FLYB_OPTIC_NOALLOC_MAX unit-flies (2 x 4 MiB + 256 B, held by every GPU that loads
+ * the library until the process exits); larger requests return FLYB_ETOOBIG. The caller still passes
+ * the state (v, adapt), the held inputs, the constants and, for a persistent launch, `status`.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current) and should come before any stream capture. Every call shares the array: calls
+ * that overlap on the GPU (other streams, other threads) race on it and must be serialised; each
+ * call recomputes dr from v and clears the barrier words, so no state carries over between calls. */
+#define FLYB_OPTIC_NOALLOC_MAX (1 << 20)
+int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream);
+
 /* y[rows][batch] (+)= clamp(alpha * (M @ x'), lo, hi) with
  * x'[j][b] = clamp(x[xmap(j)][b] / x_div, x_lo, x_hi) (xmap = identity when x_index is null;
  * a correctly rounded division, as torch's `rate / 100.0` at flyverse/optic.py:572)
