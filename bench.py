@@ -143,8 +143,10 @@ def capture(eng, steps: int):
 
 # ------------------------------------------------------------------ measurements
 def measure_batched(cfg, device, steps, warmup, fly0):
+    from flyb200 import autotune
     eng = build_engine(cfg, BATCH, device, "step", fly0)
     eng.step(max(3, warmup))
+    eng.tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
     chunk = max(1, min(25, steps))
     g = capture(eng, chunk)
     reps = max(1, math.ceil(steps / chunk))
@@ -388,6 +390,7 @@ def main() -> None:
                      "optic_bytes": roof["optic_bytes"]},
         "cpu_baseline": cpu,
         "e2e": e2e,
+        "autotune": {k: {kk: vv for kk, vv in v.items()} for k, v in eng.tuned.items()},
         "gpu_launches": eng.launches_per_step * timed_steps,
         "clocks": clocks,
     }

@@ -79,35 +79,40 @@ __device__ __forceinline__ void adj_phase2(const AdjK& k, int t, const float* __
     float acc[FPL];
 #pragma unroll
     for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+    constexpr int U = FPL <= 2 ? 8 : (FPL == 4 ? 4 : 2);
     const int e0 = k.t_ptr[j], e1 = k.t_ptr[j + 1];
-    for (int base = e0; base < e1; base += 32) {
-      const int e = base + lane;
-      int ci = 0;
-      float cw = 0.0f;
-      if (e < e1) { ci = __ldg(&k.t_col[e]); cw = __ldg(&k.t_w[e]); }
-      const int cnt = min(32, e1 - base);
-      for (int idx = 0; idx < cnt; idx += G) {
-        const int src = idx + g;
-        const int i = __shfl_sync(0xffffffffu, ci, src & 31);
-        const float wv = __shfl_sync(0xffffffffu, cw, src & 31);
-        float ge = 0.0f;
-        if (src < cnt) {
+    // lane group g takes entries e0 + g + G*k; U gathers of mu in flight per lane
+    for (int base = e0 + g; base - g < e1; base += G * U) {
+      int ii[U];
+      float ww[U];
 #pragma unroll
-          for (int q = 0; q < FPL; ++q) {
-            if (fb + q < k.batch) {
-              const float mv = mu[(size_t)i * k.batch + fb + q];
-              const float p = wv * mv;
-              acc[q] = acc[q] + p;
-              const float pg = mv * dr[q];
-              ge = ge + pg;
-            }
-          }
+      for (int u = 0; u < U; ++u) {
+        const int e = base + u * G;
+        const bool ok = e < e1;
+        ii[u] = ok ? __ldg(&k.t_col[e]) : -1;
+        ww[u] = ok ? __ldg(&k.t_w[e]) : 0.0f;
+      }
+      float mv[U][FPL];
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int q = 0; q < FPL; ++q)
+          mv[u][q] = (ii[u] >= 0 && fb + q < k.batch) ? mu[(size_t)ii[u] * k.batch + fb + q] : 0.0f;
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        float ge = 0.0f;
+#pragma unroll
+        for (int q = 0; q < FPL; ++q) {
+          const float p = ww[u] * mv[u][q];
+          acc[q] = acc[q] + p;
+          const float pg = mv[u][q] * dr[q];
+          ge = ge + pg;
         }
-        // sum the per-edge term over the F lanes of this group
+        // sum the per-edge term over the F lanes of this group (every lane takes part)
 #pragma unroll
         for (int o = 1; o < F; o <<= 1) ge = ge + __shfl_xor_sync(0xffffffffu, ge, o);
-        if (src < cnt && f == 0) {
-          const int ee = base + src;
+        if (ii[u] >= 0 && f == 0) {
+          const int ee = base + u * G;
           const int pe = k.t_perm ? k.t_perm[ee] : ee;
           k.g_edge[pe] = k.g_edge[pe] + ge;
         }

@@ -11,6 +11,8 @@
 // deterministic and equal to the C restatement in oracle/flyoracle.c bit for bit.
 //
 // Layout: state [n][batch] (fly-minor), ring [R][n][batch]; work item t = i * batch + b.
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace flyb {
@@ -93,144 +95,279 @@ __device__ __forceinline__ void advance_clock(const LifK& k, const Clk& c) {
     for (int b = threadIdx.x; b < k.batch; b += blockDim.x) k.fly_steps[b] = max(k.fly_steps[b] - k.nsteps, 0);
 }
 
-// One block processes work items [base, base + BLOCK) of local step `s`: update, then deliver.
-template <int BLOCK, bool FIXED>
-__device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, long long base, LifSmem<BLOCK>& sm) {
+// Vector access of IPT consecutive items (16-byte loads / stores when IPT == 4).
+template <int IPT, typename T>
+__device__ __forceinline__ void vload(const T* p, T (&x)[IPT]) {
+  if constexpr (IPT == 2 && sizeof(T) == 4) {
+    const float2 q = *reinterpret_cast<const float2*>(p);
+    x[0] = *reinterpret_cast<const T*>(&q.x); x[1] = *reinterpret_cast<const T*>(&q.y);
+  } else if constexpr (IPT == 2 && sizeof(T) == 8) {
+    const longlong2 a = *reinterpret_cast<const longlong2*>(p);
+    x[0] = *reinterpret_cast<const T*>(&a.x); x[1] = *reinterpret_cast<const T*>(&a.y);
+  } else if constexpr (IPT == 4 && sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    x[0] = *reinterpret_cast<const T*>(&q.x);
+    x[1] = *reinterpret_cast<const T*>(&q.y); x[2] = *reinterpret_cast<const T*>(&q.z); x[3] = *reinterpret_cast<const T*>(&q.w);
+  } else if constexpr (IPT == 4 && sizeof(T) == 8) {
+    const longlong2 a = *reinterpret_cast<const longlong2*>(p), b = *reinterpret_cast<const longlong2*>(p + 2);
+    x[0] = *reinterpret_cast<const T*>(&a.x); x[1] = *reinterpret_cast<const T*>(&a.y);
+    x[2] = *reinterpret_cast<const T*>(&b.x); x[3] = *reinterpret_cast<const T*>(&b.y);
+  } else {
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) x[q] = p[q];
+  }
+}
+
+template <int IPT, typename T>
+__device__ __forceinline__ void vstore(T* p, const T (&x)[IPT]) {
+  if constexpr (IPT == 2 && sizeof(T) == 4) {
+    float2 q;
+    q.x = *reinterpret_cast<const float*>(&x[0]); q.y = *reinterpret_cast<const float*>(&x[1]);
+    *reinterpret_cast<float2*>(p) = q;
+  } else if constexpr (IPT == 2 && sizeof(T) == 8) {
+    longlong2 a;
+    a.x = *reinterpret_cast<const long long*>(&x[0]); a.y = *reinterpret_cast<const long long*>(&x[1]);
+    *reinterpret_cast<longlong2*>(p) = a;
+  } else if constexpr (IPT == 4 && sizeof(T) == 4) {
+    float4 q;
+    q.x = *reinterpret_cast<const float*>(&x[0]); q.y = *reinterpret_cast<const float*>(&x[1]);
+    q.z = *reinterpret_cast<const float*>(&x[2]); q.w = *reinterpret_cast<const float*>(&x[3]);
+    *reinterpret_cast<float4*>(p) = q;
+  } else if constexpr (IPT == 4 && sizeof(T) == 8) {
+    longlong2 a, b;
+    a.x = *reinterpret_cast<const long long*>(&x[0]); a.y = *reinterpret_cast<const long long*>(&x[1]);
+    b.x = *reinterpret_cast<const long long*>(&x[2]); b.y = *reinterpret_cast<const long long*>(&x[3]);
+    *reinterpret_cast<longlong2*>(p) = a;
+    *reinterpret_cast<longlong2*>(p + 2) = b;
+  } else {
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) p[q] = x[q];
+  }
+}
+
+// One block processes work items [base, base + BLOCK*IPT) of local step `s`: update, then deliver.
+// Thread j owns the IPT consecutive items base + j*IPT + q (neuron-major, fly-minor order), loads
+// every state array as one vector and keeps all loads in flight before computing.
+template <int BLOCK, bool FIXED, int IPT>
+__device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, long long base,
+                                          LifSmem<BLOCK * IPT>& sm) {
+  using RingT = typename std::conditional<FIXED, long long, int>::type;
+  constexpr int NW = BLOCK / 32;
   const long long W = (long long)k.n * k.batch;
-  const long long t = base + threadIdx.x;
+  const long long t0 = base + (long long)threadIdx.x * IPT;
   const int rs = (int)(((long long)clk.ring_pos + s) % k.R);
   const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
   const size_t slot = (size_t)W;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const LifP& P = k.P;
-  bool fired = false;
-  float x = 0.0f;
-  int i = 0, b = 0;
-  if (t < W) {
-    i = (int)(t / k.batch);
-    b = (int)(t - (long long)i * k.batch);
-    const bool live = !(k.flags & FLYB_LIF_EPISODES) || s < k.fly_steps[b];
-    if (live) {
-      // 1. input due now from the ring (read; clear only what was non-zero)
-      long long c;
-      if (FIXED) {
-        long long* r = (long long*)k.ring + (size_t)rs * slot + t;
-        c = *r;
-        if (c) *r = 0;
-      } else {
-        int* r = (int*)k.ring + (size_t)rs * slot + t;
-        c = *r;
-        if (c) *r = 0;
+  const int flags = k.flags;
+  unsigned fired_bits = 0, tx_bits = 0;
+  float xq[IPT];
+  int iq[IPT], bq[IPT];
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) { xq[q] = 0.0f; iq[q] = 0; bq[q] = 0; }
+  if (t0 < W) {
+    const bool whole = t0 + IPT <= W;   // every item of the vector exists (the tail is done by items)
+    RingT c[IPT];
+    float vv[IPT], gg[IPT], ref[IPT], ad[IPT], dv[IPT], pp[IPT], rt[IPT], cn[IPT], rr[IPT];
+    RingT* rp = (RingT*)k.ring + (size_t)rs * slot + t0;
+    if (whole) {
+      vload<IPT>(rp, c);
+      vload<IPT>(k.v + t0, vv); vload<IPT>(k.g + t0, gg); vload<IPT>(k.refrac + t0, ref);
+      vload<IPT>(k.adapt + t0, ad); vload<IPT>(k.drive + t0, dv); vload<IPT>(k.rate + t0, rt);
+      if (flags & FLYB_LIF_POISSON) vload<IPT>(k.poisson_p + t0, pp);
+      if (flags & FLYB_LIF_COUNTS) vload<IPT>(k.counts + t0, cn);
+      if (flags & FLYB_LIF_STD) vload<IPT>(k.res + t0, rr);
+    } else {
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) {
+        const bool ok = t0 + q < W;
+        c[q] = ok ? rp[q] : 0;
+        vv[q] = ok ? k.v[t0 + q] : 0.0f; gg[q] = ok ? k.g[t0 + q] : 0.0f; ref[q] = ok ? k.refrac[t0 + q] : 0.0f;
+        ad[q] = ok ? k.adapt[t0 + q] : 0.0f; dv[q] = ok ? k.drive[t0 + q] : 0.0f; rt[q] = ok ? k.rate[t0 + q] : 0.0f;
+        pp[q] = (ok && (flags & FLYB_LIF_POISSON)) ? k.poisson_p[t0 + q] : 0.0f;
+        cn[q] = (ok && (flags & FLYB_LIF_COUNTS)) ? k.counts[t0 + q] : 0.0f;
+        rr[q] = (ok && (flags & FLYB_LIF_STD)) ? k.res[t0 + q] : 1.0f;
       }
+    }
+    if (!(flags & FLYB_LIF_POISSON)) {
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) pp[q] = 0.0f;
+    }
+    RingT nc[IPT];
+    float sp[IPT];
+    bool touched = false;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      const long long t = t0 + q;
+      nc[q] = c[q];
+      sp[q] = 0.0f;
+      if (t >= W) continue;
+      const int i = (int)(t / k.batch), b = (int)(t - (long long)i * k.batch);
+      iq[q] = i;
+      bq[q] = b;
+      const bool live = !(flags & FLYB_LIF_EPISODES) || s < k.fly_steps[b];
+      if (!live) { sp[q] = k.spikes[t]; continue; }
+      nc[q] = 0;
       const float act = k.active[i];
-      const float p = (k.flags & FLYB_LIF_POISSON) ? k.poisson_p[t] : 0.0f;
-      float vv = k.v[t], gg = k.g[t], ref = k.refrac[t];
-      const float ad0 = k.adapt[t], dv = k.drive[t];
       bool skip = false;
-      if ((k.flags & FLYB_LIF_SKIP_FROZEN) && act == 0.0f && p == 0.0f && c == 0) {
+      if ((flags & FLYB_LIF_SKIP_FROZEN) && act == 0.0f && pp[q] == 0.0f && c[q] == 0) {
         // frozen cell at rest: the update would leave it unchanged (neural.cu:24-26)
-        skip = vv == P.v_rest && gg == 0.0f && dv == 0.0f && ad0 == 0.0f && ref == 0.0f &&
-               k.rate[t] == 0.0f && k.spikes[t] == 0.0f && k.res[t] == 1.0f;
+        const float rres = (flags & FLYB_LIF_STD) ? rr[q] : k.res[t];
+        skip = vv[q] == P.v_rest && gg[q] == 0.0f && dv[q] == 0.0f && ad[q] == 0.0f && ref[q] == 0.0f &&
+               rt[q] == 0.0f && k.spikes[t] == 0.0f && rres == 1.0f;
       }
-      if (!skip) {
-        gg = gg * P.a_s;
-        if (c) {
-          const float inc = FIXED ? __double2float_rn((double)c * (1.0 / 4294967296.0)) : P.w_syn * (float)c;
-          gg = gg + inc;
+      if (skip) continue;           // sp stays 0 == the cell's spike value
+      touched = true;
+      // 1. synaptic input due now
+      float g1 = gg[q] * P.a_s;
+      if (c[q]) {
+        const float inc = FIXED ? __double2float_rn((double)c[q] * (1.0 / 4294967296.0)) : P.w_syn * (float)c[q];
+        g1 = g1 + inc;
+      }
+      gg[q] = g1;
+      // 2. membrane, exponential Euler with g and drive held (brain.py:839-843)
+      float target = P.v_rest + g1;
+      target = target + dv[q];
+      target = target - ad[q];
+      float u = vv[q] - target;
+      u = u * P.a_m;
+      float v1 = target + u;
+      float r1 = ref[q];
+      if (r1 > 0.0f) v1 = P.v_reset;
+      r1 = r1 - P.dt;
+      if (r1 < 0.0f) r1 = 0.0f;
+      // 3. threshold x active, Poisson forcing (brain.py:845-849)
+      float spike = (v1 >= P.v_th ? 1.0f : 0.0f) * act;
+      if (pp[q] > 0.0f) {
+        const float un = (flags & FLYB_LIF_EXT_UNIFORM)
+                             ? k.uniforms[(size_t)s * slot + t]
+                             : philox_uniform(k.seed, clk.step0 + s, (uint32_t)i, (uint32_t)(k.fly0 + b));
+        if (un < pp[q]) spike = 1.0f;
+      }
+      const bool fired = spike > 0.0f;
+      if (fired) { v1 = P.v_reset; r1 = P.t_ref; }
+      vv[q] = v1;
+      ref[q] = r1;
+      sp[q] = spike;
+      // 4. adaptation, depression, counters, rate (brain.py:853-868)
+      if (flags & FLYB_LIF_ADAPT) { float a1 = ad[q] * P.a_ad; a1 = a1 + spike * P.jump; ad[q] = a1; }
+      float x = spike;
+      if (flags & FLYB_LIF_STD) {
+        float r2 = rr[q];
+        x = spike * r2;
+        if (fired) { const float keep = 1.0f - k.std_u[i]; r2 = r2 * keep; }
+        float dep = 1.0f - r2;
+        dep = dep * P.a_std;
+        rr[q] = 1.0f - dep;
+      }
+      if (flags & FLYB_LIF_COUNTS) cn[q] = cn[q] + spike;
+      float r3 = rt[q] * P.a_r;
+      r3 = r3 + spike * P.rg;
+      rt[q] = r3;
+      if (fired) fired_bits |= 1u << q;
+      if (x != 0.0f) { tx_bits |= 1u << q; xq[q] = x; }
+    }
+    bool ring_changed = false;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) ring_changed |= nc[q] != c[q];
+    if (whole) {
+      if (ring_changed) vstore<IPT>(rp, nc);
+      if (touched) {
+        vstore<IPT>(k.g + t0, gg); vstore<IPT>(k.v + t0, vv); vstore<IPT>(k.refrac + t0, ref);
+        vstore<IPT>(k.spikes + t0, sp); vstore<IPT>(k.rate + t0, rt);
+        if (flags & FLYB_LIF_ADAPT) vstore<IPT>(k.adapt + t0, ad);
+        if (flags & FLYB_LIF_STD) vstore<IPT>(k.res + t0, rr);
+        if (flags & FLYB_LIF_COUNTS) vstore<IPT>(k.counts + t0, cn);
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < IPT; ++q) {
+        if (t0 + q >= W) continue;
+        const long long t = t0 + q;
+        if (nc[q] != c[q]) rp[q] = nc[q];
+        if (touched) {
+          k.g[t] = gg[q]; k.v[t] = vv[q]; k.refrac[t] = ref[q]; k.spikes[t] = sp[q]; k.rate[t] = rt[q];
+          if (flags & FLYB_LIF_ADAPT) k.adapt[t] = ad[q];
+          if (flags & FLYB_LIF_STD) k.res[t] = rr[q];
+          if (flags & FLYB_LIF_COUNTS) k.counts[t] = cn[q];
         }
-        k.g[t] = gg;
-        // 2. membrane, exponential Euler with g and drive held (brain.py:839-843)
-        float target = P.v_rest + gg;
-        target = target + dv;
-        target = target - ad0;
-        float u = vv - target;
-        u = u * P.a_m;
-        vv = target + u;
-        if (ref > 0.0f) vv = P.v_reset;
-        ref = ref - P.dt;
-        if (ref < 0.0f) ref = 0.0f;
-        // 3. threshold x active, Poisson forcing (brain.py:845-849)
-        float spike = (vv >= P.v_th ? 1.0f : 0.0f) * act;
-        if (p > 0.0f) {
-          const float un = (k.flags & FLYB_LIF_EXT_UNIFORM)
-                               ? k.uniforms[(size_t)s * slot + t]
-                               : philox_uniform(k.seed, clk.step0 + s, (uint32_t)i, (uint32_t)(k.fly0 + b));
-          if (un < p) spike = 1.0f;
-        }
-        fired = spike > 0.0f;
-        if (fired) { vv = P.v_reset; ref = P.t_ref; }
-        k.v[t] = vv;
-        k.refrac[t] = ref;
-        k.spikes[t] = spike;
-        // 4. adaptation, depression, counters, rate (brain.py:853-868)
-        if (k.flags & FLYB_LIF_ADAPT) { float ad = ad0 * P.a_ad; ad = ad + spike * P.jump; k.adapt[t] = ad; }
-        x = spike;
-        if (k.flags & FLYB_LIF_STD) {
-          float rr = k.res[t];
-          x = spike * rr;
-          if (fired) { const float keep = 1.0f - k.std_u[i]; rr = rr * keep; }
-          float dep = 1.0f - rr;
-          dep = dep * P.a_std;
-          rr = 1.0f - dep;
-          k.res[t] = rr;
-        }
-        if (k.flags & FLYB_LIF_COUNTS) k.counts[t] = k.counts[t] + spike;
-        float rt = k.rate[t] * P.a_r;
-        rt = rt + spike * P.rg;
-        k.rate[t] = rt;
       }
     }
   }
-  // raster word of this warp (flat bit order t)
-  const unsigned fb = __ballot_sync(0xffffffffu, fired);
-  if (k.raster && lane == 0 && base + warp * 32 < W) {
-    const size_t slot = k.raster_slots > 0 ? (size_t)(((long long)clk.raster_pos + s) % k.raster_slots) : (size_t)s;
-    k.raster[slot * k.words + (size_t)((base >> 5) + warp)] = fb;
+  // raster words: a warp covers 32 * IPT items = IPT words; lane l's IPT bits go to word l / (32/IPT)
+  if (k.raster) {
+    constexpr int LPW = 32 / IPT;            // lanes per raster word
+    unsigned v = fired_bits << (IPT * (lane % LPW));
+#pragma unroll
+    for (int o = 1; o < LPW; o <<= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+    const long long wbase = base + (long long)warp * 32 * IPT;
+    if (lane % LPW == 0 && wbase + (long long)(lane / LPW) * 32 < W) {
+      const size_t rslot = k.raster_slots > 0 ? (size_t)(((long long)clk.raster_pos + s) % k.raster_slots) : (size_t)s;
+      k.raster[rslot * k.words + (size_t)((wbase >> 5) + lane / LPW)] = v;
+    }
   }
-  // 5. compact the transmitting cells of this block (warp ballot + block prefix)
-  const unsigned tb = __ballot_sync(0xffffffffu, x != 0.0f);
-  if (lane == 0) sm.wcnt[warp] = __popc(tb);
+  // 5. compact the transmitting items of this block (per-thread bits, warp scan, block prefix)
+  const int cnt = __popc(tx_bits);
+  const int incl = warp_scan(cnt);
+  if (lane == 31) sm.wcnt[warp] = incl;
   __syncthreads();
   if (warp == 0) {
-    const int c = lane < BLOCK / 32 ? sm.wcnt[lane] : 0;
+    const int c = lane < NW ? sm.wcnt[lane] : 0;
     const int inc = warp_scan(c);
-    if (lane < BLOCK / 32) sm.woff[lane] = inc - c;
+    if (lane < NW) sm.woff[lane] = inc - c;
     if (lane == 31) sm.total = inc;
   }
   __syncthreads();
   const int L = sm.total;
   if (L == 0) return;   // block-uniform
-  int deg = 0;
-  if (x != 0.0f) {
-    const int pos = sm.woff[warp] + __popc(tb & lanemask_lt());
-    const int e0 = k.out_ptr[i];
-    deg = k.out_ptr[i + 1] - e0;
-    sm.start[pos] = e0;
-    sm.fly[pos] = b;
-    sm.x[pos] = x;
-    sm.pre[pos] = deg;   // degree for now; turned into an exclusive prefix below
+  {
+    int pos = sm.woff[warp] + incl - cnt;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      if (tx_bits & (1u << q)) {
+        const int e0 = k.out_ptr[iq[q]];
+        sm.start[pos] = e0;
+        sm.fly[pos] = bq[q];
+        sm.x[pos] = xq[q];
+        sm.pre[pos] = k.out_ptr[iq[q] + 1] - e0;   // degree for now; exclusive prefix below
+        ++pos;
+      }
+    }
   }
   __syncthreads();
-  // exclusive prefix of degrees over the L spikers
+  // exclusive prefix of the degrees over the L transmitting items (thread j: entries j*IPT..)
   {
-    const int d = threadIdx.x < L ? sm.pre[threadIdx.x] : 0;
-    const int inc = warp_scan(d);
+    int d[IPT], sum = 0;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      const int e = threadIdx.x * IPT + q;
+      d[q] = e < L ? sm.pre[e] : 0;
+      sum += d[q];
+    }
+    const int inc = warp_scan(sum);
     if (lane == 31) sm.wcnt[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-      const int c = lane < BLOCK / 32 ? sm.wcnt[lane] : 0;
+      const int c = lane < NW ? sm.wcnt[lane] : 0;
       const int winc = warp_scan(c);
-      if (lane < BLOCK / 32) sm.woff[lane] = winc - c;
+      if (lane < NW) sm.woff[lane] = winc - c;
       if (lane == 31) sm.edges = winc;
     }
     __syncthreads();
-    if (threadIdx.x < L) sm.pre[threadIdx.x] = sm.woff[warp] + inc - d;
+    int run = sm.woff[warp] + inc - sum;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      const int e = threadIdx.x * IPT + q;
+      if (e < L) sm.pre[e] = run;
+      run += d[q];
+    }
     __syncthreads();
   }
   const int E = sm.edges;
-  // 6. block-wide, edge-parallel delivery into slot ws: thread q takes edges q, q+BLOCK, ...
+  // 6. block-wide, edge-parallel delivery into slot ws: thread j takes edges j, j+BLOCK, ...
   for (int q = threadIdx.x; q < E; q += BLOCK) {
-    int lo = 0, hi = L - 1;   // last spiker with pre <= q
+    int lo = 0, hi = L - 1;   // last transmitting item with pre <= q
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (sm.pre[mid] <= q) lo = mid; else hi = mid - 1;
@@ -248,24 +385,24 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
   __syncthreads();   // shared lists are reused by the next chunk
 }
 
-template <int BLOCK, bool FIXED>
+template <int BLOCK, bool FIXED, int IPT>
 __global__ void __launch_bounds__(BLOCK) lif_step_kernel(LifK k, int s) {
-  __shared__ LifSmem<BLOCK> sm;
+  __shared__ LifSmem<BLOCK * IPT> sm;
   const Clk clk = read_clock(k);
-  lif_chunk<BLOCK, FIXED>(k, clk, s, (long long)blockIdx.x * BLOCK, sm);
+  lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, (long long)blockIdx.x * BLOCK * IPT, sm);
 }
 
 __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
 
-template <int BLOCK, bool FIXED>
+template <int BLOCK, bool FIXED, int IPT>
 __global__ void __launch_bounds__(BLOCK) lif_persistent_kernel(LifK k) {
-  __shared__ LifSmem<BLOCK> sm;
+  __shared__ LifSmem<BLOCK * IPT> sm;
   const long long W = (long long)k.n * k.batch;
   const Clk clk = read_clock(k);
   int generation = 0;
   for (int s = 0; s < k.nsteps; ++s) {
-    for (long long base = (long long)blockIdx.x * BLOCK; base < W; base += (long long)gridDim.x * BLOCK)
-      lif_chunk<BLOCK, FIXED>(k, clk, s, base, sm);
+    for (long long base = (long long)blockIdx.x * BLOCK * IPT; base < W; base += (long long)gridDim.x * BLOCK * IPT)
+      lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, base, sm);
     // the next step writes the slot this step read: every block must be done with it
     if (!grid_barrier(k.sync, k.status, generation, s)) return;
   }
@@ -273,16 +410,13 @@ __global__ void __launch_bounds__(BLOCK) lif_persistent_kernel(LifK k) {
   if (blockIdx.x == 0) advance_clock(k, clk);
 }
 
-template <int BLOCK, bool FIXED>
-static void* persistent_fn() { return (void*)lif_persistent_kernel<BLOCK, FIXED>; }
-
-template <int BLOCK, bool FIXED>
-static int run_lif(const LifK& k, int launch, int grid_cap, cudaStream_t st) {
+template <int BLOCK, bool FIXED, int IPT>
+static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st) {
   const long long W = (long long)k.n * k.batch;
-  const long long chunks = (W + BLOCK - 1) / BLOCK;
+  const long long chunks = (W + (long long)BLOCK * IPT - 1) / ((long long)BLOCK * IPT);
   if (launch == FLYB_LAUNCH_STEP) {
     for (int s = 0; s < k.nsteps; ++s) {
-      lif_step_kernel<BLOCK, FIXED><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
+      lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
       FLYB_CHECK_LAUNCH();
     }
     if (k.clock || (k.flags & FLYB_LIF_EPISODES)) {
@@ -294,7 +428,7 @@ static int run_lif(const LifK& k, int launch, int grid_cap, cudaStream_t st) {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_persistent_kernel<BLOCK, FIXED>, BLOCK, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_persistent_kernel<BLOCK, FIXED, IPT>, BLOCK, 0);
   long long grid = (long long)sms * per_sm;
   if (grid > chunks) grid = chunks;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
@@ -303,8 +437,31 @@ static int run_lif(const LifK& k, int launch, int grid_cap, cudaStream_t st) {
   if (e != cudaSuccess) return (int)e;
   LifK kk = k;
   void* args[] = {&kk};
-  e = cudaLaunchCooperativeKernel(persistent_fn<BLOCK, FIXED>(), dim3((unsigned)grid), dim3(BLOCK), args, 0, st);
+  e = cudaLaunchCooperativeKernel((void*)lif_persistent_kernel<BLOCK, FIXED, IPT>, dim3((unsigned)grid), dim3(BLOCK),
+                                  args, 0, st);
   return (int)e;
+}
+
+// `ipt` items per thread (8- or 16-byte state vectors) need every ring slot and state array
+// aligned at each thread's first item: n * batch % ipt == 0 and (4 * ipt)-byte aligned bases.
+static bool vectorizable(const LifK& k, int ipt) {
+  const long long W = (long long)k.n * k.batch;
+  if (W % ipt) return false;
+  const void* ptrs[] = {k.v, k.g, k.refrac, k.adapt, k.res, k.rate, k.counts, k.spikes, k.drive, k.poisson_p, k.ring};
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) & (4 * ipt - 1)) return false;
+  return true;
+}
+
+// Items per thread: the caller's choice when its vectors are aligned, else 4 when possible, else 1.
+template <int BLOCK, bool FIXED>
+static int run_lif(const LifK& k, int want, int launch, int grid_cap, cudaStream_t st) {
+  int ipt = want ? want : 4;
+  if (ipt != 1 && ipt != 2 && ipt != 4) return FLYB_EINVAL;
+  while (ipt > 1 && !vectorizable(k, ipt)) ipt >>= 1;
+  if (ipt == 4) return run_lif_ipt<BLOCK, FIXED, 4>(k, launch, grid_cap, st);
+  if (ipt == 2) return run_lif_ipt<BLOCK, FIXED, 2>(k, launch, grid_cap, st);
+  return run_lif_ipt<BLOCK, FIXED, 1>(k, launch, grid_cap, st);
 }
 
 // ------------------------------------------------------------------ ring deposit (checkpoint import)
@@ -403,9 +560,9 @@ __global__ void ref_events_kernel(const int* __restrict__ ptr, const int* __rest
 
 int lif_blocks_per_sm(int block) {
   int b = 0;
-  if (block == 128) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<128, false>, 128, 0);
-  else if (block == 512) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<512, false>, 512, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<256, false>, 256, 0);
+  if (block == 128) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<128, false, 4>, 128, 0);
+  else if (block == 512) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<512, false, 4>, 512, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_persistent_kernel<256, false, 4>, 256, 0);
   return b;
 }
 
@@ -445,9 +602,9 @@ FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   const bool fixed = a->ring_mode == FLYB_RING_FIXED;
   const int block = a->block ? a->block : 256;
   switch (block) {
-    case 128: return fixed ? run_lif<128, true>(k, a->launch, a->grid, st) : run_lif<128, false>(k, a->launch, a->grid, st);
-    case 256: return fixed ? run_lif<256, true>(k, a->launch, a->grid, st) : run_lif<256, false>(k, a->launch, a->grid, st);
-    case 512: return fixed ? run_lif<512, true>(k, a->launch, a->grid, st) : run_lif<512, false>(k, a->launch, a->grid, st);
+    case 128: return fixed ? run_lif<128, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<128, false>(k, a->items_per_thread, a->launch, a->grid, st);
+    case 256: return fixed ? run_lif<256, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<256, false>(k, a->items_per_thread, a->launch, a->grid, st);
+    case 512: return fixed ? run_lif<512, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<512, false>(k, a->items_per_thread, a->launch, a->grid, st);
     default: return FLYB_EINVAL;
   }
 }

@@ -16,7 +16,9 @@ namespace flyb {
 
 struct OpticK {
   int m, batch, nsteps;
-  const int* __restrict__ ptr; const int* __restrict__ col; const float* __restrict__ w;
+  const int* __restrict__ ptr; const int2* __restrict__ cw;
+  const int* __restrict__ rows;   // optional row order: rows[0, n_long) long rows, then the others
+  int n_long;
   float* __restrict__ v; float* __restrict__ adapt;
   float* buf0; float* buf1;
   const float* __restrict__ pr; const float* __restrict__ spk;
@@ -48,46 +50,62 @@ __device__ __forceinline__ void load_x(const float* __restrict__ p, float (&x)[F
   }
 }
 
-// acc[q] = sum over the row of w * x[col][f*FPL + q] for this lane's flies; full-warp result on
-// lanes of group 0 (lane < F). `vec` means batch == F * FPL exactly (aligned vector loads).
-template <int F, int FPL>
-__device__ __forceinline__ void row_product(const int* __restrict__ ptr, const int* __restrict__ col,
-                                            const float* __restrict__ w, const float* __restrict__ x, int batch,
-                                            int row, float (&acc)[FPL]) {
-  constexpr int G = 32 / F;
-  const int lane = threadIdx.x & 31, g = lane / F, f = lane % F;
+// Entries each lane keeps in flight: the gathers are L2 round trips, so a warp must issue many
+// independent ones before it consumes any (fewer when each gather is already a wide vector).
+template <int FPL>
+struct Unroll { static constexpr int U = FPL <= 2 ? 8 : (FPL == 4 ? 4 : 2); };
+
+// acc[q] = sum over the row of w * x[col][f*FPL + q] for this lane's flies, for the row of this
+// lane's slot: a warp holds 32/LPR row slots of LPR lanes; within a slot, F lanes span the flies
+// (FPL consecutive flies each) and G = LPR/F lane groups split the entries (group g takes entries
+// e0 + g + G*k). Each pass loads U interleaved {col, w} entries (8 bytes each), issues U
+// independent gathers, then accumulates them with FMAs. The result is complete on the lanes with
+// slot lane < F. `row_ok` false: the lane still takes part in the shuffles.
+template <int F, int FPL, int LPR>
+__device__ __forceinline__ void row_product(const int* __restrict__ ptr, const int2* __restrict__ cw,
+                                            const float* __restrict__ x, int batch, int row, bool row_ok,
+                                            float (&acc)[FPL], int part = 0, int parts = 1) {
+  static_assert(F <= LPR && LPR <= 32, "a row slot spans the fly lanes");
+  constexpr int G = LPR / F;
+  constexpr int U = Unroll<FPL>::U;
+  const int sl = (threadIdx.x & 31) % LPR, g = sl / F, f = sl % F;
   const int fb = f * FPL;
   const bool full = batch == F * FPL;
+  const int stride = parts * G;          // `parts` slots share a long row: slot `part` takes every parts-th group
 #pragma unroll
   for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
-  const int e0 = __ldg(&ptr[row]), e1 = __ldg(&ptr[row + 1]);
-  for (int base = e0; base < e1; base += 32) {
-    const int e = base + lane;
-    int cj = 0;
-    float cw = 0.0f;
-    if (e < e1) { cj = __ldg(&col[e]); cw = __ldg(&w[e]); }
-    const int cnt = min(32, e1 - base);
-    for (int idx = 0; idx < cnt; idx += G) {
-      const int src = idx + g;
-      const int j = __shfl_sync(0xffffffffu, cj, src & 31);
-      const float wv = __shfl_sync(0xffffffffu, cw, src & 31);
-      if (src < cnt) {
-        const float* xp = x + (size_t)j * batch + fb;
-        if (full) {
-          float xv[FPL];
-          load_x<FPL>(xp, xv);
+  if (row_ok) {
+    const int e0 = __ldg(&ptr[row]), e1 = __ldg(&ptr[row + 1]);
+    for (int base = e0 + part * G + g; base < e1; base += stride * U) {
+      int2 c[U];
 #pragma unroll
-          for (int q = 0; q < FPL; ++q) { const float p = wv * xv[q]; acc[q] = acc[q] + p; }
+      for (int u = 0; u < U; ++u) {
+        const int e = base + u * stride;
+        c[u] = e < e1 ? __ldg(&cw[e]) : make_int2(-1, 0);
+      }
+      float xv[U][FPL];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const float* xp = x + ((c[u].x < 0 ? 0 : c[u].x) * batch + fb);
+        if (full) {
+          load_x<FPL>(xp, xv[u]);
         } else {
 #pragma unroll
-          for (int q = 0; q < FPL; ++q)
-            if (fb + q < batch) { const float p = wv * __ldg(xp + q); acc[q] = acc[q] + p; }
+          for (int q = 0; q < FPL; ++q) xv[u][q] = fb + q < batch ? __ldg(xp + q) : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        if (c[u].x >= 0) {
+          const float wv = __int_as_float(c[u].y);
+#pragma unroll
+          for (int q = 0; q < FPL; ++q) acc[q] = fmaf(wv, xv[u][q], acc[q]);
         }
       }
     }
   }
 #pragma unroll
-  for (int o = F; o < 32; o <<= 1)
+  for (int o = F; o < LPR; o <<= 1)
 #pragma unroll
     for (int q = 0; q < FPL; ++q) acc[q] = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], o);
 }
@@ -117,20 +135,118 @@ __device__ __forceinline__ void optic_update(const OpticK& k, int s, size_t t, i
   dr_out[t] = r - bb;
 }
 
-template <int F, int FPL>
-__device__ __forceinline__ void optic_rows(const OpticK& k, int s, const float* dr_in, float* dr_out,
-                                           long long warp0, long long nwarps) {
-  const int lane = threadIdx.x & 31;
-  for (long long row = warp0; row < k.m; row += nwarps) {
-    float acc[FPL];
-    row_product<F, FPL>(k.ptr, k.col, k.w, dr_in, k.batch, (int)row, acc);
-    if (lane < F) {
+template <int FPL>
+__device__ __forceinline__ void store_x(float* p, const float (&x)[FPL]) {
+  if constexpr (FPL == 1) {
+    *p = x[0];
+  } else if constexpr (FPL == 2) {
+    *reinterpret_cast<float2*>(p) = make_float2(x[0], x[1]);
+  } else {
 #pragma unroll
-      for (int q = 0; q < FPL; ++q) {
-        const int bb = lane * FPL + q;
-        if (bb < k.batch) optic_update(k, s, (size_t)row * k.batch + bb, (int)row, acc[q], dr_in, dr_out);
-      }
+    for (int q = 0; q < FPL; q += 4) *reinterpret_cast<float4*>(p + q) = make_float4(x[q], x[q + 1], x[q + 2], x[q + 3]);
+  }
+}
+
+// The same update for FPL consecutive flies of one unit with vector loads and stores (batch == F*FPL).
+template <int FPL>
+__device__ __forceinline__ void optic_update_vec(const OpticK& k, int s, size_t t, int i, const float (&y)[FPL],
+                                                 const float* __restrict__ dr_in, float* __restrict__ dr_out) {
+  float old[FPL], pr[FPL], spk[FPL], ad[FPL], vv[FPL];
+  load_x<FPL>(dr_in + t, old);
+  load_x<FPL>(k.pr + t, pr);
+  load_x<FPL>(k.spk + t, spk);
+  load_x<FPL>(k.adapt + t, ad);
+  load_x<FPL>(k.v + t, vv);
+  const float ai = k.a[i], bb = k.b[i];
+  const size_t sz = (size_t)k.m * k.batch;
+  if (k.v_hist) store_x<FPL>(k.v_hist + (size_t)s * sz + t, vv);
+  float inpv[FPL], nv[FPL], na[FPL], nd[FPL];
+#pragma unroll
+  for (int q = 0; q < FPL; ++q) {
+    float inp = k.gr * y[q];
+    inp = inp + pr[q];
+    const float a2 = k.ga * ad[q];
+    inp = inp - a2;
+    inp = inp + spk[q];
+    inpv[q] = inp;
+    float dv = vv[q] - inp;
+    dv = dv * ai;
+    nv[q] = inp + dv;
+    float da = ad[q] - old[q];
+    da = da * k.aad;
+    na[q] = old[q] + da;
+    nd[q] = clip01(nv[q] + bb) - bb;
+  }
+  if (k.inp_hist) store_x<FPL>(k.inp_hist + (size_t)s * sz + t, inpv);
+  store_x<FPL>(k.v + t, nv);
+  store_x<FPL>(k.adapt + t, na);
+  store_x<FPL>(dr_out + t, nd);
+}
+
+// y (FPL flies of slot lane sl) -> the fused update of one unit.
+template <int F, int FPL>
+__device__ __forceinline__ void optic_epilogue(const OpticK& k, int s, int row, int sl, const float (&y)[FPL],
+                                               const float* dr_in, float* dr_out) {
+  if (k.batch == F * FPL) {
+    optic_update_vec<FPL>(k, s, (size_t)row * k.batch + sl * FPL, row, y, dr_in, dr_out);
+  } else {
+#pragma unroll
+    for (int q = 0; q < FPL; ++q) {
+      const int bb = sl * FPL + q;
+      if (bb < k.batch) optic_update(k, s, (size_t)row * k.batch + bb, row, y[q], dr_in, dr_out);
     }
+  }
+}
+
+template <int F, int FPL, int LPR>
+struct OpticShape {
+  static constexpr int RPW = 32 / LPR;           // row slots per warp
+  static constexpr int SLOTS = 8 * RPW;          // row slots per 256-thread block
+  static constexpr int RED = SLOTS * F * FPL;    // floats of the long-row reduction
+};
+
+// Number of block work items of one substep: one per long row, then blocks of SLOTS short rows.
+template <int F, int FPL, int LPR>
+__host__ __device__ __forceinline__ long long optic_items(int m, int n_long) {
+  constexpr int SLOTS = OpticShape<F, FPL, LPR>::SLOTS;
+  return n_long + (m - n_long + SLOTS - 1) / SLOTS;
+}
+
+// One block work item. Long rows (the first n_long of k.rows): every row slot of the block takes an
+// interleaved share of the row's entries, the shares are summed in slot order through shared
+// memory and the first slot applies the update; the longest rows thus stop bounding the substep.
+// Other rows: one row per slot.
+template <int F, int FPL, int LPR>
+__device__ __forceinline__ void optic_item(const OpticK& k, int s, const float* dr_in, float* dr_out, long long item,
+                                           float* red) {
+  using S = OpticShape<F, FPL, LPR>;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, slot = lane / LPR, sl = lane % LPR;
+  const int gslot = warp * S::RPW + slot;
+  float acc[FPL];
+  if (item < k.n_long) {
+    const int row = k.rows[item];
+    row_product<F, FPL, LPR>(k.ptr, k.cw, dr_in, k.batch, row, true, acc, gslot, S::SLOTS);
+    if (sl < F) {
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) red[gslot * F * FPL + sl * FPL + q] = acc[q];
+    }
+    __syncthreads();
+    if (gslot == 0 && sl < F) {
+      float y[FPL];
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) y[q] = red[sl * FPL + q];
+      for (int p = 1; p < S::SLOTS; ++p)
+#pragma unroll
+        for (int q = 0; q < FPL; ++q) y[q] = y[q] + red[p * F * FPL + sl * FPL + q];
+      optic_epilogue<F, FPL>(k, s, row, sl, y, dr_in, dr_out);
+    }
+    __syncthreads();
+  } else {
+    const long long r = k.n_long + (item - k.n_long) * S::SLOTS + gslot;
+    const bool ok = r < k.m;
+    const int row = ok ? (k.rows ? k.rows[r] : (int)r) : 0;
+    row_product<F, FPL, LPR>(k.ptr, k.cw, dr_in, k.batch, row, ok, acc);
+    if (ok && sl < F) optic_epilogue<F, FPL>(k, s, row, sl, acc, dr_in, dr_out);
   }
 }
 
@@ -147,38 +263,40 @@ __global__ void optic_init_kernel(OpticK k) {
   init_dr(k, k.buf0, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
 }
 
-template <int F, int FPL>
+template <int F, int FPL, int LPR>
 __global__ void __launch_bounds__(256) optic_step_kernel(OpticK k, int s) {
+  __shared__ float red[OpticShape<F, FPL, LPR>::RED];
   const float* in = (s & 1) ? k.buf1 : k.buf0;
   float* out = (s & 1) ? k.buf0 : k.buf1;
-  optic_rows<F, FPL>(k, s, in, out, ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5,
-                     ((long long)gridDim.x * blockDim.x) >> 5);
+  optic_item<F, FPL, LPR>(k, s, in, out, blockIdx.x, red);
 }
 
-template <int F, int FPL>
+template <int F, int FPL, int LPR>
 __global__ void __launch_bounds__(256) optic_persistent_kernel(OpticK k) {
+  __shared__ float red[OpticShape<F, FPL, LPR>::RED];
   int generation = 0;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
+  const long long items = optic_items<F, FPL, LPR>(k.m, k.n_long);
   init_dr(k, k.buf0, tid, nth);
   if (!grid_barrier(k.sync, k.status, generation, -1)) return;
   for (int s = 0; s < k.nsteps; ++s) {
     const float* in = (s & 1) ? k.buf1 : k.buf0;
     float* out = (s & 1) ? k.buf0 : k.buf1;
-    optic_rows<F, FPL>(k, s, in, out, tid >> 5, nth >> 5);
+    for (long long item = blockIdx.x; item < items; item += gridDim.x) optic_item<F, FPL, LPR>(k, s, in, out, item, red);
     if (s + 1 < k.nsteps && !grid_barrier(k.sync, k.status, generation, s)) return;
   }
 }
 
-template <int F, int FPL>
+template <int F, int FPL, int LPR>
 static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st) {
   const long long sz = (long long)k.m * k.batch;
   if (launch == FLYB_LAUNCH_STEP) {
     optic_init_kernel<<<(unsigned)((sz + 255) / 256), 256, 0, st>>>(k);
     FLYB_CHECK_LAUNCH();
-    const unsigned blocks = (unsigned)((k.m + 7) / 8);   // one warp per row, 8 warps per block
+    const unsigned blocks = (unsigned)optic_items<F, FPL, LPR>(k.m, k.n_long);
     for (int s = 0; s < k.nsteps; ++s) {
-      optic_step_kernel<F, FPL><<<blocks, 256, 0, st>>>(k, s);
+      optic_step_kernel<F, FPL, LPR><<<blocks, 256, 0, st>>>(k, s);
       FLYB_CHECK_LAUNCH();
     }
     return 0;
@@ -186,9 +304,9 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, optic_persistent_kernel<F, FPL>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, optic_persistent_kernel<F, FPL, LPR>, 256, 0);
   long long grid = (long long)sms * per_sm;
-  const long long need = (k.m + 7) / 8;
+  const long long need = optic_items<F, FPL, LPR>(k.m, k.n_long);
   if (grid > need) grid = need;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
   if (grid < 1) return FLYB_ECOOP;
@@ -196,7 +314,8 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
   if (e != cudaSuccess) return (int)e;
   OpticK kk = k;
   void* args[] = {&kk};
-  e = cudaLaunchCooperativeKernel((void*)optic_persistent_kernel<F, FPL>, dim3((unsigned)grid), dim3(256), args, 0, st);
+  e = cudaLaunchCooperativeKernel((void*)optic_persistent_kernel<F, FPL, LPR>, dim3((unsigned)grid), dim3(256), args, 0,
+                                  st);
   return (int)e;
 }
 
@@ -213,6 +332,33 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
     if ((B) <= 128) { constexpr int F = 32, FPL = 4; return CALL; }    \
     if ((B) <= 256) { constexpr int F = 32, FPL = 8; return CALL; }    \
     return FLYB_ETOOBIG;                                               \
+  } while (0)
+
+// (F fly lanes, FPL flies per lane, LPR lanes per row) of the optic substep for a batch; `variant`
+// 0 is the default, 1 and 2 are the alternatives the autotuner tries.
+#define FLYB_OPTIC_DISPATCH(B, V, CALL)                                                           \
+  do {                                                                                            \
+    if ((B) == 1) {                                                                               \
+      if ((V) == 1) { constexpr int F = 1, FPL = 1, LPR = 16; return CALL; }                      \
+      if ((V) == 2) { constexpr int F = 1, FPL = 1, LPR = 32; return CALL; }                      \
+      constexpr int F = 1, FPL = 1, LPR = 8; return CALL;                                         \
+    }                                                                                             \
+    if ((B) <= 2) { constexpr int F = 2, FPL = 1, LPR = 16; return CALL; }                        \
+    if ((B) <= 4) { constexpr int F = 4, FPL = 1, LPR = 16; return CALL; }                        \
+    if ((B) <= 8) { constexpr int F = 8, FPL = 1, LPR = 32; return CALL; }                        \
+    if ((B) <= 16) { constexpr int F = 16, FPL = 1, LPR = 32; return CALL; }                      \
+    if ((B) <= 32) { constexpr int F = 32, FPL = 1, LPR = 32; return CALL; }                      \
+    if ((B) <= 64) {                                                                              \
+      if ((V) == 1) { constexpr int F = 32, FPL = 2, LPR = 32; return CALL; }                     \
+      if ((V) == 2) { constexpr int F = 8, FPL = 8, LPR = 32; return CALL; }                      \
+      constexpr int F = 16, FPL = 4, LPR = 32; return CALL;                                       \
+    }                                                                                             \
+    if ((B) <= 128) {                                                                             \
+      if ((V) == 1) { constexpr int F = 16, FPL = 8, LPR = 32; return CALL; }                     \
+      constexpr int F = 32, FPL = 4, LPR = 32; return CALL;                                       \
+    }                                                                                             \
+    if ((B) <= 256) { constexpr int F = 32, FPL = 8, LPR = 32; return CALL; }                     \
+    return FLYB_ETOOBIG;                                                                          \
   } while (0)
 
 // ------------------------------------------------------------------ held-input products
@@ -234,26 +380,35 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
   float acc[FPL];
 #pragma unroll
   for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+  constexpr int U = Unroll<FPL>::U;
   const int e0 = k.ptr[row], e1 = k.ptr[row + 1];
-  for (int base = e0; base < e1; base += 32) {
-    const int e = base + lane;
-    int cj = 0;
-    float cw = 0.0f;
-    if (e < e1) { cj = k.col[e]; cw = k.w[e]; if (k.x_index) cj = k.x_index[cj]; }
-    const int cnt = min(32, e1 - base);
-    for (int idx = 0; idx < cnt; idx += G) {
-      const int src = idx + g;
-      const int j = __shfl_sync(0xffffffffu, cj, src & 31);
-      const float wv = __shfl_sync(0xffffffffu, cw, src & 31);
-      if (src < cnt) {
+  for (int base = e0 + g; base < e1; base += G * U) {
+    int jj[U];
+    float ww[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int e = base + u * G;
+      const bool ok = e < e1;
+      int j = ok ? __ldg(&k.col[e]) : -1;
+      if (ok && k.x_index) j = __ldg(&k.x_index[j]);
+      jj[u] = j;
+      ww[u] = ok ? __ldg(&k.w[e]) : 0.0f;
+    }
+    float xv[U][FPL];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+#pragma unroll
+      for (int q = 0; q < FPL; ++q)
+        xv[u][q] = (jj[u] >= 0 && fb + q < k.batch) ? __ldg(&k.x[(size_t)jj[u] * k.batch + fb + q]) : 0.0f;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (jj[u] >= 0) {
 #pragma unroll
         for (int q = 0; q < FPL; ++q) {
-          if (fb + q < k.batch) {
-            float xv = k.x[(size_t)j * k.batch + fb + q] / k.x_div;
-            xv = xv < k.x_lo ? k.x_lo : (xv > k.x_hi ? k.x_hi : xv);
-            const float p = wv * xv;
-            acc[q] = acc[q] + p;
-          }
+          float x = xv[u][q] / k.x_div;
+          x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
+          const float p = ww[u] * x;
+          acc[q] = acc[q] + p;
         }
       }
     }
@@ -334,7 +489,7 @@ __global__ void ref_csr_kernel(const int* __restrict__ ptr, const int* __restric
 
 int optic_blocks_per_sm() {
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, optic_persistent_kernel<1, 1>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, optic_persistent_kernel<1, 1, 8>, 256, 0);
   return b;
 }
 
@@ -349,11 +504,13 @@ FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
   if ((long long)a->m * a->batch >= (1ll << 31)) return FLYB_ETOOBIG;
   if (a->launch == FLYB_LAUNCH_PERSISTENT && (!a->sync || !a->status)) return FLYB_EINVAL;
   if (a->nsteps == 0) return 0;
-  OpticK k{a->m, a->batch, a->nsteps, a->ptr, a->col, a->w, a->v, a->adapt, a->dr, a->dr_tmp, a->pr, a->spk,
+  if (a->n_long < 0 || a->n_long > a->m || (a->n_long && !a->rows)) return FLYB_EINVAL;
+  OpticK k{a->m, a->batch, a->nsteps, a->ptr, (const int2*)a->cw, a->rows, a->n_long, a->v, a->adapt, a->dr, a->dr_tmp,
+           a->pr, a->spk,
            a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
            (a->flags & 1) ? a->inp_hist : nullptr, a->status, a->sync};
   cudaStream_t st = (cudaStream_t)stream;
-  FLYB_BATCH_DISPATCH(a->batch, (run_optic<F, FPL>(k, a->launch, a->grid, st)));
+  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
 }
 
 // ------------------------------------------------------------------ allocation-free variant
@@ -394,11 +551,13 @@ FLYB_API int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream) {
   const int rc = optic_noalloc_scratch(&scratch);
   if (rc) return rc;
   if (a->nsteps == 0) return 0;
-  OpticK k{a->m, a->batch, a->nsteps, a->ptr, a->col, a->w, a->v, a->adapt, scratch, scratch + FLYB_OPTIC_NOALLOC_MAX,
+  if (a->n_long < 0 || a->n_long > a->m || (a->n_long && !a->rows)) return FLYB_EINVAL;
+  OpticK k{a->m, a->batch, a->nsteps, a->ptr, (const int2*)a->cw, a->rows, a->n_long, a->v, a->adapt, scratch,
+           scratch + FLYB_OPTIC_NOALLOC_MAX,
            a->pr, a->spk, a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
            (a->flags & 1) ? a->inp_hist : nullptr, a->status, (int*)(scratch + 2 * FLYB_OPTIC_NOALLOC_MAX)};
   cudaStream_t st = (cudaStream_t)stream;
-  FLYB_BATCH_DISPATCH(a->batch, (run_optic<F, FPL>(k, a->launch, a->grid, st)));
+  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
 }
 
 FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {

@@ -37,6 +37,7 @@ class LifArgs(ct.Structure):
     _fields_ = [("n", _I), ("batch", _I), ("n_delay", _I), ("ring_slots", _I), ("ring_mode", _I),
                 ("ring_pos", _I), ("flags", _I), ("nsteps", _I), ("launch", _I), ("block", _I),
                 ("grid", _I), ("raster_slots", _I), ("raster_pos", _I), ("fly0", _I),
+                ("items_per_thread", _I), ("pad1", _I),
                 ("step0", ct.c_longlong), ("seed", ct.c_ulonglong),
                 ("out_ptr", _VP), ("out_edge", _VP),
                 ("v", _VP), ("g", _VP), ("refrac", _VP), ("adapt", _VP), ("res", _VP),
@@ -48,10 +49,10 @@ class LifArgs(ct.Structure):
 
 class OpticArgs(ct.Structure):
     _fields_ = [("m", _I), ("batch", _I), ("nsteps", _I), ("launch", _I), ("block", _I), ("grid", _I),
-                ("lanes_per_row", _I), ("flags", _I),
-                ("ptr", _VP), ("col", _VP), ("w", _VP), ("v", _VP), ("adapt", _VP), ("dr", _VP),
+                ("variant", _I), ("flags", _I),
+                ("ptr", _VP), ("cw", _VP), ("rows", _VP), ("v", _VP), ("adapt", _VP), ("dr", _VP),
                 ("dr_tmp", _VP), ("pr", _VP), ("spk", _VP), ("a", _VP), ("b", _VP),
-                ("gr", ct.c_float), ("ga", ct.c_float), ("aad", ct.c_float), ("pad0", _I),
+                ("gr", ct.c_float), ("ga", ct.c_float), ("aad", ct.c_float), ("n_long", _I),
                 ("v_hist", _VP), ("inp_hist", _VP), ("status", _VP), ("sync", _VP)]
 
 

@@ -48,6 +48,10 @@ class OpticAdjoint:
         self.core.pr_in.copy_(pr)
         self.core.spk_in.copy_(spk)
         self.WT, self.perm = self.core.W.transpose(dev)
+        # the per-edge accumulator is kept in the transposed order the reverse pass walks (coalesced,
+        # single writer); the pair reduction reads W0 and the pair ids in that order too
+        perm = self.perm.long()
+        self.W0_t, self.pair_t = self.W0[perm].contiguous(), self.pair_id[perm].contiguous()
         self.launch = launch
         M, B = self.m, self.B
         self.lam_v = torch.zeros(M, B, device=dev)
@@ -66,6 +70,7 @@ class OpticAdjoint:
     def set_params(self, gains: torch.Tensor, tau: torch.Tensor) -> None:
         g = gains.to(self.device, torch.float32)
         self.core.W.w.copy_(g[self.pair_id] * self.W0)
+        self.core.W.refresh_cw()
         self.WT.w.copy_(self.core.W.w[self.perm.long()])
         self.tau = tau.to(self.device, torch.float32)
         self.core.a.copy_(torch.exp(-self.dt / self.tau[self.type_of]))
@@ -100,7 +105,7 @@ class OpticAdjoint:
             self.core.substeps(n, self.v_hist, self.inp_hist)       # recompute with histories
             args = _abi.AdjointArgs(m=self.m, batch=self.B, nsteps=n, launch=_abi.LAUNCHES_BY_NAME[self.launch],
                                     t_ptr=self.WT.ptr.data_ptr(), t_col=self.WT.col.data_ptr(), t_w=self.WT.w.data_ptr(),
-                                    t_perm=self.perm.data_ptr(), v_hist=self.v_hist.data_ptr(),
+                                    t_perm=None, v_hist=self.v_hist.data_ptr(),
                                     inp_hist=self.inp_hist.data_ptr(), a=self.core.a.data_ptr(), b=self.core.b.data_ptr(),
                                     gr=self.gr, ga=self.ga, aad=self.aad, lam_v=self.lam_v.data_ptr(),
                                     lam_a=self.lam_a.data_ptr(), lam_tmp=self.mu1.data_ptr(), mu=self.mu0.data_ptr(),
@@ -110,8 +115,8 @@ class OpticAdjoint:
                 rc = _abi.lib().flyb_optic_adjoint(ct.byref(args), stream)
             if rc:
                 raise RuntimeError(f"flyb_optic_adjoint: error {rc}")
-        contrib = (self.gr * self.W0.double()) * self.g_edge.double()
-        d_gains = torch.zeros(self.n_pairs, dtype=torch.float64, device=self.device).index_add_(0, self.pair_id, contrib)
+        contrib = (self.gr * self.W0_t.double()) * self.g_edge.double()
+        d_gains = torch.zeros(self.n_pairs, dtype=torch.float64, device=self.device).index_add_(0, self.pair_t, contrib)
         a = self.core.a.double()
         tau_i = self.tau.double()[self.type_of]
         d_tau = torch.zeros(self.n_types, dtype=torch.float64, device=self.device).index_add_(

@@ -1,0 +1,105 @@
+"""Launch-parameter autotuner for the native steps, cached per (graph, batch, activity bucket).
+
+The best launch shape depends on the graph, the batch and how many cells spike per step: at B = 1
+the step is latency-bound and a persistent cooperative launch (one launch for many steps, a grid
+barrier per step) wins; at B = 64 the state streams from HBM and one launch per step with small
+blocks keeps more loads in flight. `tune_lif` times each candidate (block size x launch mode) for
+a few steps on a copy of the live state, restores the state, installs the fastest and caches it
+under the key; `tune_optic` does the same for the optic substep's launch mode.
+"""
+from __future__ import annotations
+
+import hashlib
+import math
+
+import numpy as np
+import torch
+
+CACHE: dict = {}
+LIF_CANDIDATES = (("step", 256, 4), ("step", 128, 4), ("step", 512, 4), ("step", 256, 2), ("step", 128, 2),
+                  ("step", 256, 1), ("persistent", 256, 4), ("persistent", 512, 2))
+
+
+def graph_key(brain) -> str:
+    h = hashlib.sha1()
+    h.update(brain._out_ptr.cpu().numpy().tobytes())
+    h.update(str((brain.n, brain.nnz, brain.ring_mode)).encode())
+    return h.hexdigest()[:16]
+
+
+def activity_bucket(brain, steps: int = 20) -> int:
+    """log2 bucket of the fraction of (neuron, fly) pairs spiking per step, measured on a copy."""
+    saved = brain.state_dict()
+    before = float(brain.spike_counts.sum())
+    rec = brain.record_activity
+    brain.record_activity = True
+    brain.step(steps)
+    rate = (float(brain.spike_counts.sum()) - before) / (steps * brain.n * brain.B)
+    brain.record_activity = rec
+    brain.load_state_dict(saved)
+    return int(math.floor(math.log2(max(rate, 1e-7))))
+
+
+def _time(fn, reps: int) -> float:
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    e.synchronize()
+    return s.elapsed_time(e) / reps
+
+
+def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
+    """Install and return the fastest (launch, block) for this brain; state is left unchanged."""
+    key = ("lif", graph_key(brain), brain.B, activity_bucket(brain))
+    if key in CACHE:
+        _apply(brain, CACHE[key])
+        return CACHE[key]
+    saved = brain.state_dict()
+    results = {}
+    for launch, block, ipt in candidates:
+        _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt})
+        brain.step(2)
+        results[(launch, block, ipt)] = _time(lambda: brain.step(steps), 1) / steps
+        brain.load_state_dict(saved)
+    best = min(results, key=results.get)
+    choice = {"launch": best[0], "block": best[1], "items_per_thread": best[2], "ms_per_step": results[best],
+              "all": {f"{k[0]}/{k[1]}/{k[2]}": v for k, v in results.items()}}
+    CACHE[key] = choice
+    _apply(brain, choice)
+    return choice
+
+
+def _apply(brain, choice: dict) -> None:
+    brain.launch, brain.block = choice["launch"], choice["block"]
+    brain.items_per_thread = choice.get("items_per_thread", 0)
+    brain._make_args()
+
+
+def tune_optic(core, steps: int = 10) -> dict:
+    """Pick the optic substep's launch mode and kernel shape (fly lanes x flies per lane x lanes
+    per row, flyb_optic_args.variant) by timing each on a copy of the state."""
+    key = ("optic", core.m, core.W.nnz, core.B)
+    if key in CACHE:
+        core.launch, core.variant = CACHE[key]["launch"], CACHE[key]["variant"]
+        return CACHE[key]
+    v, a = core.v_s.clone(), core.adapt_s.clone()
+    results = {}
+    for launch in ("step", "persistent"):
+        for variant in (0, 1, 2):
+            core.launch, core.variant = launch, variant
+            core.substeps(2)
+            results[(launch, variant)] = _time(lambda: core.substeps(steps), 1) / steps
+            core.v_s.copy_(v)
+            core.adapt_s.copy_(a)
+    best = min(results, key=results.get)
+    CACHE[key] = {"launch": best[0], "variant": best[1], "ms_per_step": results[best],
+                  "all": {f"{k[0]}/{k[1]}": t for k, t in results.items()}}
+    core.launch, core.variant = best
+    return CACHE[key]
+
+
+def summary() -> list:
+    return [{"key": list(map(str, k)), **{kk: vv for kk, vv in v.items() if kk != "all"}} for k, v in CACHE.items()]

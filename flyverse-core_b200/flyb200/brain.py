@@ -249,6 +249,7 @@ class Brain:
         st, a = self._st, _abi.LifArgs()
         a.n, a.batch, a.n_delay, a.ring_slots, a.ring_mode = self.n, self.B, self.n_delay, self.R, self.ring_mode
         a.launch, a.block = LAUNCHES[self.launch], self.block
+        a.items_per_thread = getattr(self, "items_per_thread", 0)
         a.raster_slots = self.n_delay
         a.seed = self.seed & 0xFFFFFFFFFFFFFFFF
         a.out_ptr, a.out_edge = self._out_ptr.data_ptr(), self._out_edge.data_ptr()

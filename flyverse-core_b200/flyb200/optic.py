@@ -85,6 +85,19 @@ class DeviceCSR:
         self.ptr = torch.from_numpy(M.indptr.astype(np.int32)).to(device)
         self.col = torch.from_numpy(M.indices.astype(np.int32)).to(device)
         self.w = torch.from_numpy(M.data.astype(np.float32)).to(device)
+        self._cw = None
+
+    @property
+    def cw(self) -> torch.Tensor:
+        """[nnz][2] int32 {column, float bits of the weight}: one 8-byte load per entry."""
+        if self._cw is None:
+            self._cw = torch.stack([self.col, self.w.view(torch.int32)], dim=1).contiguous()
+        return self._cw
+
+    def refresh_cw(self) -> None:
+        """Copy changed weights into the interleaved entries."""
+        if self._cw is not None:
+            self._cw[:, 1].copy_(self.w.view(torch.int32))
 
     def transpose(self, device):
         """(CSR of M^T, perm) with perm[e'] = index in M's CSR order of transposed entry e'."""
@@ -93,7 +106,7 @@ class DeviceCSR:
         order = np.lexsort((rows, cols))
         T = sp.csr_matrix((self.w.cpu().numpy()[order], (cols[order], rows[order])), shape=self.shape[::-1])
         t = DeviceCSR.__new__(DeviceCSR)
-        t.shape, t.nnz = T.shape, int(T.nnz)
+        t.shape, t.nnz, t._cw = T.shape, int(T.nnz), None
         t.ptr = torch.from_numpy(np.concatenate([[0], np.cumsum(np.bincount(cols, minlength=self.shape[1]))]).astype(np.int32)).to(device)
         t.col = torch.from_numpy(rows[order].astype(np.int32)).to(device)
         t.w = torch.from_numpy(self.w.cpu().numpy()[order]).to(device)
@@ -120,8 +133,21 @@ def spmm(M: DeviceCSR, x: torch.Tensor, y: torch.Tensor, *, x_index=None, x_div=
         raise RuntimeError(f"flyb_spmm: error {rc}")
 
 
+LONG_ROW = 192      # rows with more entries than this are split across a whole block
+
+
 class OpticCore:
-    """The rate-unit recurrence on the device: W_rr, per-unit a / b, state [M][B], held inputs."""
+    """The rate-unit recurrence on the device: W_rr, per-unit a / b, state [M][B], held inputs.
+
+    Rows run longest first (so the tail of a substep is short rows) and rows longer than
+    `long_row` entries are each shared by all warps of a block (flyb_optic_args.rows / n_long)."""
+
+    def set_long_rows(self, long_row: int) -> None:
+        deg = np.diff(self.W.ptr.cpu().numpy())
+        order = np.argsort(-deg, kind="stable").astype(np.int32)
+        self.rows = torch.from_numpy(order).to(self.device)
+        self.n_long = int((deg > long_row).sum())
+        self.long_row = int(long_row)
 
     def __init__(self, W_rr: sp.spmatrix, a: np.ndarray, b: np.ndarray, *, batch: int, device, gain_rr: float,
                  adapt_gain: float, aad: float, launch: str = "persistent"):
@@ -135,6 +161,8 @@ class OpticCore:
         self.b = torch.from_numpy(np.asarray(b, np.float32)).to(self.device)
         self.gain_rr, self.adapt_gain, self.aad = float(gain_rr), float(adapt_gain), float(aad)
         self.launch = launch
+        self.variant = 0                 # kernel shape (flyb_optic_args.variant), set by the autotuner
+        self.set_long_rows(LONG_ROW)
         M, B, dev = self.m, self.B, self.device
         self.v_s = torch.zeros(M, B, device=dev)
         self.adapt_s = torch.zeros(M, B, device=dev)
@@ -150,7 +178,8 @@ class OpticCore:
         if nsteps <= 0:
             return
         a = _abi.OpticArgs(m=self.m, batch=self.B, nsteps=int(nsteps), launch=_abi.LAUNCHES_BY_NAME[self.launch],
-                           ptr=self.W.ptr.data_ptr(), col=self.W.col.data_ptr(), w=self.W.w.data_ptr(),
+                           ptr=self.W.ptr.data_ptr(), cw=self.W.cw.data_ptr(), variant=self.variant,
+                           rows=self.rows.data_ptr(), n_long=self.n_long,
                            v=self.v_s.data_ptr(), adapt=self.adapt_s.data_ptr(), dr=self._dr.data_ptr(),
                            dr_tmp=self._dr_tmp.data_ptr(), pr=self.pr_in.data_ptr(), spk=self.spk_in.data_ptr(),
                            a=self.a.data_ptr(), b=self.b.data_ptr(), gr=self.gain_rr, ga=self.adapt_gain, aad=self.aad,

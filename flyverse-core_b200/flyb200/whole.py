@@ -45,10 +45,28 @@ class WholeFly:
         self.optic = OpticCore(o.W_rr(), a, o.b, batch=self.B, device=self.device, gain_rr=o.gain_rr,
                                adapt_gain=o.adapt_gain, aad=aad, launch="step")
         dev = self.device
-        self.W_rs, self.W_sr, self.W_rp = DeviceCSR(o.W_rs, dev), DeviceCSR(o.W_sr, dev), DeviceCSR(o.W_rp, dev)
+        # the coupling blocks keep only their non-empty rows (+ the row map): the other rows of spk_in
+        # and of the drive are never written and stay zero
+        self.W_rs, self.rs_rows = self._rows_with_entries(o.W_rs, dev)
+        self.W_sr, self.sr_rows = self._rows_with_entries(o.W_sr, dev)
+        self.W_rp = DeviceCSR(o.W_rp, dev)
         self.a_pr = torch.zeros(o.n_pr, self.B, device=dev)
-        self.launches_per_step = 4 + (1 if launch == "step" else 0) + 1   # spmm, optic init + substep, spmm, lif (+advance)
         self.steps_taken = 0
+
+    @property
+    def launches_per_step(self) -> int:
+        """Kernel launches of one step: two coupling products, the optic substep (a dr
+        initialisation + the substep, or one persistent launch) and the LIF step (+ the clock
+        advance in per-step mode)."""
+        optic = 2 if self.optic.launch == "step" else 1
+        lif = 2 if self.lif.launch == "step" else 1
+        return 2 + optic + lif
+
+    @staticmethod
+    def _rows_with_entries(M, dev):
+        M = M.tocsr()
+        rows = np.flatnonzero(np.diff(M.indptr)).astype(np.int32)
+        return DeviceCSR(M[rows], dev), torch.from_numpy(rows).to(dev)
 
     @property
     def n_neurons(self) -> int:
@@ -64,9 +82,10 @@ class WholeFly:
         lif_rate = self.lif._st["rate"]
         drive = self.lif._st["drive"]
         for _ in range(int(n)):
-            spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb)
+            spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb,
+                 y_index=self.rs_rows)
             self.optic.substeps(1)
-            spmm(self.W_sr, self.optic._dr_tmp, drive, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
+            spmm(self.W_sr, self.optic._dr_tmp, drive, y_index=self.sr_rows, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
                  y_hi=o.drive_clip_mv)
             self.lif.step(1)
         self.steps_taken += int(n)

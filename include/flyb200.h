@@ -104,6 +104,8 @@ typedef struct flyb_lif_args {
   int raster_slots;      /* 0: raster is [nsteps][words]; else a ring of that many slots */
   int raster_pos;        /* ring slot written by the first step (raster_slots > 0)   */
   int fly0;              /* global index of local fly 0 (Philox key when flies are sharded) */
+  int items_per_thread;  /* 0 auto (4 when aligned), 1, 2 or 4 consecutive items per thread */
+  int pad1;
   long long step0;       /* global step index of the first step (Philox counter)     */
   unsigned long long seed;
   /* outgoing synapses, pre-major (CSC of W[post, pre]) */
@@ -146,15 +148,19 @@ typedef struct flyb_optic_args {
   int launch;            /* FLYB_LAUNCH_*                                            */
   int block;             /* threads per block (0 = default)                          */
   int grid;              /* persistent grid cap (0 = occupancy)                      */
-  int lanes_per_row;     /* 0 = auto; else lanes cooperating on one row (1..32)      */
+  int variant;           /* kernel shape: 0 default, 1 / 2 alternatives (autotuned)  */
   int flags;             /* bit0: store per-substep history (adjoint recompute)      */
-  const int* ptr; const int* col; const float* w;    /* W_rr CSR, rows = post           */
+  const int* ptr;        /* W_rr CSR row pointers [m + 1], rows = postsynaptic units */
+  const int* cw;         /* [nnz][2] interleaved {column, float bits of weight}      */
+  const int* rows;       /* optional [m] row order: rows[0, n_long) are long rows, each
+                            split across a whole block; the rest one row per warp slot.
+                            Null: natural order and n_long = 0                       */
   float* v; float* adapt;                             /* [m][batch]                      */
   float* dr; float* dr_tmp;                           /* [m][batch] ping-pong scratch    */
   const float* pr; const float* spk;                  /* held inputs [m][batch]          */
   const float* a; const float* b;                     /* [m] exp(-dt/tau), operating point */
   float gr, ga, aad;
-  int pad0;
+  int n_long;            /* long rows at the front of `rows`                         */
   float* v_hist;         /* optional [nsteps][m][batch]: v before each substep       */
   float* inp_hist;       /* optional [nsteps][m][batch]: input of each substep       */
   int* status; int* sync;

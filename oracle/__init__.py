@@ -145,7 +145,8 @@ def optic_run(v, adapt, ptr, col, w, pr, spk, a, b, gr, ga, aad, nsteps, history
     pr, spk, a, b = _f32(pr), _f32(spk), _f32(a), _f32(b)
     vh = np.zeros((nsteps, m, B), np.float32) if history else None
     ih = np.zeros((nsteps, m, B), np.float32) if history else None
-    args = _abi.OpticArgs(m=m, batch=B, nsteps=nsteps, ptr=_p(ptr), col=_p(col), w=_p(w), v=_p(v),
+    cw = np.ascontiguousarray(np.stack([col, w.view(np.int32)], axis=1))
+    args = _abi.OpticArgs(m=m, batch=B, nsteps=nsteps, ptr=_p(ptr), cw=_p(cw), v=_p(v),
                           adapt=_p(adapt), pr=_p(pr), spk=_p(spk), a=_p(a), b=_p(b), gr=gr, ga=ga, aad=aad,
                           v_hist=_p(vh), inp_hist=_p(ih))
     assert v.dtype == np.float32 and v.flags.c_contiguous and adapt.dtype == np.float32 and adapt.flags.c_contiguous

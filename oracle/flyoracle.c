@@ -245,7 +245,10 @@ int oracle_optic_run(const flyb_optic_args* a, int threads) {
       for (int bb = 0; bb < B; ++bb) {
         const size_t t = (size_t)i * B + bb;
         float y = 0.0f;
-        for (int e = a->ptr[i]; e < a->ptr[i + 1]; ++e) { float p = a->w[e] * dr[(size_t)a->col[e] * B + bb]; y = y + p; }
+        for (int e = a->ptr[i]; e < a->ptr[i + 1]; ++e) {
+          float w; memcpy(&w, &a->cw[2 * e + 1], sizeof w);
+          float p = w * dr[(size_t)a->cw[2 * e] * B + bb]; y = y + p;
+        }
         float inp = a->gr * y;
         inp = inp + a->pr[t];
         float ad = a->ga * a->adapt[t];

@@ -13,7 +13,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda"):
+                   device="cuda", items_per_thread=0):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -33,7 +33,7 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
     P = np.ascontiguousarray(params, np.float32)
     a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
                      ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, launch=launch, block=block, grid=grid,
-                     fly0=fly0, step0=state.step, seed=seed, out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
+                     fly0=fly0, items_per_thread=items_per_thread, step0=state.step, seed=seed, out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
                      v=d["v"].data_ptr(), g=d["g"].data_ptr(), refrac=d["refrac"].data_ptr(),
                      adapt=d["adapt"].data_ptr(), res=d["res"].data_ptr(), rate=d["rate"].data_ptr(),
                      counts=d["counts"].data_ptr(), spikes=d["spikes"].data_ptr(), drive=d["drive"].data_ptr(),

@@ -77,7 +77,7 @@ def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed
                 uniforms=None, fly_steps=fs, seed=12345)
 
 
-def _compare(case, launch, block, grid=0):
+def _compare(case, launch, block, grid=0, ipt=0):
     s_ref, s_gpu = case["state"].copy(), case["state"].copy()
     fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
     fs_gpu = None if fs_ref is None else fs_ref.copy()
@@ -85,7 +85,7 @@ def _compare(case, launch, block, grid=0):
               uniforms=case["uniforms"], raster=True)
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, **kw)
     r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], fly_steps=fs_gpu, launch=launch,
-                                   block=block, grid=grid, **kw)
+                                   block=block, grid=grid, items_per_thread=ipt, **kw)
     assert unpack(r_ref, s_ref.n * s_ref.batch).sum() > 0
     np.testing.assert_array_equal(r_gpu, r_ref)                      # spike rasters
     for k in LIF_ARRAYS:
@@ -110,6 +110,12 @@ def test_19cell_depression_adaptation_native_equals_oracle(launch, block):
 @pytest.mark.parametrize("launch,block,grid", [(STEP, 256, 0), (PERS, 256, 0), (PERS, 128, 7), (PERS, 512, 0)])
 def test_batched_philox_native_equals_oracle(launch, block, grid):
     _compare(case_random(batch=64), launch, block, grid)
+
+
+@pytest.mark.parametrize("ipt", [1, 2, 4])
+@pytest.mark.parametrize("launch,batch", [(STEP, 64), (PERS, 64), (STEP, 3)])
+def test_items_per_thread_variants_equal_oracle(ipt, launch, batch):
+    _compare(case_random(batch=batch, steps=100), launch, 256, ipt=ipt)
 
 
 @pytest.mark.parametrize("batch", [1, 3, 33])

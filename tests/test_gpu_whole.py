@@ -1,0 +1,75 @@
+"""The whole-fly step (LIF + optic coupled every step) on the GPU against the oracle's step in the
+same order, on a reduced whole-fly graph; and the autotuner leaves the state untouched."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from flyb200 import _abi, autotune, synthetic
+from flyb200.brain import LIFParams, lif_coefficients, out_edges
+from flyb200.weights import lif_weights
+from flyb200.whole import WholeFly
+
+pytestmark = pytest.mark.gpu
+
+
+def small_fly():
+    return synthetic.whole_fly_config5(seed=2, n_rate=3000, n_lif=2500, n_sensory=300, edges=700_000,
+                                       optic_nnz=200_000, n_pr=300)
+
+
+def test_whole_fly_matches_oracle_step_order():
+    cfg = small_fly()
+    B, T = 4, 120
+    eng = WholeFly(cfg, B, device="cuda", seed=1, launch="step")
+    a_pr = torch.from_numpy((np.random.default_rng(0).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
+    eng.set_photoreceptors(a_pr)
+    pr = eng.optic.pr_in.cpu().numpy()
+    counts = []
+    for _ in range(T):
+        eng.step(1)
+        counts.append(eng.lif.spike_counts.sum().item())
+    # the oracle, same order: spk_in, optic substep, drive, LIF step
+    o = cfg.optic
+    p = LIFParams(**{**cfg.lif.params, "dt": 0.1})
+    W, _ = lif_weights(cfg.lif.c, p)
+    ptr, edges, mode = out_edges(W, p.w_syn)
+    n, m = cfg.n_spiking, o.m
+    st = oracle.LifState(n, B, 19, mode, p.v_rest)
+    st.poisson_p[cfg.sensory_idx, :] = np.float32(cfg.lif.poisson_hz) * np.float32(p.dt / 1000.0)
+    Wr, Wrs, Wsr = o.W_rr(), o.W_rs.tocsr(), o.W_sr.tocsr()
+    a = np.exp(-0.1 / o.tau_of_type[o.type_of].astype(np.float32)).astype(np.float32)
+    aad = float(np.exp(-0.1 / o.adapt_tau_ms))
+    v, ad = np.zeros((m, B), np.float32), np.zeros((m, B), np.float32)
+    ocounts = []
+    for _ in range(T):
+        spk = oracle.spmm(Wrs.indptr, Wrs.indices, Wrs.data, st.rate, B, rows=m, x_div=100.0, x_lo=0.0, x_hi=3.0,
+                          alpha=o.gain_fb)
+        oracle.optic_run(v, ad, Wr.indptr, Wr.indices, Wr.data, pr, spk, a, o.b, o.gain_rr, o.adapt_gain, aad, 1)
+        dr = (np.clip(v + o.b[:, None], 0, 1) - o.b[:, None]).astype(np.float32)
+        oracle.spmm(Wsr.indptr, Wsr.indices, Wsr.data, dr, B, rows=n, y=st.drive, alpha=o.gain_out_mv,
+                    y_lo=-o.drive_clip_mv, y_hi=o.drive_clip_mv)
+        oracle.lif_run(st, ptr, edges, lif_coefficients(p, False), n_delay=18,
+                       flags=_abi.LIF_POISSON | _abi.LIF_COUNTS, nsteps=1, seed=1)
+        ocounts.append(float(st.counts.sum()))
+    assert ocounts[-1] > 0
+    np.testing.assert_array_equal(np.array(counts), np.array(ocounts))          # same spikes every step
+    np.testing.assert_array_equal(eng.lif.spike_counts.t().cpu().numpy(), st.counts)
+    np.testing.assert_allclose(eng.optic.v_s.cpu().numpy(), v, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(eng.lif._st["v"].cpu().numpy(), st.v, rtol=0, atol=1e-4)
+
+
+def test_autotuner_keeps_state_and_installs_a_choice():
+    cfg = small_fly()
+    eng = WholeFly(cfg, 8, device="cuda", seed=3, launch="step")
+    eng.step(5)
+    before = {k: v.clone() for k, v in eng.lif._st.items()}
+    ring = eng.lif.ring.clone()
+    choice = autotune.tune_lif(eng.lif, steps=5)
+    assert choice["launch"] in ("step", "persistent") and choice["block"] in (128, 256, 512)
+    for k, v in before.items():
+        assert torch.equal(v, eng.lif._st[k]), k
+    assert torch.equal(ring, eng.lif.ring)
+    assert autotune.tune_lif(eng.lif) is choice                   # cached per (graph, batch, activity)
+    oc = autotune.tune_optic(eng.optic, steps=5)
+    assert oc["launch"] in ("step", "persistent")

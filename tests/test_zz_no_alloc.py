@@ -26,7 +26,7 @@ def _args(cfg, W, state, launch, status, with_scratch):
     dr_tmp = torch.zeros_like(v) if with_scratch else None
     sync = torch.zeros(64, dtype=torch.int32, device="cuda") if with_scratch else None
     args = _abi.OpticArgs(m=cfg.m, batch=v.shape[1], nsteps=15, launch=launch, ptr=W[0].data_ptr(),
-                          col=W[1].data_ptr(), w=W[2].data_ptr(), v=v.data_ptr(), adapt=ad.data_ptr(),
+                          cw=W[1].data_ptr(), v=v.data_ptr(), adapt=ad.data_ptr(),
                           dr=None if dr is None else dr.data_ptr(), dr_tmp=None if dr_tmp is None else dr_tmp.data_ptr(),
                           pr=pr.data_ptr(), spk=spk.data_ptr(), a=a.data_ptr(), b=b.data_ptr(), gr=cfg.gain_rr,
                           ga=cfg.adapt_gain, aad=cfg.aad, status=status.data_ptr(),
@@ -39,8 +39,8 @@ def test_noalloc_matches_the_allocating_entry_point_twice(launch):
     lib = _abi.lib()
     cfg = synthetic.optic_config3(seed=9, m=5000, nnz=250_000, n_pr=300, n_types=40, n_spk=400)
     Wr = cfg.W_rr()
-    W = [torch.from_numpy(Wr.indptr.astype(np.int32)).cuda(), torch.from_numpy(Wr.indices.astype(np.int32)).cuda(),
-         torch.from_numpy(Wr.data.astype(np.float32)).cuda()]
+    cw = np.stack([Wr.indices.astype(np.int32), Wr.data.astype(np.float32).view(np.int32)], axis=1)
+    W = [torch.from_numpy(Wr.indptr.astype(np.int32)).cuda(), torch.from_numpy(np.ascontiguousarray(cw)).cuda()]
     rng = np.random.default_rng(4)
     B = 3
     init = [torch.from_numpy((rng.standard_normal((cfg.m, B)) * s).astype(np.float32)).cuda() for s in (0.3, 0.05, 0.3, 0.1)]
