@@ -24,11 +24,11 @@ from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -55,13 +55,39 @@ def load_peaks() -> dict:
 
 # ------------------------------------------------------------------ clocks during the timed region
 class Clocks:
+    """SM clock and clock-event reasons sampled during the timed region, two ways: nvidia-smi's
+    clocks line every 200 ms, and NVML every 2 ms (a timed region can be shorter than 200 ms).
+    Read-only: no clock or other GPU setting is changed."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    REASONS = (("sw_power_cap", 0x4), ("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20),
+               ("hw_thermal_slowdown", 0x40), ("hw_power_brake_slowdown", 0x80))
 
     def __init__(self, index: int):
         self.index, self.proc = index, None
         self.path = Path(tempfile.mkstemp(prefix="flyb_clocks_", suffix=".csv")[1])
+        self.nvml, self.stop, self.thread, self.handle, self.max_mhz = [], threading.Event(), None, None, None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.index)
+        try:
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _sample(self):
+        nv, h = self.handle
+        while not self.stop.is_set():
+            try:
+                self.nvml.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM),
+                                  nv.nvmlDeviceGetCurrentClocksEventReasons(h)))
+            except Exception:
+                return
+            time.sleep(0.002)
 
     def __enter__(self):
         try:
@@ -70,9 +96,19 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        try:
+            self.handle = self._nvml_handle()
+            self.max_mhz = self.handle[0].nvmlDeviceGetMaxClockInfo(self.handle[1], self.handle[0].NVML_CLOCK_SM)
+            self.thread = threading.Thread(target=self._sample, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
         return self
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             self.proc.wait(timeout=10)
@@ -80,12 +116,23 @@ class Clocks:
     def summary(self) -> dict:
         rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()] if self.path.exists() else []
         self.path.unlink(missing_ok=True)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": reasons, "samples": len(rows)}
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if rows:
+            names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+            out = {"sm_mhz": float(np.median([float(r[1]) for r in rows])), "sm_max_mhz": float(rows[0][2]),
+                   "reasons": sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"}),
+                   "samples": len(rows)}
+        if self.nvml:
+            sm = [c for c, _ in self.nvml]
+            reasons = sorted({n for _, m in self.nvml for n, bit in self.REASONS if m & bit})
+            out["nvml"] = {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(min(sm)), "samples": len(sm),
+                           "reasons": reasons, "period_ms": 2}
+            if out["sm_mhz"] is None:
+                out["sm_mhz"], out["sm_max_mhz"] = float(np.median(sm)), float(self.max_mhz)
+            out["reasons"] = sorted(set(out["reasons"]) | set(reasons))
+        if not rows and not self.nvml:
+            out["reasons"] = ["unsampled"]
+        return out
 
 
 # ------------------------------------------------------------------ helpers
@@ -130,6 +177,14 @@ def photoreceptor_contrast(cfg, rad: torch.Tensor) -> torch.Tensor:
     return con.t().contiguous()
 
 
+def graph_chunk(steps: int, most: int = 26) -> int:
+    """Steps per captured graph: a divisor of `steps` (so exactly `steps` are timed), even when
+    possible (an odd count ends each replay with a copy of the optic dr back to its start buffer)."""
+    divs = [d for d in range(min(most, steps), 0, -1) if steps % d == 0]
+    even = [d for d in divs if d % 2 == 0]
+    return (even or divs)[0]
+
+
 def capture(eng, steps: int):
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
@@ -147,9 +202,10 @@ def measure_batched(cfg, device, steps, warmup, fly0):
     eng = build_engine(cfg, BATCH, device, "step", fly0)
     eng.step(max(3, warmup))
     eng.tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
-    chunk = max(1, min(25, steps))
+    eng.step(2)                    # the tuners restored the state: one step re-derives the carried dr
+    chunk = graph_chunk(steps)
     g = capture(eng, chunk)
-    reps = max(1, math.ceil(steps / chunk))
+    reps = steps // chunk
     g.replay()
     torch.cuda.synchronize()
     return eng, g, chunk, reps
@@ -169,7 +225,7 @@ def time_graph(g, reps) -> float:
 def kernel_roofline(eng, reps=20) -> dict:
     """The LIF step and the optic substep timed alone with CUDA events (B=64)."""
     lif_ms = events_time(lambda: eng.lif.step(1), reps)
-    opt_ms = events_time(lambda: eng.optic.substeps(1), reps)
+    opt_ms = events_time(lambda: eng.optic.substeps(1, carry=True), reps)
     lif_b, opt_b = eng.lif_bytes_per_step(), eng.optic_bytes_per_step()
     return {"lif_ms": lif_ms, "optic_ms": opt_ms, "lif_bytes": lif_b, "optic_bytes": opt_b}
 

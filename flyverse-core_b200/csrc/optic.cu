@@ -2,12 +2,14 @@
 // (flyverse/optic.py:_substep, optic.py:525-551; neural.cu:62-88), the held-input products
 // (optic.py:579-580, 599-602) and the reference-compatible elementwise / CSR launchers.
 //
-// Layout: state [m][batch] (unit-major, fly-minor). One warp owns one CSR row for all flies: a
-// chunk of 32 (col, w) entries is loaded coalesced, then broadcast by shuffle; each lane gathers
-// FPL consecutive flies of x[col][*] (a 4-, 8- or 16-byte vector when FPL is 1, 2 or 4), and
-// 32/F lane groups split the entries when the batch is narrower than a warp. The gathered vector
+// Layout: state [m][batch] (unit-major, fly-minor); CSR entries interleaved as int2 {col, w bits}.
+// A warp holds 32/LPR row slots; in a slot F lanes span the flies (FPL consecutive flies each: a
+// 4-, 8- or 16-byte vector gather of x[col][*]) and LPR/F lane groups split the entries, each lane
+// keeping U independent gathers in flight. Rows run longest first; rows longer than a threshold
+// are split over every slot of a block and summed through shared memory. The gathered vector
 // (dr, 0.36 MB per fly) stays L2-resident; the CSR streams from HBM once per substep for all flies.
-// Substeps ping-pong dr between two buffers, so one grid barrier per substep suffices.
+// Substeps ping-pong dr between two buffers, so one grid barrier per substep suffices, and the dr
+// of the final state is left for the next call (FLYB_OPTIC_DR_VALID).
 #include <mutex>
 
 #include "common.cuh"
@@ -26,6 +28,7 @@ struct OpticK {
   float gr, ga, aad;
   float* v_hist; float* inp_hist;
   int* status; int* sync;
+  int dr_valid;                   // buf0 already holds clip(v + b) - b: no initialisation pass
 };
 
 template <int FPL> struct VecT;
@@ -250,17 +253,17 @@ __device__ __forceinline__ void optic_item(const OpticK& k, int s, const float* 
   }
 }
 
-__device__ __forceinline__ void init_dr(const OpticK& k, float* dr, long long tid, long long nthreads) {
-  const long long sz = (long long)k.m * k.batch;
-  for (long long t = tid; t < sz; t += nthreads) {
-    const int i = (int)(t / k.batch);
-    const float bb = k.b[i];
+// dr = clip(v + b, 0, 1) - b over the state (m * batch < 2^31, checked by the entry points).
+__device__ __forceinline__ void init_dr(const OpticK& k, float* dr, int tid, int nthreads) {
+  const int sz = k.m * k.batch;
+  for (int t = tid; t < sz; t += nthreads) {
+    const float bb = __ldg(&k.b[t / k.batch]);
     dr[t] = clip01(k.v[t] + bb) - bb;
   }
 }
 
 __global__ void optic_init_kernel(OpticK k) {
-  init_dr(k, k.buf0, (long long)blockIdx.x * blockDim.x + threadIdx.x, (long long)gridDim.x * blockDim.x);
+  init_dr(k, k.buf0, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 template <int F, int FPL, int LPR>
@@ -278,8 +281,10 @@ __global__ void __launch_bounds__(256) optic_persistent_kernel(OpticK k) {
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long nth = (long long)gridDim.x * blockDim.x;
   const long long items = optic_items<F, FPL, LPR>(k.m, k.n_long);
-  init_dr(k, k.buf0, tid, nth);
-  if (!grid_barrier(k.sync, k.status, generation, -1)) return;
+  if (!k.dr_valid) {
+    init_dr(k, k.buf0, (int)tid, (int)nth);
+    if (!grid_barrier(k.sync, k.status, generation, -1)) return;
+  }
   for (int s = 0; s < k.nsteps; ++s) {
     const float* in = (s & 1) ? k.buf1 : k.buf0;
     float* out = (s & 1) ? k.buf0 : k.buf1;
@@ -292,8 +297,10 @@ template <int F, int FPL, int LPR>
 static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st) {
   const long long sz = (long long)k.m * k.batch;
   if (launch == FLYB_LAUNCH_STEP) {
-    optic_init_kernel<<<(unsigned)((sz + 255) / 256), 256, 0, st>>>(k);
-    FLYB_CHECK_LAUNCH();
+    if (!k.dr_valid) {
+      optic_init_kernel<<<(unsigned)((sz + 255) / 256), 256, 0, st>>>(k);
+      FLYB_CHECK_LAUNCH();
+    }
     const unsigned blocks = (unsigned)optic_items<F, FPL, LPR>(k.m, k.n_long);
     for (int s = 0; s < k.nsteps; ++s) {
       optic_step_kernel<F, FPL, LPR><<<blocks, 256, 0, st>>>(k, s);
@@ -371,44 +378,53 @@ struct SpmmK {
   float alpha, y_lo, y_hi;
 };
 
-template <int F, int FPL>
+// WPR warps share one row (RB = 8 / WPR rows per 256-thread block): warp `part` of a row takes the
+// entry groups part, part + WPR, ... of it, the partial sums meet in shared memory and the row's
+// first warp applies alpha, the clamp and the store. Lanes: F across the flies (FPL each), G = 32/F
+// entry groups per warp.
+template <int F, int FPL, int WPR>
 __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
-  constexpr int G = 32 / F;
-  const int lane = threadIdx.x & 31, g = lane / F, f = lane % F, fb = f * FPL;
-  const long long row = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (row >= k.rows) return;
+  constexpr int G = 32 / F, RB = 8 / WPR;
+  constexpr int U = Unroll<FPL>::U;
+  __shared__ float red[WPR > 1 ? 8 * F * FPL : 1];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane / F, f = lane % F, fb = f * FPL;
+  const int part = warp % WPR;
+  const long long row = (long long)blockIdx.x * RB + warp / WPR;
+  const bool ok = row < k.rows;
   float acc[FPL];
 #pragma unroll
   for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
-  constexpr int U = Unroll<FPL>::U;
-  const int e0 = k.ptr[row], e1 = k.ptr[row + 1];
-  for (int base = e0 + g; base < e1; base += G * U) {
-    int jj[U];
-    float ww[U];
+  if (ok) {
+    const int e0 = k.ptr[row], e1 = k.ptr[row + 1];
+    constexpr int stride = WPR * G;
+    for (int base = e0 + part * G + g; base < e1; base += stride * U) {
+      int jj[U];
+      float ww[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      const int e = base + u * G;
-      const bool ok = e < e1;
-      int j = ok ? __ldg(&k.col[e]) : -1;
-      if (ok && k.x_index) j = __ldg(&k.x_index[j]);
-      jj[u] = j;
-      ww[u] = ok ? __ldg(&k.w[e]) : 0.0f;
-    }
-    float xv[U][FPL];
+      for (int u = 0; u < U; ++u) {
+        const int e = base + u * stride;
+        const bool in = e < e1;
+        int j = in ? __ldg(&k.col[e]) : -1;
+        if (in && k.x_index) j = __ldg(&k.x_index[j]);
+        jj[u] = j;
+        ww[u] = in ? __ldg(&k.w[e]) : 0.0f;
+      }
+      float xv[U][FPL];
 #pragma unroll
-    for (int u = 0; u < U; ++u)
+      for (int u = 0; u < U; ++u)
 #pragma unroll
-      for (int q = 0; q < FPL; ++q)
-        xv[u][q] = (jj[u] >= 0 && fb + q < k.batch) ? __ldg(&k.x[(size_t)jj[u] * k.batch + fb + q]) : 0.0f;
+        for (int q = 0; q < FPL; ++q)
+          xv[u][q] = (jj[u] >= 0 && fb + q < k.batch) ? __ldg(&k.x[(size_t)jj[u] * k.batch + fb + q]) : 0.0f;
 #pragma unroll
-    for (int u = 0; u < U; ++u) {
-      if (jj[u] >= 0) {
+      for (int u = 0; u < U; ++u) {
+        if (jj[u] >= 0) {
 #pragma unroll
-        for (int q = 0; q < FPL; ++q) {
-          float x = xv[u][q] / k.x_div;
-          x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
-          const float p = ww[u] * x;
-          acc[q] = acc[q] + p;
+          for (int q = 0; q < FPL; ++q) {
+            float x = xv[u][q] / k.x_div;
+            x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
+            const float p = ww[u] * x;
+            acc[q] = acc[q] + p;
+          }
         }
       }
     }
@@ -417,7 +433,17 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
   for (int o = F; o < 32; o <<= 1)
 #pragma unroll
     for (int q = 0; q < FPL; ++q) acc[q] = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], o);
-  if (lane < F) {
+  if (WPR > 1) {
+    if (lane < F)
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) red[(warp * F + f) * FPL + q] = acc[q];
+    __syncthreads();
+    if (part == 0 && lane < F)
+      for (int p = 1; p < WPR; ++p)
+#pragma unroll
+        for (int q = 0; q < FPL; ++q) acc[q] = acc[q] + red[((warp + p) * F + f) * FPL + q];
+  }
+  if (ok && part == 0 && lane < F) {
     const long long yi = k.y_index ? k.y_index[row] : row;
 #pragma unroll
     for (int q = 0; q < FPL; ++q) {
@@ -433,9 +459,17 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
 }
 
 template <int F, int FPL>
-static int run_spmm(const SpmmK& k, cudaStream_t st) {
-  const unsigned blocks = (unsigned)((k.rows + 7) / 8);
-  if (blocks) spmm_kernel<F, FPL><<<blocks, 256, 0, st>>>(k);
+static int run_spmm(const SpmmK& k, int wpr, cudaStream_t st) {
+  const long long rb = 8 / wpr;
+  const unsigned blocks = (unsigned)((k.rows + rb - 1) / rb);
+  if (!blocks) return 0;
+  switch (wpr) {
+    case 1: spmm_kernel<F, FPL, 1><<<blocks, 256, 0, st>>>(k); break;
+    case 2: spmm_kernel<F, FPL, 2><<<blocks, 256, 0, st>>>(k); break;
+    case 4: spmm_kernel<F, FPL, 4><<<blocks, 256, 0, st>>>(k); break;
+    case 8: spmm_kernel<F, FPL, 8><<<blocks, 256, 0, st>>>(k); break;
+    default: return FLYB_EINVAL;
+  }
   return (int)cudaGetLastError();
 }
 
@@ -507,8 +541,9 @@ FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
   if (a->n_long < 0 || a->n_long > a->m || (a->n_long && !a->rows)) return FLYB_EINVAL;
   OpticK k{a->m, a->batch, a->nsteps, a->ptr, (const int2*)a->cw, a->rows, a->n_long, a->v, a->adapt, a->dr, a->dr_tmp,
            a->pr, a->spk,
-           a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
-           (a->flags & 1) ? a->inp_hist : nullptr, a->status, a->sync};
+           a->a, a->b, a->gr, a->ga, a->aad, (a->flags & FLYB_OPTIC_HISTORY) ? a->v_hist : nullptr,
+           (a->flags & FLYB_OPTIC_HISTORY) ? a->inp_hist : nullptr, a->status, a->sync,
+           (a->flags & FLYB_OPTIC_DR_VALID) ? 1 : 0};
   cudaStream_t st = (cudaStream_t)stream;
   FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
 }
@@ -554,8 +589,9 @@ FLYB_API int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream) {
   if (a->n_long < 0 || a->n_long > a->m || (a->n_long && !a->rows)) return FLYB_EINVAL;
   OpticK k{a->m, a->batch, a->nsteps, a->ptr, (const int2*)a->cw, a->rows, a->n_long, a->v, a->adapt, scratch,
            scratch + FLYB_OPTIC_NOALLOC_MAX,
-           a->pr, a->spk, a->a, a->b, a->gr, a->ga, a->aad, (a->flags & 1) ? a->v_hist : nullptr,
-           (a->flags & 1) ? a->inp_hist : nullptr, a->status, (int*)(scratch + 2 * FLYB_OPTIC_NOALLOC_MAX)};
+           a->pr, a->spk, a->a, a->b, a->gr, a->ga, a->aad, (a->flags & FLYB_OPTIC_HISTORY) ? a->v_hist : nullptr,
+           (a->flags & FLYB_OPTIC_HISTORY) ? a->inp_hist : nullptr, a->status,
+           (int*)(scratch + 2 * FLYB_OPTIC_NOALLOC_MAX), 0};
   cudaStream_t st = (cudaStream_t)stream;
   FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
 }
@@ -567,7 +603,9 @@ FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
   SpmmK k{a->rows, a->batch, a->accumulate, a->ptr, a->col, a->w, a->x, a->x_index, a->x_div, a->x_lo, a->x_hi,
           a->y, a->y_index, a->alpha, a->y_lo, a->y_hi};
   cudaStream_t st = (cudaStream_t)stream;
-  FLYB_BATCH_DISPATCH(a->batch, (run_spmm<F, FPL>(k, st)));
+  const int wpr = a->warps_per_row ? a->warps_per_row : 1;
+  if (wpr != 1 && wpr != 2 && wpr != 4 && wpr != 8) return FLYB_EINVAL;
+  FLYB_BATCH_DISPATCH(a->batch, (run_spmm<F, FPL>(k, wpr, st)));
 }
 
 FLYB_API int launch_optic_dr(void** p, int n, int batch, void* stream) {

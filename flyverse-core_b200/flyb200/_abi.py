@@ -27,7 +27,7 @@ LAUNCHES_BY_NAME = {"step": LAUNCH_STEP, "persistent": LAUNCH_PERSISTENT}
 (P_V_REST, P_V_RESET, P_V_TH, P_A_M, P_A_S, P_DT, P_T_REF, P_ADAPT_JUMP, P_A_AD, P_A_STD, P_A_R,
  P_RATE_GAIN, P_W_SYN, LIF_NPARAM) = range(14)
 LIF_SYNC_WORDS = 64
-OPTIC_HISTORY = 1
+OPTIC_HISTORY, OPTIC_DR_VALID = 1, 2
 
 _VP = ct.c_void_p
 _I = ct.c_int
@@ -63,7 +63,7 @@ class SpmmArgs(ct.Structure):
                 ("x_div", ct.c_float), ("x_lo", ct.c_float), ("x_hi", ct.c_float),
                 ("y", _VP), ("y_index", _VP), ("y_rows", _I),
                 ("alpha", ct.c_float), ("y_lo", ct.c_float), ("y_hi", ct.c_float),
-                ("lanes_per_row", _I)]
+                ("warps_per_row", _I)]
 
 
 class AdjointArgs(ct.Structure):

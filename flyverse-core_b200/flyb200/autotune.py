@@ -91,7 +91,7 @@ def tune_optic(core, steps: int = 10) -> dict:
         for variant in (0, 1, 2):
             core.launch, core.variant = launch, variant
             core.substeps(2)
-            results[(launch, variant)] = _time(lambda: core.substeps(steps), 1) / steps
+            results[(launch, variant)] = _time(lambda: core.substeps(steps, carry=True), 1) / steps
             core.v_s.copy_(v)
             core.adapt_s.copy_(a)
     best = min(results, key=results.get)

@@ -113,8 +113,22 @@ class DeviceCSR:
         return t, torch.from_numpy(order.astype(np.int32)).to(device)
 
 
+def spmm_warps_per_row(nnz: int, rows: int, batch: int) -> int:
+    """Warps sharing one row of flyb_spmm: enough that one pass (U = 8 entries per lane group,
+    32 / F lane groups per warp with F = min(batch, 32) fly lanes) covers a row of mean length."""
+    if rows <= 0:
+        return 1
+    per_pass = 8 * max(1, 32 // min(max(batch, 1), 32))
+    mean = -(-nnz // rows)
+    wpr = 1
+    while wpr < 8 and wpr * per_pass < mean:
+        wpr *= 2
+    return wpr
+
+
 def spmm(M: DeviceCSR, x: torch.Tensor, y: torch.Tensor, *, x_index=None, x_div=1.0, x_lo=-math.inf,
-         x_hi=math.inf, y_index=None, alpha=1.0, y_lo=-math.inf, y_hi=math.inf, accumulate=False) -> None:
+         x_hi=math.inf, y_index=None, alpha=1.0, y_lo=-math.inf, y_hi=math.inf, accumulate=False,
+         warps_per_row: int | None = None) -> None:
     """y[ymap(i)][b] (+)= clamp(alpha * sum_e w_e * clamp(x[xmap(col_e)][b] / x_div, x_lo, x_hi), y_lo, y_hi).
 
     x, y: contiguous fly-minor storage [rows][B] on the device (include/flyb200.h: flyb_spmm)."""
@@ -127,7 +141,8 @@ def spmm(M: DeviceCSR, x: torch.Tensor, y: torch.Tensor, *, x_index=None, x_div=
                       col=M.col.data_ptr(), w=M.w.data_ptr(), x=x.data_ptr(),
                       x_index=None if x_index is None else x_index.data_ptr(), x_rows=x.shape[0], x_div=x_div,
                       x_lo=x_lo, x_hi=x_hi, y=y.data_ptr(), y_index=None if y_index is None else y_index.data_ptr(),
-                      y_rows=y.shape[0], alpha=alpha, y_lo=y_lo, y_hi=y_hi)
+                      y_rows=y.shape[0], alpha=alpha, y_lo=y_lo, y_hi=y_hi,
+                      warps_per_row=warps_per_row or spmm_warps_per_row(M.nnz, M.shape[0], B))
     rc = _abi.lib().flyb_spmm(ct.byref(a), torch.cuda.current_stream(x.device).cuda_stream)
     if rc:
         raise RuntimeError(f"flyb_spmm: error {rc}")
@@ -168,29 +183,57 @@ class OpticCore:
         self.adapt_s = torch.zeros(M, B, device=dev)
         self.pr_in = torch.zeros(M, B, device=dev)
         self.spk_in = torch.zeros(M, B, device=dev)
-        self._dr = torch.zeros(M, B, device=dev)
-        self._dr_tmp = torch.zeros(M, B, device=dev)
+        # dr ping-pong: _bufs[_cur] holds clip(v + b, 0, 1) - b of the current state after every call;
+        # _dr_key records (v, b) versions then, so a later call can skip recomputing it (carry=True)
+        self._bufs = (torch.zeros(M, B, device=dev), torch.zeros(M, B, device=dev))
+        self._cur = 0
+        self._dr_key = None
         self._status = torch.zeros(4, dtype=torch.int32, device=dev)
         self._sync = torch.zeros(64, dtype=torch.int32, device=dev)
         self._WT = None
 
-    def substeps(self, nsteps: int, v_hist: torch.Tensor | None = None, inp_hist: torch.Tensor | None = None) -> None:
+    def _state_key(self):
+        return (self.v_s._version, self.b._version, self.v_s.data_ptr(), self.b.data_ptr())
+
+    def substeps(self, nsteps: int, v_hist: torch.Tensor | None = None, inp_hist: torch.Tensor | None = None,
+                 carry: bool = False) -> None:
+        """Run `nsteps` substeps. `carry`: reuse the dr the previous call left (FLYB_OPTIC_DR_VALID)
+        when v and b have not been written since (tensor version counters), saving one pass over
+        the state; the kernels themselves never bump the counters."""
         if nsteps <= 0:
             return
+        flags = _abi.OPTIC_HISTORY if v_hist is not None else 0
+        if carry and self._dr_key == self._state_key():
+            flags |= _abi.OPTIC_DR_VALID
+        dr, dr_tmp = self._bufs[self._cur], self._bufs[1 - self._cur]
         a = _abi.OpticArgs(m=self.m, batch=self.B, nsteps=int(nsteps), launch=_abi.LAUNCHES_BY_NAME[self.launch],
                            ptr=self.W.ptr.data_ptr(), cw=self.W.cw.data_ptr(), variant=self.variant,
                            rows=self.rows.data_ptr(), n_long=self.n_long,
-                           v=self.v_s.data_ptr(), adapt=self.adapt_s.data_ptr(), dr=self._dr.data_ptr(),
-                           dr_tmp=self._dr_tmp.data_ptr(), pr=self.pr_in.data_ptr(), spk=self.spk_in.data_ptr(),
+                           v=self.v_s.data_ptr(), adapt=self.adapt_s.data_ptr(), dr=dr.data_ptr(),
+                           dr_tmp=dr_tmp.data_ptr(), pr=self.pr_in.data_ptr(), spk=self.spk_in.data_ptr(),
                            a=self.a.data_ptr(), b=self.b.data_ptr(), gr=self.gain_rr, ga=self.adapt_gain, aad=self.aad,
-                           flags=_abi.OPTIC_HISTORY if v_hist is not None else 0,
-                           v_hist=None if v_hist is None else v_hist.data_ptr(),
+                           flags=flags, v_hist=None if v_hist is None else v_hist.data_ptr(),
                            inp_hist=None if inp_hist is None else inp_hist.data_ptr(),
                            status=self._status.data_ptr(), sync=self._sync.data_ptr())
         with torch.cuda.device(self.device):
             rc = self._lib.flyb_optic_run(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
         if rc:
             raise RuntimeError(f"flyb_optic_run: error {rc}")
+        self._cur ^= int(nsteps) & 1
+        self._dr_key = self._state_key()
+
+    @property
+    def dr_out(self) -> torch.Tensor:
+        """The device buffer holding clip(v + b, 0, 1) - b of the state the last call left, [M][B]."""
+        return self._bufs[self._cur]
+
+    def pin_dr(self, cur: int) -> None:
+        """Move the current dr into buffer `cur` (stream-ordered copy when it is elsewhere): a CUDA
+        graph of an odd number of substeps must end with dr where it started."""
+        if self._cur != cur:
+            self._bufs[cur].copy_(self._bufs[self._cur])
+            self._cur = cur
+            self._dr_key = self._state_key()
 
     def dr(self) -> torch.Tensor:
         """clip(v + b, 0, 1) - b, [M][B]."""

@@ -1,19 +1,62 @@
 """A short, eager run of the whole-fly step for profilers (every kernel launched separately).
 
     python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic]
+                              [--lif-block 256] [--lif-ipt 0|1|2|4]
+    python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
 `--steps` steps of the chosen part. Used for the launch list and the per-kernel captures whose
-summaries live in profiles/.
+summaries live in profiles/. `--breakdown` instead times each stage of the step on its own with
+CUDA events (stream-ordered, warm L2) and prints one JSON line of microseconds per stage.
 """
 from __future__ import annotations
 
 import argparse
+import json
 
 import torch
 
 from . import synthetic
+from .optic import spmm
 from .whole import WholeFly
+
+
+def _time_us(fn, reps: int) -> float:
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(reps):
+        fn()
+    e.record()
+    e.synchronize()
+    return 1000.0 * s.elapsed_time(e) / reps
+
+
+def breakdown(eng: WholeFly, reps: int) -> dict:
+    """Microseconds per stage of one whole-fly step, each stage repeated alone `reps` times."""
+    o = eng.cfg.optic
+    rate, drive = eng.lif._st["rate"], eng.lif._st["drive"]
+    stages = {
+        "spk_in = W_rs rate": lambda: spmm(eng.W_rs, rate, eng.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0,
+                                           alpha=o.gain_fb, y_index=eng.rs_rows),
+        "optic substep": lambda: eng.optic.substeps(1, carry=True),
+        "drive = W_sr dr": lambda: spmm(eng.W_sr, eng.optic.dr_out, drive, y_index=eng.sr_rows, alpha=o.gain_out_mv,
+                                        y_lo=-o.drive_clip_mv, y_hi=o.drive_clip_mv),
+        "lif step": lambda: eng.lif.step(1),
+        "whole step (eager)": lambda: eng.step(1),
+    }
+    out = {k: _time_us(f, reps) for k, f in stages.items()}
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            eng.step(10)
+    torch.cuda.current_stream().wait_stream(s)
+    out["whole step (graph of 10)"] = _time_us(g.replay, max(1, reps // 10)) / 10
+    del g
+    return out
 
 
 def main() -> None:
@@ -22,19 +65,29 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--part", default="whole", choices=["whole", "lif", "optic"])
+    ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--lif-block", type=int, default=256)
+    ap.add_argument("--lif-ipt", type=int, default=0, help="LIF items per thread (0: automatic)")
     args = ap.parse_args()
     cfg = synthetic.whole_fly_config5(seed=0)
     eng = WholeFly(cfg, args.batch, device="cuda", seed=1, launch="step")
+    eng.lif.block, eng.lif.items_per_thread = args.lif_block, args.lif_ipt
+    eng.lif._make_args()
     eng.optic.pr_in.normal_(0.0, 0.2)
     eng.step(args.warmup)
     torch.cuda.synchronize()
+    if args.breakdown:
+        res = breakdown(eng, max(10, args.steps))
+        eng.lif.check()
+        print(json.dumps({"batch": args.batch, "us": res}))
+        return
     for _ in range(args.steps):
         if args.part == "whole":
             eng.step(1)
         elif args.part == "lif":
             eng.lif.step(1)
         else:
-            eng.optic.substeps(1)
+            eng.optic.substeps(1, carry=True)
     torch.cuda.synchronize()
     eng.lif.check()
     print(f"profiled {args.steps} {args.part} steps at batch {args.batch}: {eng.n_neurons:,} neurons")

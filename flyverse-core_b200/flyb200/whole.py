@@ -55,12 +55,10 @@ class WholeFly:
 
     @property
     def launches_per_step(self) -> int:
-        """Kernel launches of one step: two coupling products, the optic substep (a dr
-        initialisation + the substep, or one persistent launch) and the LIF step (+ the clock
-        advance in per-step mode)."""
-        optic = 2 if self.optic.launch == "step" else 1
-        lif = 2 if self.lif.launch == "step" else 1
-        return 2 + optic + lif
+        """Kernel launches of one step once running: two coupling products, the optic substep (its
+        dr carried over from the previous step), the LIF step and its device-clock advance (one
+        launch per step, or one persistent launch)."""
+        return 5 if self.lif.launch == "step" else 4
 
     @staticmethod
     def _rows_with_entries(M, dev):
@@ -78,16 +76,23 @@ class WholeFly:
         spmm(self.W_rp, self.a_pr, self.optic.pr_in, alpha=self.cfg.optic.gain_in)
 
     def step(self, n: int = 1) -> None:
+        """Advance every fly n steps. Each optic substep reuses the dr the previous one wrote. Under
+        CUDA-graph capture the recorded steps end with that dr in the buffer they started from, so
+        the graph replays back to back; a graph replay assumes nothing else wrote the optic state
+        since the capture (a write is seen at capture time only)."""
         o = self.cfg.optic
         lif_rate = self.lif._st["rate"]
         drive = self.lif._st["drive"]
+        cur0 = self.optic._cur
         for _ in range(int(n)):
             spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb,
                  y_index=self.rs_rows)
-            self.optic.substeps(1)
-            spmm(self.W_sr, self.optic._dr_tmp, drive, y_index=self.sr_rows, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
+            self.optic.substeps(1, carry=True)
+            spmm(self.W_sr, self.optic.dr_out, drive, y_index=self.sr_rows, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
                  y_hi=o.drive_clip_mv)
             self.lif.step(1)
+        if torch.cuda.is_current_stream_capturing():
+            self.optic.pin_dr(cur0)
         self.steps_taken += int(n)
 
     # ------------------------------------------------------------------ algorithmic bytes (roofline)

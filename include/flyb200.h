@@ -140,7 +140,15 @@ int flyb_lif_run(const flyb_lif_args* a, void* stream);
 int flyb_ring_deposit(int n, int batch, int ring_mode, const int* out_ptr, const int* out_edge,
                       const float* x, void* ring_slot, void* stream);
 
-/* Optic lobe: `nsteps` fused substeps of y = W_rr @ dr and the rate update, state [m][batch]. */
+/* Optic lobe: `nsteps` fused substeps of y = W_rr @ dr and the rate update, state [m][batch].
+ * Substep s reads dr from (s even ? dr : dr_tmp) and writes the next one to the other buffer, so
+ * after the call the dr of the final state, clip(v + b, 0, 1) - b, is in `dr` when nsteps is even
+ * and in `dr_tmp` when it is odd. */
+#define FLYB_OPTIC_HISTORY   1   /* store v and the input of every substep (adjoint recompute)   */
+#define FLYB_OPTIC_DR_VALID  2   /* `dr` already holds clip(v + b, 0, 1) - b of the current v (the
+                                    final dr of the previous call, buffers swapped by the caller):
+                                    the initialisation pass over the state is skipped. Ignored by
+                                    flyb_optic_run_noalloc, whose buffers the caller cannot see. */
 typedef struct flyb_optic_args {
   int m;                 /* rate units                                               */
   int batch;
@@ -149,7 +157,7 @@ typedef struct flyb_optic_args {
   int block;             /* threads per block (0 = default)                          */
   int grid;              /* persistent grid cap (0 = occupancy)                      */
   int variant;           /* kernel shape: 0 default, 1 / 2 alternatives (autotuned)  */
-  int flags;             /* bit0: store per-substep history (adjoint recompute)      */
+  int flags;             /* FLYB_OPTIC_*                                             */
   const int* ptr;        /* W_rr CSR row pointers [m + 1], rows = postsynaptic units */
   const int* cw;         /* [nnz][2] interleaved {column, float bits of weight}      */
   const int* rows;       /* optional [m] row order: rows[0, n_long) are long rows, each
@@ -196,7 +204,7 @@ typedef struct flyb_spmm_args {
   float x_div, x_lo, x_hi;
   float* y; const int* y_index; int y_rows;
   float alpha, y_lo, y_hi;
-  int lanes_per_row;
+  int warps_per_row;     /* 1, 2, 4 or 8 warps share one row (0 = 1): more for long rows */
 } flyb_spmm_args;
 
 int flyb_spmm(const flyb_spmm_args* a, void* stream);

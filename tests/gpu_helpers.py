@@ -13,7 +13,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda", items_per_thread=0):
+                   device="cuda", items_per_thread=0, with_sync=True):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -40,7 +40,7 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
                      poisson_p=d["poisson_p"].data_ptr(), active=active.data_ptr(), std_u=std_u.data_ptr(),
                      params=P.ctypes.data, ring=ring.data_ptr(), uniforms=None if uni is None else uni.data_ptr(),
                      fly_steps=None if fs is None else fs.data_ptr(), raster=None if r is None else r.data_ptr(),
-                     events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr())
+                     events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr() if with_sync else None)
     rc = _abi.lib().flyb_lif_run(ct.byref(a), torch.cuda.current_stream(dev).cuda_stream)
     if rc:
         raise RuntimeError(f"flyb_lif_run: error {rc}")

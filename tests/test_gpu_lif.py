@@ -77,7 +77,7 @@ def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed
                 uniforms=None, fly_steps=fs, seed=12345)
 
 
-def _compare(case, launch, block, grid=0, ipt=0):
+def _compare(case, launch, block, grid=0, ipt=0, with_sync=True):
     s_ref, s_gpu = case["state"].copy(), case["state"].copy()
     fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
     fs_gpu = None if fs_ref is None else fs_ref.copy()
@@ -85,7 +85,7 @@ def _compare(case, launch, block, grid=0, ipt=0):
               uniforms=case["uniforms"], raster=True)
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, **kw)
     r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], fly_steps=fs_gpu, launch=launch,
-                                   block=block, grid=grid, items_per_thread=ipt, **kw)
+                                   block=block, grid=grid, items_per_thread=ipt, with_sync=with_sync, **kw)
     assert unpack(r_ref, s_ref.n * s_ref.batch).sum() > 0
     np.testing.assert_array_equal(r_gpu, r_ref)                      # spike rasters
     for k in LIF_ARRAYS:
@@ -123,9 +123,11 @@ def test_uneven_batches_and_fixed_ring(batch):
     _compare(case_random(batch=batch, fixed=True, steps=120), PERS, 256)
 
 
-@pytest.mark.parametrize("launch", [STEP, PERS])
-def test_uneven_episodes_native_equals_oracle(launch):
-    _compare(case_random(batch=16, steps=150, episodes=True), launch, 256)
+@pytest.mark.parametrize("launch,with_sync", [(STEP, True), (STEP, False), (PERS, True)])
+def test_uneven_episodes_native_equals_oracle(launch, with_sync):
+    """Episode counters gate the update and are lowered after the run; per-step launches need no
+    sync words."""
+    _compare(case_random(batch=16, steps=150, episodes=True), launch, 256, with_sync=with_sync)
 
 
 def test_sharded_flies_equal_one_batch():

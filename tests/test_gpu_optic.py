@@ -74,8 +74,48 @@ def test_fp64_error_of_fp32_substeps_is_small():
     assert np.abs(r_gpu - r_64).max() < 1e-4
 
 
-@pytest.mark.parametrize("batch", [1, 3, 64])
-def test_held_input_products_match_oracle(batch):
+@pytest.mark.parametrize("launch", ["step", "persistent"])
+def test_carried_dr_equals_fresh_initialisation(launch):
+    """Substeps that reuse the previous call's dr (FLYB_OPTIC_DR_VALID) give the same bits as calls
+    that recompute it; a host write to v between calls is seen and forces the recompute."""
+    cfg = small_optic(seed=7)
+    W = cfg.W_rr()
+    B = 8
+    rng = np.random.default_rng(3)
+    v0 = (rng.standard_normal((cfg.m, B)) * 0.3).astype(np.float32)
+    pr = (rng.standard_normal((cfg.m, B)) * 0.3).astype(np.float32)
+    v_mid = (rng.standard_normal((cfg.m, B)) * 0.3).astype(np.float32)
+    cores = []
+    for carry in (True, False):
+        core = OpticCore(W, cfg.a, cfg.b, batch=B, device="cuda", gain_rr=cfg.gain_rr, adapt_gain=cfg.adapt_gain,
+                         aad=cfg.aad, launch=launch)
+        core.v_s.copy_(torch.from_numpy(v0))
+        core.pr_in.copy_(torch.from_numpy(pr))
+        for k, n in enumerate((1, 2, 1, 3, 1, 1)):
+            if k == 3:
+                core.v_s[: cfg.m // 2].copy_(torch.from_numpy(v_mid[: cfg.m // 2]))
+            core.substeps(n, carry=carry)
+            torch.cuda.synchronize()
+            np.testing.assert_array_equal(core.dr_out.cpu().numpy(), core.dr().cpu().numpy())
+        core.check()
+        cores.append(core)
+    for name in ("v_s", "adapt_s"):
+        np.testing.assert_array_equal(getattr(cores[0], name).cpu().numpy(), getattr(cores[1], name).cpu().numpy())
+    # and both equal the oracle run the same way
+    v, ad = v0.copy(), np.zeros_like(v0)
+    spk = np.zeros_like(v0)
+    for k, n in enumerate((1, 2, 1, 3, 1, 1)):
+        if k == 3:
+            v[: cfg.m // 2] = v_mid[: cfg.m // 2]
+        oracle.optic_run(v, ad, W.indptr, W.indices, W.data, pr, spk, cfg.a, cfg.b, cfg.gain_rr, cfg.adapt_gain,
+                         cfg.aad, n)
+    np.testing.assert_allclose(cores[0].v_s.cpu().numpy(), v, rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("batch,wpr", [(1, None), (3, None), (64, None), (64, 1), (5, 2), (64, 4), (40, 8), (1, 8)])
+def test_held_input_products_match_oracle(batch, wpr):
+    """The held-input products with the warps-per-row split chosen from the mean row length, or
+    forced to each allowed value."""
     cfg = small_optic(seed=6)
     rng = np.random.default_rng(1)
     rates = (rng.random((cfg.W_rs.shape[1] + 50, batch)) * 500).astype(np.float32)   # [N][B] Hz
@@ -83,7 +123,7 @@ def test_held_input_products_match_oracle(batch):
     M = DeviceCSR(cfg.W_rs, "cuda")
     y = torch.zeros(cfg.m, batch, device="cuda")
     spmm(M, torch.from_numpy(rates).cuda(), y, x_index=torch.from_numpy(x_index).cuda(), x_div=100.0, x_lo=0.0,
-         x_hi=3.0, alpha=0.5)
+         x_hi=3.0, alpha=0.5, warps_per_row=wpr)
     W = cfg.W_rs.tocsr()
     ref = oracle.spmm(W.indptr, W.indices, W.data, rates, batch, rows=W.shape[0], x_index=x_index, x_div=100.0,
                       x_lo=0.0, x_hi=3.0, alpha=0.5)
@@ -93,7 +133,7 @@ def test_held_input_products_match_oracle(batch):
     y_index = rng.permutation(W.shape[0] + 10)[: W.shape[0]].astype(np.int32)
     out = torch.zeros(W.shape[0] + 10, batch, device="cuda")
     spmm(DeviceCSR(W, "cuda"), torch.from_numpy(d).cuda(), out, y_index=torch.from_numpy(y_index).cuda(), alpha=100.0,
-         y_lo=-35.0, y_hi=35.0)
+         y_lo=-35.0, y_hi=35.0, warps_per_row=wpr)
     ref = np.zeros((W.shape[0] + 10, batch), np.float32)
     oracle.spmm(W.indptr, W.indices, W.data, d, batch, rows=W.shape[0], y=ref, y_index=y_index, alpha=100.0,
                 y_lo=-35.0, y_hi=35.0)

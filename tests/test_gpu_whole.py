@@ -59,6 +59,44 @@ def test_whole_fly_matches_oracle_step_order():
     np.testing.assert_allclose(eng.lif._st["v"].cpu().numpy(), st.v, rtol=0, atol=1e-4)
 
 
+@pytest.mark.parametrize("chunk", [2, 3])
+def test_graph_replay_equals_eager_steps(chunk):
+    """A CUDA graph of `chunk` whole-fly steps replayed back to back gives the bits of eager steps:
+    the carried optic dr ends each replay in the buffer it started from (an odd chunk adds a copy)
+    and the LIF device clock gives every replay fresh Philox counters and ring slots."""
+    cfg = small_fly()
+    B = 4
+    a_pr = torch.from_numpy((np.random.default_rng(5).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
+    engs = []
+    for _ in range(2):
+        eng = WholeFly(cfg, B, device="cuda", seed=7, launch="step")
+        eng.set_photoreceptors(a_pr)
+        eng.step(3)
+        engs.append(eng)
+    graphed, eager = engs
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            graphed.step(chunk)
+    torch.cuda.current_stream().wait_stream(s)
+    reps = 5
+    for _ in range(reps):
+        g.replay()
+    eager.step(chunk * reps)
+    torch.cuda.synchronize()
+    graphed.lif.check()
+    graphed.optic.check()
+    for k in ("v", "g", "rate", "spike_counts", "spikes", "adapt"):
+        assert torch.equal(graphed.lif._st[k], eager.lif._st[k]), k
+    assert torch.equal(graphed.lif.ring, eager.lif.ring)
+    assert torch.equal(graphed.optic.v_s, eager.optic.v_s)
+    assert torch.equal(graphed.optic.adapt_s, eager.optic.adapt_s)
+    assert torch.equal(graphed.optic.dr_out, eager.optic.dr_out)
+    del g
+
+
 def test_autotuner_keeps_state_and_installs_a_choice():
     cfg = small_fly()
     eng = WholeFly(cfg, 8, device="cuda", seed=3, launch="step")
