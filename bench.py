@@ -271,7 +271,7 @@ def measure_e2e(cfg, eng, device, steps) -> dict:
     o, B = cfg.optic, eng.B
     rad_host = torch.from_numpy(o.grating(0.0, B, seed=0)).pin_memory()
     rad_dev = torch.empty_like(rad_host, device=device)
-    groups = np.array_split(np.asarray(cfg.vpn_idx[:900]), 90)
+    groups = np.array_split(eng.lif_position[np.asarray(cfg.vpn_idx[:900])], 90)   # stored LIF order
     ptr = torch.tensor(np.r_[0, np.cumsum([len(g) for g in groups])], dtype=torch.int32, device=device)
     idx = torch.tensor(np.concatenate(groups), dtype=torch.int32, device=device)
     out_host = torch.empty(B, 90, dtype=torch.float64).pin_memory()

@@ -23,6 +23,9 @@ struct LifP {
 
 struct LifK {
   int n, batch, n_delay, R, flags, nsteps, ring_pos, words, raster_slots, raster_pos, fly0;
+  unsigned bdiv_m;      // item t -> neuron t / batch as (umulhi(t, bdiv_m) + t) >> bdiv_s (t < 2^31)
+  int bdiv_s;
+  int t_begin, t_end;   // items [t_begin, t_end) = neurons [n_first, n_first + n_count) x batch
   long long step0;
   unsigned long long seed;
   const int* __restrict__ out_ptr;
@@ -53,6 +56,20 @@ struct LifSmem {
   int fly[BLOCK];     // fly of each spiker
   float x[BLOCK];     // transmitted amount (1, or spike * resource under depression)
 };
+
+// Division by the batch width with a precomputed multiplier (Granlund & Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994: the round-up variant with an added dividend):
+// exact for every 0 <= t < 2^31.
+__device__ __forceinline__ int neuron_of(const LifK& k, int t) {
+  return (int)((__umulhi((unsigned)t, k.bdiv_m) + (unsigned)t) >> k.bdiv_s);
+}
+
+static void batch_divider(int d, unsigned* m, int* s) {
+  int l = 0;
+  while ((1ll << l) < d) ++l;
+  *m = (unsigned)(((1ull << 32) * ((1ull << l) - (unsigned long long)d)) / (unsigned long long)d + 1ull);
+  *s = l;
+}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -145,6 +162,149 @@ __device__ __forceinline__ void vstore(T* p, const T (&x)[IPT]) {
   }
 }
 
+// Steps 1-4 of one live item (neuron i, fly b) whose ring entry due now is c, in the reference
+// order (brain.py:829-868, neural.cu:18-52), every float operation separately rounded. Returns the
+// spike value; x is the amount transmitted (the spike, times the resource under depression).
+template <bool FIXED, typename RingT>
+__device__ __forceinline__ float lif_update(const LifK& k, const Clk& clk, int s, size_t slot, size_t t, int i, int b,
+                                            RingT c, float act, float pp, float dv, float& v, float& g, float& ref,
+                                            float& ad, float& rt, float& cn, float& rr, float& x) {
+  const LifP& P = k.P;
+  const int flags = k.flags;
+  // 1. synaptic input due now
+  float g1 = g * P.a_s;
+  if (c) {
+    const float inc = FIXED ? __double2float_rn((double)c * (1.0 / 4294967296.0)) : P.w_syn * (float)c;
+    g1 = g1 + inc;
+  }
+  g = g1;
+  // 2. membrane, exponential Euler with g and drive held (brain.py:839-843)
+  float target = P.v_rest + g1;
+  target = target + dv;
+  target = target - ad;
+  float u = v - target;
+  u = u * P.a_m;
+  float v1 = target + u;
+  float r1 = ref;
+  if (r1 > 0.0f) v1 = P.v_reset;
+  r1 = r1 - P.dt;
+  if (r1 < 0.0f) r1 = 0.0f;
+  // 3. threshold x active, Poisson forcing (brain.py:845-849)
+  float spike = (v1 >= P.v_th ? 1.0f : 0.0f) * act;
+  if (pp > 0.0f) {
+    const float un = (flags & FLYB_LIF_EXT_UNIFORM)
+                         ? k.uniforms[(size_t)s * slot + t]
+                         : philox_uniform(k.seed, clk.step0 + s, (uint32_t)i, (uint32_t)(k.fly0 + b));
+    if (un < pp) spike = 1.0f;
+  }
+  const bool fired = spike > 0.0f;
+  if (fired) { v1 = P.v_reset; r1 = P.t_ref; }
+  v = v1;
+  ref = r1;
+  // 4. adaptation, depression, counters, rate (brain.py:853-868)
+  if (flags & FLYB_LIF_ADAPT) { float a1 = ad * P.a_ad; a1 = a1 + spike * P.jump; ad = a1; }
+  x = spike;
+  if (flags & FLYB_LIF_STD) {
+    float r2 = rr;
+    x = spike * r2;
+    if (fired) { const float keep = 1.0f - k.std_u[i]; r2 = r2 * keep; }
+    float dep = 1.0f - r2;
+    dep = dep * P.a_std;
+    rr = 1.0f - dep;
+  }
+  if (flags & FLYB_LIF_COUNTS) cn = cn + spike;
+  float r3 = rt * P.a_r;
+  r3 = r3 + spike * P.rg;
+  rt = r3;
+  return spike;
+}
+
+// 5-6. Compact the transmitting items of a block (per-thread bits over IPT items, warp scan, block
+// prefix), prefix their out-degrees, then deliver every out-edge edge-parallel into ring slot `ws`
+// with integer red.global.add. tx bit q of a thread describes its item q: neuron iq[q], fly bq[q],
+// transmitted amount xq[q].
+template <int BLOCK, bool FIXED, int IPT>
+__device__ __forceinline__ void deliver(const LifK& k, LifSmem<BLOCK * IPT>& sm, unsigned tx_bits, const int (&iq)[IPT],
+                                        const int (&bq)[IPT], const float (&xq)[IPT], int ws, size_t slot) {
+  constexpr int NW = BLOCK / 32;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cnt = __popc(tx_bits);
+  const int incl = warp_scan(cnt);
+  if (lane == 31) sm.wcnt[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const int c = lane < NW ? sm.wcnt[lane] : 0;
+    const int inc = warp_scan(c);
+    if (lane < NW) sm.woff[lane] = inc - c;
+    if (lane == 31) sm.total = inc;
+  }
+  __syncthreads();
+  const int L = sm.total;
+  if (L == 0) return;   // block-uniform
+  {
+    int pos = sm.woff[warp] + incl - cnt;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      if (tx_bits & (1u << q)) {
+        const int e0 = k.out_ptr[iq[q]];
+        sm.start[pos] = e0;
+        sm.fly[pos] = bq[q];
+        sm.x[pos] = xq[q];
+        sm.pre[pos] = k.out_ptr[iq[q] + 1] - e0;   // degree for now; exclusive prefix below
+        ++pos;
+      }
+    }
+  }
+  __syncthreads();
+  // exclusive prefix of the degrees over the L transmitting items (thread j: entries j*IPT..)
+  {
+    int d[IPT], sum = 0;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      const int e = threadIdx.x * IPT + q;
+      d[q] = e < L ? sm.pre[e] : 0;
+      sum += d[q];
+    }
+    const int inc = warp_scan(sum);
+    if (lane == 31) sm.wcnt[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      const int c = lane < NW ? sm.wcnt[lane] : 0;
+      const int winc = warp_scan(c);
+      if (lane < NW) sm.woff[lane] = winc - c;
+      if (lane == 31) sm.edges = winc;
+    }
+    __syncthreads();
+    int run = sm.woff[warp] + inc - sum;
+#pragma unroll
+    for (int q = 0; q < IPT; ++q) {
+      const int e = threadIdx.x * IPT + q;
+      if (e < L) sm.pre[e] = run;
+      run += d[q];
+    }
+    __syncthreads();
+  }
+  const int E = sm.edges;
+  // 6. block-wide, edge-parallel delivery into slot ws: thread j takes edges j, j+BLOCK, ...
+  for (int q = threadIdx.x; q < E; q += BLOCK) {
+    int lo = 0, hi = L - 1;   // last transmitting item with pre <= q
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sm.pre[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const int2 ed = __ldg(&k.out_edge[sm.start[lo] + (q - sm.pre[lo])]);
+    const size_t dst = (size_t)ws * slot + (size_t)ed.x * k.batch + sm.fly[lo];
+    if (FIXED) {
+      const long long f = __double2ll_rn((double)__int_as_float(ed.y) * (double)sm.x[lo] * 4294967296.0);
+      atomicAdd((unsigned long long*)k.ring + dst, (unsigned long long)f);
+    } else {
+      atomicAdd((int*)k.ring + dst, ed.y);
+    }
+  }
+  if (k.events && threadIdx.x == 0) atomicAdd(k.events, (unsigned long long)E);
+  __syncthreads();   // shared lists are reused by the next chunk
+}
+
 // One block processes work items [base, base + BLOCK*IPT) of local step `s`: update, then deliver.
 // Thread j owns the IPT consecutive items base + j*IPT + q (neuron-major, fly-minor order), loads
 // every state array as one vector and keeps all loads in flight before computing.
@@ -152,12 +312,11 @@ template <int BLOCK, bool FIXED, int IPT>
 __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, long long base,
                                           LifSmem<BLOCK * IPT>& sm) {
   using RingT = typename std::conditional<FIXED, long long, int>::type;
-  constexpr int NW = BLOCK / 32;
-  const long long W = (long long)k.n * k.batch;
+  const long long W = k.t_end;                         // items of this launch end here
   const long long t0 = base + (long long)threadIdx.x * IPT;
   const int rs = (int)(((long long)clk.ring_pos + s) % k.R);
   const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
-  const size_t slot = (size_t)W;
+  const size_t slot = (size_t)k.n * k.batch;            // ring slot stride
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const LifP& P = k.P;
   const int flags = k.flags;
@@ -219,6 +378,8 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
       }
       if (skip) continue;           // sp stays 0 == the cell's spike value
       touched = true;
+      // steps 1-4, the arithmetic of lif_update written out over the item vectors (kept inline: the
+      // vector path's register allocation, and with it its occupancy, depends on it)
       // 1. synaptic input due now
       float g1 = gg[q] * P.a_s;
       if (c[q]) {
@@ -307,119 +468,283 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
       k.raster[rslot * k.words + (size_t)((wbase >> 5) + lane / LPW)] = v;
     }
   }
-  // 5. compact the transmitting items of this block (per-thread bits, warp scan, block prefix)
-  const int cnt = __popc(tx_bits);
-  const int incl = warp_scan(cnt);
-  if (lane == 31) sm.wcnt[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    const int c = lane < NW ? sm.wcnt[lane] : 0;
-    const int inc = warp_scan(c);
-    if (lane < NW) sm.woff[lane] = inc - c;
-    if (lane == 31) sm.total = inc;
-  }
-  __syncthreads();
-  const int L = sm.total;
-  if (L == 0) return;   // block-uniform
-  {
-    int pos = sm.woff[warp] + incl - cnt;
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      if (tx_bits & (1u << q)) {
-        const int e0 = k.out_ptr[iq[q]];
-        sm.start[pos] = e0;
-        sm.fly[pos] = bq[q];
-        sm.x[pos] = xq[q];
-        sm.pre[pos] = k.out_ptr[iq[q] + 1] - e0;   // degree for now; exclusive prefix below
-        ++pos;
-      }
-    }
-  }
-  __syncthreads();
-  // exclusive prefix of the degrees over the L transmitting items (thread j: entries j*IPT..)
-  {
-    int d[IPT], sum = 0;
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      const int e = threadIdx.x * IPT + q;
-      d[q] = e < L ? sm.pre[e] : 0;
-      sum += d[q];
-    }
-    const int inc = warp_scan(sum);
-    if (lane == 31) sm.wcnt[warp] = inc;
-    __syncthreads();
-    if (warp == 0) {
-      const int c = lane < NW ? sm.wcnt[lane] : 0;
-      const int winc = warp_scan(c);
-      if (lane < NW) sm.woff[lane] = winc - c;
-      if (lane == 31) sm.edges = winc;
-    }
-    __syncthreads();
-    int run = sm.woff[warp] + inc - sum;
-#pragma unroll
-    for (int q = 0; q < IPT; ++q) {
-      const int e = threadIdx.x * IPT + q;
-      if (e < L) sm.pre[e] = run;
-      run += d[q];
-    }
-    __syncthreads();
-  }
-  const int E = sm.edges;
-  // 6. block-wide, edge-parallel delivery into slot ws: thread j takes edges j, j+BLOCK, ...
-  for (int q = threadIdx.x; q < E; q += BLOCK) {
-    int lo = 0, hi = L - 1;   // last transmitting item with pre <= q
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (sm.pre[mid] <= q) lo = mid; else hi = mid - 1;
-    }
-    const int2 ed = __ldg(&k.out_edge[sm.start[lo] + (q - sm.pre[lo])]);
-    const size_t dst = (size_t)ws * slot + (size_t)ed.x * k.batch + sm.fly[lo];
-    if (FIXED) {
-      const long long f = __double2ll_rn((double)__int_as_float(ed.y) * (double)sm.x[lo] * 4294967296.0);
-      atomicAdd((unsigned long long*)k.ring + dst, (unsigned long long)f);
-    } else {
-      atomicAdd((int*)k.ring + dst, ed.y);
-    }
-  }
-  if (k.events && threadIdx.x == 0) atomicAdd(k.events, (unsigned long long)E);
-  __syncthreads();   // shared lists are reused by the next chunk
+  deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
 }
 
 template <int BLOCK, bool FIXED, int IPT>
 __global__ void __launch_bounds__(BLOCK) lif_step_kernel(LifK k, int s) {
   __shared__ LifSmem<BLOCK * IPT> sm;
   const Clk clk = read_clock(k);
-  lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, (long long)blockIdx.x * BLOCK * IPT, sm);
+  lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, k.t_begin + (long long)blockIdx.x * BLOCK * IPT, sm);
 }
 
 __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
 
+// A run ends by advancing the device clock / episode counters unless the caller does it later.
+static bool needs_advance(const LifK& k) {
+  return (k.clock || (k.flags & FLYB_LIF_EPISODES)) && !(k.flags & FLYB_LIF_NO_ADVANCE);
+}
+
 template <int BLOCK, bool FIXED, int IPT>
 __global__ void __launch_bounds__(BLOCK) lif_persistent_kernel(LifK k) {
   __shared__ LifSmem<BLOCK * IPT> sm;
-  const long long W = (long long)k.n * k.batch;
   const Clk clk = read_clock(k);
   int generation = 0;
   for (int s = 0; s < k.nsteps; ++s) {
-    for (long long base = (long long)blockIdx.x * BLOCK * IPT; base < W; base += (long long)gridDim.x * BLOCK * IPT)
+    for (long long base = k.t_begin + (long long)blockIdx.x * BLOCK * IPT; base < k.t_end;
+         base += (long long)gridDim.x * BLOCK * IPT)
       lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, base, sm);
     // the next step writes the slot this step read: every block must be done with it
     if (!grid_barrier(k.sync, k.status, generation, s)) return;
   }
   // every block has read the clock and the episode counters: advance them
-  if (blockIdx.x == 0) advance_clock(k, clk);
+  if (blockIdx.x == 0 && !(k.flags & FLYB_LIF_NO_ADVANCE)) advance_clock(k, clk);
+}
+
+// ------------------------------------------------------------------ staged (bulk-copy) step
+// One step, per-step launch, blocks looping over chunks of CH = BLOCK * IPT items. A chunk's state
+// arrays are copied global -> shared by the async proxy (cp.async.bulk, completion on an mbarrier)
+// while the block updates and delivers the previous chunk from the other stage; the updated arrays
+// go back shared -> global the same way. Thread j handles items j + r * BLOCK of a chunk (r < IPT),
+// one at a time from shared memory, so the registers hold one item and the copies in flight
+// replace the vector loads of the register path.
+template <int BLOCK, bool FIXED, int IPT>
+struct StagedLayout {
+  using RingT = typename std::conditional<FIXED, long long, int>::type;
+  static constexpr int CH = BLOCK * IPT;
+  enum { V, G, REF, AD, DV, RT, PP, CN, RR, NF };             // float arrays of a stage; DV holds spikes out
+  static constexpr size_t RING = (size_t)CH * sizeof(RingT);
+  static constexpr size_t STAGE = RING + (size_t)NF * CH * sizeof(float);
+  static constexpr size_t BARS = 128;                          // two mbarriers, padded
+  static constexpr size_t LISTS = BARS + 2 * STAGE;
+  static constexpr size_t BYTES = LISTS + sizeof(LifSmem<CH>);
+};
+
+// Loads of the chunk starting at item `base` (items up to W) into `stage`, on barrier `bar`.
+template <int BLOCK, bool FIXED, int IPT>
+__device__ __forceinline__ void staged_issue_loads(const LifK& k, unsigned char* stage, long long base, long long W,
+                                                   const void* ring_rd, uint64_t* bar) {
+  using L = StagedLayout<BLOCK, FIXED, IPT>;
+  using RingT = typename L::RingT;
+  const long long n = W - base < L::CH ? W - base : L::CH;      // a multiple of 4 (checked on the host)
+  const uint32_t fb = (uint32_t)(n * sizeof(float)), rb = (uint32_t)(n * sizeof(RingT));
+  float* f = reinterpret_cast<float*>(stage + L::RING);
+  const int flags = k.flags;
+  const int nf = 6 + ((flags & FLYB_LIF_POISSON) ? 1 : 0) + ((flags & FLYB_LIF_COUNTS) ? 1 : 0) +
+                 ((flags & FLYB_LIF_STD) ? 1 : 0);
+  mbar_arrive_expect(bar, rb + (uint32_t)nf * fb);
+  bulk_load(stage, (const RingT*)ring_rd + base, rb, bar);
+  bulk_load(f + L::V * L::CH, k.v + base, fb, bar);
+  bulk_load(f + L::G * L::CH, k.g + base, fb, bar);
+  bulk_load(f + L::REF * L::CH, k.refrac + base, fb, bar);
+  bulk_load(f + L::AD * L::CH, k.adapt + base, fb, bar);
+  bulk_load(f + L::DV * L::CH, k.drive + base, fb, bar);
+  bulk_load(f + L::RT * L::CH, k.rate + base, fb, bar);
+  if (flags & FLYB_LIF_POISSON) bulk_load(f + L::PP * L::CH, k.poisson_p + base, fb, bar);
+  if (flags & FLYB_LIF_COUNTS) bulk_load(f + L::CN * L::CH, k.counts + base, fb, bar);
+  if (flags & FLYB_LIF_STD) bulk_load(f + L::RR * L::CH, k.res + base, fb, bar);
+}
+
+template <int BLOCK, bool FIXED, int IPT>
+__device__ __forceinline__ void staged_issue_stores(const LifK& k, unsigned char* stage, long long base, long long W) {
+  using L = StagedLayout<BLOCK, FIXED, IPT>;
+  const long long n = W - base < L::CH ? W - base : L::CH;
+  const uint32_t fb = (uint32_t)(n * sizeof(float));
+  float* f = reinterpret_cast<float*>(stage + L::RING);
+  const int flags = k.flags;
+  bulk_store(k.v + base, f + L::V * L::CH, fb);
+  bulk_store(k.g + base, f + L::G * L::CH, fb);
+  bulk_store(k.refrac + base, f + L::REF * L::CH, fb);
+  bulk_store(k.spikes + base, f + L::DV * L::CH, fb);
+  bulk_store(k.rate + base, f + L::RT * L::CH, fb);
+  if (flags & FLYB_LIF_ADAPT) bulk_store(k.adapt + base, f + L::AD * L::CH, fb);
+  if (flags & FLYB_LIF_COUNTS) bulk_store(k.counts + base, f + L::CN * L::CH, fb);
+  if (flags & FLYB_LIF_STD) bulk_store(k.res + base, f + L::RR * L::CH, fb);
+  bulk_commit();
+}
+
+template <int BLOCK, bool FIXED, int IPT>
+__global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
+  using L = StagedLayout<BLOCK, FIXED, IPT>;
+  using RingT = typename L::RingT;
+  constexpr int CH = L::CH;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  LifSmem<CH>& sm = *reinterpret_cast<LifSmem<CH>*>(smem + L::LISTS);
+  __shared__ int ok;
+  const long long W = k.t_end;                                 // items [t_begin, t_end) of this launch
+  const long long nchunks = (W - k.t_begin + CH - 1) / CH;
+  const size_t slot = (size_t)k.n * k.batch;                  // ring slot stride
+  if ((long long)blockIdx.x >= nchunks) return;                 // block-uniform, before any copy
+  const Clk clk = read_clock(k);
+  const int rs = (int)(((long long)clk.ring_pos + s) % k.R);
+  const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
+  RingT* ring_rd = (RingT*)k.ring + (size_t)rs * slot;
+  const LifP& P = k.P;
+  const int flags = k.flags;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    staged_issue_loads<BLOCK, FIXED, IPT>(k, smem + L::BARS, k.t_begin + (long long)blockIdx.x * CH, W, ring_rd,
+                                          &bar[0]);
+  }
+  uint32_t parity = 0u;                                        // bit st: phase parity of stage st
+  int it = 0;
+  for (long long c = blockIdx.x; c < nchunks; c += gridDim.x, ++it) {
+    const int st = it & 1;
+    unsigned char* stage = smem + L::BARS + (size_t)st * L::STAGE;
+    const long long base = k.t_begin + c * CH;
+    if (threadIdx.x == 0) {
+      const long long cn = c + gridDim.x;
+      if (cn < nchunks) {
+        bulk_wait_read_all();     // the other stage's stores (previous chunk) have read it out
+        staged_issue_loads<BLOCK, FIXED, IPT>(k, smem + L::BARS + (size_t)(st ^ 1) * L::STAGE, k.t_begin + cn * CH,
+                                              W, ring_rd, &bar[st ^ 1]);
+      }
+      ok = mbar_wait_bounded(&bar[st], (parity >> st) & 1u, k.status, kMbarLimit, 4, s) ? 1 : 0;
+      // on a timeout, let this block's other copy in flight land before it leaves
+      if (!ok && cn < nchunks) mbar_wait_bounded(&bar[st ^ 1], (parity >> (st ^ 1)) & 1u, k.status, kMbarLimit, 4, s);
+    }
+    __syncthreads();
+    if (!ok) {
+      if (threadIdx.x == 0) bulk_wait_all();
+      return;
+    }
+    mbar_try_wait(&bar[st], (parity >> st) & 1u);   // completed: each thread observes the phase (acquire)
+    parity ^= 1u << st;
+    RingT* ring = reinterpret_cast<RingT*>(stage);
+    float* f = reinterpret_cast<float*>(stage + L::RING);
+    unsigned tx_bits = 0;
+    float xq[IPT];
+    int iq[IPT], bq[IPT];
+#pragma unroll
+    for (int r = 0; r < IPT; ++r) {
+      const int j = threadIdx.x + r * BLOCK;
+      const int t = (int)base + j;                              // n * batch < 2^31
+      bool fired = false;
+      xq[r] = 0.0f; iq[r] = 0; bq[r] = 0;
+      if (t < W) {
+        const int i = neuron_of(k, t), b = t - i * k.batch;
+        iq[r] = i;
+        bq[r] = b;
+        const RingT c0 = ring[j];
+        const bool live = !(flags & FLYB_LIF_EPISODES) || s < k.fly_steps[b];
+        if (!live) {
+          f[L::DV * CH + j] = k.spikes[t];                      // unchanged state, spike kept
+        } else {
+          if (c0) ring_rd[t] = 0;
+          float vv = f[L::V * CH + j], gg = f[L::G * CH + j], ref = f[L::REF * CH + j], ad = f[L::AD * CH + j];
+          const float dv = f[L::DV * CH + j];
+          float rt = f[L::RT * CH + j];
+          const float pp = (flags & FLYB_LIF_POISSON) ? f[L::PP * CH + j] : 0.0f;
+          float cn = (flags & FLYB_LIF_COUNTS) ? f[L::CN * CH + j] : 0.0f;
+          float rr = (flags & FLYB_LIF_STD) ? f[L::RR * CH + j] : 1.0f;
+          const float act = k.active[i];
+          bool skip = false;
+          if ((flags & FLYB_LIF_SKIP_FROZEN) && act == 0.0f && pp == 0.0f && c0 == 0) {
+            const float rres = (flags & FLYB_LIF_STD) ? rr : k.res[t];
+            skip = vv == P.v_rest && gg == 0.0f && dv == 0.0f && ad == 0.0f && ref == 0.0f && rt == 0.0f &&
+                   k.spikes[t] == 0.0f && rres == 1.0f;
+          }
+          if (skip) {
+            f[L::DV * CH + j] = 0.0f;
+          } else {
+            float x;
+            const float spike = lif_update<FIXED>(k, clk, s, slot, (size_t)t, i, b, c0, act, pp, dv, vv, gg, ref, ad,
+                                                  rt, cn, rr, x);
+            fired = spike > 0.0f;
+            f[L::V * CH + j] = vv; f[L::G * CH + j] = gg; f[L::REF * CH + j] = ref; f[L::AD * CH + j] = ad;
+            f[L::DV * CH + j] = spike; f[L::RT * CH + j] = rt;
+            if (flags & FLYB_LIF_COUNTS) f[L::CN * CH + j] = cn;
+            if (flags & FLYB_LIF_STD) f[L::RR * CH + j] = rr;
+            if (x != 0.0f) { tx_bits |= 1u << r; xq[r] = x; }
+          }
+        }
+      }
+      // raster: lanes of a warp hold 32 consecutive items of the chunk = one word
+      if (k.raster) {
+        const unsigned word = __ballot_sync(0xffffffffu, fired);
+        const int wfirst = (int)base + r * BLOCK + warp * 32;
+        if (lane == 0 && wfirst < W) {
+          const size_t rslot = k.raster_slots > 0 ? (size_t)(((long long)clk.raster_pos + s) % k.raster_slots) : (size_t)s;
+          k.raster[rslot * k.words + (size_t)(wfirst >> 5)] = word;
+        }
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) staged_issue_stores<BLOCK, FIXED, IPT>(k, stage, base, W);
+    deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) bulk_wait_all();
+}
+
+// Shared memory of the staged kernel, opted in once per instantiation (above the 48 KB default).
+template <int BLOCK, bool FIXED, int IPT>
+static int staged_prepare(int* blocks_per_sm) {
+  using L = StagedLayout<BLOCK, FIXED, IPT>;
+  static int per_sm = -1;
+  if (per_sm < 0) {
+    cudaError_t e = cudaFuncSetAttribute(lif_staged_kernel<BLOCK, FIXED, IPT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
+    if (e != cudaSuccess) return (int)e;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_staged_kernel<BLOCK, FIXED, IPT>, BLOCK, L::BYTES);
+    if (e != cudaSuccess) return (int)e;
+    per_sm = b;
+  }
+  *blocks_per_sm = per_sm;
+  return 0;
+}
+
+// The staged path's requirements: 16-byte aligned chunk copies (items of the launch a multiple of
+// 4 starting on a multiple of 4, 16-byte aligned arrays).
+static bool stageable(const LifK& k) {
+  if ((k.t_end - k.t_begin) % 4 || k.t_begin % 4) return false;
+  const void* ptrs[] = {k.v, k.g, k.refrac, k.adapt, k.res, k.rate, k.counts, k.spikes, k.drive, k.poisson_p, k.ring};
+  for (const void* p : ptrs)
+    if (reinterpret_cast<uintptr_t>(p) & 15) return false;
+  return true;
+}
+
+template <int BLOCK, bool FIXED, int IPT>
+static int run_lif_staged(const LifK& k, int grid_cap, cudaStream_t st) {
+  using L = StagedLayout<BLOCK, FIXED, IPT>;
+  if constexpr (L::BYTES > 227 * 1024) return FLYB_EINVAL;   // beyond one block's shared memory
+  int per_sm = 0;
+  int rc = staged_prepare<BLOCK, FIXED, IPT>(&per_sm);
+  if (rc) return rc;
+  if (per_sm < 1) return FLYB_ECOOP;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long grid = (long long)sms * per_sm;
+  const long long chunks = ((long long)k.t_end - k.t_begin + L::CH - 1) / L::CH;
+  if (grid > chunks) grid = chunks;
+  if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
+  for (int s = 0; s < k.nsteps; ++s) {
+    lif_staged_kernel<BLOCK, FIXED, IPT><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
+    FLYB_CHECK_LAUNCH();
+  }
+  if (needs_advance(k)) {
+    lif_advance_kernel<<<1, 256, 0, st>>>(k);
+    FLYB_CHECK_LAUNCH();
+  }
+  return 0;
 }
 
 template <int BLOCK, bool FIXED, int IPT>
 static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st) {
-  const long long W = (long long)k.n * k.batch;
+  const long long W = (long long)k.t_end - k.t_begin;
   const long long chunks = (W + (long long)BLOCK * IPT - 1) / ((long long)BLOCK * IPT);
   if (launch == FLYB_LAUNCH_STEP) {
     for (int s = 0; s < k.nsteps; ++s) {
       lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
       FLYB_CHECK_LAUNCH();
     }
-    if (k.clock || (k.flags & FLYB_LIF_EPISODES)) {
+    if (needs_advance(k)) {
       lif_advance_kernel<<<1, 256, 0, st>>>(k);
       FLYB_CHECK_LAUNCH();
     }
@@ -445,8 +770,7 @@ static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st)
 // `ipt` items per thread (8- or 16-byte state vectors) need every ring slot and state array
 // aligned at each thread's first item: n * batch % ipt == 0 and (4 * ipt)-byte aligned bases.
 static bool vectorizable(const LifK& k, int ipt) {
-  const long long W = (long long)k.n * k.batch;
-  if (W % ipt) return false;
+  if ((k.t_end - k.t_begin) % ipt || k.t_begin % ipt) return false;
   const void* ptrs[] = {k.v, k.g, k.refrac, k.adapt, k.res, k.rate, k.counts, k.spikes, k.drive, k.poisson_p, k.ring};
   for (const void* p : ptrs)
     if (reinterpret_cast<uintptr_t>(p) & (4 * ipt - 1)) return false;
@@ -454,10 +778,14 @@ static bool vectorizable(const LifK& k, int ipt) {
 }
 
 // Items per thread: the caller's choice when its vectors are aligned, else 4 when possible, else 1.
+// `staged` per-step launches take the bulk-copy path when its alignment holds (2 or 4 items per
+// thread there: 1 runs as 2).
 template <int BLOCK, bool FIXED>
-static int run_lif(const LifK& k, int want, int launch, int grid_cap, cudaStream_t st) {
+static int run_lif(const LifK& k, int want, int launch, int grid_cap, int staged, cudaStream_t st) {
   int ipt = want ? want : 4;
   if (ipt != 1 && ipt != 2 && ipt != 4) return FLYB_EINVAL;
+  if (staged && launch == FLYB_LAUNCH_STEP && stageable(k))
+    return ipt == 4 ? run_lif_staged<BLOCK, FIXED, 4>(k, grid_cap, st) : run_lif_staged<BLOCK, FIXED, 2>(k, grid_cap, st);
   while (ipt > 1 && !vectorizable(k, ipt)) ipt >>= 1;
   if (ipt == 4) return run_lif_ipt<BLOCK, FIXED, 4>(k, launch, grid_cap, st);
   if (ipt == 2) return run_lif_ipt<BLOCK, FIXED, 2>(k, launch, grid_cap, st);
@@ -570,7 +898,8 @@ int lif_blocks_per_sm(int block) {
 
 using namespace flyb;
 
-FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
+// Validates the arguments and fills the kernel view; 0 or an FLYB_E* code.
+static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   if (!a || a->n <= 0 || a->batch <= 0 || a->n_delay < 1 || a->ring_slots < a->n_delay + 1 || a->nsteps < 0 ||
       !a->out_ptr || !a->v || !a->g || !a->refrac || !a->adapt || !a->res || !a->rate ||
       !a->counts || !a->spikes || !a->drive || !a->poisson_p || !a->active || !a->params || !a->ring ||
@@ -581,9 +910,14 @@ FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   if ((a->flags & FLYB_LIF_EXT_UNIFORM) && !a->uniforms) return FLYB_EINVAL;
   if ((a->flags & FLYB_LIF_EPISODES) && !a->fly_steps) return FLYB_EINVAL;
   if (a->launch == FLYB_LAUNCH_PERSISTENT && (!a->sync || !a->status)) return FLYB_EINVAL;
-  if (a->nsteps == 0) return 0;
-  LifK k;
+  const int count = a->n_count ? a->n_count : a->n - a->n_first;
+  if (a->n_first < 0 || a->n_first >= a->n || a->n_count < 0 || count <= 0 || (long long)a->n_first + count > a->n ||
+      ((long long)a->n_first * a->batch) % 32)
+    return FLYB_EINVAL;
   k.n = a->n; k.batch = a->batch; k.n_delay = a->n_delay; k.R = a->ring_slots; k.flags = a->flags;
+  batch_divider(a->batch, &k.bdiv_m, &k.bdiv_s);
+  k.t_begin = a->n_first * a->batch;
+  k.t_end = (a->n_first + count) * a->batch;
   k.nsteps = a->nsteps; k.ring_pos = ((a->ring_pos % k.R) + k.R) % k.R;
   k.words = (int)(((long long)a->n * a->batch + 31) / 32);
   k.step0 = a->step0; k.seed = a->seed;
@@ -598,13 +932,33 @@ FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   k.P = LifP{P[FLYB_P_V_REST], P[FLYB_P_V_RESET], P[FLYB_P_V_TH], P[FLYB_P_A_M], P[FLYB_P_A_S], P[FLYB_P_DT],
              P[FLYB_P_T_REF], P[FLYB_P_ADAPT_JUMP], P[FLYB_P_A_AD], P[FLYB_P_A_STD], P[FLYB_P_A_R],
              P[FLYB_P_RATE_GAIN], P[FLYB_P_W_SYN]};
+  return 0;
+}
+
+FLYB_API int flyb_lif_advance(const flyb_lif_args* a, void* stream) {
+  LifK k;
+  const int rc = make_lif_k(a, k);
+  if (rc) return rc;
+  if (a->nsteps == 0 || !(k.clock || (k.flags & FLYB_LIF_EPISODES))) return 0;
+  lif_advance_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(k);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
+  LifK k;
+  const int rc = make_lif_k(a, k);
+  if (rc) return rc;
+  if (a->nsteps == 0) return 0;
   cudaStream_t st = (cudaStream_t)stream;
   const bool fixed = a->ring_mode == FLYB_RING_FIXED;
   const int block = a->block ? a->block : 256;
   switch (block) {
-    case 128: return fixed ? run_lif<128, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<128, false>(k, a->items_per_thread, a->launch, a->grid, st);
-    case 256: return fixed ? run_lif<256, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<256, false>(k, a->items_per_thread, a->launch, a->grid, st);
-    case 512: return fixed ? run_lif<512, true>(k, a->items_per_thread, a->launch, a->grid, st) : run_lif<512, false>(k, a->items_per_thread, a->launch, a->grid, st);
+    case 128: return fixed ? run_lif<128, true>(k, a->items_per_thread, a->launch, a->grid, a->staged, st)
+                     : run_lif<128, false>(k, a->items_per_thread, a->launch, a->grid, a->staged, st);
+    case 256: return fixed ? run_lif<256, true>(k, a->items_per_thread, a->launch, a->grid, a->staged, st)
+                     : run_lif<256, false>(k, a->items_per_thread, a->launch, a->grid, a->staged, st);
+    case 512: return fixed ? run_lif<512, true>(k, a->items_per_thread, a->launch, a->grid, a->staged, st)
+                     : run_lif<512, false>(k, a->items_per_thread, a->launch, a->grid, a->staged, st);
     default: return FLYB_EINVAL;
   }
 }

@@ -20,7 +20,7 @@ _LIB = None
 # ------------------------------------------------------------------ constants (flyb200.h)
 OK, EINVAL, EBARRIER, ECOOP, ETOOBIG = 0, 1001, 1002, 1003, 1004
 LIF_POISSON, LIF_STD, LIF_COUNTS, LIF_ADAPT = 1, 2, 4, 8
-LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES = 16, 32, 64
+LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES, LIF_NO_ADVANCE = 16, 32, 64, 128
 RING_COUNT, RING_FIXED = 0, 1
 LAUNCH_STEP, LAUNCH_PERSISTENT = 0, 1
 LAUNCHES_BY_NAME = {"step": LAUNCH_STEP, "persistent": LAUNCH_PERSISTENT}
@@ -37,7 +37,7 @@ class LifArgs(ct.Structure):
     _fields_ = [("n", _I), ("batch", _I), ("n_delay", _I), ("ring_slots", _I), ("ring_mode", _I),
                 ("ring_pos", _I), ("flags", _I), ("nsteps", _I), ("launch", _I), ("block", _I),
                 ("grid", _I), ("raster_slots", _I), ("raster_pos", _I), ("fly0", _I),
-                ("items_per_thread", _I), ("pad1", _I),
+                ("items_per_thread", _I), ("staged", _I), ("n_first", _I), ("n_count", _I),
                 ("step0", ct.c_longlong), ("seed", ct.c_ulonglong),
                 ("out_ptr", _VP), ("out_edge", _VP),
                 ("v", _VP), ("g", _VP), ("refrac", _VP), ("adapt", _VP), ("res", _VP),
@@ -98,6 +98,7 @@ SIGNATURES = {
     "launch_events": [_P, _I, _I, _I, _I, _VP],
     "launch_means": [_P, _I, _I, _I, _I, _VP],
     "flyb_lif_run": [ct.POINTER(LifArgs), _VP],
+    "flyb_lif_advance": [ct.POINTER(LifArgs), _VP],
     "flyb_ring_deposit": [_I, _I, _I, _VP, _VP, _VP, _VP, _VP],
     "flyb_optic_run": [ct.POINTER(OpticArgs), _VP],
     "flyb_optic_run_noalloc": [ct.POINTER(OpticArgs), _VP],

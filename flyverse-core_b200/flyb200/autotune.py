@@ -2,10 +2,11 @@
 
 The best launch shape depends on the graph, the batch and how many cells spike per step: at B = 1
 the step is latency-bound and a persistent cooperative launch (one launch for many steps, a grid
-barrier per step) wins; at B = 64 the state streams from HBM and one launch per step with small
-blocks keeps more loads in flight. `tune_lif` times each candidate (block size x launch mode) for
-a few steps on a copy of the live state, restores the state, installs the fastest and caches it
-under the key; `tune_optic` does the same for the optic substep's launch mode.
+barrier per step) wins; at B = 64 the state streams from HBM and one launch per step, with the
+state staged through shared memory by bulk copies, keeps more bytes in flight. `tune_lif` times
+each candidate (launch mode x block size x items per thread x staged) for a few steps on a copy of
+the live state, restores the state, installs the fastest and caches it under the key;
+`tune_optic` does the same for the optic substep's launch mode and kernel shape.
 """
 from __future__ import annotations
 
@@ -16,8 +17,10 @@ import numpy as np
 import torch
 
 CACHE: dict = {}
-LIF_CANDIDATES = (("step", 256, 4), ("step", 128, 4), ("step", 512, 4), ("step", 256, 2), ("step", 128, 2),
-                  ("step", 256, 1), ("persistent", 256, 4), ("persistent", 512, 2))
+# (launch, block, items per thread, staged): staged = per-step launches through the bulk-copy kernel
+LIF_CANDIDATES = (("step", 256, 4, 0), ("step", 512, 4, 0), ("step", 256, 2, 0), ("step", 256, 1, 0),
+                  ("step", 256, 2, 1), ("step", 256, 4, 1), ("step", 512, 2, 1), ("step", 128, 4, 1),
+                  ("persistent", 256, 4, 0), ("persistent", 512, 2, 0))
 
 
 def graph_key(brain) -> str:
@@ -52,21 +55,22 @@ def _time(fn, reps: int) -> float:
 
 
 def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
-    """Install and return the fastest (launch, block) for this brain; state is left unchanged."""
+    """Install and return the fastest LIF launch choice for this brain; state is left unchanged."""
     key = ("lif", graph_key(brain), brain.B, activity_bucket(brain))
     if key in CACHE:
         _apply(brain, CACHE[key])
         return CACHE[key]
     saved = brain.state_dict()
     results = {}
-    for launch, block, ipt in candidates:
-        _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt})
+    for launch, block, ipt, staged in candidates:
+        _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt, "staged": staged})
         brain.step(2)
-        results[(launch, block, ipt)] = _time(lambda: brain.step(steps), 1) / steps
+        results[(launch, block, ipt, staged)] = _time(lambda: brain.step(steps), 1) / steps
         brain.load_state_dict(saved)
     best = min(results, key=results.get)
-    choice = {"launch": best[0], "block": best[1], "items_per_thread": best[2], "ms_per_step": results[best],
-              "all": {f"{k[0]}/{k[1]}/{k[2]}": v for k, v in results.items()}}
+    choice = {"launch": best[0], "block": best[1], "items_per_thread": best[2], "staged": best[3],
+              "ms_per_step": results[best],
+              "all": {f"{k[0]}{'-staged' if k[3] else ''}/{k[1]}/{k[2]}": v for k, v in results.items()}}
     CACHE[key] = choice
     _apply(brain, choice)
     return choice
@@ -75,6 +79,7 @@ def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
 def _apply(brain, choice: dict) -> None:
     brain.launch, brain.block = choice["launch"], choice["block"]
     brain.items_per_thread = choice.get("items_per_thread", 0)
+    brain.staged = bool(choice.get("staged", 0))
     brain._make_args()
 
 

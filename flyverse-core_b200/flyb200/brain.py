@@ -250,6 +250,7 @@ class Brain:
         a.n, a.batch, a.n_delay, a.ring_slots, a.ring_mode = self.n, self.B, self.n_delay, self.R, self.ring_mode
         a.launch, a.block = LAUNCHES[self.launch], self.block
         a.items_per_thread = getattr(self, "items_per_thread", 0)
+        a.staged = int(bool(getattr(self, "staged", False)))
         a.raster_slots = self.n_delay
         a.seed = self.seed & 0xFFFFFFFFFFFFFFFF
         a.out_ptr, a.out_edge = self._out_ptr.data_ptr(), self._out_edge.data_ptr()
@@ -298,6 +299,37 @@ class Brain:
             rc = self._lib.flyb_lif_run(ct.byref(a), stream)
         if rc:
             raise RuntimeError(f"flyb_lif_run: error {rc}")
+        self.buf_pos = (self.buf_pos + n_steps) % self.R
+        self.t += n_steps * self.p.dt
+        self.step_count += n_steps
+
+    def step_range(self, n_first: int, n_count: int) -> None:
+        """Update neurons [n_first, n_first + n_count) by one step on the current stream, leaving
+        the device clock where it is (FLYB_LIF_NO_ADVANCE): the ranges of one step may run on
+        different streams, after which `advance(1)` ends the step. n_first * B must be a multiple
+        of 32. Spikes of the range are delivered to every postsynaptic neuron as in `step`."""
+        a = self._args
+        a.flags = self._flags(False) | _abi.LIF_NO_ADVANCE
+        a.nsteps, a.uniforms = 1, None
+        a.n_first, a.n_count = int(n_first), int(n_count)
+        try:
+            with torch.cuda.device(self.device):
+                rc = self._lib.flyb_lif_run(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
+        finally:
+            a.n_first, a.n_count = 0, 0
+        if rc:
+            raise RuntimeError(f"flyb_lif_run: error {rc}")
+
+    def advance(self, n_steps: int = 1) -> None:
+        """End `n_steps` steps run by ranges: move the device clock (ring and history positions,
+        Philox step) on, as the end of `step` does."""
+        a = self._args
+        a.flags = self._flags(False)
+        a.nsteps = int(n_steps)
+        with torch.cuda.device(self.device):
+            rc = self._lib.flyb_lif_advance(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError(f"flyb_lif_advance: error {rc}")
         self.buf_pos = (self.buf_pos + n_steps) % self.R
         self.t += n_steps * self.p.dt
         self.step_count += n_steps

@@ -10,6 +10,13 @@ refreshed every step instead of every 10 ms frame:
   4. one fused LIF step over the spiking population       (flyb_lif_run)
 and, every `frame_steps` steps, the photoreceptor stage and pr_in = gain_in * W_rp a_pr. All
 buffers are allocated at construction, so `capture(k)` records k steps into one CUDA graph.
+
+Only the LIF neurons that receive the VPN drive (rows of W_sr) need stage 3 before their update;
+the others depend on the previous step alone. The spiking population is therefore stored in an
+order (`lif_order`) whose tail, from a multiple of 32 on, holds the driven neurons, and with
+`overlap` the LIF update of the head runs on a second stream concurrently with stages 2-3; the
+tail follows stage 3, and the device clock advances once both are done. Every neuron sees the same
+inputs as in the serial order and the ring sums are exact, so the result is bit-identical.
 """
 from __future__ import annotations
 
@@ -26,7 +33,7 @@ from .synthetic import WholeFlyConfig
 
 class WholeFly:
     def __init__(self, cfg: WholeFlyConfig, batch: int, *, device="cuda", seed: int = 0, dt_ms: float = 0.1,
-                 launch: str = "step", poisson_hz=None, record_activity: bool = True):
+                 launch: str = "step", poisson_hz=None, record_activity: bool = True, overlap: bool = True):
         self.cfg, self.B = cfg, int(batch)
         self.device = torch.device(device)
         if self.device.index is None:
@@ -35,10 +42,22 @@ class WholeFly:
         self.dt_ms = dt_ms
         params = dict(cfg.lif.params)
         params["dt"] = dt_ms
-        self.lif = Brain(cfg.lif.c, LIFParams(**params), device=self.device, seed=seed, batch=self.B, launch=launch)
+        # spiking population order: undriven neurons, then (from a multiple of 32) the driven ones
+        n = cfg.n_spiking
+        driven = np.unique(o.W_sr.tocoo().row)
+        head = np.setdiff1d(np.arange(n), driven)
+        self.lif_order = np.concatenate([head, driven]).astype(np.int64)
+        self.split = len(head) - len(head) % 32           # neurons [split, n) update after the drive
+        self.lif_position = np.empty(n, np.int64)         # original spiking index -> stored position
+        self.lif_position[self.lif_order] = np.arange(n)
+        self.lif_connectome = cfg.lif.c.subset(self.lif_order)
+        self.sensory_idx = self.lif_position[np.asarray(cfg.sensory_idx)]
+        self.lif = Brain(self.lif_connectome, LIFParams(**params), device=self.device, seed=seed, batch=self.B,
+                         launch=launch)
         self.lif.record_activity = record_activity
         hz = cfg.lif.poisson_hz if poisson_hz is None else poisson_hz
-        self.lif.set_poisson(cfg.sensory_idx, torch.as_tensor(hz, dtype=torch.float32))
+        self.lif.set_poisson(self.sensory_idx, torch.as_tensor(hz, dtype=torch.float32))
+        self.overlap = bool(overlap)
         tau = o.tau_of_type[o.type_of].astype(np.float32)
         a = np.exp(-dt_ms / tau).astype(np.float32)
         aad = float(np.exp(-dt_ms / o.adapt_tau_ms))
@@ -47,18 +66,29 @@ class WholeFly:
         dev = self.device
         # the coupling blocks keep only their non-empty rows (+ the row map): the other rows of spk_in
         # and of the drive are never written and stay zero
-        self.W_rs, self.rs_rows = self._rows_with_entries(o.W_rs, dev)
-        self.W_sr, self.sr_rows = self._rows_with_entries(o.W_sr, dev)
+        self.W_rs_host = o.W_rs.tocsc()[:, self.lif_order].tocsr()    # columns in stored LIF order
+        self.W_sr_host = o.W_sr.tocsr()[self.lif_order]                # rows in stored LIF order
+        self.W_rs, self.rs_rows = self._rows_with_entries(self.W_rs_host, dev)
+        self.W_sr, self.sr_rows = self._rows_with_entries(self.W_sr_host, dev)
         self.W_rp = DeviceCSR(o.W_rp, dev)
         self.a_pr = torch.zeros(o.n_pr, self.B, device=dev)
         self.steps_taken = 0
+        self._fork = (torch.cuda.Stream(self.device, priority=-1), torch.cuda.Stream(self.device))
 
     @property
     def launches_per_step(self) -> int:
         """Kernel launches of one step once running: two coupling products, the optic substep (its
-        dr carried over from the previous step), the LIF step and its device-clock advance (one
-        launch per step, or one persistent launch)."""
+        dr carried over from the previous step), the LIF step (two ranges when overlapped) and its
+        device-clock advance (or one persistent launch)."""
+        if self.overlapping:
+            return 6
         return 5 if self.lif.launch == "step" else 4
+
+    @property
+    def overlapping(self) -> bool:
+        """Whether steps fork the undriven LIF update onto a second stream (per-step launches only:
+        a persistent cooperative launch must own the whole device)."""
+        return self.overlap and self.lif.launch == "step" and self.optic.launch == "step" and 0 < self.split
 
     @staticmethod
     def _rows_with_entries(M, dev):
@@ -84,16 +114,36 @@ class WholeFly:
         lif_rate = self.lif._st["rate"]
         drive = self.lif._st["drive"]
         cur0 = self.optic._cur
+        overlap = self.overlapping
+        main = torch.cuda.current_stream(self.device)
+        hi, side = self._fork
         for _ in range(int(n)):
             spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb,
                  y_index=self.rs_rows)
-            self.optic.substeps(1, carry=True)
-            spmm(self.W_sr, self.optic.dr_out, drive, y_index=self.sr_rows, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
-                 y_hi=o.drive_clip_mv)
-            self.lif.step(1)
+            if overlap:
+                # the optic chain on a high-priority stream, the undriven LIF neurons beside it
+                hi.wait_stream(main)
+                side.wait_stream(main)
+                with torch.cuda.stream(side):
+                    self.lif.step_range(0, self.split)
+                with torch.cuda.stream(hi):
+                    self._optic_and_drive(drive)
+                    self.lif.step_range(self.split, self.cfg.n_spiking - self.split)
+                main.wait_stream(hi)
+                main.wait_stream(side)
+                self.lif.advance(1)
+            else:
+                self._optic_and_drive(drive)
+                self.lif.step(1)
         if torch.cuda.is_current_stream_capturing():
             self.optic.pin_dr(cur0)
         self.steps_taken += int(n)
+
+    def _optic_and_drive(self, drive: torch.Tensor) -> None:
+        o = self.cfg.optic
+        self.optic.substeps(1, carry=True)
+        spmm(self.W_sr, self.optic.dr_out, drive, y_index=self.sr_rows, alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
+             y_hi=o.drive_clip_mv)
 
     # ------------------------------------------------------------------ algorithmic bytes (roofline)
     def lif_bytes_per_step(self) -> int:

@@ -70,6 +70,9 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
 #define FLYB_LIF_EXT_UNIFORM  16   /* Poisson uniforms from `uniforms` instead of Philox      */
 #define FLYB_LIF_SKIP_FROZEN  32   /* frozen cells at rest are left untouched                 */
 #define FLYB_LIF_EPISODES     64   /* per-fly remaining-step counters gate the update         */
+#define FLYB_LIF_NO_ADVANCE   128  /* leave `clock` and `fly_steps` as they are: other launches of
+                                      the same steps cover the other neurons; flyb_lif_advance
+                                      moves them on once all have run                           */
 
 /* Delay-ring element types */
 #define FLYB_RING_COUNT  0   /* int32 signed synapse counts; g += w_syn * count (exact sum)     */
@@ -105,7 +108,16 @@ typedef struct flyb_lif_args {
   int raster_pos;        /* ring slot written by the first step (raster_slots > 0)   */
   int fly0;              /* global index of local fly 0 (Philox key when flies are sharded) */
   int items_per_thread;  /* 0 auto (4 when aligned), 1, 2 or 4 consecutive items per thread */
-  int pad1;
+  int staged;            /* per-step launches only: 1 stages each block's state chunks through
+                            shared memory with bulk async copies, the next chunk loading while
+                            the current one is updated and delivered (needs the items of the
+                            launch, n_count * batch, and n_first * batch to be multiples of 4
+                            and 16-byte aligned arrays; otherwise the register path runs) */
+  int n_first;           /* update neurons [n_first, n_first + n_count) only (n_count 0: to
+                            the end); n_first * batch must be a multiple of 32. Their spikes
+                            are delivered to every postsynaptic neuron as usual; the state
+                            of the other neurons is not touched */
+  int n_count;
   long long step0;       /* global step index of the first step (Philox counter)     */
   unsigned long long seed;
   /* outgoing synapses, pre-major (CSC of W[post, pre]) */
@@ -134,6 +146,11 @@ typedef struct flyb_lif_args {
 } flyb_lif_args;
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);
+
+/* Advance `clock` by a->nsteps and lower `fly_steps` (FLYB_LIF_EPISODES) as the end of a
+ * flyb_lif_run does: for runs split over neuron ranges with FLYB_LIF_NO_ADVANCE, after all of
+ * them. One small launch on `stream`. No counterpart in the reference (it has one update per step). */
+int flyb_lif_advance(const flyb_lif_args* a, void* stream);
 
 /* Deposit transmitted spikes x[n][batch] into ring slot `slot` (checkpoint import of a
  * reference spike buffer). COUNT rings need x in {0, 1}. */

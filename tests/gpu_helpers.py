@@ -13,7 +13,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda", items_per_thread=0, with_sync=True):
+                   device="cuda", items_per_thread=0, with_sync=True, staged=0):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -33,7 +33,7 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
     P = np.ascontiguousarray(params, np.float32)
     a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
                      ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, launch=launch, block=block, grid=grid,
-                     fly0=fly0, items_per_thread=items_per_thread, step0=state.step, seed=seed, out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
+                     fly0=fly0, items_per_thread=items_per_thread, staged=staged, step0=state.step, seed=seed, out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
                      v=d["v"].data_ptr(), g=d["g"].data_ptr(), refrac=d["refrac"].data_ptr(),
                      adapt=d["adapt"].data_ptr(), res=d["res"].data_ptr(), rate=d["rate"].data_ptr(),
                      counts=d["counts"].data_ptr(), spikes=d["spikes"].data_ptr(), drive=d["drive"].data_ptr(),
@@ -56,3 +56,66 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
     if fly_steps is not None:
         fly_steps[...] = fs.cpu().numpy()
     return (r.cpu().numpy().view(np.uint32) if raster else None), int(events.item())
+
+
+def native_lif_run_split(state, out_ptr, out_edge, params, *, split, n_delay, flags, nsteps, seed=0, fly_steps=None,
+                         block=256, items_per_thread=0, staged=0, device="cuda"):
+    """oracle.lif_run's contract (raster always on), but every step runs as two neuron ranges,
+    [0, split) and [split, n), launched on two streams that overlap, each with
+    FLYB_LIF_NO_ADVANCE, then flyb_lif_advance on the joined stream (the device clock keeps the
+    step counter, ring slot and raster slot)."""
+    dev = torch.device(device)
+    n, B = state.n, state.batch
+    words = (n * B + 31) // 32
+    d = {k: torch.from_numpy(getattr(state, k)).to(dev) for k in LIF_ARRAYS}
+    active = torch.from_numpy(state.active).to(dev)
+    std_u = torch.from_numpy(state.std_u).to(dev)
+    ring = torch.from_numpy(state.ring).to(dev)
+    ptr = torch.from_numpy(np.ascontiguousarray(out_ptr, np.int32)).to(dev)
+    edge = torch.from_numpy(np.ascontiguousarray(out_edge, np.int32)).to(dev)
+    fs = None if fly_steps is None else torch.from_numpy(np.ascontiguousarray(fly_steps, np.int32)).to(dev)
+    r = torch.zeros(nsteps, words, dtype=torch.int32, device=dev)
+    clock = torch.tensor([state.step, state.ring_pos, 0], dtype=torch.int64, device=dev)
+    events = torch.zeros(1, dtype=torch.int64, device=dev)
+    status = torch.zeros(4, dtype=torch.int32, device=dev)
+    P = np.ascontiguousarray(params, np.float32)
+    a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
+                     ring_pos=0, flags=flags | _abi.LIF_NO_ADVANCE, nsteps=1, launch=_abi.LAUNCH_STEP, block=block,
+                     raster_slots=nsteps, raster_pos=0, items_per_thread=items_per_thread, staged=staged, seed=seed,
+                     out_ptr=ptr.data_ptr(), out_edge=edge.data_ptr(),
+                     v=d["v"].data_ptr(), g=d["g"].data_ptr(), refrac=d["refrac"].data_ptr(),
+                     adapt=d["adapt"].data_ptr(), res=d["res"].data_ptr(), rate=d["rate"].data_ptr(),
+                     counts=d["counts"].data_ptr(), spikes=d["spikes"].data_ptr(), drive=d["drive"].data_ptr(),
+                     poisson_p=d["poisson_p"].data_ptr(), active=active.data_ptr(), std_u=std_u.data_ptr(),
+                     params=P.ctypes.data, ring=ring.data_ptr(), fly_steps=None if fs is None else fs.data_ptr(),
+                     clock=clock.data_ptr(), raster=r.data_ptr(), events=events.data_ptr(), status=status.data_ptr())
+    lib = _abi.lib()
+    main = torch.cuda.current_stream(dev)
+    s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    for _ in range(nsteps):
+        for stream, first, count in ((s1, 0, split), (s2, split, n - split)):
+            stream.wait_stream(main)
+            a.n_first, a.n_count = first, count
+            rc = lib.flyb_lif_run(ct.byref(a), stream.cuda_stream)
+            if rc:
+                torch.cuda.synchronize(dev)
+                raise RuntimeError(f"flyb_lif_run: error {rc}")
+        main.wait_stream(s1)
+        main.wait_stream(s2)
+        a.flags = flags
+        rc = lib.flyb_lif_advance(ct.byref(a), main.cuda_stream)
+        a.flags = flags | _abi.LIF_NO_ADVANCE
+        if rc:
+            raise RuntimeError(f"flyb_lif_advance: error {rc}")
+    torch.cuda.synchronize(dev)
+    st = status.cpu().numpy()
+    if st[0]:
+        raise RuntimeError(f"kernel status {st.tolist()}")
+    for k in LIF_ARRAYS:
+        getattr(state, k)[...] = d[k].cpu().numpy()
+    state.ring[...] = ring.cpu().numpy()
+    state.ring_pos = (state.ring_pos + nsteps) % state.ring_slots
+    state.step += nsteps
+    if fly_steps is not None:
+        fly_steps[...] = fs.cpu().numpy()
+    return r.cpu().numpy().view(np.uint32), int(events.item())

@@ -11,7 +11,7 @@ import oracle
 from flyb200 import _abi, synthetic
 from flyb200.brain import Brain, LIFParams, lif_coefficients, out_edges
 from flyb200.weights import DEFAULT_STD_U_BY_TYPE, lif_weights, per_type
-from gpu_helpers import LIF_ARRAYS, native_lif_run
+from gpu_helpers import LIF_ARRAYS, native_lif_run, native_lif_run_split
 from helpers import connectome_from_fixture, golden, torch_uniforms, unpack
 
 pytestmark = pytest.mark.gpu
@@ -55,7 +55,8 @@ def case_19cell():
                 uniforms=np.ascontiguousarray(U))
 
 
-def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed=False, seed=3):
+def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed=False, seed=3, std=False,
+                ext_uniform=False):
     rng = np.random.default_rng(seed)
     pre, post = rng.integers(0, n, edges), rng.integers(0, n, edges)
     sign = np.where(rng.random(n) < 0.65, 1.0, -1.0).astype(np.float32)
@@ -63,7 +64,7 @@ def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed
                       shape=(n, n), dtype=np.float32)
     p = LIFParams(conn_cap=0.0, input_norm_alpha=0.0, path_gain=[], type_path_gain=[], same_type_gain=1.0,
                   adapt_jump=1.5, receptor_model=None, dt=0.1)
-    ptr, e, mode = out_edges(W, p.w_syn, "fixed" if fixed else "auto")
+    ptr, e, mode = out_edges(W, p.w_syn, "fixed" if (fixed or std) else "auto", std_on=std)
     st = oracle.LifState(n, batch, 19, mode, p.v_rest)
     st.poisson_p[rng.choice(n, n // 10, replace=False), :] = rng.uniform(0.002, 0.02, (n // 10, batch)).astype(np.float32)
     st.drive[:] = rng.uniform(5.0, 7.5, (n, batch)).astype(np.float32)
@@ -73,11 +74,18 @@ def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed
     if episodes:
         flags |= _abi.LIF_EPISODES
         fs = rng.integers(0, steps + 1, batch).astype(np.int32)
-    return dict(state=st, ptr=ptr, edges=e, P=lif_coefficients(p, False), n_delay=18, flags=flags, nsteps=steps,
-                uniforms=None, fly_steps=fs, seed=12345)
+    if std:
+        flags |= _abi.LIF_STD
+        st.std_u[:] = rng.uniform(0.1, 0.5, n).astype(np.float32)
+    uni = None
+    if ext_uniform:
+        flags |= _abi.LIF_EXT_UNIFORM
+        uni = rng.random((steps, n, batch), dtype=np.float32)
+    return dict(state=st, ptr=ptr, edges=e, P=lif_coefficients(p, std), n_delay=18, flags=flags, nsteps=steps,
+                uniforms=uni, fly_steps=fs, seed=12345)
 
 
-def _compare(case, launch, block, grid=0, ipt=0, with_sync=True):
+def _compare(case, launch, block, grid=0, ipt=0, with_sync=True, staged=0):
     s_ref, s_gpu = case["state"].copy(), case["state"].copy()
     fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
     fs_gpu = None if fs_ref is None else fs_ref.copy()
@@ -85,7 +93,8 @@ def _compare(case, launch, block, grid=0, ipt=0, with_sync=True):
               uniforms=case["uniforms"], raster=True)
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, **kw)
     r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], fly_steps=fs_gpu, launch=launch,
-                                   block=block, grid=grid, items_per_thread=ipt, with_sync=with_sync, **kw)
+                                   block=block, grid=grid, items_per_thread=ipt, with_sync=with_sync, staged=staged,
+                                   **kw)
     assert unpack(r_ref, s_ref.n * s_ref.batch).sum() > 0
     np.testing.assert_array_equal(r_gpu, r_ref)                      # spike rasters
     for k in LIF_ARRAYS:
@@ -116,6 +125,60 @@ def test_batched_philox_native_equals_oracle(launch, block, grid):
 @pytest.mark.parametrize("launch,batch", [(STEP, 64), (PERS, 64), (STEP, 3)])
 def test_items_per_thread_variants_equal_oracle(ipt, launch, batch):
     _compare(case_random(batch=batch, steps=100), launch, 256, ipt=ipt)
+
+
+@pytest.mark.parametrize("block,ipt", [(256, 2), (256, 4), (128, 2), (512, 4)])
+@pytest.mark.parametrize("kind", ["count", "fixed", "episodes"])
+def test_staged_step_equals_oracle(block, ipt, kind):
+    """The bulk-copy (staged) per-step kernel: every state bit, ring, raster and event count equal
+    the oracle, in both ring modes and with uneven episodes; chunks end mid-array (n * batch is not
+    a multiple of the chunk)."""
+    case = case_random(batch=20, n=2999, steps=80, fixed=kind == "fixed", episodes=kind == "episodes")
+    _compare(case, STEP, block, ipt=ipt, staged=1)
+
+
+def test_staged_request_falls_back_when_unaligned():
+    """n * batch % 4 != 0: the staged request runs the register path, same results."""
+    _compare(case_random(batch=3, n=2999, steps=60), STEP, 256, staged=1)
+
+
+def test_staged_depression_and_external_uniforms():
+    _compare(case_random(batch=8, n=2999, steps=60, std=True, ext_uniform=True), STEP, 256, ipt=2, staged=1)
+    _compare(case_random(batch=8, n=2999, steps=60, std=True), STEP, 256, ipt=4, staged=1)
+
+
+def test_depression_random_graph_register_paths():
+    for launch in (STEP, PERS):
+        _compare(case_random(batch=8, n=2999, steps=60, std=True, ext_uniform=True), launch, 256)
+
+
+@pytest.mark.parametrize("staged,ipt", [(0, 4), (0, 1), (1, 2), (1, 4)])
+@pytest.mark.parametrize("kind", ["count", "fixed-episodes"])
+def test_neuron_ranges_on_two_streams_equal_oracle(staged, ipt, kind):
+    """Each step as two neuron ranges launched on overlapping streams (FLYB_LIF_NO_ADVANCE), then
+    flyb_lif_advance: every state bit, ring, raster and event count equal the oracle's whole steps."""
+    case = case_random(batch=8, n=2999, steps=60, fixed=kind != "count", episodes=kind != "count")
+    s_ref, s_gpu = case["state"].copy(), case["state"].copy()
+    fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
+    fs_gpu = None if fs_ref is None else fs_ref.copy()
+    kw = dict(n_delay=case["n_delay"], flags=case["flags"], nsteps=case["nsteps"], seed=case["seed"])
+    r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, raster=True, **kw)
+    r_gpu, ev_gpu = native_lif_run_split(s_gpu, case["ptr"], case["edges"], case["P"], split=1504, fly_steps=fs_gpu,
+                                         items_per_thread=ipt, staged=staged, **kw)
+    np.testing.assert_array_equal(r_gpu, r_ref)
+    for k in LIF_ARRAYS:
+        np.testing.assert_array_equal(getattr(s_gpu, k), getattr(s_ref, k), err_msg=k)
+    np.testing.assert_array_equal(s_gpu.ring, s_ref.ring)
+    assert ev_gpu == ev_ref
+    if fs_ref is not None:
+        np.testing.assert_array_equal(fs_gpu, fs_ref)
+
+
+def test_neuron_range_must_start_on_a_raster_word():
+    case = case_random(batch=3, n=200, steps=2)
+    with pytest.raises(RuntimeError, match="1001"):
+        native_lif_run_split(case["state"].copy(), case["ptr"], case["edges"], case["P"], split=7,
+                             n_delay=case["n_delay"], flags=case["flags"], nsteps=1)
 
 
 @pytest.mark.parametrize("batch", [1, 3, 33])

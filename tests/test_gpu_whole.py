@@ -18,10 +18,15 @@ def small_fly():
                                        optic_nnz=200_000, n_pr=300)
 
 
-def test_whole_fly_matches_oracle_step_order():
+@pytest.mark.parametrize("overlap", [True, False])
+def test_whole_fly_matches_oracle_step_order(overlap):
+    """Bit-identical spikes every step whether the undriven LIF neurons update concurrently with
+    the optic chain (overlap) or after it; the oracle runs the stages serially on the engine's
+    stored neuron order."""
     cfg = small_fly()
     B, T = 4, 120
-    eng = WholeFly(cfg, B, device="cuda", seed=1, launch="step")
+    eng = WholeFly(cfg, B, device="cuda", seed=1, launch="step", overlap=overlap)
+    assert eng.overlapping == overlap
     a_pr = torch.from_numpy((np.random.default_rng(0).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
     eng.set_photoreceptors(a_pr)
     pr = eng.optic.pr_in.cpu().numpy()
@@ -32,12 +37,12 @@ def test_whole_fly_matches_oracle_step_order():
     # the oracle, same order: spk_in, optic substep, drive, LIF step
     o = cfg.optic
     p = LIFParams(**{**cfg.lif.params, "dt": 0.1})
-    W, _ = lif_weights(cfg.lif.c, p)
+    W, _ = lif_weights(eng.lif_connectome, p)
     ptr, edges, mode = out_edges(W, p.w_syn)
     n, m = cfg.n_spiking, o.m
     st = oracle.LifState(n, B, 19, mode, p.v_rest)
-    st.poisson_p[cfg.sensory_idx, :] = np.float32(cfg.lif.poisson_hz) * np.float32(p.dt / 1000.0)
-    Wr, Wrs, Wsr = o.W_rr(), o.W_rs.tocsr(), o.W_sr.tocsr()
+    st.poisson_p[eng.sensory_idx, :] = np.float32(cfg.lif.poisson_hz) * np.float32(p.dt / 1000.0)
+    Wr, Wrs, Wsr = o.W_rr(), eng.W_rs_host, eng.W_sr_host
     a = np.exp(-0.1 / o.tau_of_type[o.type_of].astype(np.float32)).astype(np.float32)
     aad = float(np.exp(-0.1 / o.adapt_tau_ms))
     v, ad = np.zeros((m, B), np.float32), np.zeros((m, B), np.float32)
@@ -57,6 +62,16 @@ def test_whole_fly_matches_oracle_step_order():
     np.testing.assert_array_equal(eng.lif.spike_counts.t().cpu().numpy(), st.counts)
     np.testing.assert_allclose(eng.optic.v_s.cpu().numpy(), v, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(eng.lif._st["v"].cpu().numpy(), st.v, rtol=0, atol=1e-4)
+
+
+def test_stored_order_puts_driven_neurons_last():
+    cfg = small_fly()
+    eng = WholeFly(cfg, 3, device="cuda", seed=1)
+    driven = np.unique(cfg.optic.W_sr.tocoo().row)
+    assert eng.split % 32 == 0 and eng.split <= cfg.n_spiking - len(driven)
+    assert set(eng.lif_position[driven]) <= set(range(eng.split, cfg.n_spiking))
+    np.testing.assert_array_equal(np.sort(eng.lif_order), np.arange(cfg.n_spiking))
+    np.testing.assert_array_equal(eng.lif_position[eng.lif_order], np.arange(cfg.n_spiking))
 
 
 @pytest.mark.parametrize("chunk", [2, 3])
