@@ -675,6 +675,8 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
     fence_proxy_async_smem();
     __syncthreads();
     if (threadIdx.x == 0) staged_issue_stores<BLOCK, FIXED, IPT>(k, stage, base, W);
+    // block-wide delivery: the edges of a chunk's spikers are spread over all its threads (a
+    // warp-local delivery leaves one warp with a high out-degree spiker's whole edge list)
     deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
     __syncthreads();
   }

@@ -64,13 +64,12 @@ struct Unroll { static constexpr int U = FPL <= 2 ? 8 : (FPL == 4 ? 4 : 2); };
 // e0 + g + G*k). Each pass loads U interleaved {col, w} entries (8 bytes each), issues U
 // independent gathers, then accumulates them with FMAs. The result is complete on the lanes with
 // slot lane < F. `row_ok` false: the lane still takes part in the shuffles.
-template <int F, int FPL, int LPR>
+template <int F, int FPL, int LPR, int U = Unroll<FPL>::U>
 __device__ __forceinline__ void row_product(const int* __restrict__ ptr, const int2* __restrict__ cw,
                                             const float* __restrict__ x, int batch, int row, bool row_ok,
                                             float (&acc)[FPL], int part = 0, int parts = 1) {
   static_assert(F <= LPR && LPR <= 32, "a row slot spans the fly lanes");
   constexpr int G = LPR / F;
-  constexpr int U = Unroll<FPL>::U;
   const int sl = (threadIdx.x & 31) % LPR, g = sl / F, f = sl % F;
   const int fb = f * FPL;
   const bool full = batch == F * FPL;
@@ -219,7 +218,7 @@ __host__ __device__ __forceinline__ long long optic_items(int m, int n_long) {
 // interleaved share of the row's entries, the shares are summed in slot order through shared
 // memory and the first slot applies the update; the longest rows thus stop bounding the substep.
 // Other rows: one row per slot.
-template <int F, int FPL, int LPR>
+template <int F, int FPL, int LPR, int U>
 __device__ __forceinline__ void optic_item(const OpticK& k, int s, const float* dr_in, float* dr_out, long long item,
                                            float* red) {
   using S = OpticShape<F, FPL, LPR>;
@@ -228,7 +227,7 @@ __device__ __forceinline__ void optic_item(const OpticK& k, int s, const float* 
   float acc[FPL];
   if (item < k.n_long) {
     const int row = k.rows[item];
-    row_product<F, FPL, LPR>(k.ptr, k.cw, dr_in, k.batch, row, true, acc, gslot, S::SLOTS);
+    row_product<F, FPL, LPR, U>(k.ptr, k.cw, dr_in, k.batch, row, true, acc, gslot, S::SLOTS);
     if (sl < F) {
 #pragma unroll
       for (int q = 0; q < FPL; ++q) red[gslot * F * FPL + sl * FPL + q] = acc[q];
@@ -248,7 +247,7 @@ __device__ __forceinline__ void optic_item(const OpticK& k, int s, const float* 
     const long long r = k.n_long + (item - k.n_long) * S::SLOTS + gslot;
     const bool ok = r < k.m;
     const int row = ok ? (k.rows ? k.rows[r] : (int)r) : 0;
-    row_product<F, FPL, LPR>(k.ptr, k.cw, dr_in, k.batch, row, ok, acc);
+    row_product<F, FPL, LPR, U>(k.ptr, k.cw, dr_in, k.batch, row, ok, acc);
     if (ok && sl < F) optic_epilogue<F, FPL>(k, s, row, sl, acc, dr_in, dr_out);
   }
 }
@@ -266,16 +265,18 @@ __global__ void optic_init_kernel(OpticK k) {
   init_dr(k, k.buf0, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
-template <int F, int FPL, int LPR>
-__global__ void __launch_bounds__(256) optic_step_kernel(OpticK k, int s) {
+// MINB: blocks per SM the registers must allow (launch bounds); 8 caps them at 32 per thread so a
+// full SM of 64 warps keeps gathers in flight.
+template <int F, int FPL, int LPR, int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) optic_step_kernel(OpticK k, int s) {
   __shared__ float red[OpticShape<F, FPL, LPR>::RED];
   const float* in = (s & 1) ? k.buf1 : k.buf0;
   float* out = (s & 1) ? k.buf0 : k.buf1;
-  optic_item<F, FPL, LPR>(k, s, in, out, blockIdx.x, red);
+  optic_item<F, FPL, LPR, U>(k, s, in, out, blockIdx.x, red);
 }
 
-template <int F, int FPL, int LPR>
-__global__ void __launch_bounds__(256) optic_persistent_kernel(OpticK k) {
+template <int F, int FPL, int LPR, int U, int MINB>
+__global__ void __launch_bounds__(256, MINB) optic_persistent_kernel(OpticK k) {
   __shared__ float red[OpticShape<F, FPL, LPR>::RED];
   int generation = 0;
   const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -288,12 +289,12 @@ __global__ void __launch_bounds__(256) optic_persistent_kernel(OpticK k) {
   for (int s = 0; s < k.nsteps; ++s) {
     const float* in = (s & 1) ? k.buf1 : k.buf0;
     float* out = (s & 1) ? k.buf0 : k.buf1;
-    for (long long item = blockIdx.x; item < items; item += gridDim.x) optic_item<F, FPL, LPR>(k, s, in, out, item, red);
+    for (long long item = blockIdx.x; item < items; item += gridDim.x) optic_item<F, FPL, LPR, U>(k, s, in, out, item, red);
     if (s + 1 < k.nsteps && !grid_barrier(k.sync, k.status, generation, s)) return;
   }
 }
 
-template <int F, int FPL, int LPR>
+template <int F, int FPL, int LPR, int U = Unroll<FPL>::U, int MINB = 1>
 static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st) {
   const long long sz = (long long)k.m * k.batch;
   if (launch == FLYB_LAUNCH_STEP) {
@@ -303,7 +304,7 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
     }
     const unsigned blocks = (unsigned)optic_items<F, FPL, LPR>(k.m, k.n_long);
     for (int s = 0; s < k.nsteps; ++s) {
-      optic_step_kernel<F, FPL, LPR><<<blocks, 256, 0, st>>>(k, s);
+      optic_step_kernel<F, FPL, LPR, U, MINB><<<blocks, 256, 0, st>>>(k, s);
       FLYB_CHECK_LAUNCH();
     }
     return 0;
@@ -311,7 +312,7 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, optic_persistent_kernel<F, FPL, LPR>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, optic_persistent_kernel<F, FPL, LPR, U, MINB>, 256, 0);
   long long grid = (long long)sms * per_sm;
   const long long need = optic_items<F, FPL, LPR>(k.m, k.n_long);
   if (grid > need) grid = need;
@@ -321,7 +322,7 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
   if (e != cudaSuccess) return (int)e;
   OpticK kk = k;
   void* args[] = {&kk};
-  e = cudaLaunchCooperativeKernel((void*)optic_persistent_kernel<F, FPL, LPR>, dim3((unsigned)grid), dim3(256), args, 0,
+  e = cudaLaunchCooperativeKernel((void*)optic_persistent_kernel<F, FPL, LPR, U, MINB>, dim3((unsigned)grid), dim3(256), args, 0,
                                   st);
   return (int)e;
 }
@@ -341,30 +342,45 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
     return FLYB_ETOOBIG;                                               \
   } while (0)
 
-// (F fly lanes, FPL flies per lane, LPR lanes per row) of the optic substep for a batch; `variant`
-// 0 is the default, 1 and 2 are the alternatives the autotuner tries.
+// (F fly lanes, FPL flies per lane, LPR lanes per row, U gathers in flight per lane, MINB blocks per
+// SM) of the optic substep for a batch; `variant` 0 is the default, the others are alternatives the
+// autotuner tries (more warps with fewer registers each, or wider lanes); an unknown variant is an
+// error.
 #define FLYB_OPTIC_DISPATCH(B, V, CALL)                                                           \
   do {                                                                                            \
     if ((B) == 1) {                                                                               \
-      if ((V) == 1) { constexpr int F = 1, FPL = 1, LPR = 16; return CALL; }                      \
-      if ((V) == 2) { constexpr int F = 1, FPL = 1, LPR = 32; return CALL; }                      \
-      constexpr int F = 1, FPL = 1, LPR = 8; return CALL;                                         \
+      if ((V) == 0) { constexpr int F = 1, FPL = 1, LPR = 8, U = 8, MINB = 1; return CALL; }      \
+      if ((V) == 1) { constexpr int F = 1, FPL = 1, LPR = 16, U = 8, MINB = 1; return CALL; }     \
+      if ((V) == 2) { constexpr int F = 1, FPL = 1, LPR = 32, U = 8, MINB = 1; return CALL; }     \
+      if ((V) == 3) { constexpr int F = 1, FPL = 1, LPR = 8, U = 4, MINB = 8; return CALL; }      \
+      if ((V) == 4) { constexpr int F = 1, FPL = 1, LPR = 16, U = 4, MINB = 8; return CALL; }     \
+      return FLYB_EINVAL;                                                                         \
     }                                                                                             \
-    if ((B) <= 2) { constexpr int F = 2, FPL = 1, LPR = 16; return CALL; }                        \
-    if ((B) <= 4) { constexpr int F = 4, FPL = 1, LPR = 16; return CALL; }                        \
-    if ((B) <= 8) { constexpr int F = 8, FPL = 1, LPR = 32; return CALL; }                        \
-    if ((B) <= 16) { constexpr int F = 16, FPL = 1, LPR = 32; return CALL; }                      \
-    if ((B) <= 32) { constexpr int F = 32, FPL = 1, LPR = 32; return CALL; }                      \
+    if ((V) != 0 && (B) <= 32) return FLYB_EINVAL;                                                \
+    if ((B) <= 2) { constexpr int F = 2, FPL = 1, LPR = 16, U = 8, MINB = 1; return CALL; }       \
+    if ((B) <= 4) { constexpr int F = 4, FPL = 1, LPR = 16, U = 8, MINB = 1; return CALL; }       \
+    if ((B) <= 8) { constexpr int F = 8, FPL = 1, LPR = 32, U = 8, MINB = 1; return CALL; }       \
+    if ((B) <= 16) { constexpr int F = 16, FPL = 1, LPR = 32, U = 8, MINB = 1; return CALL; }     \
+    if ((B) <= 32) { constexpr int F = 32, FPL = 1, LPR = 32, U = 8, MINB = 1; return CALL; }     \
     if ((B) <= 64) {                                                                              \
-      if ((V) == 1) { constexpr int F = 32, FPL = 2, LPR = 32; return CALL; }                     \
-      if ((V) == 2) { constexpr int F = 8, FPL = 8, LPR = 32; return CALL; }                      \
-      constexpr int F = 16, FPL = 4, LPR = 32; return CALL;                                       \
+      if ((V) == 0) { constexpr int F = 16, FPL = 4, LPR = 32, U = 4, MINB = 1; return CALL; }    \
+      if ((V) == 1) { constexpr int F = 32, FPL = 2, LPR = 32, U = 8, MINB = 1; return CALL; }    \
+      if ((V) == 2) { constexpr int F = 8, FPL = 8, LPR = 32, U = 2, MINB = 1; return CALL; }     \
+      if ((V) == 3) { constexpr int F = 16, FPL = 4, LPR = 32, U = 2, MINB = 8; return CALL; }    \
+      if ((V) == 4) { constexpr int F = 32, FPL = 2, LPR = 32, U = 4, MINB = 8; return CALL; }    \
+      if ((V) == 5) { constexpr int F = 16, FPL = 4, LPR = 32, U = 4, MINB = 6; return CALL; }    \
+      return FLYB_EINVAL;                                                                         \
     }                                                                                             \
     if ((B) <= 128) {                                                                             \
-      if ((V) == 1) { constexpr int F = 16, FPL = 8, LPR = 32; return CALL; }                     \
-      constexpr int F = 32, FPL = 4, LPR = 32; return CALL;                                       \
+      if ((V) == 0) { constexpr int F = 32, FPL = 4, LPR = 32, U = 4, MINB = 1; return CALL; }    \
+      if ((V) == 1) { constexpr int F = 16, FPL = 8, LPR = 32, U = 2, MINB = 1; return CALL; }    \
+      if ((V) == 3) { constexpr int F = 32, FPL = 4, LPR = 32, U = 2, MINB = 8; return CALL; }    \
+      return FLYB_EINVAL;                                                                         \
     }                                                                                             \
-    if ((B) <= 256) { constexpr int F = 32, FPL = 8, LPR = 32; return CALL; }                     \
+    if ((B) <= 256) {                                                                             \
+      if ((V) == 0) { constexpr int F = 32, FPL = 8, LPR = 32, U = 2, MINB = 1; return CALL; }    \
+      return FLYB_EINVAL;                                                                         \
+    }                                                                                             \
     return FLYB_ETOOBIG;                                                                          \
   } while (0)
 
@@ -376,6 +392,7 @@ struct SpmmK {
   float x_div, x_lo, x_hi;
   float* y; const int* __restrict__ y_index;
   float alpha, y_lo, y_hi;
+  int xvec;   // batch == F * FPL and x aligned to FPL floats: one vector gather per entry and lane
 };
 
 // WPR warps share one row (RB = 8 / WPR rows per 256-thread block): warp `part` of a row takes the
@@ -411,16 +428,22 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
       }
       float xv[U][FPL];
 #pragma unroll
-      for (int u = 0; u < U; ++u)
+      for (int u = 0; u < U; ++u) {
+        if (k.xvec) {
+          load_x<FPL>(k.x + (size_t)(jj[u] < 0 ? 0 : jj[u]) * k.batch + fb, xv[u]);
+        } else {
 #pragma unroll
-        for (int q = 0; q < FPL; ++q)
-          xv[u][q] = (jj[u] >= 0 && fb + q < k.batch) ? __ldg(&k.x[(size_t)jj[u] * k.batch + fb + q]) : 0.0f;
+          for (int q = 0; q < FPL; ++q)
+            xv[u][q] = (jj[u] >= 0 && fb + q < k.batch) ? __ldg(&k.x[(size_t)jj[u] * k.batch + fb + q]) : 0.0f;
+        }
+      }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         if (jj[u] >= 0) {
 #pragma unroll
           for (int q = 0; q < FPL; ++q) {
-            float x = xv[u][q] / k.x_div;
+            float x = xv[u][q];
+            if (k.x_div != 1.0f) x = x / k.x_div;     // x / 1 == x exactly: skip the IEEE division
             x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
             const float p = ww[u] * x;
             acc[q] = acc[q] + p;
@@ -459,7 +482,9 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
 }
 
 template <int F, int FPL>
-static int run_spmm(const SpmmK& k, int wpr, cudaStream_t st) {
+static int run_spmm(const SpmmK& k0, int wpr, cudaStream_t st) {
+  SpmmK k = k0;
+  k.xvec = k.batch == F * FPL && (reinterpret_cast<uintptr_t>(k.x) % (FPL * sizeof(float))) == 0;
   const long long rb = 8 / wpr;
   const unsigned blocks = (unsigned)((k.rows + rb - 1) / rb);
   if (!blocks) return 0;
@@ -523,7 +548,7 @@ __global__ void ref_csr_kernel(const int* __restrict__ ptr, const int* __restric
 
 int optic_blocks_per_sm() {
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, optic_persistent_kernel<1, 1, 8>, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, optic_persistent_kernel<1, 1, 8, 8, 1>, 256, 0);
   return b;
 }
 
@@ -545,7 +570,7 @@ FLYB_API int flyb_optic_run(const flyb_optic_args* a, void* stream) {
            (a->flags & FLYB_OPTIC_HISTORY) ? a->inp_hist : nullptr, a->status, a->sync,
            (a->flags & FLYB_OPTIC_DR_VALID) ? 1 : 0};
   cudaStream_t st = (cudaStream_t)stream;
-  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
+  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR, U, MINB>(k, a->launch, a->grid, st)));
 }
 
 // ------------------------------------------------------------------ allocation-free variant
@@ -593,7 +618,7 @@ FLYB_API int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream) {
            (a->flags & FLYB_OPTIC_HISTORY) ? a->inp_hist : nullptr, a->status,
            (int*)(scratch + 2 * FLYB_OPTIC_NOALLOC_MAX), 0};
   cudaStream_t st = (cudaStream_t)stream;
-  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR>(k, a->launch, a->grid, st)));
+  FLYB_OPTIC_DISPATCH(a->batch, a->variant, (run_optic<F, FPL, LPR, U, MINB>(k, a->launch, a->grid, st)));
 }
 
 FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
@@ -601,7 +626,7 @@ FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
     return FLYB_EINVAL;
   if (a->rows == 0) return 0;
   SpmmK k{a->rows, a->batch, a->accumulate, a->ptr, a->col, a->w, a->x, a->x_index, a->x_div, a->x_lo, a->x_hi,
-          a->y, a->y_index, a->alpha, a->y_lo, a->y_hi};
+          a->y, a->y_index, a->alpha, a->y_lo, a->y_hi, 0};
   cudaStream_t st = (cudaStream_t)stream;
   const int wpr = a->warps_per_row ? a->warps_per_row : 1;
   if (wpr != 1 && wpr != 2 && wpr != 4 && wpr != 8) return FLYB_EINVAL;

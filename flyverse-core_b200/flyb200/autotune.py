@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 CACHE: dict = {}
+OPTIC_VARIANTS = 6          # flyb_optic_args.variant values; a batch width has a subset of them
 # (launch, block, items per thread, staged): staged = per-step launches through the bulk-copy kernel
 LIF_CANDIDATES = (("step", 256, 4, 0), ("step", 512, 4, 0), ("step", 256, 2, 0), ("step", 256, 1, 0),
                   ("step", 256, 2, 1), ("step", 256, 4, 1), ("step", 512, 2, 1), ("step", 128, 4, 1),
@@ -93,9 +94,12 @@ def tune_optic(core, steps: int = 10) -> dict:
     v, a = core.v_s.clone(), core.adapt_s.clone()
     results = {}
     for launch in ("step", "persistent"):
-        for variant in (0, 1, 2):
+        for variant in range(OPTIC_VARIANTS):
             core.launch, core.variant = launch, variant
-            core.substeps(2)
+            try:
+                core.substeps(2)
+            except RuntimeError:                 # no such shape for this batch width
+                continue
             results[(launch, variant)] = _time(lambda: core.substeps(steps, carry=True), 1) / steps
             core.v_s.copy_(v)
             core.adapt_s.copy_(a)

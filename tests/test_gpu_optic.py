@@ -54,6 +54,42 @@ def test_fused_substeps_match_oracle(batch, launch):
     np.testing.assert_allclose(ih.cpu().numpy(), oih, rtol=RTOL, atol=ATOL)
 
 
+@pytest.mark.parametrize("batch,variant", [(1, 1), (1, 2), (1, 3), (1, 4), (64, 1), (64, 2), (64, 3), (64, 4),
+                                           (64, 5), (100, 1), (100, 3), (48, 3)])
+@pytest.mark.parametrize("launch", ["step", "persistent"])
+def test_kernel_shape_variants_match_oracle(batch, variant, launch):
+    """Every kernel shape the autotuner may pick (flyb_optic_args.variant) against the FP32 oracle."""
+    cfg = small_optic(seed=8)
+    W = cfg.W_rr()
+    rng = np.random.default_rng(variant)
+    v = (rng.standard_normal((cfg.m, batch)) * 0.3).astype(np.float32)
+    ad = (rng.standard_normal((cfg.m, batch)) * 0.05).astype(np.float32)
+    pr = (rng.standard_normal((cfg.m, batch)) * 0.3).astype(np.float32)
+    spk = (rng.standard_normal((cfg.m, batch)) * 0.1).astype(np.float32)
+    core = OpticCore(W, cfg.a, cfg.b, batch=batch, device="cuda", gain_rr=cfg.gain_rr, adapt_gain=cfg.adapt_gain,
+                     aad=cfg.aad, launch=launch)
+    core.variant = variant
+    core.v_s.copy_(torch.from_numpy(v))
+    core.adapt_s.copy_(torch.from_numpy(ad))
+    core.pr_in.copy_(torch.from_numpy(pr))
+    core.spk_in.copy_(torch.from_numpy(spk))
+    core.substeps(20)
+    torch.cuda.synchronize()
+    core.check()
+    oracle.optic_run(v, ad, W.indptr, W.indices, W.data, pr, spk, cfg.a, cfg.b, cfg.gain_rr, cfg.adapt_gain, cfg.aad, 20)
+    np.testing.assert_allclose(core.v_s.cpu().numpy(), v, rtol=RTOL, atol=ATOL)
+    np.testing.assert_allclose(core.adapt_s.cpu().numpy(), ad, rtol=RTOL, atol=ATOL)
+
+
+def test_unknown_kernel_shape_is_rejected():
+    cfg = small_optic(seed=8)
+    core = OpticCore(cfg.W_rr(), cfg.a, cfg.b, batch=8, device="cuda", gain_rr=cfg.gain_rr,
+                     adapt_gain=cfg.adapt_gain, aad=cfg.aad, launch="step")
+    core.variant = 3                     # batch widths 2-32 have one shape only
+    with pytest.raises(RuntimeError, match="1001"):
+        core.substeps(1)
+
+
 def test_fp64_error_of_fp32_substeps_is_small():
     cfg = small_optic(seed=5)
     W = cfg.W_rr()
