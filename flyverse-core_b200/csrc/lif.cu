@@ -42,8 +42,15 @@ struct LifK {
   unsigned long long* events;
   int* status;
   int* sync;
+  int4* spike_list;   // deferred delivery: {fly, first edge, edges, x bits} per chunk of a spiker's edges
+  unsigned* spike_n;  // entries appended this step
+  long long spike_cap;
   LifP P;
 };
+
+// Out-edges per deferred-delivery entry: a spiker's edge list is cut into chunks of at most this
+// many, so one block of the scatter kernel never walks more (out-degrees reach 10^4 and beyond).
+constexpr int kEdgeChunk = 1024;
 
 template <int BLOCK>
 struct LifSmem {
@@ -305,10 +312,73 @@ __device__ __forceinline__ void deliver(const LifK& k, LifSmem<BLOCK * IPT>& sm,
   __syncthreads();   // shared lists are reused by the next chunk
 }
 
+// Deferred delivery, update side: a warp with transmitting items reserves list entries with one
+// atomicAdd (each item takes one entry per kEdgeChunk of its out-edges) and writes them; the
+// scatter kernel of the same step delivers them. Entries beyond spike_cap are not written and set
+// FLYB_ETOOBIG (the host sizes the list so that this cannot happen).
+template <int IPT>
+__device__ __forceinline__ void append_spikes(const LifK& k, int s, unsigned tx_bits, const int (&iq)[IPT],
+                                              const int (&bq)[IPT], const float (&xq)[IPT]) {
+  const int lane = threadIdx.x & 31;
+  if (!__any_sync(0xffffffffu, tx_bits != 0)) return;   // nearly every warp: nothing fired
+  int e0[IPT], deg[IPT], cnt = 0;
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    e0[q] = 0; deg[q] = 0;
+    if (tx_bits & (1u << q)) {
+      e0[q] = k.out_ptr[iq[q]];
+      deg[q] = k.out_ptr[iq[q] + 1] - e0[q];
+      cnt += (deg[q] + kEdgeChunk - 1) / kEdgeChunk;
+    }
+  }
+  const int incl = warp_scan(cnt);
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned base = 0;
+  if (lane == 31 && total) base = atomicAdd(k.spike_n, (unsigned)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  long long pos = (long long)base + incl - cnt;
+#pragma unroll
+  for (int q = 0; q < IPT; ++q) {
+    for (int c = 0; c < deg[q]; c += kEdgeChunk, ++pos) {
+      if (pos >= k.spike_cap) { set_error(k.status, FLYB_ETOOBIG, 5, s); break; }
+      const int len = deg[q] - c < kEdgeChunk ? deg[q] - c : kEdgeChunk;
+      k.spike_list[pos] = make_int4(bq[q], e0[q] + c, len, __float_as_int(xq[q]));
+    }
+  }
+}
+
+// Deferred delivery, scatter side: one block per list entry (at most kEdgeChunk edges), blocks
+// striding over the entries the update kernel of step `s` appended; same integer red.global.add
+// into the write slot as the fused path, so the ring sums are identical.
+template <bool FIXED>
+__global__ void __launch_bounds__(256) lif_scatter_kernel(LifK k, int s) {
+  const Clk clk = read_clock(k);
+  const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
+  const size_t slot = (size_t)k.n * k.batch;
+  const long long n = (long long)*k.spike_n < k.spike_cap ? (long long)*k.spike_n : k.spike_cap;
+  unsigned long long edges = 0;
+  for (long long j = blockIdx.x; j < n; j += gridDim.x) {
+    const int4 en = k.spike_list[j];
+    const float x = __int_as_float(en.w);
+    for (int q = threadIdx.x; q < en.z; q += blockDim.x) {
+      const int2 ed = __ldg(&k.out_edge[en.y + q]);
+      const size_t dst = (size_t)ws * slot + (size_t)ed.x * k.batch + en.x;
+      if (FIXED) {
+        const long long f = __double2ll_rn((double)__int_as_float(ed.y) * (double)x * 4294967296.0);
+        atomicAdd((unsigned long long*)k.ring + dst, (unsigned long long)f);
+      } else {
+        atomicAdd((int*)k.ring + dst, ed.y);
+      }
+    }
+    edges += (unsigned long long)en.z;
+  }
+  if (k.events && threadIdx.x == 0 && edges) atomicAdd(k.events, edges);
+}
+
 // One block processes work items [base, base + BLOCK*IPT) of local step `s`: update, then deliver.
 // Thread j owns the IPT consecutive items base + j*IPT + q (neuron-major, fly-minor order), loads
 // every state array as one vector and keeps all loads in flight before computing.
-template <int BLOCK, bool FIXED, int IPT>
+template <int BLOCK, bool FIXED, int IPT, bool DEFER = false>
 __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, long long base,
                                           LifSmem<BLOCK * IPT>& sm) {
   using RingT = typename std::conditional<FIXED, long long, int>::type;
@@ -468,14 +538,17 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
       k.raster[rslot * k.words + (size_t)((wbase >> 5) + lane / LPW)] = v;
     }
   }
-  deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
+  if constexpr (DEFER)
+    append_spikes<IPT>(k, s, tx_bits, iq, bq, xq);
+  else
+    deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
 }
 
-template <int BLOCK, bool FIXED, int IPT>
+template <int BLOCK, bool FIXED, int IPT, bool DEFER = false>
 __global__ void __launch_bounds__(BLOCK) lif_step_kernel(LifK k, int s) {
   __shared__ LifSmem<BLOCK * IPT> sm;
   const Clk clk = read_clock(k);
-  lif_chunk<BLOCK, FIXED, IPT>(k, clk, s, k.t_begin + (long long)blockIdx.x * BLOCK * IPT, sm);
+  lif_chunk<BLOCK, FIXED, IPT, DEFER>(k, clk, s, k.t_begin + (long long)blockIdx.x * BLOCK * IPT, sm);
 }
 
 __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
@@ -742,8 +815,23 @@ static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st)
   const long long W = (long long)k.t_end - k.t_begin;
   const long long chunks = (W + (long long)BLOCK * IPT - 1) / ((long long)BLOCK * IPT);
   if (launch == FLYB_LAUNCH_STEP) {
+    int scatter_grid = 0;
+    if (k.spike_list) {
+      int dev = 0, sms = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      scatter_grid = sms * 8;
+    }
     for (int s = 0; s < k.nsteps; ++s) {
-      lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
+      if (k.spike_list) {   // deferred delivery: update + list, then the balanced scatter
+        cudaError_t e = cudaMemsetAsync(k.spike_n, 0, sizeof(unsigned), st);
+        if (e != cudaSuccess) return (int)e;
+        lif_step_kernel<BLOCK, FIXED, IPT, true><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
+        FLYB_CHECK_LAUNCH();
+        lif_scatter_kernel<FIXED><<<scatter_grid, 256, 0, st>>>(k, s);
+      } else {
+        lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
+      }
       FLYB_CHECK_LAUNCH();
     }
     if (needs_advance(k)) {
@@ -900,6 +988,18 @@ int lif_blocks_per_sm(int block) {
 
 using namespace flyb;
 
+FLYB_API long long flyb_lif_spike_capacity(const flyb_lif_args* a) {
+  if (!a || a->n <= 0 || a->batch <= 0 || !a->out_ptr) return -1;
+  const int first = a->n_first, count = a->n_count ? a->n_count : a->n - a->n_first;
+  if (first < 0 || count <= 0 || (long long)first + count > a->n) return -1;
+  // every item of the launch fires: one entry per item plus one per full kEdgeChunk of its edges
+  int lo = 0, hi = 0;
+  if (cudaMemcpy(&lo, a->out_ptr + first, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&hi, a->out_ptr + first + count, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return (long long)count * a->batch + ((long long)(hi - lo) / kEdgeChunk) * a->batch;
+}
+
 // Validates the arguments and fills the kernel view; 0 or an FLYB_E* code.
 static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   if (!a || a->n <= 0 || a->batch <= 0 || a->n_delay < 1 || a->ring_slots < a->n_delay + 1 || a->nsteps < 0 ||
@@ -930,6 +1030,13 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.clock = a->clock;
   k.raster = a->raster; k.raster_slots = a->raster_slots; k.raster_pos = a->raster_pos; k.fly0 = a->fly0;
   k.events = a->events; k.status = a->status; k.sync = a->sync;
+  k.spike_list = nullptr; k.spike_n = nullptr; k.spike_cap = 0;
+  if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
+    // per-step launches of the register path only; the list must hold every entry a step can make
+    if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP || a->staged)
+      return FLYB_EINVAL;
+    k.spike_list = (int4*)a->spike_list; k.spike_n = a->spike_n; k.spike_cap = a->spike_cap;
+  }
   const float* P = a->params;
   k.P = LifP{P[FLYB_P_V_REST], P[FLYB_P_V_RESET], P[FLYB_P_V_TH], P[FLYB_P_A_M], P[FLYB_P_A_S], P[FLYB_P_DT],
              P[FLYB_P_T_REF], P[FLYB_P_ADAPT_JUMP], P[FLYB_P_A_AD], P[FLYB_P_A_STD], P[FLYB_P_A_R],

@@ -318,6 +318,12 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
   if (grid > need) grid = need;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
   if (grid < 1) return FLYB_ECOOP;
+  if (k.nsteps == 1 && k.dr_valid) {
+    // one substep on a carried dr reaches no grid barrier: an ordinary launch of `grid` blocks
+    // looping over the items, which other kernels may share the SMs with
+    optic_persistent_kernel<F, FPL, LPR, U, MINB><<<(unsigned)grid, 256, 0, st>>>(k);
+    return (int)cudaGetLastError();
+  }
   cudaError_t e = cudaMemsetAsync(k.sync, 0, 2 * sizeof(int), st);
   if (e != cudaSuccess) return (int)e;
   OpticK kk = k;

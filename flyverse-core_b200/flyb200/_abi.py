@@ -20,7 +20,7 @@ _LIB = None
 # ------------------------------------------------------------------ constants (flyb200.h)
 OK, EINVAL, EBARRIER, ECOOP, ETOOBIG = 0, 1001, 1002, 1003, 1004
 LIF_POISSON, LIF_STD, LIF_COUNTS, LIF_ADAPT = 1, 2, 4, 8
-LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES, LIF_NO_ADVANCE = 16, 32, 64, 128
+LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES, LIF_NO_ADVANCE, LIF_DEFER_DELIVERY = 16, 32, 64, 128, 256
 RING_COUNT, RING_FIXED = 0, 1
 LAUNCH_STEP, LAUNCH_PERSISTENT = 0, 1
 LAUNCHES_BY_NAME = {"step": LAUNCH_STEP, "persistent": LAUNCH_PERSISTENT}
@@ -44,7 +44,7 @@ class LifArgs(ct.Structure):
                 ("rate", _VP), ("counts", _VP), ("spikes", _VP), ("drive", _VP), ("poisson_p", _VP),
                 ("active", _VP), ("std_u", _VP), ("params", _VP), ("ring", _VP), ("uniforms", _VP),
                 ("fly_steps", _VP), ("clock", _VP), ("raster", _VP), ("events", _VP), ("status", _VP),
-                ("sync", _VP)]
+                ("sync", _VP), ("spike_list", _VP), ("spike_n", _VP), ("spike_cap", ct.c_longlong)]
 
 
 class OpticArgs(ct.Structure):
@@ -99,6 +99,7 @@ SIGNATURES = {
     "launch_means": [_P, _I, _I, _I, _I, _VP],
     "flyb_lif_run": [ct.POINTER(LifArgs), _VP],
     "flyb_lif_advance": [ct.POINTER(LifArgs), _VP],
+    "flyb_lif_spike_capacity": [ct.POINTER(LifArgs)],
     "flyb_ring_deposit": [_I, _I, _I, _VP, _VP, _VP, _VP, _VP],
     "flyb_optic_run": [ct.POINTER(OpticArgs), _VP],
     "flyb_optic_run_noalloc": [ct.POINTER(OpticArgs), _VP],
@@ -110,7 +111,7 @@ SIGNATURES = {
     "flyb_version": [],
     "flyb_abi_sizes": [ct.POINTER(_I), _I],
 }
-RESTYPES = {"flyb_version": ct.c_char_p}
+RESTYPES = {"flyb_version": ct.c_char_p, "flyb_lif_spike_capacity": ct.c_longlong}
 
 
 def library_path() -> Path:

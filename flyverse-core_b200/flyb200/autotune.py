@@ -4,8 +4,8 @@ The best launch shape depends on the graph, the batch and how many cells spike p
 the step is latency-bound and a persistent cooperative launch (one launch for many steps, a grid
 barrier per step) wins; at B = 64 the state streams from HBM and one launch per step, with the
 state staged through shared memory by bulk copies, keeps more bytes in flight. `tune_lif` times
-each candidate (launch mode x block size x items per thread x staged) for a few steps on a copy of
-the live state, restores the state, installs the fastest and caches it under the key;
+each candidate (launch mode x block size x items per thread x spike delivery) for a few steps on a
+copy of the live state, restores the state, installs the fastest and caches it under the key;
 `tune_optic` does the same for the optic substep's launch mode and kernel shape.
 """
 from __future__ import annotations
@@ -18,10 +18,13 @@ import torch
 
 CACHE: dict = {}
 OPTIC_VARIANTS = 6          # flyb_optic_args.variant values; a batch width has a subset of them
-# (launch, block, items per thread, staged): staged = per-step launches through the bulk-copy kernel
-LIF_CANDIDATES = (("step", 256, 4, 0), ("step", 512, 4, 0), ("step", 256, 2, 0), ("step", 256, 1, 0),
-                  ("step", 256, 2, 1), ("step", 256, 4, 1), ("step", 512, 2, 1), ("step", 128, 4, 1),
-                  ("persistent", 256, 4, 0), ("persistent", 512, 2, 0))
+# (launch, block, items per thread, delivery): "fused" delivers spikes inside the update kernel,
+# "staged" runs per-step launches through the bulk-copy kernel, "defer" lists the spikers and
+# delivers them from a second, load-balanced kernel
+LIF_CANDIDATES = (("step", 256, 4, "fused"), ("step", 256, 2, "fused"), ("step", 256, 1, "fused"),
+                  ("step", 256, 2, "staged"), ("step", 512, 2, "staged"), ("step", 256, 4, "staged"),
+                  ("step", 256, 2, "defer"), ("step", 256, 1, "defer"), ("step", 128, 2, "defer"),
+                  ("step", 256, 4, "defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"))
 
 
 def graph_key(brain) -> str:
@@ -63,15 +66,15 @@ def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
         return CACHE[key]
     saved = brain.state_dict()
     results = {}
-    for launch, block, ipt, staged in candidates:
-        _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt, "staged": staged})
+    for launch, block, ipt, delivery in candidates:
+        _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt, "delivery": delivery})
         brain.step(2)
-        results[(launch, block, ipt, staged)] = _time(lambda: brain.step(steps), 1) / steps
+        results[(launch, block, ipt, delivery)] = _time(lambda: brain.step(steps), 1) / steps
         brain.load_state_dict(saved)
     best = min(results, key=results.get)
-    choice = {"launch": best[0], "block": best[1], "items_per_thread": best[2], "staged": best[3],
+    choice = {"launch": best[0], "block": best[1], "items_per_thread": best[2], "delivery": best[3],
               "ms_per_step": results[best],
-              "all": {f"{k[0]}{'-staged' if k[3] else ''}/{k[1]}/{k[2]}": v for k, v in results.items()}}
+              "all": {f"{k[0]}-{k[3]}/{k[1]}/{k[2]}": v for k, v in results.items()}}
     CACHE[key] = choice
     _apply(brain, choice)
     return choice
@@ -80,7 +83,8 @@ def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
 def _apply(brain, choice: dict) -> None:
     brain.launch, brain.block = choice["launch"], choice["block"]
     brain.items_per_thread = choice.get("items_per_thread", 0)
-    brain.staged = bool(choice.get("staged", 0))
+    delivery = choice.get("delivery", "fused")
+    brain.staged, brain.defer = delivery == "staged", delivery == "defer"
     brain._make_args()
 
 

@@ -249,6 +249,7 @@ class Brain:
         st, a = self._st, _abi.LifArgs()
         a.n, a.batch, a.n_delay, a.ring_slots, a.ring_mode = self.n, self.B, self.n_delay, self.R, self.ring_mode
         a.launch, a.block = LAUNCHES[self.launch], self.block
+        a.grid = int(getattr(self, "grid", 0))        # persistent / staged launches: block cap
         a.items_per_thread = getattr(self, "items_per_thread", 0)
         a.staged = int(bool(getattr(self, "staged", False)))
         a.raster_slots = self.n_delay
@@ -263,9 +264,34 @@ class Brain:
         a.ring, a.clock, a.raster = self.ring.data_ptr(), self._clock.data_ptr(), self._hist.data_ptr()
         a.events, a.status, a.sync = self._events.data_ptr(), self._status.data_ptr(), self._sync.data_ptr()
         self._args = a
+        self._lists = {}          # deferred-delivery lists per neuron range, sized on first use
+
+    def _defer_active(self) -> bool:
+        """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step register launches."""
+        return bool(getattr(self, "defer", False)) and self.launch == "step" and not getattr(self, "staged", False)
+
+    def _set_delivery(self, a, n_first: int, n_count: int) -> None:
+        """Point the arguments at the spike list of this neuron range (one list per range, so
+        ranges running on different streams never share one), or at none."""
+        if not self._defer_active():
+            a.spike_list, a.spike_n, a.spike_cap = None, None, 0
+            return
+        key = (int(n_first), int(n_count))
+        lst = self._lists.get(key)
+        if lst is None:
+            a.n_first, a.n_count = key
+            cap = int(self._lib.flyb_lif_spike_capacity(ct.byref(a)))
+            if cap <= 0:
+                raise RuntimeError("flyb_lif_spike_capacity failed")
+            lst = (torch.empty(cap, 4, dtype=torch.int32, device=self.device),
+                   torch.zeros(1, dtype=torch.int32, device=self.device), cap)
+            self._lists[key] = lst
+        a.spike_list, a.spike_n, a.spike_cap = lst[0].data_ptr(), lst[1].data_ptr(), lst[2]
 
     def _flags(self, external: bool) -> int:
         f = 0
+        if self._defer_active():
+            f |= _abi.LIF_DEFER_DELIVERY
         if self._poisson_on:
             f |= _abi.LIF_POISSON
         if self._std_on:
@@ -294,6 +320,8 @@ class Brain:
         a.flags = self._flags(ext is not None)
         a.nsteps = n_steps
         a.uniforms = ext.data_ptr() if ext is not None else None
+        self._set_delivery(a, 0, 0)
+        a.n_first, a.n_count = 0, 0
         stream = torch.cuda.current_stream(self.device).cuda_stream
         with torch.cuda.device(self.device):
             rc = self._lib.flyb_lif_run(ct.byref(a), stream)
@@ -311,6 +339,7 @@ class Brain:
         a = self._args
         a.flags = self._flags(False) | _abi.LIF_NO_ADVANCE
         a.nsteps, a.uniforms = 1, None
+        self._set_delivery(a, n_first, n_count)
         a.n_first, a.n_count = int(n_first), int(n_count)
         try:
             with torch.cuda.device(self.device):
@@ -324,7 +353,7 @@ class Brain:
         """End `n_steps` steps run by ranges: move the device clock (ring and history positions,
         Philox step) on, as the end of `step` does."""
         a = self._args
-        a.flags = self._flags(False)
+        a.flags = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY
         a.nsteps = int(n_steps)
         with torch.cuda.device(self.device):
             rc = self._lib.flyb_lif_advance(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)

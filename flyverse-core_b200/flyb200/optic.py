@@ -177,6 +177,7 @@ class OpticCore:
         self.gain_rr, self.adapt_gain, self.aad = float(gain_rr), float(adapt_gain), float(aad)
         self.launch = launch
         self.variant = 0                 # kernel shape (flyb_optic_args.variant), set by the autotuner
+        self.grid = 0                    # persistent launches: block cap (0 = every resident block)
         self.set_long_rows(LONG_ROW)
         M, B, dev = self.m, self.B, self.device
         self.v_s = torch.zeros(M, B, device=dev)
@@ -207,7 +208,7 @@ class OpticCore:
             flags |= _abi.OPTIC_DR_VALID
         dr, dr_tmp = self._bufs[self._cur], self._bufs[1 - self._cur]
         a = _abi.OpticArgs(m=self.m, batch=self.B, nsteps=int(nsteps), launch=_abi.LAUNCHES_BY_NAME[self.launch],
-                           ptr=self.W.ptr.data_ptr(), cw=self.W.cw.data_ptr(), variant=self.variant,
+                           grid=int(self.grid), ptr=self.W.ptr.data_ptr(), cw=self.W.cw.data_ptr(), variant=self.variant,
                            rows=self.rows.data_ptr(), n_long=self.n_long,
                            v=self.v_s.data_ptr(), adapt=self.adapt_s.data_ptr(), dr=dr.data_ptr(),
                            dr_tmp=dr_tmp.data_ptr(), pr=self.pr_in.data_ptr(), spk=self.spk_in.data_ptr(),

@@ -1,7 +1,9 @@
 """A short, eager run of the whole-fly step for profilers (every kernel launched separately).
 
     python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic]
-                              [--lif-block 256] [--lif-ipt 0|1|2|4] [--lif-staged] [--no-overlap]
+                              [--lif-block 256] [--lif-ipt 0|1|2|4] [--lif-staged] [--lif-defer] [--lif-grid 0]
+                              [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
+                              [--no-overlap]
     python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
@@ -70,10 +72,17 @@ def main() -> None:
     ap.add_argument("--lif-ipt", type=int, default=0, help="LIF items per thread (0: automatic)")
     ap.add_argument("--lif-staged", action="store_true", help="LIF step through the bulk-copy kernel")
     ap.add_argument("--no-overlap", action="store_true", help="run the LIF step after the optic chain")
+    ap.add_argument("--lif-grid", type=int, default=0, help="staged LIF block cap (0: every resident block)")
+    ap.add_argument("--lif-defer", action="store_true", help="LIF spikes delivered by a second kernel")
+    ap.add_argument("--optic-launch", default="step", choices=["step", "persistent"])
+    ap.add_argument("--optic-variant", type=int, default=0)
+    ap.add_argument("--optic-grid", type=int, default=0, help="persistent optic block cap")
     args = ap.parse_args()
     cfg = synthetic.whole_fly_config5(seed=0)
     eng = WholeFly(cfg, args.batch, device="cuda", seed=1, launch="step", overlap=not args.no_overlap)
     eng.lif.block, eng.lif.items_per_thread, eng.lif.staged = args.lif_block, args.lif_ipt, args.lif_staged
+    eng.lif.grid, eng.lif.defer = args.lif_grid, args.lif_defer
+    eng.optic.launch, eng.optic.variant, eng.optic.grid = args.optic_launch, args.optic_variant, args.optic_grid
     eng.lif._make_args()
     eng.optic.pr_in.normal_(0.0, 0.2)
     eng.step(args.warmup)

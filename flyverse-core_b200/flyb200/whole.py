@@ -86,9 +86,11 @@ class WholeFly:
 
     @property
     def overlapping(self) -> bool:
-        """Whether steps fork the undriven LIF update onto a second stream (per-step launches only:
-        a persistent cooperative launch must own the whole device)."""
-        return self.overlap and self.lif.launch == "step" and self.optic.launch == "step" and 0 < self.split
+        """Whether steps fork the undriven LIF update onto a second stream. The LIF must use
+        per-step launches (a persistent cooperative launch owns the device); the optic substep may
+        be persistent, since one substep on a carried dr is an ordinary launch (with
+        `optic.grid` blocks, leaving SMs room for the LIF blocks)."""
+        return self.overlap and self.lif.launch == "step" and 0 < self.split
 
     @staticmethod
     def _rows_with_entries(M, dev):

@@ -70,6 +70,10 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
 #define FLYB_LIF_EXT_UNIFORM  16   /* Poisson uniforms from `uniforms` instead of Philox      */
 #define FLYB_LIF_SKIP_FROZEN  32   /* frozen cells at rest are left untouched                 */
 #define FLYB_LIF_EPISODES     64   /* per-fly remaining-step counters gate the update         */
+#define FLYB_LIF_DEFER_DELIVERY 256 /* per-step register launches: the update kernel lists the
+                                      transmitting items (one entry per 1024 out-edges) in
+                                      `spike_list` and a second kernel delivers them, one block
+                                      per entry; needs spike_list / spike_n / spike_cap       */
 #define FLYB_LIF_NO_ADVANCE   128  /* leave `clock` and `fly_steps` as they are: other launches of
                                       the same steps cover the other neurons; flyb_lif_advance
                                       moves them on once all have run                           */
@@ -143,9 +147,17 @@ typedef struct flyb_lif_args {
   unsigned long long* events; /* optional [1]: += synaptic events (edges delivered)    */
   int* status;           /* [4] device words: [0] error code, [1] where, [2] step    */
   int* sync;             /* [FLYB_LIF_SYNC_WORDS] zeroed device scratch (persistent) */
+  void* spike_list;      /* FLYB_LIF_DEFER_DELIVERY: [spike_cap] int4 entries (device)  */
+  unsigned* spike_n;     /* FLYB_LIF_DEFER_DELIVERY: one device word (reset each step)  */
+  long long spike_cap;   /* entries spike_list holds: flyb_lif_spike_capacity(a) or more */
 } flyb_lif_args;
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);
+
+/* Entries a FLYB_LIF_DEFER_DELIVERY step of these arguments can write when every item of the
+ * neuron range fires (n_count * batch + batch * out-edges of the range / 1024); reads two row
+ * pointers from the device, so call it at set-up, not during stream capture. -1 on bad input. */
+long long flyb_lif_spike_capacity(const flyb_lif_args* a);
 
 /* Advance `clock` by a->nsteps and lower `fly_steps` (FLYB_LIF_EPISODES) as the end of a
  * flyb_lif_run does: for runs split over neuron ranges with FLYB_LIF_NO_ADVANCE, after all of

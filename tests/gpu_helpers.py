@@ -13,7 +13,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda", items_per_thread=0, with_sync=True, staged=0):
+                   device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -41,6 +41,13 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
                      params=P.ctypes.data, ring=ring.data_ptr(), uniforms=None if uni is None else uni.data_ptr(),
                      fly_steps=None if fs is None else fs.data_ptr(), raster=None if r is None else r.data_ptr(),
                      events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr() if with_sync else None)
+    if defer:
+        a.flags |= _abi.LIF_DEFER_DELIVERY
+        cap = int(_abi.lib().flyb_lif_spike_capacity(ct.byref(a)))
+        assert cap > 0
+        spike_list = torch.empty(cap, 4, dtype=torch.int32, device=dev)
+        spike_n = torch.zeros(1, dtype=torch.int32, device=dev)
+        a.spike_list, a.spike_n, a.spike_cap = spike_list.data_ptr(), spike_n.data_ptr(), cap
     rc = _abi.lib().flyb_lif_run(ct.byref(a), torch.cuda.current_stream(dev).cuda_stream)
     if rc:
         raise RuntimeError(f"flyb_lif_run: error {rc}")
@@ -59,7 +66,7 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
 
 
 def native_lif_run_split(state, out_ptr, out_edge, params, *, split, n_delay, flags, nsteps, seed=0, fly_steps=None,
-                         block=256, items_per_thread=0, staged=0, device="cuda"):
+                         block=256, items_per_thread=0, staged=0, device="cuda", defer=False):
     """oracle.lif_run's contract (raster always on), but every step runs as two neuron ranges,
     [0, split) and [split, n), launched on two streams that overlap, each with
     FLYB_LIF_NO_ADVANCE, then flyb_lif_advance on the joined stream (the device clock keeps the
@@ -92,17 +99,29 @@ def native_lif_run_split(state, out_ptr, out_edge, params, *, split, n_delay, fl
     lib = _abi.lib()
     main = torch.cuda.current_stream(dev)
     s1, s2 = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    lists = {}
+    if defer:
+        flags |= _abi.LIF_DEFER_DELIVERY
+        a.flags = flags | _abi.LIF_NO_ADVANCE
+        for first, count in ((0, split), (split, n - split)):
+            a.n_first, a.n_count = first, count
+            cap = int(lib.flyb_lif_spike_capacity(ct.byref(a)))
+            lists[first] = (torch.empty(cap, 4, dtype=torch.int32, device=dev),
+                            torch.zeros(1, dtype=torch.int32, device=dev), cap)
     for _ in range(nsteps):
         for stream, first, count in ((s1, 0, split), (s2, split, n - split)):
             stream.wait_stream(main)
             a.n_first, a.n_count = first, count
+            if defer:
+                lst = lists[first]
+                a.spike_list, a.spike_n, a.spike_cap = lst[0].data_ptr(), lst[1].data_ptr(), lst[2]
             rc = lib.flyb_lif_run(ct.byref(a), stream.cuda_stream)
             if rc:
                 torch.cuda.synchronize(dev)
                 raise RuntimeError(f"flyb_lif_run: error {rc}")
         main.wait_stream(s1)
         main.wait_stream(s2)
-        a.flags = flags
+        a.flags = flags & ~_abi.LIF_DEFER_DELIVERY
         rc = lib.flyb_lif_advance(ct.byref(a), main.cuda_stream)
         a.flags = flags | _abi.LIF_NO_ADVANCE
         if rc:

@@ -85,7 +85,7 @@ def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed
                 uniforms=uni, fly_steps=fs, seed=12345)
 
 
-def _compare(case, launch, block, grid=0, ipt=0, with_sync=True, staged=0):
+def _compare(case, launch, block, grid=0, ipt=0, with_sync=True, staged=0, defer=False):
     s_ref, s_gpu = case["state"].copy(), case["state"].copy()
     fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
     fs_gpu = None if fs_ref is None else fs_ref.copy()
@@ -94,7 +94,7 @@ def _compare(case, launch, block, grid=0, ipt=0, with_sync=True, staged=0):
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, **kw)
     r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], fly_steps=fs_gpu, launch=launch,
                                    block=block, grid=grid, items_per_thread=ipt, with_sync=with_sync, staged=staged,
-                                   **kw)
+                                   defer=defer, **kw)
     assert unpack(r_ref, s_ref.n * s_ref.batch).sum() > 0
     np.testing.assert_array_equal(r_gpu, r_ref)                      # spike rasters
     for k in LIF_ARRAYS:
@@ -137,6 +137,31 @@ def test_staged_step_equals_oracle(block, ipt, kind):
     _compare(case, STEP, block, ipt=ipt, staged=1)
 
 
+@pytest.mark.parametrize("block,ipt", [(256, 1), (256, 2), (128, 4), (512, 2)])
+@pytest.mark.parametrize("kind", ["count", "fixed", "episodes"])
+def test_deferred_delivery_equals_oracle(block, ipt, kind):
+    """Spikes listed by the update kernel (one entry per 1024 out-edges) and delivered by the
+    scatter kernel: every state bit, ring, raster and event count equal the oracle."""
+    case = case_random(batch=20, n=2999, steps=80, fixed=kind == "fixed", episodes=kind == "episodes")
+    _compare(case, STEP, block, ipt=ipt, defer=True)
+
+
+def test_deferred_delivery_splits_high_out_degree_spikers():
+    """A hub with more out-edges than one list entry covers (and uneven batch 3) still delivers
+    every edge once."""
+    case = case_random(batch=3, n=3000, edges=60_000, steps=60)
+    rng = np.random.default_rng(11)
+    ptr, e = case["ptr"].copy(), case["edges"].copy()
+    hub_extra = 5000                                   # neuron 0 gets 5000 more targets
+    w = 1 if case["state"].ring_mode == _abi.RING_COUNT else int(np.float32(0.275).view(np.int32))
+    extra = np.stack([rng.integers(0, 3000, hub_extra), np.full(hub_extra, w, np.int64)], 1).astype(np.int32)
+    e = np.concatenate([e[: ptr[1]], extra, e[ptr[1]:]]).astype(np.int32)
+    ptr = np.concatenate([[0], ptr[1:] + hub_extra]).astype(np.int32)
+    case["ptr"], case["edges"] = ptr, e
+    case["state"].poisson_p[0, :] = 0.5                # the hub fires often
+    _compare(case, STEP, 256, ipt=1, defer=True)
+
+
 def test_staged_request_falls_back_when_unaligned():
     """n * batch % 4 != 0: the staged request runs the register path, same results."""
     _compare(case_random(batch=3, n=2999, steps=60), STEP, 256, staged=1)
@@ -152,9 +177,10 @@ def test_depression_random_graph_register_paths():
         _compare(case_random(batch=8, n=2999, steps=60, std=True, ext_uniform=True), launch, 256)
 
 
-@pytest.mark.parametrize("staged,ipt", [(0, 4), (0, 1), (1, 2), (1, 4)])
+@pytest.mark.parametrize("staged,ipt,defer", [(0, 4, False), (0, 1, False), (1, 2, False), (1, 4, False),
+                                              (0, 2, True)])
 @pytest.mark.parametrize("kind", ["count", "fixed-episodes"])
-def test_neuron_ranges_on_two_streams_equal_oracle(staged, ipt, kind):
+def test_neuron_ranges_on_two_streams_equal_oracle(staged, ipt, defer, kind):
     """Each step as two neuron ranges launched on overlapping streams (FLYB_LIF_NO_ADVANCE), then
     flyb_lif_advance: every state bit, ring, raster and event count equal the oracle's whole steps."""
     case = case_random(batch=8, n=2999, steps=60, fixed=kind != "count", episodes=kind != "count")
@@ -164,7 +190,7 @@ def test_neuron_ranges_on_two_streams_equal_oracle(staged, ipt, kind):
     kw = dict(n_delay=case["n_delay"], flags=case["flags"], nsteps=case["nsteps"], seed=case["seed"])
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, raster=True, **kw)
     r_gpu, ev_gpu = native_lif_run_split(s_gpu, case["ptr"], case["edges"], case["P"], split=1504, fly_steps=fs_gpu,
-                                         items_per_thread=ipt, staged=staged, **kw)
+                                         items_per_thread=ipt, staged=staged, defer=defer, **kw)
     np.testing.assert_array_equal(r_gpu, r_ref)
     for k in LIF_ARRAYS:
         np.testing.assert_array_equal(getattr(s_gpu, k), getattr(s_ref, k), err_msg=k)

@@ -81,6 +81,32 @@ def test_kernel_shape_variants_match_oracle(batch, variant, launch):
     np.testing.assert_allclose(core.adapt_s.cpu().numpy(), ad, rtol=RTOL, atol=ATOL)
 
 
+def test_single_carried_persistent_substeps_with_a_block_cap_equal_step_launches():
+    """One substep on a carried dr is an ordinary launch of a capped grid looping over the rows:
+    bit-identical to one launch per substep."""
+    cfg = small_optic(seed=9)
+    W = cfg.W_rr()
+    B = 64
+    rng = np.random.default_rng(4)
+    v0 = (rng.standard_normal((cfg.m, B)) * 0.3).astype(np.float32)
+    pr = (rng.standard_normal((cfg.m, B)) * 0.3).astype(np.float32)
+    cores = []
+    for launch, grid in (("step", 0), ("persistent", 37)):
+        core = OpticCore(W, cfg.a, cfg.b, batch=B, device="cuda", gain_rr=cfg.gain_rr, adapt_gain=cfg.adapt_gain,
+                         aad=cfg.aad, launch=launch)
+        core.grid = grid
+        core.v_s.copy_(torch.from_numpy(v0))
+        core.pr_in.copy_(torch.from_numpy(pr))
+        for _ in range(7):
+            core.substeps(1, carry=True)
+        torch.cuda.synchronize()
+        core.check()
+        cores.append(core)
+    assert torch.equal(cores[0].v_s, cores[1].v_s)
+    assert torch.equal(cores[0].adapt_s, cores[1].adapt_s)
+    assert torch.equal(cores[0].dr_out, cores[1].dr_out)
+
+
 def test_unknown_kernel_shape_is_rejected():
     cfg = small_optic(seed=8)
     core = OpticCore(cfg.W_rr(), cfg.a, cfg.b, batch=8, device="cuda", gain_rr=cfg.gain_rr,

@@ -18,14 +18,20 @@ def small_fly():
                                        optic_nnz=200_000, n_pr=300)
 
 
-@pytest.mark.parametrize("overlap", [True, False])
-def test_whole_fly_matches_oracle_step_order(overlap):
+@pytest.mark.parametrize("overlap,capped,defer", [(True, False, False), (False, False, False), (True, True, False),
+                                                  (True, False, True)])
+def test_whole_fly_matches_oracle_step_order(overlap, capped, defer):
     """Bit-identical spikes every step whether the undriven LIF neurons update concurrently with
-    the optic chain (overlap) or after it; the oracle runs the stages serially on the engine's
-    stored neuron order."""
+    the optic chain (overlap) or after it, also with a capped persistent optic grid beside capped
+    staged LIF blocks; the oracle runs the stages serially on the engine's stored neuron order."""
     cfg = small_fly()
     B, T = 4, 120
     eng = WholeFly(cfg, B, device="cuda", seed=1, launch="step", overlap=overlap)
+    if capped:
+        eng.optic.launch, eng.optic.grid = "persistent", 20
+        eng.lif.staged, eng.lif.grid = True, 7
+        eng.lif._make_args()
+    eng.lif.defer = defer
     assert eng.overlapping == overlap
     a_pr = torch.from_numpy((np.random.default_rng(0).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
     eng.set_photoreceptors(a_pr)
