@@ -432,7 +432,10 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
       nc[q] = c[q];
       sp[q] = 0.0f;
       if (t >= W) continue;
-      const int i = (int)(t / k.batch), b = (int)(t - (long long)i * k.batch);
+      // the fused path keeps the 64-bit division: its register allocation (and occupancy) depends
+      // on it; the deferred path divides by multiply-shift
+      const int i = DEFER ? neuron_of(k, (int)t) : (int)(t / k.batch);
+      const int b = DEFER ? (int)t - i * k.batch : (int)(t - (long long)i * k.batch);
       iq[q] = i;
       bq[q] = b;
       const bool live = !(flags & FLYB_LIF_EPISODES) || s < k.fly_steps[b];
@@ -544,8 +547,10 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
     deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
 }
 
+// The deferred-delivery update at 1-2 items per thread is bounded to 64 registers (32 warps per SM
+// stay resident; at 4 items the bound would spill).
 template <int BLOCK, bool FIXED, int IPT, bool DEFER = false>
-__global__ void __launch_bounds__(BLOCK) lif_step_kernel(LifK k, int s) {
+__global__ void __launch_bounds__(BLOCK, (DEFER && IPT <= 2) ? 1024 / BLOCK : 1) lif_step_kernel(LifK k, int s) {
   __shared__ LifSmem<BLOCK * IPT> sm;
   const Clk clk = read_clock(k);
   lif_chunk<BLOCK, FIXED, IPT, DEFER>(k, clk, s, k.t_begin + (long long)blockIdx.x * BLOCK * IPT, sm);

@@ -35,8 +35,24 @@ def _time_us(fn, reps: int) -> float:
     return 1000.0 * s.elapsed_time(e) / reps
 
 
+def _graph_us(fn, reps: int = 20) -> float:
+    """Device microseconds of one fn() call, from a CUDA graph of `reps` calls (no host gaps)."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(reps):
+                fn()
+    torch.cuda.current_stream().wait_stream(s)
+    us = _time_us(g.replay, 5) / reps
+    del g
+    return us
+
+
 def breakdown(eng: WholeFly, reps: int) -> dict:
-    """Microseconds per stage of one whole-fly step, each stage repeated alone `reps` times."""
+    """Microseconds per stage of one whole-fly step, each stage repeated alone inside a CUDA graph
+    (so small kernels are not measured through host launch gaps)."""
     o = eng.cfg.optic
     rate, drive = eng.lif._st["rate"], eng.lif._st["drive"]
     stages = {
@@ -48,7 +64,14 @@ def breakdown(eng: WholeFly, reps: int) -> dict:
         "lif step": lambda: eng.lif.step(1),
         "whole step (eager)": lambda: eng.step(1),
     }
-    out = {k: _time_us(f, reps) for k, f in stages.items()}
+    for wpr in (1, 2, 4, 8):
+        stages[f"W_rs, {wpr} warps/row"] = (lambda w=wpr: spmm(eng.W_rs, rate, eng.optic.spk_in, x_div=100.0, x_lo=0.0,
+                                                              x_hi=3.0, alpha=o.gain_fb, y_index=eng.rs_rows,
+                                                              warps_per_row=w))
+        stages[f"W_sr, {wpr} warps/row"] = (lambda w=wpr: spmm(eng.W_sr, eng.optic.dr_out, drive, y_index=eng.sr_rows,
+                                                              alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv,
+                                                              y_hi=o.drive_clip_mv, warps_per_row=w))
+    out = {k: (_time_us(f, reps) if "eager" in k else _graph_us(f)) for k, f in stages.items()}
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     g = torch.cuda.CUDAGraph()
