@@ -223,11 +223,56 @@ def time_graph(g, reps) -> float:
 
 
 def kernel_roofline(eng, reps=20) -> dict:
-    """The LIF step and the optic substep timed alone with CUDA events (B=64)."""
+    """The LIF step and the optic substep timed alone with CUDA events (B=64), after one untimed
+    call of each (the first whole-range LIF step sizes its spike list)."""
+    eng.lif.step(1)
+    eng.optic.substeps(1, carry=True)
+    torch.cuda.synchronize()
     lif_ms = events_time(lambda: eng.lif.step(1), reps)
     opt_ms = events_time(lambda: eng.optic.substeps(1, carry=True), reps)
     lif_b, opt_b = eng.lif_bytes_per_step(), eng.optic_bytes_per_step()
     return {"lif_ms": lif_ms, "optic_ms": opt_ms, "lif_bytes": lif_b, "optic_bytes": opt_b}
+
+
+def measure_l2_gather(device, rows: int = 89_390, n_idx: int = 6_000_000) -> dict:
+    """L2 -> SM gather ceiling on this GPU: flyb_gather_probe reads n_idx random 256-byte rows of a
+    [rows][64] float array (the optic substep's dr gathers at 64 flies, L2-resident), best of 8 and
+    16 blocks per SM; TB/s of row bytes + index bytes."""
+    import ctypes as ct
+    from flyb200 import _abi
+    lib = _abi.lib()
+    g = torch.Generator(device="cpu").manual_seed(7)
+    idx = torch.randint(0, rows, (n_idx,), generator=g, dtype=torch.int32).to(device)
+    x = torch.zeros(rows, 64, device=device)
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    out = torch.empty(sms * 16 * 256, device=device)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    best = 0.0
+    for bps in (8, 16):
+        call = lambda: lib.flyb_gather_probe(ct.c_void_p(x.data_ptr()), rows, ct.c_void_p(idx.data_ptr()), n_idx,
+                                             ct.c_void_p(out.data_ptr()), bps, ct.c_void_p(stream))
+        for _ in range(3):
+            if call():
+                raise RuntimeError("flyb_gather_probe failed")
+        ms = events_time(call, 10)
+        best = max(best, (n_idx * 256 + n_idx * 4) / (ms / 1000.0) / 1e12)
+    return {"tbs": best, "rows": rows, "gathers": n_idx, "row_bytes": 256}
+
+
+def read_traffic() -> dict:
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the ncu captures
+    summarised in profiles/traffic.txt: one `<kernel> <bytes>` pair per line."""
+    tp = ROOT / "profiles" / "traffic.txt"
+    out = {}
+    if tp.exists():
+        for line in tp.read_text().splitlines():
+            parts = line.split()
+            if len(parts) >= 2 and not line.startswith("#"):
+                try:
+                    out[parts[0]] = float(parts[1])
+                except ValueError:
+                    pass
+    return out
 
 
 def measure_plain(cfg, device, steps, warmup):
@@ -419,10 +464,10 @@ def main() -> None:
     batch1 = N / (plain_ms / 1000.0)
     adj = measure_adjoint(device)
     e2e = measure_e2e(cfg, eng, device, args.steps)
-    traffic = None
-    tp = ROOT / "profiles" / "traffic.json"
-    if tp.exists():
-        traffic = json.loads(tp.read_text()).get(dom)
+    traffic = read_traffic().get(dom)
+    l2 = measure_l2_gather(device)
+    o = cfg.optic
+    optic_l2_bytes = int(o.W0.nnz) * BATCH * 4 + roof["optic_bytes"]     # dr gathers + the streamed bytes
     cpu = None
     if not args.no_cpu_baseline:
         cpu = cpu_port_rate(cfg, 8, 3, os.cpu_count() or 1)
@@ -443,7 +488,13 @@ def main() -> None:
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "lif_gbs": lif_gbs, "optic_gbs": opt_gbs,
                      "lif_ms": roof["lif_ms"], "optic_ms": roof["optic_ms"], "lif_bytes": roof["lif_bytes"],
-                     "optic_bytes": roof["optic_bytes"]},
+                     "optic_bytes": roof["optic_bytes"],
+                     "l2_gather": {"kernel": "optic step (B=64)", "bytes": optic_l2_bytes,
+                                   "achieved_tbs": optic_l2_bytes / (roof["optic_ms"] / 1000.0) / 1e12,
+                                   "peak_tbs": l2["tbs"],
+                                   "frac": optic_l2_bytes / (roof["optic_ms"] / 1000.0) / 1e12 / l2["tbs"],
+                                   "peak_source": "flyb_gather_probe, measured in this run",
+                                   "note": "the optic substep gathers nnz x 64 x 4 B of L2-resident dr"}},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "autotune": {k: {kk: vv for kk, vv in v.items()} for k, v in eng.tuned.items()},

@@ -102,10 +102,23 @@ struct Clk {
   int ring_pos, raster_pos;
 };
 
+// v mod m in [0, m) for m > 0: a compare when v already is in range (the clock keeps its positions
+// reduced), a 64-bit modulo only otherwise. Every thread reads the clock, so this stays cheap.
+__device__ __forceinline__ int wrap_pos(long long v, int m) {
+  if (v >= 0 && v < m) return (int)v;
+  const long long q = v % m;
+  return (int)(q < 0 ? q + m : q);
+}
+
+// (pos + d) mod m for 0 <= pos < m and d >= 0, in 32-bit arithmetic.
+__device__ __forceinline__ int slot_after(int pos, int d, int m) {
+  const int v = pos + d;
+  return v < m ? v : v % m;
+}
+
 __device__ __forceinline__ Clk read_clock(const LifK& k) {
   if (!k.clock) return Clk{k.step0, k.ring_pos, k.raster_pos};
-  const long long r = k.clock[1], h = k.clock[2];
-  return Clk{k.clock[0], (int)(((r % k.R) + k.R) % k.R), k.raster_slots > 0 ? (int)(((h % k.raster_slots) + k.raster_slots) % k.raster_slots) : 0};
+  return Clk{k.clock[0], wrap_pos(k.clock[1], k.R), k.raster_slots > 0 ? wrap_pos(k.clock[2], k.raster_slots) : 0};
 }
 
 // After the last step: advance the device clock and lower the per-fly remaining-step counters.
@@ -353,7 +366,7 @@ __device__ __forceinline__ void append_spikes(const LifK& k, int s, unsigned tx_
 template <bool FIXED>
 __global__ void __launch_bounds__(256) lif_scatter_kernel(LifK k, int s) {
   const Clk clk = read_clock(k);
-  const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
+  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
   const size_t slot = (size_t)k.n * k.batch;
   const long long n = (long long)*k.spike_n < k.spike_cap ? (long long)*k.spike_n : k.spike_cap;
   unsigned long long edges = 0;
@@ -384,8 +397,8 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
   using RingT = typename std::conditional<FIXED, long long, int>::type;
   const long long W = k.t_end;                         // items of this launch end here
   const long long t0 = base + (long long)threadIdx.x * IPT;
-  const int rs = (int)(((long long)clk.ring_pos + s) % k.R);
-  const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
+  const int rs = slot_after(clk.ring_pos, s, k.R);
+  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
   const size_t slot = (size_t)k.n * k.batch;            // ring slot stride
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const LifP& P = k.P;
@@ -537,7 +550,7 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
     for (int o = 1; o < LPW; o <<= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
     const long long wbase = base + (long long)warp * 32 * IPT;
     if (lane % LPW == 0 && wbase + (long long)(lane / LPW) * 32 < W) {
-      const size_t rslot = k.raster_slots > 0 ? (size_t)(((long long)clk.raster_pos + s) % k.raster_slots) : (size_t)s;
+      const size_t rslot = k.raster_slots > 0 ? (size_t)slot_after(clk.raster_pos, s, k.raster_slots) : (size_t)s;
       k.raster[rslot * k.words + (size_t)((wbase >> 5) + lane / LPW)] = v;
     }
   }
@@ -655,8 +668,8 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
   const size_t slot = (size_t)k.n * k.batch;                  // ring slot stride
   if ((long long)blockIdx.x >= nchunks) return;                 // block-uniform, before any copy
   const Clk clk = read_clock(k);
-  const int rs = (int)(((long long)clk.ring_pos + s) % k.R);
-  const int ws = (int)(((long long)clk.ring_pos + s + k.n_delay) % k.R);
+  const int rs = slot_after(clk.ring_pos, s, k.R);
+  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
   RingT* ring_rd = (RingT*)k.ring + (size_t)rs * slot;
   const LifP& P = k.P;
   const int flags = k.flags;
@@ -745,7 +758,7 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
         const unsigned word = __ballot_sync(0xffffffffu, fired);
         const int wfirst = (int)base + r * BLOCK + warp * 32;
         if (lane == 0 && wfirst < W) {
-          const size_t rslot = k.raster_slots > 0 ? (size_t)(((long long)clk.raster_pos + s) % k.raster_slots) : (size_t)s;
+          const size_t rslot = k.raster_slots > 0 ? (size_t)slot_after(clk.raster_pos, s, k.raster_slots) : (size_t)s;
           k.raster[rslot * k.words + (size_t)(wfirst >> 5)] = word;
         }
       }
@@ -1026,6 +1039,7 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.t_begin = a->n_first * a->batch;
   k.t_end = (a->n_first + count) * a->batch;
   k.nsteps = a->nsteps; k.ring_pos = ((a->ring_pos % k.R) + k.R) % k.R;
+  if (a->raster_slots < 0) return FLYB_EINVAL;
   k.words = (int)(((long long)a->n * a->batch + 31) / 32);
   k.step0 = a->step0; k.seed = a->seed;
   k.out_ptr = a->out_ptr; k.out_edge = (const int2*)a->out_edge;
@@ -1033,7 +1047,8 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.counts = a->counts; k.spikes = a->spikes; k.drive = a->drive; k.poisson_p = a->poisson_p;
   k.active = a->active; k.std_u = a->std_u; k.ring = a->ring; k.uniforms = a->uniforms; k.fly_steps = a->fly_steps;
   k.clock = a->clock;
-  k.raster = a->raster; k.raster_slots = a->raster_slots; k.raster_pos = a->raster_pos; k.fly0 = a->fly0;
+  k.raster = a->raster; k.raster_slots = a->raster_slots; k.fly0 = a->fly0;
+  k.raster_pos = a->raster_slots > 0 ? ((a->raster_pos % a->raster_slots) + a->raster_slots) % a->raster_slots : 0;
   k.events = a->events; k.status = a->status; k.sync = a->sync;
   k.spike_list = nullptr; k.spike_n = nullptr; k.spike_cap = 0;
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {

@@ -348,6 +348,23 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
     return FLYB_ETOOBIG;                                               \
   } while (0)
 
+// (F fly lanes, FPL flies per lane) of the held-input products: from 32 flies on, 4 flies per lane
+// so that a warp instruction covers 2-4 entries (the per-entry index and weight work is shared by
+// more products).
+#define FLYB_SPMM_DISPATCH(B, CALL)                                    \
+  do {                                                                 \
+    if ((B) == 1) { constexpr int F = 1, FPL = 1; return CALL; }       \
+    if ((B) <= 2) { constexpr int F = 2, FPL = 1; return CALL; }       \
+    if ((B) <= 4) { constexpr int F = 4, FPL = 1; return CALL; }       \
+    if ((B) <= 8) { constexpr int F = 8, FPL = 1; return CALL; }       \
+    if ((B) <= 16) { constexpr int F = 16, FPL = 1; return CALL; }     \
+    if ((B) <= 32) { constexpr int F = 8, FPL = 4; return CALL; }      \
+    if ((B) <= 64) { constexpr int F = 16, FPL = 4; return CALL; }     \
+    if ((B) <= 128) { constexpr int F = 32, FPL = 4; return CALL; }    \
+    if ((B) <= 256) { constexpr int F = 32, FPL = 8; return CALL; }    \
+    return FLYB_ETOOBIG;                                               \
+  } while (0)
+
 // (F fly lanes, FPL flies per lane, LPR lanes per row, U gathers in flight per lane, MINB blocks per
 // SM) of the optic substep for a batch; `variant` 0 is the default, the others are alternatives the
 // autotuner tries (more warps with fewer registers each, or wider lanes); an unknown variant is an
@@ -636,7 +653,7 @@ FLYB_API int flyb_spmm(const flyb_spmm_args* a, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   const int wpr = a->warps_per_row ? a->warps_per_row : 1;
   if (wpr != 1 && wpr != 2 && wpr != 4 && wpr != 8) return FLYB_EINVAL;
-  FLYB_BATCH_DISPATCH(a->batch, (run_spmm<F, FPL>(k, wpr, st)));
+  FLYB_SPMM_DISPATCH(a->batch, (run_spmm<F, FPL>(k, wpr, st)));
 }
 
 FLYB_API int launch_optic_dr(void** p, int n, int batch, void* stream) {

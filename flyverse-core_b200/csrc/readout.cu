@@ -76,6 +76,33 @@ __global__ void selftest_wait_kernel(const int* flag, int* status, long long spi
   if (threadIdx.x == 0 && blockIdx.x == 0) bounded_wait_ne(flag, 0, status, spins, 2, -1);
 }
 
+// Gather-rate probe: half-warps (16 lanes x float4) read random 256-byte rows x[idx[e]][0:64] of an
+// L2-resident array, 8 rows in flight per half-warp, and sum them. The access pattern of the optic
+// substep at 64 flies without its arithmetic: its rate bounds that kernel from above.
+__global__ void __launch_bounds__(256) gather_probe_kernel(const float4* __restrict__ x, int rows,
+                                                           const int* __restrict__ idx, int n_idx, float* out) {
+  constexpr int U = 8;
+  const int lane = threadIdx.x & 31, sub = lane >> 4, l = lane & 15;
+  const long long hw = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + sub;
+  const long long nhw = (long long)gridDim.x * blockDim.x / 16;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (long long e0 = hw; e0 < n_idx; e0 += nhw * U) {
+    int r[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const long long e = e0 + (long long)u * nhw;
+      const int v = e < n_idx ? __ldg(&idx[e]) : -1;
+      r[u] = (v >= 0 && v < rows) ? v : -1;
+    }
+    float4 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) v[u] = r[u] >= 0 ? __ldg(&x[(size_t)r[u] * 16 + l]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < U; ++u) { acc.x += v[u].x; acc.y += v[u].y; acc.z += v[u].z; acc.w += v[u].w; }
+  }
+  out[(size_t)blockIdx.x * blockDim.x + threadIdx.x] = acc.x + acc.y + acc.z + acc.w;
+}
+
 int lif_blocks_per_sm(int block);
 int optic_blocks_per_sm();
 int adjoint_blocks_per_sm();
@@ -120,6 +147,17 @@ FLYB_API int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_
   else if (kind == 2) b = adjoint_blocks_per_sm();
   else return FLYB_EINVAL;
   if (blocks_per_sm) *blocks_per_sm = b;
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_gather_probe(const float* x, int rows, const int* idx, int n_idx, float* out, int blocks_per_sm,
+                               void* stream) {
+  if (!x || !idx || !out || rows <= 0 || n_idx < 0 || blocks_per_sm < 1 || blocks_per_sm > 16) return FLYB_EINVAL;
+  if (reinterpret_cast<uintptr_t>(x) & 15) return FLYB_EINVAL;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  gather_probe_kernel<<<sms * blocks_per_sm, 256, 0, (cudaStream_t)stream>>>((const float4*)x, rows, idx, n_idx, out);
   return (int)cudaGetLastError();
 }
 

@@ -108,6 +108,7 @@ SIGNATURES = {
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
     "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
     "flyb_selftest_wait": [_VP, _VP, ct.c_longlong, _VP],
+    "flyb_gather_probe": [_VP, _I, _VP, _I, _VP, _I, _VP],
     "flyb_version": [],
     "flyb_abi_sizes": [ct.POINTER(_I), _I],
 }

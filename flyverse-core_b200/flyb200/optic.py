@@ -114,11 +114,16 @@ class DeviceCSR:
 
 
 def spmm_warps_per_row(nnz: int, rows: int, batch: int) -> int:
-    """Warps sharing one row of flyb_spmm: enough that one pass (U = 8 entries per lane group,
-    32 / F lane groups per warp with F = min(batch, 32) fly lanes) covers a row of mean length."""
+    """Warps sharing one row of flyb_spmm: enough that one pass (U entries per lane group, 32 / F
+    lane groups per warp; F, FPL as the library picks them for the batch) covers a row of mean
+    length."""
     if rows <= 0:
         return 1
-    per_pass = 8 * max(1, 32 // min(max(batch, 1), 32))
+    lanes = {1: 1, 2: 2, 4: 4, 8: 8, 16: 16}
+    f, fpl = next(((f, 1) for b, f in lanes.items() if batch <= b), None) or \
+        ((8, 4) if batch <= 32 else (16, 4) if batch <= 64 else (32, 4) if batch <= 128 else (32, 8))
+    unroll = 8 if fpl <= 2 else (4 if fpl == 4 else 2)
+    per_pass = unroll * (32 // f)
     mean = -(-nnz // rows)
     wpr = 1
     while wpr < 8 and wpr * per_pass < mean:

@@ -298,6 +298,14 @@ int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm);
  * status instead of a hang. No counterpart in the reference. */
 int flyb_selftest_wait(const int* flag, int* status, long long spins, void* stream);
 
+/* Measurement aid, no counterpart in the reference: gathers n_idx random rows of 64 floats
+ * (x[idx[e]][0:64], x is [rows][64], 16-byte aligned) the way the optic substep gathers dr at 64
+ * flies, without its arithmetic, with SMs x blocks_per_sm (1-16) blocks of 256 threads; `out`
+ * takes one float per thread (SMs x blocks_per_sm x 256). Timing it gives the L2 -> SM gather rate
+ * that bounds the optic kernel. Out-of-range indices are skipped. */
+int flyb_gather_probe(const float* x, int rows, const int* idx, int n_idx, float* out, int blocks_per_sm,
+                      void* stream);
+
 /* Library version string. */
 const char* flyb_version(void);
 

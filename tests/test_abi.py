@@ -11,7 +11,7 @@ HEADER = Path(__file__).resolve().parents[1] / "include" / "flyb200.h"
 
 def declared_functions() -> set[str]:
     text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
-    return set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(\w+)\s*\([^;{]*\)\s*;", text, flags=re.M))
+    return set(re.findall(r"^\s*(?:const\s+)?(?:long\s+long|\w+)\s*\*?\s*(\w+)\s*\([^;{]*\)\s*;", text, flags=re.M))
 
 
 def test_library_builds_and_exports_every_declared_symbol():

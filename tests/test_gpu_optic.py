@@ -311,3 +311,27 @@ def test_compat_lif_update_matches_torch_step():
     torch.testing.assert_close(br.spikes, spikes, rtol=0, atol=0)
     torch.testing.assert_close(br.spike_buf[1], spikes * before["res"], rtol=0, atol=0)
     torch.testing.assert_close(br.spike_counts, before["spike_counts"] + spikes, rtol=0, atol=0)
+
+
+def test_gather_probe_reads_every_row_once():
+    """flyb_gather_probe (the L2 gather-rate measurement of bench.py): with every element 1 the
+    thread sums add up to 64 per gathered row; out-of-range indices are skipped."""
+    import ctypes as ct
+    from flyb200 import _abi
+    rows, n_idx = 1000, 100_003
+    x = torch.ones(rows, 64, device="cuda")
+    idx = torch.randint(0, rows, (n_idx,), dtype=torch.int32, device="cuda")
+    idx[::1000] = rows + 5                                       # skipped
+    skipped = int((idx >= rows).sum().item())
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    out = torch.zeros(sms * 16 * 256, device="cuda")
+    lib = _abi.lib()
+    for bps in (1, 16):
+        out.zero_()
+        rc = lib.flyb_gather_probe(ct.c_void_p(x.data_ptr()), rows, ct.c_void_p(idx.data_ptr()), n_idx,
+                                   ct.c_void_p(out.data_ptr()), bps, ct.c_void_p(torch.cuda.current_stream().cuda_stream))
+        assert rc == 0
+        torch.cuda.synchronize()
+        assert out.double().sum().item() == 64.0 * (n_idx - skipped)
+    assert lib.flyb_gather_probe(ct.c_void_p(x.data_ptr()), rows, ct.c_void_p(idx.data_ptr()), n_idx,
+                                 ct.c_void_p(out.data_ptr()), 17, None) == _abi.EINVAL
