@@ -422,7 +422,9 @@ struct SpmmK {
 // entry groups part, part + WPR, ... of it, the partial sums meet in shared memory and the row's
 // first warp applies alpha, the clamp and the store. Lanes: F across the flies (FPL each), G = 32/F
 // entry groups per warp.
-template <int F, int FPL, int WPR>
+// XT: the input has a transform (x / x_div clamped to [x_lo, x_hi]); without one the products are
+// plain w * x.
+template <int F, int FPL, int WPR, bool XT>
 __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
   constexpr int G = 32 / F, RB = 8 / WPR;
   constexpr int U = Unroll<FPL>::U;
@@ -466,8 +468,10 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
 #pragma unroll
           for (int q = 0; q < FPL; ++q) {
             float x = xv[u][q];
-            if (k.x_div != 1.0f) x = x / k.x_div;     // x / 1 == x exactly: skip the IEEE division
-            x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
+            if (XT) {
+              if (k.x_div != 1.0f) x = x / k.x_div;   // x / 1 == x exactly: skip the IEEE division
+              x = x < k.x_lo ? k.x_lo : (x > k.x_hi ? k.x_hi : x);
+            }
             const float p = ww[u] * x;
             acc[q] = acc[q] + p;
           }
@@ -504,6 +508,18 @@ __global__ void __launch_bounds__(256) spmm_kernel(SpmmK k) {
   }
 }
 
+template <int F, int FPL, bool XT>
+static int run_spmm_xt(const SpmmK& k, int wpr, unsigned blocks, cudaStream_t st) {
+  switch (wpr) {
+    case 1: spmm_kernel<F, FPL, 1, XT><<<blocks, 256, 0, st>>>(k); break;
+    case 2: spmm_kernel<F, FPL, 2, XT><<<blocks, 256, 0, st>>>(k); break;
+    case 4: spmm_kernel<F, FPL, 4, XT><<<blocks, 256, 0, st>>>(k); break;
+    case 8: spmm_kernel<F, FPL, 8, XT><<<blocks, 256, 0, st>>>(k); break;
+    default: return FLYB_EINVAL;
+  }
+  return (int)cudaGetLastError();
+}
+
 template <int F, int FPL>
 static int run_spmm(const SpmmK& k0, int wpr, cudaStream_t st) {
   SpmmK k = k0;
@@ -511,14 +527,8 @@ static int run_spmm(const SpmmK& k0, int wpr, cudaStream_t st) {
   const long long rb = 8 / wpr;
   const unsigned blocks = (unsigned)((k.rows + rb - 1) / rb);
   if (!blocks) return 0;
-  switch (wpr) {
-    case 1: spmm_kernel<F, FPL, 1><<<blocks, 256, 0, st>>>(k); break;
-    case 2: spmm_kernel<F, FPL, 2><<<blocks, 256, 0, st>>>(k); break;
-    case 4: spmm_kernel<F, FPL, 4><<<blocks, 256, 0, st>>>(k); break;
-    case 8: spmm_kernel<F, FPL, 8><<<blocks, 256, 0, st>>>(k); break;
-    default: return FLYB_EINVAL;
-  }
-  return (int)cudaGetLastError();
+  const bool xt = k.x_div != 1.0f || k.x_lo > -INFINITY || k.x_hi < INFINITY;
+  return xt ? run_spmm_xt<F, FPL, true>(k, wpr, blocks, st) : run_spmm_xt<F, FPL, false>(k, wpr, blocks, st);
 }
 
 // ------------------------------------------------------------------ reference-compatible launchers

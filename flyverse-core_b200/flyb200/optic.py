@@ -113,10 +113,21 @@ class DeviceCSR:
         return t, torch.from_numpy(order.astype(np.int32)).to(device)
 
 
-def spmm_warps_per_row(nnz: int, rows: int, batch: int) -> int:
-    """Warps sharing one row of flyb_spmm: enough that one pass (U entries per lane group, 32 / F
-    lane groups per warp; F, FPL as the library picks them for the batch) covers a row of mean
-    length."""
+_SMS: dict = {}
+
+
+def _sm_count(device) -> int:
+    if device not in _SMS:
+        _SMS[device] = torch.cuda.get_device_properties(device).multi_processor_count
+    return _SMS[device]
+
+
+def spmm_warps_per_row(nnz: int, rows: int, batch: int, sms: int = 148) -> int:
+    """Warps sharing one row of flyb_spmm (1, 2, 4, 8; a block holds 8 warps): the fewest that
+    still give about two blocks per SM, or that keep a warp within 16 passes of U entries per lane
+    group over a row of mean length (F, FPL as the library picks them for the batch). Measured at
+    64 flies on the whole-fly coupling blocks: 3,885 rows of 50 entries run best at 1 warp per row,
+    1,787 rows of 20 at 2."""
     if rows <= 0:
         return 1
     lanes = {1: 1, 2: 2, 4: 4, 8: 8, 16: 16}
@@ -126,7 +137,7 @@ def spmm_warps_per_row(nnz: int, rows: int, batch: int) -> int:
     per_pass = unroll * (32 // f)
     mean = -(-nnz // rows)
     wpr = 1
-    while wpr < 8 and wpr * per_pass < mean:
+    while wpr < 8 and (rows * wpr / 8 < 2 * sms or mean > wpr * per_pass * 16):
         wpr *= 2
     return wpr
 
@@ -147,7 +158,7 @@ def spmm(M: DeviceCSR, x: torch.Tensor, y: torch.Tensor, *, x_index=None, x_div=
                       x_index=None if x_index is None else x_index.data_ptr(), x_rows=x.shape[0], x_div=x_div,
                       x_lo=x_lo, x_hi=x_hi, y=y.data_ptr(), y_index=None if y_index is None else y_index.data_ptr(),
                       y_rows=y.shape[0], alpha=alpha, y_lo=y_lo, y_hi=y_hi,
-                      warps_per_row=warps_per_row or spmm_warps_per_row(M.nnz, M.shape[0], B))
+                      warps_per_row=warps_per_row or spmm_warps_per_row(M.nnz, M.shape[0], B, _sm_count(x.device)))
     rc = _abi.lib().flyb_spmm(ct.byref(a), torch.cuda.current_stream(x.device).cuda_stream)
     if rc:
         raise RuntimeError(f"flyb_spmm: error {rc}")
