@@ -77,12 +77,13 @@ class WholeFly:
 
     @property
     def launches_per_step(self) -> int:
-        """Kernel launches of one step once running: two coupling products, the optic substep (its
-        dr carried over from the previous step), the LIF step (two ranges when overlapped) and its
-        device-clock advance (or one persistent launch)."""
-        if self.overlapping:
-            return 6
-        return 5 if self.lif.launch == "step" else 4
+        """Kernels launched by one step once running: two coupling products, the optic substep (its
+        dr carried over), the LIF update (two ranges when overlapped; each followed by its scatter
+        under deferred delivery) and the device-clock advance (or one persistent launch)."""
+        n = 6 if self.overlapping else (5 if self.lif.launch == "step" else 4)
+        if self.lif._defer_active():
+            n += 2 if self.overlapping else 1          # the scatter kernel of each LIF launch
+        return n
 
     @property
     def overlapping(self) -> bool:
