@@ -158,7 +158,8 @@ def events_time(fn, reps: int, flush=None) -> float:
 def build_engine(cfg, batch, device, launch, fly0=0):
     from flyb200.whole import WholeFly
     eng = WholeFly(cfg, batch, device=device, seed=1, launch=launch)
-    eng.lif._args.fly0 = fly0
+    eng.lif.fly0 = fly0              # this rank's flies draw their own Poisson streams
+    eng.lif._make_args()
     o = cfg.optic
     rad = torch.from_numpy(o.grating(0.0, batch, seed=fly0)).to(device)
     a_pr = photoreceptor_contrast(cfg, rad)
@@ -197,9 +198,9 @@ def capture(eng, steps: int):
 
 
 # ------------------------------------------------------------------ measurements
-def measure_batched(cfg, device, steps, warmup, fly0):
+def measure_batched(cfg, device, steps, warmup, fly0, batch=BATCH):
     from flyb200 import autotune
-    eng = build_engine(cfg, BATCH, device, "step", fly0)
+    eng = build_engine(cfg, batch, device, "step", fly0)
     eng.step(max(3, warmup))
     eng.tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
     eng.step(2)                    # the tuners restored the state: one step re-derives the carried dr
@@ -470,6 +471,14 @@ def main() -> None:
     opt_gbs = roof["optic_bytes"] / (roof["optic_ms"] / 1000.0) / 1e9
     dom = "lif" if roof["lif_ms"] >= roof["optic_ms"] else "optic"
     achieved = lif_gbs if dom == "lif" else opt_gbs
+    # the whole-fly configuration at 256 flies (its uneven-rollout variant runs through BatchSim)
+    n256 = min(args.steps, 40)
+    eng256, g256, c256, r256 = measure_batched(cfg, device, n256, args.warmup, fly0=0, batch=256)
+    ms256 = time_graph(g256, r256) / (c256 * r256)
+    batch256 = {"value": N * 256 / (ms256 / 1000.0), "ms_per_step": ms256, "steps": c256 * r256,
+                "autotune": {k: {kk: vv for kk, vv in v.items() if kk != "all"} for k, v in eng256.tuned.items()}}
+    del g256, eng256
+    torch.cuda.empty_cache()
     plain_eng, plain_ms = measure_plain(cfg, device, args.steps, args.warmup)
     batch1 = N / (plain_ms / 1000.0)
     adj = measure_adjoint(device)
@@ -489,6 +498,7 @@ def main() -> None:
         "batch1": {"value": batch1, "ms_per_step": plain_ms, "l2": "flushed between timed steps",
                    "launches": "one launch per kernel per step"},
         "batched_over_plain": value / world / batch1,
+        "batch256": batch256,
         "adjoint": adj,
         "synaptic_events_per_s": events_per_step * world * timed_steps / (ms / 1000.0),
         "roofline": {"bound": "hbm", "kernel": f"{dom} step (B=64)", "achieved": achieved, "peak": peaks["hbm_gbs"],

@@ -252,6 +252,7 @@ class Brain:
         a.grid = int(getattr(self, "grid", 0))        # persistent / staged launches: block cap
         a.items_per_thread = getattr(self, "items_per_thread", 0)
         a.staged = int(bool(getattr(self, "staged", False)))
+        a.fly0 = int(getattr(self, "fly0", 0))       # global index of local fly 0 (Philox key when sharded)
         a.raster_slots = self.n_delay
         a.seed = self.seed & 0xFFFFFFFFFFFFFFFF
         a.out_ptr, a.out_edge = self._out_ptr.data_ptr(), self._out_edge.data_ptr()

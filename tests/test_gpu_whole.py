@@ -132,3 +132,30 @@ def test_autotuner_keeps_state_and_installs_a_choice():
     assert autotune.tune_lif(eng.lif) is choice                   # cached per (graph, batch, activity)
     oc = autotune.tune_optic(eng.optic, steps=5)
     assert oc["launch"] in ("step", "persistent")
+
+
+def test_fly_shards_equal_one_batch_after_argument_rebuilds():
+    """The per-rank fly offset (Brain.fly0) keys the Poisson streams by the global fly index and
+    survives argument rebuilds (the autotuner's): two 4-fly shards of the spiking population equal
+    one 8-fly batch bit for bit."""
+    from flyb200.brain import Brain
+    cfg = small_fly()
+    p = LIFParams(**{**cfg.lif.params, "dt": 0.1})
+    hz = torch.as_tensor(cfg.lif.poisson_hz, dtype=torch.float32)
+    whole = Brain(cfg.lif.c, p, device="cuda", seed=11, batch=8, launch="step")
+    whole.record_activity = True
+    whole.set_poisson(cfg.sensory_idx, hz)
+    whole.step(80)
+    for lo in (0, 4):
+        part = Brain(cfg.lif.c, p, device="cuda", seed=11, batch=4, launch="step")
+        part.record_activity = True
+        part.set_poisson(cfg.sensory_idx, hz)
+        part.fly0 = lo
+        part._make_args()
+        part.items_per_thread = 1                          # another rebuild, as the autotuner does
+        part._make_args()
+        part.step(80)
+        torch.cuda.synchronize()
+        assert whole.spike_counts.sum().item() > 0
+        assert torch.equal(part.spike_counts, whole.spike_counts[lo:lo + 4])
+        assert torch.equal(part._st["v"], whole._st["v"][:, lo:lo + 4])
