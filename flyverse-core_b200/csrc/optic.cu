@@ -402,6 +402,9 @@ static int run_optic(const OpticK& k, int launch, int grid_cap, cudaStream_t st)
     }                                                                                             \
     if ((B) <= 256) {                                                                             \
       if ((V) == 0) { constexpr int F = 32, FPL = 8, LPR = 32, U = 2, MINB = 1; return CALL; }    \
+      if ((V) == 1) { constexpr int F = 32, FPL = 8, LPR = 32, U = 2, MINB = 4; return CALL; }    \
+      if ((V) == 3) { constexpr int F = 32, FPL = 8, LPR = 32, U = 1, MINB = 6; return CALL; }    \
+      if ((V) == 5) { constexpr int F = 32, FPL = 8, LPR = 32, U = 1, MINB = 8; return CALL; }    \
       return FLYB_EINVAL;                                                                         \
     }                                                                                             \
     return FLYB_ETOOBIG;                                                                          \

@@ -55,7 +55,8 @@ def test_fused_substeps_match_oracle(batch, launch):
 
 
 @pytest.mark.parametrize("batch,variant", [(1, 1), (1, 2), (1, 3), (1, 4), (64, 1), (64, 2), (64, 3), (64, 4),
-                                           (64, 5), (100, 1), (100, 3), (48, 3)])
+                                           (64, 5), (100, 1), (100, 3), (48, 3), (256, 1), (256, 3), (256, 5),
+                                           (200, 3)])
 @pytest.mark.parametrize("launch", ["step", "persistent"])
 def test_kernel_shape_variants_match_oracle(batch, variant, launch):
     """Every kernel shape the autotuner may pick (flyb_optic_args.variant) against the FP32 oracle."""
