@@ -45,6 +45,7 @@ struct LifK {
   int4* spike_list;   // deferred delivery: {fly, first edge, edges, x bits} per chunk of a spiker's edges
   unsigned* spike_n;  // entries appended this step
   long long spike_cap;
+  const float* __restrict__ adapt_jump;   // per-neuron adaptation jump, or null (P.jump)
   LifP P;
 };
 
@@ -222,7 +223,11 @@ __device__ __forceinline__ float lif_update(const LifK& k, const Clk& clk, int s
   v = v1;
   ref = r1;
   // 4. adaptation, depression, counters, rate (brain.py:853-868)
-  if (flags & FLYB_LIF_ADAPT) { float a1 = ad * P.a_ad; a1 = a1 + spike * P.jump; ad = a1; }
+  if (flags & FLYB_LIF_ADAPT) {
+    float a1 = ad * P.a_ad;
+    a1 = a1 + spike * (k.adapt_jump ? __ldg(&k.adapt_jump[i]) : P.jump);
+    ad = a1;
+  }
   x = spike;
   if (flags & FLYB_LIF_STD) {
     float r2 = rr;
@@ -498,7 +503,11 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
       ref[q] = r1;
       sp[q] = spike;
       // 4. adaptation, depression, counters, rate (brain.py:853-868)
-      if (flags & FLYB_LIF_ADAPT) { float a1 = ad[q] * P.a_ad; a1 = a1 + spike * P.jump; ad[q] = a1; }
+      if (flags & FLYB_LIF_ADAPT) {
+        float a1 = ad[q] * P.a_ad;
+        a1 = a1 + spike * (k.adapt_jump ? __ldg(&k.adapt_jump[i]) : P.jump);
+        ad[q] = a1;
+      }
       float x = spike;
       if (flags & FLYB_LIF_STD) {
         float r2 = rr[q];
@@ -1051,6 +1060,7 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.raster_pos = a->raster_slots > 0 ? ((a->raster_pos % a->raster_slots) + a->raster_slots) % a->raster_slots : 0;
   k.events = a->events; k.status = a->status; k.sync = a->sync;
   k.spike_list = nullptr; k.spike_n = nullptr; k.spike_cap = 0;
+  k.adapt_jump = a->adapt_jump;
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
     if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP || a->staged)

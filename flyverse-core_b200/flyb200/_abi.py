@@ -44,7 +44,8 @@ class LifArgs(ct.Structure):
                 ("rate", _VP), ("counts", _VP), ("spikes", _VP), ("drive", _VP), ("poisson_p", _VP),
                 ("active", _VP), ("std_u", _VP), ("params", _VP), ("ring", _VP), ("uniforms", _VP),
                 ("fly_steps", _VP), ("clock", _VP), ("raster", _VP), ("events", _VP), ("status", _VP),
-                ("sync", _VP), ("spike_list", _VP), ("spike_n", _VP), ("spike_cap", ct.c_longlong)]
+                ("sync", _VP), ("spike_list", _VP), ("spike_n", _VP), ("spike_cap", ct.c_longlong),
+                ("adapt_jump", _VP)]
 
 
 class OpticArgs(ct.Structure):

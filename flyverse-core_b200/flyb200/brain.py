@@ -78,7 +78,7 @@ _STATE = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_cou
 LAUNCHES = {"step": _abi.LAUNCH_STEP, "persistent": _abi.LAUNCH_PERSISTENT}
 
 
-def lif_coefficients(p: LIFParams, std_on: bool) -> np.ndarray:
+def lif_coefficients(p: LIFParams, std_on: bool, adapt_on: bool | None = None) -> np.ndarray:
     """The float32 coefficient vector of the native step (the reference's `_cuda_P`, brain.py:493-520,
     plus tau_syn's decay and w_syn), with the exponentials taken in double as the reference does."""
     a_r = math.exp(-p.dt / p.rate_tau)
@@ -87,7 +87,8 @@ def lif_coefficients(p: LIFParams, std_on: bool) -> np.ndarray:
     P[_abi.P_A_M], P[_abi.P_A_S] = math.exp(-p.dt / p.tau_m), math.exp(-p.dt / p.tau_syn)
     P[_abi.P_DT], P[_abi.P_T_REF] = p.dt, p.t_ref
     P[_abi.P_ADAPT_JUMP] = p.adapt_jump
-    P[_abi.P_A_AD] = math.exp(-p.dt / p.adapt_tau) if p.adapt_jump > 0 else 0.0
+    adapt_on = p.adapt_jump > 0 if adapt_on is None else adapt_on       # per-type jumps keep the decay on
+    P[_abi.P_A_AD] = math.exp(-p.dt / p.adapt_tau) if adapt_on else 0.0
     P[_abi.P_A_STD] = math.exp(-p.dt / p.std_tau) if std_on else 1.0
     P[_abi.P_A_R], P[_abi.P_RATE_GAIN] = a_r, (1 - a_r) * 1000.0 / p.dt
     P[_abi.P_W_SYN] = p.w_syn
@@ -128,8 +129,6 @@ def _unsupported(p: LIFParams, metal_kernels, cuda_kernels, cuda_sparse) -> None
         raise NotImplementedError("per-module clocks (dt_by_module) are not in the native LIF step")
     if p.receptor_model == "full":
         raise NotImplementedError("the slow receptor term (receptor_model='full') is not in the native LIF step")
-    if (DEFAULT_ADAPT_BY_TYPE if p.adapt_by_type is None else p.adapt_by_type):
-        raise NotImplementedError("per-type adaptation (adapt_by_type) is not in the native LIF step")
     if p.weight_dtype not in ("float32", "float16"):
         raise ValueError("weight_dtype must be float32 or float16")
     if p.event_driven is False:
@@ -175,9 +174,13 @@ class Brain:
         self._a_m = math.exp(-p.dt / p.tau_m)
         self._a_s = math.exp(-p.dt / p.tau_syn)
         self._a_r = math.exp(-p.dt / p.rate_tau)
-        self._a_ad = math.exp(-p.dt / p.adapt_tau) if p.adapt_jump > 0 else 0.0
+        # per-type adaptation (brain.py:497-506): a per-neuron jump, and the decay always on
+        adapt_map = DEFAULT_ADAPT_BY_TYPE if p.adapt_by_type is None else p.adapt_by_type
+        self.adapt_jump_vec = torch.from_numpy(per_type(c, adapt_map, p.adapt_jump)).to(dev) if adapt_map else None
+        self._adapt_on = p.adapt_jump > 0 or self.adapt_jump_vec is not None
+        self._a_ad = math.exp(-p.dt / p.adapt_tau) if self._adapt_on else 0.0
         self._a_std = math.exp(-p.dt / p.std_tau) if self._std_on else 1.0
-        self._P = lif_coefficients(p, self._std_on)
+        self._P = lif_coefficients(p, self._std_on, self._adapt_on)
         # state: [N][B] storage, (B, N) public views
         self._st = {k: torch.zeros(N, B, device=dev) for k in _STATE}
         self._st["v"].fill_(p.v_rest)
@@ -264,6 +267,7 @@ class Brain:
         a.params = self._P.ctypes.data
         a.ring, a.clock, a.raster = self.ring.data_ptr(), self._clock.data_ptr(), self._hist.data_ptr()
         a.events, a.status, a.sync = self._events.data_ptr(), self._status.data_ptr(), self._sync.data_ptr()
+        a.adapt_jump = None if self.adapt_jump_vec is None else self.adapt_jump_vec.data_ptr()
         self._args = a
         self._lists = {}          # deferred-delivery lists per neuron range, sized on first use
 
@@ -299,7 +303,7 @@ class Brain:
             f |= _abi.LIF_STD
         if self.record_activity:
             f |= _abi.LIF_COUNTS
-        if self.p.adapt_jump > 0:
+        if self._adapt_on:
             f |= _abi.LIF_ADAPT
         if self.cuda_compact:
             f |= _abi.LIF_SKIP_FROZEN

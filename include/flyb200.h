@@ -150,6 +150,9 @@ typedef struct flyb_lif_args {
   void* spike_list;      /* FLYB_LIF_DEFER_DELIVERY: [spike_cap] int4 entries (device)  */
   unsigned* spike_n;     /* FLYB_LIF_DEFER_DELIVERY: one device word (reset each step)  */
   long long spike_cap;   /* entries spike_list holds: flyb_lif_spike_capacity(a) or more */
+  const float* adapt_jump; /* optional [n]: per-neuron adaptation jump (mV per spike) under
+                            FLYB_LIF_ADAPT, the reference's adapt_by_type (brain.py:497-506);
+                            null = params[FLYB_P_ADAPT_JUMP] for every neuron             */
 } flyb_lif_args;
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);

@@ -126,7 +126,11 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     if (fired) { v = v_reset; ref = t_ref; }
     a->v[t] = v; a->refrac[t] = ref; a->spikes[t] = spike;
     /* 4. adaptation, depression, counters, rate (brain.py:853-868) */
-    if (flags & FLYB_LIF_ADAPT) { float ad = a->adapt[t] * a_ad; ad = ad + spike * jump; a->adapt[t] = ad; }
+    if (flags & FLYB_LIF_ADAPT) {
+      float ad = a->adapt[t] * a_ad;
+      ad = ad + spike * (a->adapt_jump ? a->adapt_jump[i] : jump);
+      a->adapt[t] = ad;
+    }
     float x = spike;
     if (flags & FLYB_LIF_STD) {
       float res = a->res[t];

@@ -13,6 +13,8 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
   lif_19cell.npz  the same Brain with the default model constants (receptor_model=None) on the
                   19-cell graph of tests/test_bit_identity.py::graph(), batch 2, depression and
                   adaptation on: the shaped weights, rasters and final state.
+  lif_19cell_adapt_by_type.npz  the same run with per-type adaptation jumps (ADAPT_BY_TYPE, the
+                  reference's adapt_by_type): its per-neuron jump vector, rasters and final state.
   optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
                   of tests/test_optic_hooks.py::hex_graph(), batch 2, three frames.
   optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
@@ -85,12 +87,15 @@ def _table(n: pd.DataFrame) -> dict:
         {"nrn_bodyId": n.bodyId.to_numpy().astype(np.int64)}
 
 
-def lif_19cell(ref) -> dict:
+ADAPT_BY_TYPE = {"^ORN_": 3.0, "^JO-": 0.4, "^DNp": 2.5}
+
+
+def lif_19cell(ref, adapt_by_type=None) -> dict:
     brain = ref["brain"]
     tb = ref["test_bit_identity"]
     c = tb.graph()
     B, steps, seed = 2, 400, 7
-    p = brain.LIFParams(receptor_model=None, event_driven=True)
+    p = brain.LIFParams(receptor_model=None, event_driven=True, adapt_by_type=adapt_by_type)
     b = brain.Brain(c, p, device="cpu", seed=seed, batch=B)
     frozen = np.flatnonzero((c.neurons.superclass == "ol_intrinsic").to_numpy())
     b.freeze(frozen)
@@ -115,7 +120,11 @@ def lif_19cell(ref) -> dict:
                                "steps": np.int64(steps), "batch": np.int64(B)}
     for key in ("v", "g", "refrac", "adapt", "res", "rate", "spike_counts", "spikes"):
         out[f"final_{key}"] = getattr(b, key).numpy().copy()
-    print(f"lif_19cell: {int(ras.sum())} spikes, {W.nnz} shaped entries")
+    if adapt_by_type:
+        out["adapt_jump_vec"] = b.adapt_jump_vec.numpy().copy()
+        out["adapt_patterns"] = np.array(list(adapt_by_type), dtype="U")
+        out["adapt_values"] = np.array(list(adapt_by_type.values()), np.float32)
+    print(f"lif_19cell (adapt_by_type={adapt_by_type}): {int(ras.sum())} spikes, {W.nnz} shaped entries")
     return out
 
 
@@ -180,6 +189,7 @@ def optic_synth(ref) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--only", default=None, help="regenerate one fixture (its file stem)")
     args = ap.parse_args()
     sys.path.insert(1, args.reference)
     sys.path.insert(2, str(Path(args.reference) / "tests"))
@@ -189,10 +199,12 @@ def main() -> None:
                                                       ("test_bit_identity", "test_bit_identity"),
                                                       ("test_optic_hooks", "test_optic_hooks"))}
     torch.set_num_threads(1)
-    np.savez_compressed(HERE / "lif_c1.npz", **lif_c1(ref))
-    np.savez_compressed(HERE / "lif_19cell.npz", **lif_19cell(ref))
-    np.savez_compressed(HERE / "optic_hex.npz", **optic_hex(ref))
-    np.savez_compressed(HERE / "optic_synth.npz", **optic_synth(ref))
+    fixtures = {"lif_c1": lambda: lif_c1(ref), "lif_19cell": lambda: lif_19cell(ref),
+                "lif_19cell_adapt_by_type": lambda: lif_19cell(ref, ADAPT_BY_TYPE),
+                "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref)}
+    for name, make in fixtures.items():
+        if args.only in (None, name):
+            np.savez_compressed(HERE / f"{name}.npz", **make())
 
 
 if __name__ == "__main__":

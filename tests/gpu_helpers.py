@@ -13,7 +13,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False):
+                   device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False, adapt_jump=None):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -41,6 +41,8 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
                      params=P.ctypes.data, ring=ring.data_ptr(), uniforms=None if uni is None else uni.data_ptr(),
                      fly_steps=None if fs is None else fs.data_ptr(), raster=None if r is None else r.data_ptr(),
                      events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr() if with_sync else None)
+    aj = None if adapt_jump is None else torch.from_numpy(np.ascontiguousarray(adapt_jump, np.float32)).to(dev)
+    a.adapt_jump = None if aj is None else aj.data_ptr()
     if defer:
         a.flags |= _abi.LIF_DEFER_DELIVERY
         cap = int(_abi.lib().flyb_lif_spike_capacity(ct.byref(a)))

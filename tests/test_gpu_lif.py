@@ -33,10 +33,15 @@ def case_c1(ring="auto", regime_seed=1, drive=6.5):
                 nsteps=cfg.steps, uniforms=np.ascontiguousarray(U))
 
 
-def case_19cell():
-    z = golden("lif_19cell")
+def _abt(z):
+    """The fixture's adapt_by_type map, or None."""
+    return dict(zip(z["adapt_patterns"].tolist(), z["adapt_values"].tolist())) if "adapt_patterns" in z else None
+
+
+def case_19cell(fixture="lif_19cell"):
+    z = golden(fixture)
     c = connectome_from_fixture(z)
-    p = LIFParams(receptor_model=None)
+    p = LIFParams(receptor_model=None, adapt_by_type=_abt(z))
     W = sp.csr_matrix((z["shaped_data"], z["shaped_indices"], z["shaped_indptr"]), shape=(c.n, c.n))
     ptr, edges, mode = out_edges(W, p.w_syn, "auto", std_on=True)
     B, T = int(z["batch"]), int(z["steps"])
@@ -51,8 +56,9 @@ def case_19cell():
     U = torch_uniforms(int(z["seed"]), T, (B, c.n)).transpose(0, 2, 1)
     flags = (_abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD |
              _abi.LIF_SKIP_FROZEN)
-    return dict(state=st, ptr=ptr, edges=edges, P=lif_coefficients(p, True), n_delay=4, flags=flags, nsteps=T,
-                uniforms=np.ascontiguousarray(U))
+    jumps = per_type(c, p.adapt_by_type, p.adapt_jump) if p.adapt_by_type else None
+    return dict(state=st, ptr=ptr, edges=edges, P=lif_coefficients(p, True, True), n_delay=4, flags=flags, nsteps=T,
+                uniforms=np.ascontiguousarray(U), adapt_jump=jumps)
 
 
 def case_random(batch=64, n=3000, edges=60_000, steps=200, episodes=False, fixed=False, seed=3, std=False,
@@ -90,7 +96,7 @@ def _compare(case, launch, block, grid=0, ipt=0, with_sync=True, staged=0, defer
     fs_ref = None if case.get("fly_steps") is None else case["fly_steps"].copy()
     fs_gpu = None if fs_ref is None else fs_ref.copy()
     kw = dict(n_delay=case["n_delay"], flags=case["flags"], nsteps=case["nsteps"], seed=case.get("seed", 0),
-              uniforms=case["uniforms"], raster=True)
+              uniforms=case["uniforms"], raster=True, adapt_jump=case.get("adapt_jump"))
     r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], fly_steps=fs_ref, **kw)
     r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], fly_steps=fs_gpu, launch=launch,
                                    block=block, grid=grid, items_per_thread=ipt, with_sync=with_sync, staged=staged,
@@ -112,8 +118,9 @@ def test_config1_native_equals_oracle(launch, ring):
 
 
 @pytest.mark.parametrize("launch,block", [(STEP, 128), (PERS, 256), (PERS, 512)])
-def test_19cell_depression_adaptation_native_equals_oracle(launch, block):
-    _compare(case_19cell(), launch, block)
+@pytest.mark.parametrize("fixture", ["lif_19cell", "lif_19cell_adapt_by_type"])
+def test_19cell_depression_adaptation_native_equals_oracle(launch, block, fixture):
+    _compare(case_19cell(fixture), launch, block)
 
 
 @pytest.mark.parametrize("launch,block,grid", [(STEP, 256, 0), (PERS, 256, 0), (PERS, 128, 7), (PERS, 512, 0)])
@@ -259,11 +266,13 @@ def test_brain_config1_rasters_equal_reference_golden():
         b.check()
 
 
-def test_brain_19cell_drop_in_equals_reference_golden():
-    z = golden("lif_19cell")
+@pytest.mark.parametrize("fixture", ["lif_19cell", "lif_19cell_adapt_by_type"])
+def test_brain_19cell_drop_in_equals_reference_golden(fixture):
+    z = golden(fixture)
     c = connectome_from_fixture(z)
     B, T = int(z["batch"]), int(z["steps"])
-    b = Brain(c, LIFParams(receptor_model=None), device="cuda", seed=int(z["seed"]), batch=B, launch="step")
+    b = Brain(c, LIFParams(receptor_model=None, adapt_by_type=_abt(z)), device="cuda", seed=int(z["seed"]), batch=B,
+              launch="step")
     b.freeze(z["frozen"])
     b.prune(z["frozen"])
     b.record_activity = True

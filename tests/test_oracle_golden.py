@@ -63,10 +63,11 @@ def test_lif_config1_fixed_ring_matches_reference():
     np.testing.assert_allclose(st.v[:, 0], z["drive65_v"], rtol=0, atol=2e-5)
 
 
-def _nineteen():
-    z = golden("lif_19cell")
+def _nineteen(name="lif_19cell"):
+    z = golden(name)
     c = connectome_from_fixture(z)
-    p = LIFParams(receptor_model=None)
+    abt = dict(zip(z["adapt_patterns"].tolist(), z["adapt_values"].tolist())) if "adapt_patterns" in z else None
+    p = LIFParams(receptor_model=None, adapt_by_type=abt)
     return z, c, p
 
 
@@ -83,9 +84,11 @@ def test_lif_19cell_weights_identical_to_reference():
     np.testing.assert_array_equal(W.data, z["shaped_data"])        # float32 bit for bit
 
 
-def test_lif_19cell_rasters_match_reference():
-    """Default model constants: fan-in scale, cap, gains, adaptation, depression on ORNs -> Q32.32 ring."""
-    z, c, p = _nineteen()
+@pytest.mark.parametrize("fixture", ["lif_19cell", "lif_19cell_adapt_by_type"])
+def test_lif_19cell_rasters_match_reference(fixture):
+    """Default model constants: fan-in scale, cap, gains, adaptation, depression on ORNs -> Q32.32 ring;
+    and the same with per-type adaptation jumps (adapt_by_type)."""
+    z, c, p = _nineteen(fixture)
     import scipy.sparse as sp
     W = sp.csr_matrix((z["shaped_data"], z["shaped_indices"], z["shaped_indptr"]), shape=(c.n, c.n))
     u = per_type(c, DEFAULT_STD_U_BY_TYPE, p.std_u)
@@ -103,8 +106,12 @@ def test_lif_19cell_rasters_match_reference():
     U = torch_uniforms(int(z["seed"]), T, (B, n))
     assert sha(U) == str(z["uniform_sha"])
     flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD | _abi.LIF_SKIP_FROZEN
-    r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True), n_delay=4, flags=flags, nsteps=T,
-                          uniforms=U.transpose(0, 2, 1), raster=True)
+    jumps = None
+    if p.adapt_by_type:
+        jumps = per_type(c, p.adapt_by_type, p.adapt_jump)
+        np.testing.assert_array_equal(jumps, z["adapt_jump_vec"])              # the reference's per-neuron jumps
+    r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True, True), n_delay=4, flags=flags, nsteps=T,
+                          uniforms=U.transpose(0, 2, 1), raster=True, adapt_jump=jumps)
     ras = unpack(r, n * B).reshape(T, n, B).transpose(0, 2, 1)
     assert ras.sum() > 20
     np.testing.assert_array_equal(ras, z["raster"])
