@@ -17,6 +17,19 @@ __global__ void ref_means_kernel(const int* __restrict__ ptr, const int* __restr
   out[(size_t)b * stride + k] = count ? sum / count : 0.0;
 }
 
+// Native-layout motor readout: rates are [n][batch] (fly-minor); thread (k, b) sums group k of fly b
+// in member order in double, so consecutive threads of a group read consecutive flies.
+__global__ void group_means_kernel(const int* __restrict__ ptr, const int* __restrict__ idx,
+                                   const float* __restrict__ rates, double* out, int groups, int batch) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)groups * batch) return;
+  const int k = (int)(t / batch), b = (int)(t - (long long)k * batch);
+  double sum = 0.0;
+  for (int j = ptr[k]; j < ptr[k + 1]; ++j) sum += (double)rates[(size_t)idx[j] * batch + b];
+  const int count = ptr[k + 1] - ptr[k];
+  out[(size_t)b * groups + k] = count ? sum / count : 0.0;
+}
+
 struct PhotoK {
   int n_pr, n_col, batch;
   const float* __restrict__ rad; const int* __restrict__ pr_column; const float* __restrict__ sens;
@@ -116,6 +129,17 @@ FLYB_API int launch_means(void** p, int n, int groups, int batch, int stride, vo
   if (total > 0)
     ref_means_kernel<<<(unsigned)((total + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
         (int*)p[0], (int*)p[1], (float*)p[2], (double*)p[3], n, groups, batch, stride);
+  return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_group_means(const int* ptr, const int* idx, const float* rates, double* out, int groups, int batch,
+                              void* stream) {
+  if (!ptr || !rates || !out || groups < 0 || batch <= 0) return FLYB_EINVAL;
+  const long long total = (long long)groups * batch;
+  if (total >= (1ll << 31)) return FLYB_ETOOBIG;
+  if (total)
+    group_means_kernel<<<(unsigned)((total + 127) / 128), 128, 0, (cudaStream_t)stream>>>(ptr, idx, rates, out, groups,
+                                                                                          batch);
   return (int)cudaGetLastError();
 }
 

@@ -107,6 +107,7 @@ SIGNATURES = {
     "flyb_spmm": [ct.POINTER(SpmmArgs), _VP],
     "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
+    "flyb_group_means": [_VP, _VP, _VP, _VP, _I, _I, _VP],
     "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
     "flyb_selftest_wait": [_VP, _VP, ct.c_longlong, _VP],
     "flyb_gather_probe": [_VP, _I, _VP, _I, _VP, _I, _VP],

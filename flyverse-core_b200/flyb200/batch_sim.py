@@ -47,6 +47,7 @@ class BatchSim:
         self.episode_frames = episode_frames
         self.frames_left = self._draw(self.B)
         self.groups = groups or {}
+        self.fb.set_motor(self.groups or None)
         self.stimulus = stimulus
         self.stats = EpisodeStats()
         self.frame = 0
@@ -64,7 +65,7 @@ class BatchSim:
             for name, (idx, hz) in (inputs or {}).items():
                 self.fb.set_input(name, idx, hz)
         self.fb.step(self.FRAME_MS)
-        out = self.fb.motor(self.groups) if self.groups else {}
+        out = self.fb.motor() if self.groups else {}
         self.frame += 1
         self.stats.frames += self.B
         self.frames_left -= 1

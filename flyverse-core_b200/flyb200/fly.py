@@ -8,16 +8,20 @@ from `stimulate` end on a LIF step boundary, and with `cuda_graphs=True` each di
 Captured frames advance the device step clock themselves, so replays draw fresh Poisson numbers.
 Senses, motor programs and the body of the reference are outside the brain step; inputs arrive as
 Poisson rates (`set_input`, `stimulate`) and radiance (`vision`), outputs as group means (`motor`).
+Groups registered with `set_motor` are reduced at the end of every frame, inside the captured
+graph, straight from the fly-minor rate state, and copied asynchronously into pinned host memory;
+`motor()` then only waits for that copy.
 """
 from __future__ import annotations
 
+import ctypes as ct
 import math
 from dataclasses import asdict
 
 import numpy as np
 import torch
 
-from . import cuda as fcuda
+from . import _abi
 from .brain import Brain, LIFParams
 from .connectome import PHOTORECEPTOR_TYPES
 from .optic import OpticLobe, OpticParams
@@ -58,6 +62,8 @@ class FlyBrain:
         self._inputs_on = {}
         self._pulses = []
         self._activity_ms = np.zeros(self.B)
+        self._motor = None                # (names, ptr, idx, device means, pinned means, event)
+        self._motor_fresh = False
 
     @property
     def t(self) -> float:
@@ -126,6 +132,7 @@ class FlyBrain:
             return 0.0
         if self.cuda_graphs and not any(p[2] < self.t + elapsed - 1e-9 for p in self._pulses):
             self._graph_frame(steps)
+            self._mark_readout()
             if self._pulses:
                 self._refresh_poisson()
             self._activity_ms += elapsed
@@ -141,6 +148,8 @@ class FlyBrain:
             remaining -= count
             if self._pulses:
                 self._refresh_poisson()
+        self._readout()
+        self._mark_readout()
         self._activity_ms += elapsed
         return elapsed
 
@@ -151,6 +160,7 @@ class FlyBrain:
     def _frame(self, steps: int) -> None:
         self._vision_frame(steps * self.brain.p.dt)
         self.brain.step(steps)
+        self._readout()
 
     def _graph_frame(self, steps: int) -> None:
         b, o = self.brain, self.optic
@@ -184,17 +194,81 @@ class FlyBrain:
             o._pending_ms = max(0.0, total - int(math.floor((total + 1e-9) / o.p.dt_ms)) * o.p.dt_ms)
 
     # ------------------------------------------------------------------ outputs
-    def motor(self, groups: dict) -> dict:
-        """{name: (B,) mean rate in Hz} of named neuron groups, one GPU reduction and one copy
-        (the native motor readout, flyverse/motor.py:232-270)."""
+    def _group_table(self, groups: dict):
         names = list(groups)
-        idx = [np.asarray(groups[k], np.int64) for k in names]
+        idx = [np.asarray(groups[k], np.int64).ravel() for k in names]
+        for i in idx:
+            if len(i) and (i.min() < 0 or i.max() >= self.brain.n):
+                raise IndexError("motor group index out of range")
         ptr = torch.tensor(np.r_[0, np.cumsum([len(i) for i in idx])], dtype=torch.int32, device=self.device)
         flat = torch.tensor(np.concatenate(idx) if idx else np.zeros(0, np.int64), dtype=torch.int32, device=self.device)
-        means = fcuda.group_means(ptr, flat, self.brain.rate.contiguous()).cpu().numpy()
+        return names, ptr, flat
+
+    def _launch_means(self, ptr, flat, out) -> None:
+        groups = ptr.numel() - 1
+        if not groups:
+            return
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        rc = _abi.lib().flyb_group_means(ct.c_void_p(ptr.data_ptr()), ct.c_void_p(flat.data_ptr()),
+                                         ct.c_void_p(self.brain._st["rate"].data_ptr()), ct.c_void_p(out.data_ptr()),
+                                         groups, self.B, ct.c_void_p(stream))
+        if rc:
+            raise RuntimeError(f"flyb_group_means: error {rc}")
+
+    def set_motor(self, groups: dict | None) -> None:
+        """Register the motor groups that every frame reads out (None to stop): {name: neuron
+        indices}. The group means are reduced on the device at the end of each frame, inside the
+        captured graph, and copied without a synchronisation into pinned host memory."""
+        self._graphs.clear()                    # captured frames hold the previous readout buffers
+        self._motor, self._motor_fresh = None, False
+        if not groups:
+            return
+        names, ptr, flat = self._group_table(groups)
+        out = torch.zeros(self.B, len(names), dtype=torch.float64, device=self.device)
+        host = torch.zeros(self.B, len(names), dtype=torch.float64, pin_memory=True)
+        self._motor = (names, ptr, flat, out, host, torch.cuda.Event())
+        self._motor_groups = {k: np.asarray(groups[k], np.int64).ravel().copy() for k in names}
+
+    def _readout(self) -> None:
+        """Queue the registered readout on the current stream (recorded when a frame is captured)."""
+        if self._motor is not None:
+            _, ptr, flat, out, host, _ = self._motor
+            self._launch_means(ptr, flat, out)
+            host.copy_(out, non_blocking=True)
+
+    def _mark_readout(self) -> None:
+        if self._motor is not None:
+            self._motor[5].record(torch.cuda.current_stream(self.device))
+            self._motor_fresh = True
+
+    def _same_groups(self, groups: dict) -> bool:
+        held = getattr(self, "_motor_groups", None)
+        return held is not None and list(groups) == list(held) and \
+            all(np.array_equal(np.asarray(groups[k], np.int64).ravel(), held[k]) for k in held)
+
+    def motor(self, groups: dict | None = None) -> dict:
+        """{name: (B,) mean rate in Hz} of named neuron groups (the native motor readout,
+        flyverse/motor.py:232-270). With no argument, or the groups given to `set_motor`, the means
+        of the last frame come from the frame's own readout; other groups cost one reduction and
+        one synchronising copy."""
+        if self._motor is not None and (groups is None or self._same_groups(groups)):
+            if not self._motor_fresh:           # no frame since registration, reset or restore
+                self._readout()
+                self._mark_readout()
+            names, _, _, _, host, event = self._motor
+            event.synchronize()
+            means = host.numpy().copy()
+            return {k: means[:, n] for n, k in enumerate(names)}
+        if groups is None:
+            raise ValueError("no motor groups registered; pass groups or call set_motor")
+        names, ptr, flat = self._group_table(groups)
+        out = torch.zeros(self.B, len(names), dtype=torch.float64, device=self.device)
+        self._launch_means(ptr, flat, out)
+        means = out.cpu().numpy()
         return {k: means[:, n] for n, k in enumerate(names)}
 
     def reset(self, rows=None) -> None:
+        self._motor_fresh = False
         self.brain.reset(rows)
         if self.optic is not None:
             self.optic.reset(rows)
@@ -234,6 +308,7 @@ class FlyBrain:
         if state["lif_params"] != asdict(self.brain.p):
             raise ValueError("state simulation parameters do not match")
         self._graphs.clear()
+        self._motor_fresh = False
         self.brain.load_state_dict(state["brain"])
         o = self.optic
         if o is not None:

@@ -291,6 +291,12 @@ typedef struct flyb_photo_args {
 
 int flyb_photoreceptor(const flyb_photo_args* a, void* stream);
 
+/* Motor readout on the native layout: out[b * groups + k] = mean of rates[i][b] over the members
+ * i = idx[ptr[k]:ptr[k+1]] of group k, summed in member order in double (the reference's
+ * launch_means, neural.cu:133-144, without the batch-major copy of the rates); rates [n][batch]. */
+int flyb_group_means(const int* ptr, const int* idx, const float* rates, double* out, int groups, int batch,
+                     void* stream);
+
 /* Device facts for grid sizing: SM count and co-resident blocks per SM for the persistent
  * kernels at `block` threads. kind: 0 LIF, 1 optic, 2 adjoint. */
 int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm);

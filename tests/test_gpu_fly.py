@@ -85,3 +85,48 @@ def test_batch_sim_uneven_episodes_reset_their_rows():
             resets += 1
         assert out["lc"].shape == (4,)
     assert resets == sim.stats.finished > 0
+
+
+def _member_order_means(rates, groups):
+    out = {}
+    for k, idx in groups.items():
+        acc = np.zeros(rates.shape[0])
+        for i in idx:
+            acc += rates[:, i]
+        out[k] = acc / len(idx) if len(idx) else acc
+    return out
+
+
+def test_motor_readout_inside_captured_frames():
+    """Registered groups are reduced inside every (captured or eager) frame and copied to pinned
+    memory; the result equals a member-order double sum of the rates on the host, the reference's
+    launcher on the batch-major copy, and a fresh reduction after a reset."""
+    from flyb200 import cuda as fcuda
+    for graphs in (True, False):
+        fb = make(graphs)
+        rng = np.random.default_rng(4)
+        groups = {"spk": [int(i) for i in fb.optic.spk_idx[:7]], "rand": rng.integers(0, fb.brain.n, 40).tolist(),
+                  "empty": [], "one": [int(fb.optic.spk_idx[0])]}
+        fb.set_motor(groups)
+        first = fb.motor()                                  # before any frame: reduced on demand
+        assert all(np.all(v == 0) or np.all(np.isfinite(v)) for v in first.values())
+        for ms in (10.0, 10.0, 13.3, 10.0):
+            fb.step(ms)
+            got = fb.motor()
+            rates = fb.brain.rate.double().cpu().numpy()
+            want = _member_order_means(rates, groups)
+            for k in groups:
+                np.testing.assert_array_equal(got[k], want[k], err_msg=k)
+            ptr = torch.tensor(np.r_[0, np.cumsum([len(groups[k]) for k in groups])], dtype=torch.int32, device="cuda")
+            flat = torch.tensor(sum((groups[k] for k in groups), []), dtype=torch.int32, device="cuda")
+            ref = fcuda.group_means(ptr, flat, fb.brain.rate.contiguous()).cpu().numpy()
+            np.testing.assert_array_equal(np.stack([got[k] for k in groups], 1), ref)
+            assert fb.motor(dict(groups)) .keys() == got.keys()
+            other = fb.motor({"x": groups["rand"][:5]})     # unregistered groups: one explicit reduction
+            np.testing.assert_array_equal(other["x"], _member_order_means(rates, {"x": groups["rand"][:5]})["x"])
+        assert float(np.abs(got["spk"]).sum()) > 0
+        fb.reset([0])
+        after = fb.motor()
+        np.testing.assert_array_equal(after["spk"][0], 0.0)
+        if graphs:
+            assert len(fb._graphs) >= 1
