@@ -17,6 +17,9 @@ Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthet
   e2e            the same B=64 step through the public API with, every step, the radiance copied in
                  from pinned host memory and the motor readout copied out
   roofline       the LIF step kernel: algorithmic bytes / CUDA-event time against measured HBM copy
+  tracer         the eye's ray tracer at 64 flies x 1,634 columns x 7 rays: device time, the frame
+                 path beside the reference's own torch tracer on the same GPU (baseline/_ref), and
+                 the C oracle on host cores
   cpu_baseline   the C oracle port (oracle/) on this host's cores, a bounded sample of the workload
 `--impl reference` times that CPU port alone on the same config and prints the same line.
 """
@@ -389,6 +392,111 @@ def cpu_port_rate(cfg, batch: int, steps: int, threads: int) -> dict:
             "kind": "port", "sample": f"{steps} whole-fly steps x {batch} flies ({m + n:,} neurons) on the C oracle"}
 
 
+def measure_tracer(device, batch: int = BATCH, reps: int = 50, cpu: bool = True) -> dict:
+    """The eye's ray tracer: 1,634 columns x 7 rays per fly in its own make_room scene, fused
+    column sums, at `batch` flies. Device time of the one launch; the frame-level path (poses from
+    the host, column radiance on the device) beside the reference's own torch tracer run on this
+    GPU from baseline/_ref when it is installed; the C oracle on host cores."""
+    from flyb200 import synthetic
+    from flyb200 import world as W
+    from flyb200.batch_world import BatchWorld
+    _, dirs, w = synthetic.eye_grid()
+    n_col, k = dirs.shape[:2]
+    scenes = [W.make_room(i)[0] for i in range(batch)]
+    bw = BatchWorld(scenes, device)
+    bw.set_eye(dirs, w)
+    pose = synthetic.fly_poses(batch, seed=0)
+    bw.set_pose(*pose)
+    out = torch.empty(batch, n_col, 4, device=device)
+    for _ in range(3):
+        bw.trace_eye(out)
+    ms = events_time(lambda: bw.trace_eye(out), reps)
+    rays = batch * n_col * k
+
+    def frame():
+        bw.column_radiance(*pose, out=out)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(3):
+        frame()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        frame()
+    frame_ms = (time.perf_counter() - t0) / reps * 1000.0
+    res = {"workload": f"{batch} flies x {n_col} columns x {k} rays, make_room scenes (20 spheres, 8 boxes, "
+                       "6 planes), shadows and value-noise detail, column sums fused",
+           "rays_per_frame": rays, "ms": ms, "rays_per_s": rays / (ms / 1000.0),
+           "frame_ms": frame_ms, "frame_note": "poses from host numpy -> column radiance on the device, synchronised"}
+    ref = reference_tracer(device, scenes, dirs, w, pose, out, reps=max(3, reps // 10))
+    if ref is not None:
+        res["reference_gpu"] = ref
+        res["frame_speedup_vs_reference"] = ref["frame_ms"] / frame_ms
+    if cpu:
+        import oracle
+        sample = 8
+        blob = np.stack([W.pack_scene(sc) for sc in scenes[:sample]])
+        args = dict(origins=pose[0][:sample], eye_dirs=dirs.reshape(-1, 3),
+                    pose=np.concatenate([v[:sample] for v in pose[1:]], 1), weights=w, shared_origin=True, batch=sample)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        cols = oracle.trace(blob, bw._scene_shape, bw.detail, threads=threads, **args)
+        dt = time.perf_counter() - t0
+        res["cpu_baseline"] = {"value": sample * n_col * k / dt, "unit": "rays/s", "cores": threads, "kind": "port",
+                               "sample": f"{sample} of the {batch} flies on the C oracle"}
+        res["oracle_bit_exact"] = bool(np.array_equal(cols, out[:sample].cpu().numpy()))
+    return res
+
+
+def reference_tracer(device, scenes, dirs, w, pose, ours, reps: int):
+    """The reference's stock tracer (flyverse.world / batch_world from baseline/_ref) on this GPU
+    for the same scenes and poses, as BatchSim.column_radiance calls it (host numpy turn, captured
+    trace, weighted sum); None when it is not installed."""
+    ref_dir = ROOT / "baseline" / "_ref"
+    if not (ref_dir / "flyverse" / "world.py").exists():
+        return None
+    sys.path.insert(0, str(ref_dir))
+    try:
+        from flyverse import batch_world as rbw
+        from flyverse import world as rw
+    except Exception as e:               # noqa: BLE001 - report, do not fail the bench
+        return {"unavailable": f"import failed: {e}"}
+    finally:
+        sys.path.remove(str(ref_dir))
+    worlds = []
+    for i in range(len(scenes)):
+        wr = rw.make_room(i)[0]
+        wr.device = device
+        worlds.append(wr)
+    bw = rbw.BatchWorld(worlds, device)
+    wts = torch.as_tensor(w, dtype=torch.float32, device=device)
+    eye, f, left, up = pose
+
+    def frame():
+        rotation = np.stack([f, left, up], axis=2)
+        directions = dirs.reshape(1, -1, 3) @ rotation.transpose(0, 2, 1)
+        origins = np.broadcast_to(eye[:, None], directions.shape)
+        rad = bw.trace(torch.from_numpy(np.ascontiguousarray(origins, dtype=np.float32)),
+                       torch.from_numpy(np.ascontiguousarray(directions, dtype=np.float32)), cuda_graphs=True)
+        col = (rad.reshape(len(worlds), *dirs.shape[:2], 4) * wts[None, None, :, None]).sum(2)
+        torch.cuda.current_stream().synchronize()
+        return col
+
+    col = frame()
+    for _ in range(2):
+        frame()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        frame()
+    frame_ms = (time.perf_counter() - t0) / reps * 1000.0
+    diff = (col - ours).abs()
+    res = {"frame_ms": frame_ms, "reps": reps, "max_abs_diff": float(diff.max()),
+           "columns_differing_over_1e-4": int((diff > 1e-4).any(-1).sum()),
+           "note": "the reference's torch tracer on this GPU (CUDA-graph captured), same scenes and poses"}
+    del bw, worlds
+    torch.cuda.empty_cache()
+    return res
+
+
 # ------------------------------------------------------------------ arms
 def arm_config(world: int) -> dict:
     """The workload both arms report (the reference arm times a bounded sample of it)."""
@@ -482,6 +590,7 @@ def main() -> None:
     plain_eng, plain_ms = measure_plain(cfg, device, args.steps, args.warmup)
     batch1 = N / (plain_ms / 1000.0)
     adj = measure_adjoint(device)
+    tracer = measure_tracer(device, cpu=not args.no_cpu_baseline)
     e2e = measure_e2e(cfg, eng, device, args.steps)
     traffic = read_traffic().get(dom)
     l2 = measure_l2_gather(device)
@@ -500,6 +609,7 @@ def main() -> None:
         "batched_over_plain": value / world / batch1,
         "batch256": batch256,
         "adjoint": adj,
+        "tracer": tracer,
         "synaptic_events_per_s": events_per_step * world * timed_steps / (ms / 1000.0),
         "roofline": {"bound": "hbm", "kernel": f"{dom} step (B=64)", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,

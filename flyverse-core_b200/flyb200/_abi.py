@@ -87,7 +87,14 @@ class PhotoArgs(ct.Structure):
                 ("a_pr", _VP)]
 
 
-STRUCTS = (LifArgs, OpticArgs, SpmmArgs, AdjointArgs, PhotoArgs)
+class TraceArgs(ct.Structure):
+    _fields_ = [("batch", _I), ("rays", _I), ("n_sph", _I), ("n_box", _I), ("n_pln", _I), ("shared_origin", _I),
+                ("samples", _I), ("detail", ct.c_float),
+                ("scene", _VP), ("origins", _VP), ("dirs", _VP), ("eye_dirs", _VP), ("pose", _VP), ("weights", _VP),
+                ("out", _VP)]
+
+
+STRUCTS = (LifArgs, OpticArgs, SpmmArgs, AdjointArgs, PhotoArgs, TraceArgs)
 
 # Every symbol include/flyb200.h declares, with its ctypes signature.
 _P = ct.POINTER(ct.c_void_p)
@@ -108,6 +115,8 @@ SIGNATURES = {
     "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
     "flyb_group_means": [_VP, _VP, _VP, _VP, _I, _I, _VP],
+    "flyb_trace_scene_floats": [_I, _I, _I],
+    "flyb_trace": [ct.POINTER(TraceArgs), _VP],
     "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
     "flyb_selftest_wait": [_VP, _VP, ct.c_longlong, _VP],
     "flyb_gather_probe": [_VP, _I, _VP, _I, _VP, _I, _VP],

@@ -2,11 +2,13 @@
 flyverse/batch_sim.py:86-343).
 
 Every row is an independent fly sharing the graph. `step()` runs one 10 ms frame for all rows:
-the caller's stimulus (radiance and/or Poisson rates per row) goes in, the frame runs through
+the caller's stimulus (radiance and/or Poisson rates per row) goes in, or, with `world` (a
+BatchWorld, one scene per fly) and `pose(frame, fb) -> (eye, forward, left, up)`, every eye is
+ray traced on the device (batch_sim.py:192-201), then the frame runs through
 FlyBrain (graph-captured when `cuda_graphs`), the motor groups' mean rates come out. Rows whose
 episode length is used up are reset on their own (`FlyBrain.reset(rows)`, batch_sim.py:282-304)
 and start a new episode of a freshly drawn length; the shared clock and Poisson streams go on.
-The world, body and behaviour programs of the reference are not part of the brain step.
+The body and behaviour programs of the reference are not part of the brain step.
 """
 from __future__ import annotations
 
@@ -30,7 +32,8 @@ class BatchSim:
 
     def __init__(self, batch: int = 1, *, c, seed: int = 0, device=None, brain_dt: float = 0.5, optic_dt: float = 1.0,
                  cuda_graphs: bool = False, lif_params: LIFParams | None = None, optic_params: OpticParams | None = None,
-                 episode_frames=(50, 400), groups: dict | None = None, stimulus=None, retina=None):
+                 episode_frames=(50, 400), groups: dict | None = None, stimulus=None, retina=None, world=None,
+                 pose=None):
         if not isinstance(batch, (int, np.integer)) or batch < 1:
             raise ValueError("batch must be a positive integer")
         if not np.isfinite(brain_dt) or brain_dt <= 0 or not np.isclose(self.FRAME_MS / brain_dt,
@@ -49,6 +52,9 @@ class BatchSim:
         self.groups = groups or {}
         self.fb.set_motor(self.groups or None)
         self.stimulus = stimulus
+        if (world is None) != (pose is None):
+            raise ValueError("a traced world needs a pose callback and vice versa")
+        self.world, self.pose = world, pose
         self.stats = EpisodeStats()
         self.frame = 0
 
@@ -64,6 +70,8 @@ class BatchSim:
                 self.fb.vision(radiance)
             for name, (idx, hz) in (inputs or {}).items():
                 self.fb.set_input(name, idx, hz)
+        if self.world is not None:
+            self.fb.look(self.world, *self.pose(self.frame, self.fb))
         self.fb.step(self.FRAME_MS)
         out = self.fb.motor() if self.groups else {}
         self.frame += 1

@@ -86,6 +86,20 @@ class FlyBrain:
         else:
             self._radiance.copy_(value)
 
+    def look(self, world, eye, forward, left, up) -> None:
+        """Trace every fly's eye in its own scene of `world` (a BatchWorld, one scene per fly) from
+        eye positions (B, 3) and orientations forward/left/up (B, 3 each), and hold the column
+        radiance as `vision` does; the radiance stays on the device (one trace launch)."""
+        if self.optic is None:
+            raise ValueError("vision is absent from this connectome subset")
+        if getattr(world, "B", None) != self.B:
+            raise ValueError("the world must hold one scene per fly")
+        if world._eye is None or world._eye[2] != self.retina.n_columns:
+            world.set_eye(*self.retina.ray_directions())
+        if self._radiance is None:
+            self._radiance = torch.zeros(self.B, self.retina.n_columns, 4, device=self.device)
+        world.column_radiance(eye, forward, left, up, out=self._radiance)
+
     def set_input(self, name: str, idx, hz) -> None:
         """A held sensory Poisson input (the reference's `_input`, fly.py:312-324)."""
         ti = self.brain._idx(idx)

@@ -1,6 +1,6 @@
 """A short, eager run of the whole-fly step for profilers (every kernel launched separately).
 
-    python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic]
+    python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic|tracer]
                               [--lif-block 256] [--lif-ipt 0|1|2|4] [--lif-staged] [--lif-defer] [--lif-grid 0]
                               [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
                               [--no-overlap]
@@ -84,12 +84,27 @@ def breakdown(eng: WholeFly, reps: int) -> dict:
     return out
 
 
+def trace_eyes(args) -> None:
+    """`--batch` flies' eyes (1,634 columns x 7 rays) traced in their own rooms, `--steps` times."""
+    from . import world as W
+    from .batch_world import BatchWorld
+    _, dirs, w = synthetic.eye_grid()
+    bw = BatchWorld([W.make_room(i)[0] for i in range(args.batch)], "cuda")
+    bw.set_eye(dirs, w)
+    bw.set_pose(*synthetic.fly_poses(args.batch, seed=0))
+    for _ in range(args.warmup + args.steps):
+        out = bw.trace_eye()
+    torch.cuda.synchronize()
+    print(f"traced {args.steps} frames of {args.batch} eyes: {out.shape[1]} columns, mean radiance "
+          f"{float(out.mean()):.4f}")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
-    ap.add_argument("--part", default="whole", choices=["whole", "lif", "optic"])
+    ap.add_argument("--part", default="whole", choices=["whole", "lif", "optic", "tracer"])
     ap.add_argument("--breakdown", action="store_true")
     ap.add_argument("--lif-block", type=int, default=256)
     ap.add_argument("--lif-ipt", type=int, default=0, help="LIF items per thread (0: automatic)")
@@ -101,6 +116,9 @@ def main() -> None:
     ap.add_argument("--optic-variant", type=int, default=0)
     ap.add_argument("--optic-grid", type=int, default=0, help="persistent optic block cap")
     args = ap.parse_args()
+    if args.part == "tracer":
+        trace_eyes(args)
+        return
     cfg = synthetic.whole_fly_config5(seed=0)
     eng = WholeFly(cfg, args.batch, device="cuda", seed=1, launch="step", overlap=not args.no_overlap)
     eng.lif.block, eng.lif.items_per_thread, eng.lif.staged = args.lif_block, args.lif_ipt, args.lif_staged

@@ -17,6 +17,9 @@ reference's headline numbers are quoted on:
                 (operating point 0) whose inhibitory inputs from 35 "delayed inhibition" types
                 (tau 10 ms) carry a x5 pair gain; 5,895 photoreceptors on a hex eye driven by a
                 drifting sinusoidal grating in 4 spectral channels.
+  eye_grid      the eye the ray tracer casts: two hexagonal column patches of radius 16 (817
+                columns each, 1,634 in all, about the ommatidia of a fly's pair of eyes) through
+                the retina's own geometry, 7 sample rays per column.
 """
 from __future__ import annotations
 
@@ -304,3 +307,29 @@ def whole_fly_config5(seed: int = 0, n_rate: int = 89_390, n_lif: int = 71_618, 
     vpn = np.unique(optic.W_sr.tocoo().row)
     return WholeFlyConfig(lif=lif, optic=optic, sensory_idx=sensory, vpn_idx=vpn, n_rate=n_rate, n_spiking=n_spk,
                           edges=int(W.nnz + optic.W0.nnz + coupling))
+
+
+def eye_grid(radius: int = 16):
+    """(retina, ray directions (n_col, k, 3), weights (k,)) of two hexagonal column patches."""
+    from .retina import EyeGeometry, Retina, column_directions
+    cells = [(h1, h2) for h1 in range(-radius, radius + 1) for h2 in range(-radius, radius + 1) if abs(h1 - h2) <= radius]
+    side = np.array(["L"] * len(cells) + ["R"] * len(cells))
+    hexes = np.array(cells + cells, dtype=float)
+    col_dir, az_el = column_directions(side, hexes, EyeGeometry())
+    r = Retina(pr_index=np.zeros(0, np.int64), pr_column=np.zeros(0, np.int64), pr_sens=np.zeros((0, 4), np.float32),
+               col_side=side, col_hex=hexes, col_dir=col_dir, col_az_el=az_el)
+    return (r, *r.ray_directions())
+
+
+def fly_poses(batch: int, seed: int = 0):
+    """Eye positions and orientations (eye, forward, left, up) of flies walking and hovering over
+    the table and floor of `world.make_room`, heading and pitch uniform."""
+    rng = np.random.default_rng(seed)
+    heading, pitch = rng.uniform(-np.pi, np.pi, batch), rng.uniform(-0.4, 0.4, batch)
+    on_table = rng.random(batch) < 0.5
+    eye = np.c_[rng.uniform(-1.5, 1.5, batch), rng.uniform(-1.5, 1.5, batch), rng.uniform(0.01, 1.5, batch)]
+    eye[on_table] = np.c_[rng.uniform(-0.5, 0.5, on_table.sum()), rng.uniform(-0.3, 0.3, on_table.sum()),
+                          0.751 + rng.uniform(0, 0.05, on_table.sum())]
+    f = np.c_[np.cos(pitch) * np.cos(heading), np.cos(pitch) * np.sin(heading), np.sin(pitch)]
+    left = np.c_[-np.sin(heading), np.cos(heading), np.zeros(batch)]
+    return eye, f, left, np.cross(f, left)

@@ -297,6 +297,45 @@ int flyb_photoreceptor(const flyb_photo_args* a, void* stream);
 int flyb_group_means(const int* ptr, const int* idx, const float* rates, double* out, int groups, int batch,
                      void* stream);
 
+/* ---------------------------------------------------------------- the eye's ray tracer
+ * Replaces World.trace / BatchWorld.trace (flyverse/world.py:214, flyverse/batch_world.py:77) and the
+ * column averaging of BatchSim.column_radiance (flyverse/batch_sim.py:192-201). Every scene of a
+ * batch has the same primitive counts; scene b is flyb_trace_scene_floats(...) floats at
+ * scene + b * that count:
+ *   spheres [n_sph][6] centre xyz, radii xyz; boxes [n_box][6] lo xyz, hi xyz;
+ *   planes [n_pln][6] point xyz, unit normal xyz;
+ *   materials [n_sph + n_box + n_pln + 1][16] reflectance 4, second reflectance 4, emission 4,
+ *     pattern period, pattern id (0 plain, 1 checks, 2 wall stripes, 3 planks), 2 unused; the last
+ *     row belongs to rays that hit nothing;
+ *   light [12] position xyz, colour 4, ambient 4, 1 unused.
+ * Rays: explicit origins and directions ([batch][rays][3] each), or one origin per scene
+ * (shared_origin) with explicit directions, or one origin per scene with body-frame directions
+ * eye_dirs [rays][3] turned by pose [batch][9] (forward, left, up: d = x f + y l + z u, in double,
+ * then rounded to float). With samples > 1, each run of `samples` consecutive rays is one output,
+ * the weighted sum of their radiance in sample order. out is [batch][rays / samples][4], 16-byte
+ * aligned. */
+typedef struct flyb_trace_args {
+  int batch;
+  int rays;
+  int n_sph;
+  int n_box;
+  int n_pln;
+  int shared_origin;
+  int samples;
+  float detail;           /* surface-noise amplitude; 0 = flat colours */
+  const float* scene;
+  const float* origins;
+  const float* dirs;
+  const double* eye_dirs;
+  const double* pose;
+  const float* weights;   /* [samples] */
+  float* out;
+} flyb_trace_args;
+
+/* floats per packed scene, or -1 for negative counts or more than 512 primitives */
+int flyb_trace_scene_floats(int n_sph, int n_box, int n_pln);
+int flyb_trace(const flyb_trace_args* a, void* stream);
+
 /* Device facts for grid sizing: SM count and co-resident blocks per SM for the persistent
  * kernels at `block` threads. kind: 0 LIF, 1 optic, 2 adjoint. */
 int flyb_occupancy(int kind, int block, int* sm_count, int* blocks_per_sm);

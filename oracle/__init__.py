@@ -4,6 +4,8 @@ Only tests/, __graft_entry__.smoke() and bench.py (its cpu_baseline leg and `--i
 arm) import this package, always as the checker or as the timed CPU port, never as the thing
 measured or shipped. It wraps:
 
+  tracer.c      plain-C restatement of the eye's ray tracer (scenes, shadows, patterns, value
+                noise, pose turn and column sums);
   flyoracle.c   plain-C restatement of the LIF step over an exact delay ring, Philox4x32-10, the
                 optic substep (FP32 reference order, FP64) and the held-input products;
   optic64.py    FP64 numpy restatement of the optic dynamics parameterised by per-type-pair gains
@@ -36,14 +38,14 @@ from flyb200 import _abi  # noqa: E402  (struct layouts of include/flyb200.h onl
 
 def build(force: bool = False) -> Path:
     """Compile flyoracle.c with gcc (no contraction of multiply-adds, OpenMP over flies)."""
-    src = HERE / "flyoracle.c"
-    if LIB.exists() and not force and LIB.stat().st_mtime >= max(src.stat().st_mtime,
-                                                                 (ROOT / "include" / "flyb200.h").stat().st_mtime):
+    srcs = [HERE / "flyoracle.c", HERE / "tracer.c"]
+    if LIB.exists() and not force and LIB.stat().st_mtime >= max([s.stat().st_mtime for s in srcs] +
+                                                                 [(ROOT / "include" / "flyb200.h").stat().st_mtime]):
         return LIB
     BUILD.mkdir(exist_ok=True)
     tmp = BUILD / f"libflyoracle.{os.getpid()}.so"
     cmd = ["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
-           str(src), "-o", str(tmp), "-lm"]
+           *map(str, srcs), "-o", str(tmp), "-lm"]
     subprocess.run(cmd, check=True, capture_output=True, text=True)
     tmp.replace(LIB)
     return LIB
@@ -61,6 +63,7 @@ def lib():
         L.oracle_uniform.restype = ct.c_float
         L.oracle_philox.argtypes = [ct.c_uint64] + [ct.c_uint32] * 4 + [ct.POINTER(ct.c_uint32)]
         L.oracle_optic_run_f64.argtypes = [ct.c_int] * 3 + [ct.c_void_p] * 9 + [ct.c_double] * 3
+        L.oracle_trace.argtypes = [ct.POINTER(_abi.TraceArgs), ct.c_int]
         _lib = L
     return _lib
 
@@ -183,3 +186,24 @@ def spmm(ptr, col, w, x, batch, *, rows, x_index=None, x_div=1.0, x_lo=-np.inf, 
                          y=_p(y), y_index=_p(yi), y_rows=y.shape[0], alpha=alpha, y_lo=y_lo, y_hi=y_hi)
     lib().oracle_spmm(ct.byref(args))
     return y
+
+
+def trace(scene, shape, detail, *, origins, dirs=None, eye_dirs=None, pose=None, weights=None,
+          shared_origin=False, batch=1, threads=0):
+    """The tracer restatement on host arrays, arguments as flyb_trace_args: returns
+    (batch, rays / samples, 4) float32."""
+    scene, origins = _f32(scene), _f32(origins)
+    dirs = None if dirs is None else _f32(dirs)
+    eye_dirs = None if eye_dirs is None else np.ascontiguousarray(eye_dirs, dtype=np.float64)
+    pose = None if pose is None else np.ascontiguousarray(pose, dtype=np.float64)
+    weights = None if weights is None else _f32(weights)
+    rays = (len(eye_dirs.reshape(-1, 3)) if eye_dirs is not None else dirs.reshape(batch, -1, 3).shape[1])
+    samples = 1 if weights is None else weights.size
+    out = np.zeros((batch, rays // samples, 4), np.float32)
+    a = _abi.TraceArgs(batch=batch, rays=rays, n_sph=shape[0], n_box=shape[1], n_pln=shape[2],
+                       shared_origin=int(shared_origin), samples=samples, detail=float(detail), scene=_p(scene),
+                       origins=_p(origins), dirs=_p(dirs), eye_dirs=_p(eye_dirs), pose=_p(pose),
+                       weights=_p(weights), out=_p(out))
+    if lib().oracle_trace(ct.byref(a), threads or os.cpu_count() or 1):
+        raise ValueError("oracle_trace: invalid arguments")
+    return out

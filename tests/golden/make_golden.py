@@ -19,6 +19,11 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
                   of tests/test_optic_hooks.py::hex_graph(), batch 2, three frames.
   optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
                   synthetic 3,000-unit lobe from flyb200.synthetic.optic_config3, 60 substeps.
+  tracer.npz      flyverse.world / flyverse.batch_world (CPU): the reference tests' rays in
+                  make_room(0), a 48 x 32 camera image, three batched rooms before and after a
+                  per-row sphere move, and the eye: flyverse.retina.build_retina on a two-eye
+                  hex grid (column directions, 7 sample rays per column) traced from four fly
+                  poses and averaged into columns as BatchSim.column_radiance does.
 """
 from __future__ import annotations
 
@@ -186,6 +191,97 @@ def optic_synth(ref) -> dict:
             "adapt": lobe.adapt.numpy().copy(), "aad": np.float64(cfg.aad)}
 
 
+def eye_grid(radius: int = 6) -> pd.DataFrame:
+    """One R1-R6 photoreceptor per column of a hex patch on each side (ids 1000 + k)."""
+    cells = [(h1, h2) for h1 in range(-radius, radius + 1) for h2 in range(-radius, radius + 1) if abs(h1 - h2) <= radius]
+    sites = [(side, h1, h2) for side in ("L", "R") for h1, h2 in cells]
+    return pd.DataFrame([dict(bodyId=1000 + k, type="R1-R6", superclass="ol_sensory", nt="histamine", hex1=h1, hex2=h2,
+                              hex_side=side) for k, (side, h1, h2) in enumerate(sites)])
+
+
+def tracer(ref) -> dict:
+    world, bworld, rt, cn = ref["world"], ref["batch_world"], ref["retina"], ref["connectome"]
+    out = {}
+    # known answers of the reference's tests (tests/test_world.py:18-28)
+    w = world.World(spheres=[world.Sphere((1, 0, 0), (.2, .2, .2), "apple")], device="cpu", detail=0,
+                    ambient=(1, 1, 1, 1), light_color=(0, 0, 0, 0))
+    out["known_apple"] = w.trace(torch.zeros(1, 3), torch.tensor([[1., 0, 0]])).numpy()
+    # the room and the reference tests' rays (test_world.py:9-14, 43-50)
+    room, _ = world.make_room(0)
+    room.device = "cpu"
+
+    def rays(n, seed):
+        g = torch.Generator().manual_seed(seed)
+        d = torch.randn(n, 3, generator=g)
+        d /= d.norm(dim=-1, keepdim=True)
+        return torch.tensor([-.5, .05, .7512]).expand_as(d).contiguous(), d
+
+    o1, d1 = rays(67, 0)
+    o2, d2 = rays(134, 8)
+    o2, d2 = (o2[::2] + .03).contiguous(), d2[::2].contiguous()
+    for k, (o, d) in enumerate(((o1, d1), (o2, d2))):
+        out[f"room_o{k}"], out[f"room_d{k}"] = o.numpy(), d.numpy()
+        out[f"room_rad{k}"] = room.trace(o, d).numpy()
+    # the same room without texture detail, and seen from a camera
+    room.detail = 0
+    room.invalidate()
+    out["room_flat_rad0"] = room.trace(o1, d1).numpy()
+    room.detail = 1.4
+    room.invalidate()
+    out["camera"] = room.render_camera((0, 0, 1), (1, 0, 0), (0, 0, 1), width=48, height=32).numpy()
+    # three batched rooms (tests/test_batch_sim.py:141-161)
+    scenes = [world.make_room(i)[0] for i in range(3)]
+    for sc in scenes:
+        sc.device = "cpu"
+    scenes[1].spheres[0].material = "black"
+    scenes[2].light_pos = (1, 0, 2)
+    batched = bworld.BatchWorld(scenes, "cpu")
+    gen = torch.Generator().manual_seed(12)
+    dirs = torch.randn(3, 74, 3, generator=gen)[:, ::2]
+    dirs = (dirs / dirs.norm(dim=-1, keepdim=True)).contiguous()
+    org = torch.tensor([-.5, .05, .7512]).expand_as(dirs).contiguous()
+    out["batch_o"], out["batch_d"] = org.numpy(), dirs.numpy()
+    out["batch_rad"] = batched.trace(org, dirs).numpy()
+    batched.move_sphere(0, (-.45, .05, .77), (.05,) * 3, rows=[1])
+    out["batch_rad_moved"] = batched.trace(org, dirs).numpy()
+    # the eye: the reference's retina geometry on a two-eye hex grid, traced from four poses
+    n = eye_grid()
+    n["class"] = ""; n["subclass"] = ""; n["somaSide"] = n.hex_side; n["instance"] = n.type + "_x"
+    n["sign"] = np.array([cn.NT_SIGN[x] for x in n.nt], dtype=np.float32)
+    c = cn.Connectome(n, sp.csr_matrix((len(n), len(n)), dtype=np.float32), pd.Series(np.arange(len(n)), index=n.bodyId.to_numpy()))
+    r = rt.build_retina(c)
+    eye_dirs, wts = r.ray_directions()
+    out.update({"eye_hex1": n.hex1.to_numpy(np.float64), "eye_hex2": n.hex2.to_numpy(np.float64),
+                "eye_side": n.hex_side.to_numpy().astype("U"), "eye_col_dir": r.col_dir, "eye_col_az_el": r.col_az_el,
+                "eye_dirs": eye_dirs, "eye_w": wts, "eye_pr_column": r.pr_column})
+    B = 4
+    rooms = [world.make_room(i)[0] for i in range(B)]
+    for sc in rooms:
+        sc.device = "cpu"
+    rooms[3].spheres[0].material = "lamp"
+    eyes = bworld.BatchWorld(rooms, "cpu")
+    rng = np.random.default_rng(21)
+    heading = rng.uniform(-np.pi, np.pi, B)
+    pitch = rng.uniform(-0.3, 0.3, B)
+    eye = np.c_[rng.uniform(-0.5, 0.5, B), rng.uniform(-0.3, 0.3, B), 0.76 + rng.uniform(0, 0.1, B)]
+    f = np.c_[np.cos(pitch) * np.cos(heading), np.cos(pitch) * np.sin(heading), np.sin(pitch)]
+    left = np.c_[-np.sin(heading), np.cos(heading), np.zeros(B)]
+    up = np.cross(f, left)
+    # BatchSim.column_radiance (batch_sim.py:192-201)
+    rotation = np.stack([f, left, up], axis=2)
+    directions = eye_dirs.reshape(1, -1, 3) @ rotation.transpose(0, 2, 1)
+    origins = np.broadcast_to(eye[:, None], directions.shape)
+    rad = eyes.trace(torch.from_numpy(np.ascontiguousarray(origins, dtype=np.float32)),
+                     torch.from_numpy(np.ascontiguousarray(directions, dtype=np.float32)))
+    wts_t = torch.as_tensor(wts, dtype=torch.float32)
+    out["eye_rad"] = rad.numpy()
+    out["eye_columns"] = (rad.reshape(B, *eye_dirs.shape[:2], 4) * wts_t[None, None, :, None]).sum(2).numpy()
+    out.update({"eye_pos": eye, "eye_f": f, "eye_left": left, "eye_up": up,
+                "eye_ray_d": np.ascontiguousarray(directions, dtype=np.float32)})
+    print(f"tracer: {r.n_columns} columns x {eye_dirs.shape[1]} rays, {B} poses")
+    return out
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -197,11 +293,13 @@ def main() -> None:
     ref = {k: importlib.import_module(m) for k, m in (("connectome", "flyverse.connectome"), ("brain", "flyverse.brain"),
                                                       ("optic", "flyverse.optic"), ("retina", "flyverse.retina"),
                                                       ("test_bit_identity", "test_bit_identity"),
-                                                      ("test_optic_hooks", "test_optic_hooks"))}
+                                                      ("test_optic_hooks", "test_optic_hooks"),
+                                                      ("world", "flyverse.world"), ("batch_world", "flyverse.batch_world"))}
     torch.set_num_threads(1)
     fixtures = {"lif_c1": lambda: lif_c1(ref), "lif_19cell": lambda: lif_19cell(ref),
                 "lif_19cell_adapt_by_type": lambda: lif_19cell(ref, ADAPT_BY_TYPE),
-                "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref)}
+                "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
+                "tracer": lambda: tracer(ref)}
     for name, make in fixtures.items():
         if args.only in (None, name):
             np.savez_compressed(HERE / f"{name}.npz", **make())

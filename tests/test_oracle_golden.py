@@ -8,7 +8,7 @@ from oracle import frame as oframe
 from flyb200 import _abi, synthetic
 from flyb200.brain import LIFParams, lif_coefficients, out_edges
 from flyb200.optic import OpticParams, lobe_matrices
-from flyb200.retina import Retina
+from flyb200.retina import build_retina
 from flyb200.weights import lif_weights, per_type, DEFAULT_STD_U_BY_TYPE
 from helpers import connectome_from_fixture, golden, sha, torch_uniforms, unpack
 
@@ -146,8 +146,12 @@ def hex_lobe():
     z = golden("optic_hex")
     c = connectome_from_fixture(z, extra=())
     c.neurons["hex1"], c.neurons["hex2"], c.neurons["hex_side"] = z["hex1"], z["hex2"], z["hex_side"]
-    r = Retina(pr_index=z["pr_index"], pr_column=z["pr_column"], pr_sens=z["pr_sens"],
-               col_side=np.array(["L"] * int(z["n_columns"])), col_hex=np.zeros((int(z["n_columns"]), 2)))
+    c.neurons["hex_side"] = c.neurons.hex_side.replace("", None)
+    r = build_retina(c)
+    np.testing.assert_array_equal(r.pr_index, z["pr_index"])
+    np.testing.assert_array_equal(r.pr_column, z["pr_column"])
+    np.testing.assert_array_equal(r.pr_sens, z["pr_sens"])
+    assert r.n_columns == int(z["n_columns"])
     return z, c, r
 
 
