@@ -56,15 +56,21 @@ __device__ __forceinline__ float lattice_hash(long long lin) {
   long long h = lin % 2147483647ll;
   if (h < 0) h += 2147483647ll;
   h = mod_mersenne31((unsigned long long)(h ^ (h >> 13)) * 1274126177ull);
-  return (float)(h % 65536) / 32768.0f - 1.0f;
+  return (float)(int)(h & 65535) / 32768.0f - 1.0f;  // h >= 0
+}
+
+// int64 of an integer-valued float, through the 32-bit conversion when it fits
+__device__ __forceinline__ long long to_int64(float f) {
+  return fabsf(f) < 2147483648.f ? (long long)(int)f : (long long)f;
 }
 
 // trilinear value noise at period `scale` (world.py:28-43), corners in (dx, dy, dz) order
 __device__ float value_noise(float px, float py, float pz, float scale) {
   const float qx = px / scale, qy = py / scale, qz = pz / scale;
   const float flx = floorf(qx), fly = floorf(qy), flz = floorf(qz);
-  const long long ix = (long long)flx, iy = (long long)fly, iz = (long long)flz;
-  float fx = qx - (float)ix, fy = qy - (float)iy, fz = qz - (float)iz;
+  const long long ix = to_int64(flx), iy = to_int64(fly), iz = to_int64(flz);
+  // floor() is integer valued, so converting it to int64 and back returns it unchanged
+  float fx = qx - flx, fy = qy - fly, fz = qz - flz;
   fx = (fx * fx) * (3.f - 2.f * fx);
   fy = (fy * fy) * (3.f - 2.f * fy);
   fz = (fz * fz) * (3.f - 2.f * fz);
@@ -96,6 +102,7 @@ struct SceneSm {
   const float* mat;    // [ns + nb + np + 1][16]
   const float* light;  // [12]
   const float* occ;    // [ns][4] per-sphere (o - c) / r and |(o - c) / r|^2 - 1 for a shared origin, or null
+  const int* shadow_order;  // spheres enclosing the light first: the likeliest blockers of a shadow ray
 };
 
 struct Hit {
@@ -116,10 +123,14 @@ __device__ __forceinline__ float sphere_t(const float* s, const float* occ, floa
   const float a = (ddx * ddx + ddy * ddy) + ddz * ddz;
   const float b = 2.f * ((ocx * ddx + ocy * ddy) + ocz * ddz);
   const float disc = b * b - (4.f * a) * c;
-  const float sq = sqrtf(fmaxf(disc, 0.f));
-  const float t0 = (-b - sq) / (2.f * a), t1 = (-b + sq) / (2.f * a);
-  const float t = t0 > kEps ? t0 : t1;
-  return (disc > 0.f && t > kEps) ? t : kInf;
+  // the reference's where(disc > 0 & t > eps, t, INF) with t = t0 > eps ? t0 : t1, evaluating
+  // the square root and each quotient only where the result depends on it
+  if (!(disc > 0.f)) return kInf;
+  const float sq = sqrtf(disc);
+  const float t0 = (-b - sq) / (2.f * a);
+  if (t0 > kEps) return t0;
+  const float t1 = (-b + sq) / (2.f * a);
+  return t1 > kEps ? t1 : kInf;
 }
 
 __device__ __forceinline__ float box_t(const float* bx, float ox, float oy, float oz, float ix, float iy, float iz,
@@ -140,9 +151,11 @@ __device__ __forceinline__ float plane_t(const float* pl, float ox, float oy, fl
                                          float* denom_out) {
   const float denom = (dx * pl[3] + dy * pl[4]) + dz * pl[5];
   const float num = ((pl[0] - ox) * pl[3] + (pl[1] - oy) * pl[4]) + (pl[2] - oz) * pl[5];
-  const float t = num / (fabsf(denom) < kTiny ? kTiny : denom);
   *denom_out = denom;
-  return (t > kEps && fabsf(denom) > kTiny) ? t : kInf;
+  // t = num / denom > eps > 0 needs |denom| > tiny and num, denom of one sign; only then divide
+  if (!(fabsf(denom) > kTiny) || !((num > 0.f && denom > 0.f) || (num < 0.f && denom < 0.f))) return kInf;
+  const float t = num / denom;
+  return t > kEps ? t : kInf;
 }
 
 __device__ __forceinline__ float guard(float d) { return fabsf(d) < kTiny ? kTiny : d; }
@@ -198,8 +211,10 @@ __device__ Hit nearest(const SceneSm& s, float ox, float oy, float oz, float dx,
 
 // 1 when nothing lies nearer than `dist` along the shadow ray (world.py:276-277: ts >= dist)
 __device__ float unshadowed(const SceneSm& s, float ox, float oy, float oz, float dx, float dy, float dz, float dist) {
-  for (int k = 0; k < s.ns; ++k)
+  for (int q = 0; q < s.ns; ++q) {
+    const int k = s.shadow_order[q];
     if (sphere_t(s.sph + 6 * k, nullptr, ox, oy, oz, dx, dy, dz) < dist) return 0.f;
+  }
   if (s.nb) {
     const float ix = 1.f / guard(dx), iy = 1.f / guard(dy), iz = 1.f / guard(dz);
     for (int k = 0; k < s.nb; ++k) {
@@ -276,13 +291,27 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(TraceK k) {
   for (int i = threadIdx.x; i < k.floats; i += blockDim.x) sm[i] = src[i];
   float* occ = sm + ((k.floats + 3) & ~3);            // [ns][4], 16-byte aligned
   float4* partial = reinterpret_cast<float4*>(occ + 4 * k.ns);
+  int* order = reinterpret_cast<int*>(partial + (k.samples > 1 ? kThreads : 0));  // [ns]
   SceneSm s;
   s.ns = k.ns, s.nb = k.nb, s.np = k.np;
   s.sph = sm, s.box = sm + 6 * k.ns, s.pln = sm + 6 * (k.ns + k.nb);
   s.mat = sm + 6 * (k.ns + k.nb + k.np);
   s.light = s.mat + kMatFloats * (k.ns + k.nb + k.np + 1);
   s.occ = nullptr;
+  s.shadow_order = order;
   __syncthreads();
+  if (threadIdx.x == 0) {
+    // any order finds "some primitive nearer than the light" equally; enclosing spheres first
+    const float* L = s.light;
+    int q = 0;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int i = 0; i < k.ns; ++i) {
+        const float* sp = s.sph + 6 * i;
+        const float ex = (L[0] - sp[0]) / sp[3], ey = (L[1] - sp[1]) / sp[4], ez = (L[2] - sp[2]) / sp[5];
+        const bool encloses = (ex * ex + ey * ey) + ez * ez < 1.f;
+        if (encloses == (pass == 0)) order[q++] = i;
+      }
+  }
   float ox = 0.f, oy = 0.f, oz = 0.f;
   if (k.shared_origin) {
     ox = k.origins[3 * b], oy = k.origins[3 * b + 1], oz = k.origins[3 * b + 2];
@@ -292,8 +321,8 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(TraceK k) {
       occ[4 * i] = x, occ[4 * i + 1] = y, occ[4 * i + 2] = z, occ[4 * i + 3] = ((x * x + y * y) + z * z) - 1.f;
     }
     s.occ = occ;
-    __syncthreads();
   }
+  __syncthreads();
   const int local = threadIdx.x / k.samples, j = threadIdx.x - local * k.samples;
   const int col = blockIdx.x * k.per_block + local;
   const bool active = local < k.per_block && col < k.outputs;
@@ -343,16 +372,17 @@ FLYB_API int flyb_trace_scene_floats(int n_sph, int n_box, int n_pln) {
 }
 
 FLYB_API int flyb_trace(const flyb_trace_args* a, void* stream) {
-  if (!a || !a->scene || !a->out || !a->origins || a->batch <= 0 || a->rays < 0 || a->samples < 1 ||
-      a->samples > kThreads || a->n_sph < 0 || a->n_box < 0 || a->n_pln < 0)
+  if (!a || a->batch <= 0 || a->rays < 0 || a->samples < 1 || a->samples > kThreads || a->n_sph < 0 || a->n_box < 0 ||
+      a->n_pln < 0)
     return FLYB_EINVAL;
+  if (!a->rays) return 0;  // nothing to trace; empty outputs may have no address
+  if (!a->scene || !a->out || !a->origins) return FLYB_EINVAL;
   if (a->n_sph + a->n_box + a->n_pln > kMaxObjects) return FLYB_ETOOBIG;
   if (reinterpret_cast<uintptr_t>(a->out) & 15) return FLYB_EINVAL;  // float4 stores
   if (a->rays % a->samples || (a->samples > 1 && !a->weights) || (a->pose ? !a->eye_dirs : !a->dirs) ||
       (a->pose && !a->shared_origin) || !(a->detail >= 0.f))
     return FLYB_EINVAL;
   if (a->batch > 65535 || (long long)a->batch * a->rays * 3 >= (1ll << 40)) return FLYB_ETOOBIG;
-  if (!a->rays) return 0;
   TraceK k;
   k.batch = a->batch, k.rays = a->rays, k.samples = a->samples;
   k.ns = a->n_sph, k.nb = a->n_box, k.np = a->n_pln, k.shared_origin = a->shared_origin ? 1 : 0;
@@ -364,7 +394,7 @@ FLYB_API int flyb_trace(const flyb_trace_args* a, void* stream) {
   k.weights = a->weights, k.out = a->out;
   // scene (rounded up to 16 bytes), per-sphere origin terms, per-thread radiance for the sample sums
   const size_t bytes = (size_t)(((k.floats + 3) & ~3) + 4 * k.ns) * sizeof(float) +
-                       (a->samples > 1 ? kThreads * sizeof(float4) : 0);
+                       (a->samples > 1 ? kThreads * sizeof(float4) : 0) + (size_t)k.ns * sizeof(int);
   if (bytes > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return (int)e;

@@ -125,6 +125,8 @@ def launch_trace(scene: torch.Tensor, shape: tuple, detail: float, out: torch.Te
                  pose: torch.Tensor | None = None, weights: torch.Tensor | None = None, shared_origin: bool = False,
                  rays: int, batch: int) -> None:
     """One flyb_trace launch on the current stream (arguments as in include/flyb200.h)."""
+    if rays == 0:
+        return
     tensors = [t for t in (scene, origins, dirs, eye_dirs, pose, weights, out) if t is not None]
     for t in tensors:
         if t.device != out.device or t.device.type != "cuda" or not t.is_contiguous():
