@@ -51,12 +51,28 @@ __device__ __forceinline__ long long mod_mersenne31(unsigned long long x) {
   return (long long)(x >= m ? x - m : x);
 }
 
+// second stage of the lattice hash from the first residue h in [0, 2^31 - 1)
+__device__ __forceinline__ float hash_tail(long long h) {
+  h = mod_mersenne31((unsigned long long)(h ^ (h >> 13)) * 1274126177ull);
+  return (float)(int)(h & 65535) / 32768.0f - 1.0f;  // h >= 0
+}
+
 // lattice hash in [-1, 1] (world.py:21-25); the linear form wraps in 64 bits like torch's int64
 __device__ __forceinline__ float lattice_hash(long long lin) {
   long long h = lin % 2147483647ll;
   if (h < 0) h += 2147483647ll;
-  h = mod_mersenne31((unsigned long long)(h ^ (h >> 13)) * 1274126177ull);
-  return (float)(int)(h & 65535) / 32768.0f - 1.0f;  // h >= 0
+  return hash_tail(h);
+}
+
+// x mod (2^31 - 1), non-negative, for |x| < 2^62: 2^31 is 1 modulo 2^31 - 1, so the high and low
+// halves fold together
+__device__ __forceinline__ long long residue_m31(long long x) {
+  const long long m = 2147483647ll;
+  x = (x >> 31) + (x & m);
+  x = (x >> 31) + (x & m);
+  if (x < 0) x += m;
+  if (x >= m) x -= m;
+  return x;
 }
 
 // int64 of an integer-valued float, through the 32-bit conversion when it fits
@@ -74,9 +90,33 @@ __device__ float value_noise(float px, float py, float pz, float scale) {
   fx = (fx * fx) * (3.f - 2.f * fx);
   fy = (fy * fy) * (3.f - 2.f * fy);
   fz = (fz * fz) * (3.f - 2.f * fz);
+  float out = 0.f;
+  if (fabsf(flx) < 1073741824.f && fabsf(fly) < 1073741824.f && fabsf(flz) < 1073741824.f) {
+    // |i| < 2^30: the linear form cannot wrap, so its residue is the sum of the per-axis residues;
+    // the z coefficient is the modulus itself, so z drops out and corners (x, y, 0), (x, y, 1)
+    // share one hash
+    const long long m = 2147483647ll;
+    long long hx[2], hy[2];
+    hx[0] = residue_m31(ix * 374761393ll);
+    hy[0] = residue_m31(iy * 668265263ll);
+    hx[1] = hx[0] + 374761393ll >= m ? hx[0] + 374761393ll - m : hx[0] + 374761393ll;
+    hy[1] = hy[0] + 668265263ll >= m ? hy[0] + 668265263ll - m : hy[0] + 668265263ll;
+#pragma unroll
+    for (int dx = 0; dx < 2; ++dx) {
+      const float wx = dx ? fx : 1.f - fx;
+#pragma unroll
+      for (int dy = 0; dy < 2; ++dy) {
+        const float wy = dy ? fy : 1.f - fy;
+        const long long h = hx[dx] + hy[dy];
+        const float g = hash_tail(h >= m ? h - m : h);
+        out = out + ((wx * wy) * (1.f - fz)) * g;
+        out = out + ((wx * wy) * fz) * g;
+      }
+    }
+    return out;
+  }
   const unsigned long long A = 374761393ull, Bc = 668265263ull, C = 2147483647ull;
   const unsigned long long base = (unsigned long long)ix * A + (unsigned long long)iy * Bc + (unsigned long long)iz * C;
-  float out = 0.f;
 #pragma unroll
   for (int dx = 0; dx < 2; ++dx) {
     const float wx = dx ? fx : 1.f - fx;
