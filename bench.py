@@ -324,16 +324,15 @@ def measure_e2e(cfg, eng, device, steps) -> dict:
     ptr = torch.tensor(np.r_[0, np.cumsum([len(g) for g in groups])], dtype=torch.int32, device=device)
     idx = torch.tensor(np.concatenate(groups), dtype=torch.int32, device=device)
     out_host = torch.empty(B, 90, dtype=torch.float64).pin_memory()
-    rate = eng.lif.rate                               # (B, N) view; the readout reads it batch-major
-    rate_bm = torch.empty(B, cfg.n_spiking, device=device)
+    out_dev = torch.empty(B, 90, dtype=torch.float64, device=device)
+    rate_nb = eng.lif._st["rate"]                     # [N][B]: the readout reads the native layout
     n = min(steps, 100)
 
     def one():
         rad_dev.copy_(rad_host, non_blocking=True)
         eng.set_photoreceptors(photoreceptor_contrast(cfg, rad_dev))
         eng.step(1)
-        rate_bm.copy_(rate)
-        out_host.copy_(fcuda.group_means(ptr, idx, rate_bm), non_blocking=True)
+        out_host.copy_(fcuda.group_means_native(ptr, idx, rate_nb, out_dev), non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
     for _ in range(3):

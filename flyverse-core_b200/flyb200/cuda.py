@@ -109,6 +109,27 @@ def event_scatter(ptr, idx, weights, x, g, pre_ids=None):
           int(weights.dtype == torch.float16), -1 if pre_ids is None else pre_ids.numel())
 
 
+def group_means_native(ptr, idx, rates_nb, out):
+    """out (B, groups) float64 = group means of the fly-minor rates [N][B] (flyb_group_means: the
+    reduction of `group_means` without a batch-major copy of the rates)."""
+    if ptr.dtype != torch.int32 or idx.dtype != torch.int32 or rates_nb.dtype != torch.float32 or rates_nb.ndim != 2:
+        raise ValueError("group indices must be int32 vectors; rates must be a float32 (N, B) matrix")
+    groups, batch = ptr.numel() - 1, rates_nb.shape[1]
+    if out.dtype != torch.float64 or tuple(out.shape) != (batch, groups):
+        raise ValueError(f"out must be float64 of shape ({batch}, {groups})")
+    for t in (ptr, idx, rates_nb, out):
+        if t.device != out.device or t.device.type != "cuda" or not t.is_contiguous():
+            raise ValueError("CUDA kernels require contiguous tensors on the same CUDA device")
+    if groups <= 0:
+        return out
+    with torch.cuda.device(out.device):
+        error = _abi.lib().flyb_group_means(ptr.data_ptr(), idx.data_ptr(), rates_nb.data_ptr(), out.data_ptr(),
+                                            groups, batch, torch.cuda.current_stream(out.device).cuda_stream)
+    if error:
+        raise RuntimeError(f"flyb_group_means: CUDA error {error}")
+    return out
+
+
 def group_means(ptr, idx, rates, spikes=None):
     """(B, groups [+1]) float64 means of rates over index groups (+ spike totals)."""
     if ptr.dtype != torch.int32 or idx.dtype != torch.int32 or ptr.ndim != 1 or idx.ndim != 1 or rates.ndim != 2:

@@ -14,14 +14,13 @@ graph, straight from the fly-minor rate state, and copied asynchronously into pi
 """
 from __future__ import annotations
 
-import ctypes as ct
 import math
 from dataclasses import asdict
 
 import numpy as np
 import torch
 
-from . import _abi
+from . import cuda as fcuda
 from .brain import Brain, LIFParams
 from .connectome import PHOTORECEPTOR_TYPES
 from .optic import OpticLobe, OpticParams
@@ -219,15 +218,7 @@ class FlyBrain:
         return names, ptr, flat
 
     def _launch_means(self, ptr, flat, out) -> None:
-        groups = ptr.numel() - 1
-        if not groups:
-            return
-        stream = torch.cuda.current_stream(self.device).cuda_stream
-        rc = _abi.lib().flyb_group_means(ct.c_void_p(ptr.data_ptr()), ct.c_void_p(flat.data_ptr()),
-                                         ct.c_void_p(self.brain._st["rate"].data_ptr()), ct.c_void_p(out.data_ptr()),
-                                         groups, self.B, ct.c_void_p(stream))
-        if rc:
-            raise RuntimeError(f"flyb_group_means: error {rc}")
+        fcuda.group_means_native(ptr, flat, self.brain._st["rate"], out)
 
     def set_motor(self, groups: dict | None) -> None:
         """Register the motor groups that every frame reads out (None to stop): {name: neuron
