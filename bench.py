@@ -409,7 +409,14 @@ def measure_tracer(device, batch: int = BATCH, reps: int = 50, cpu: bool = True)
     out = torch.empty(batch, n_col, 4, device=device)
     for _ in range(3):
         bw.trace_eye(out)
-    ms = events_time(lambda: bw.trace_eye(out), reps)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(reps):                 # back to back: device time per launch, no host gaps
+        bw.trace_eye(out)
+    t1.record()
+    t1.synchronize()
+    ms = t0.elapsed_time(t1) / reps
     rays = batch * n_col * k
 
     def frame():

@@ -26,7 +26,10 @@ constexpr float kTiny = 1e-9f;    // division guard of box slabs and planes
 constexpr int kMatFloats = 16;    // refl 4, refl2 4, emit 4, pattern scale, pattern id, 2 spare
 constexpr int kLightFloats = 12;  // position 3, colour 4, ambient 4, 1 spare
 constexpr int kMaxObjects = 512;
-constexpr int kThreads = 256;
+#ifndef FLYB_TRACE_THREADS
+#define FLYB_TRACE_THREADS 256
+#endif
+constexpr int kThreads = FLYB_TRACE_THREADS;  // rays per block
 
 __host__ __device__ inline int scene_floats(int ns, int nb, int np) {
   return 6 * (ns + nb + np) + kMatFloats * (ns + nb + np + 1) + kLightFloats;
@@ -332,6 +335,9 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(TraceK k) {
   float* occ = sm + ((k.floats + 3) & ~3);            // [ns][4], 16-byte aligned
   float4* partial = reinterpret_cast<float4*>(occ + 4 * k.ns);
   int* order = reinterpret_cast<int*>(partial + (k.samples > 1 ? kThreads : 0));  // [ns]
+  int* arrived = order + k.ns;                        // [per_block] samples finished per column
+  if (k.samples > 1)
+    for (int i = threadIdx.x; i < k.per_block; i += blockDim.x) arrived[i] = 0;
   SceneSm s;
   s.ns = k.ns, s.nb = k.nb, s.np = k.np;
   s.sph = sm, s.box = sm + 6 * k.ns, s.pln = sm + 6 * (k.ns + k.nb);
@@ -391,17 +397,21 @@ __global__ void __launch_bounds__(kThreads) trace_kernel(TraceK k) {
     if (active) dst[col] = rad;
     return;
   }
+  if (!active) return;
+  // the last sample of a column to finish sums the column in sample order: no block barrier, so
+  // a warp of cheap rays does not wait for the block's slowest one
   partial[threadIdx.x] = rad;
-  __syncthreads();
-  if (active && j == 0) {
-    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int q = 0; q < k.samples; ++q) {
-      const float w = k.weights[q];
-      const float4 v = partial[threadIdx.x + q];
-      acc.x = acc.x + v.x * w, acc.y = acc.y + v.y * w, acc.z = acc.z + v.z * w, acc.w = acc.w + v.w * w;
-    }
-    dst[col] = acc;
+  __threadfence_block();
+  if (atomicAdd(&arrived[local], 1) != k.samples - 1) return;
+  __threadfence_block();
+  const int first = local * k.samples;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int q = 0; q < k.samples; ++q) {
+    const float w = k.weights[q];
+    const float4 v = partial[first + q];
+    acc.x = acc.x + v.x * w, acc.y = acc.y + v.y * w, acc.z = acc.z + v.z * w, acc.w = acc.w + v.w * w;
   }
+  dst[col] = acc;
 }
 
 }  // namespace
@@ -434,7 +444,7 @@ FLYB_API int flyb_trace(const flyb_trace_args* a, void* stream) {
   k.weights = a->weights, k.out = a->out;
   // scene (rounded up to 16 bytes), per-sphere origin terms, per-thread radiance for the sample sums
   const size_t bytes = (size_t)(((k.floats + 3) & ~3) + 4 * k.ns) * sizeof(float) +
-                       (a->samples > 1 ? kThreads * sizeof(float4) : 0) + (size_t)k.ns * sizeof(int);
+                       (a->samples > 1 ? kThreads * sizeof(float4) : 0) + (size_t)(k.ns + k.per_block) * sizeof(int);
   if (bytes > 48 * 1024) {
     const cudaError_t e = cudaFuncSetAttribute(trace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return (int)e;
