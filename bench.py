@@ -15,7 +15,9 @@ Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthet
   adjoint        optic-lobe adjoint over 200 substeps (89,390 units, 6 M nnz, checkpoint 20) over
                  the forward pass time
   e2e            the same B=64 step through the public API with, every step, the radiance copied in
-                 from pinned host memory and the motor readout copied out
+                 from pinned host memory and the motor readout copied out, the calls captured once
+                 as a CUDA graph and the host synchronising on every step's readout (the eager
+                 launch-by-launch figure is reported beside it)
   roofline       the LIF step kernel: algorithmic bytes / CUDA-event time against measured HBM copy
   tracer         the eye's ray tracer at 64 flies x 1,634 columns x 7 rays: device time, the frame
                  path beside the reference's own torch tracer on the same GPU (baseline/_ref), and
@@ -170,12 +172,14 @@ def build_engine(cfg, batch, device, launch, fly0=0):
     return eng
 
 
-def photoreceptor_contrast(cfg, rad: torch.Tensor) -> torch.Tensor:
+def photoreceptor_contrast(cfg, rad: torch.Tensor, tables=None) -> torch.Tensor:
     """Held photoreceptor activity [n_pr][B] of a radiance frame (B, n_col, 4): channel-weighted
-    intensity, contrast against the frame mean (the stage's steady state)."""
+    intensity, contrast against the frame mean (the stage's steady state). `tables` = the device
+    copies of (sensitivity, photoreceptor column) when the call is captured in a graph."""
     o = cfg.optic
-    sens = torch.from_numpy(o.sens).to(rad.device)
-    col = torch.from_numpy(o.pr_column.astype(np.int64)).to(rad.device)
+    if tables is None:
+        tables = (torch.from_numpy(o.sens).to(rad.device), torch.from_numpy(o.pr_column.astype(np.int64)).to(rad.device))
+    sens, col = tables
     ip = (rad[:, col, :] * sens[None]).sum(-1)                            # (B, n_pr)
     con = ((ip - ip.mean(1, keepdim=True)) / (ip.mean(1, keepdim=True) + 0.02)).clamp(-1.0, 2.0)
     return con.t().contiguous()
@@ -326,24 +330,42 @@ def measure_e2e(cfg, eng, device, steps) -> dict:
     out_host = torch.empty(B, 90, dtype=torch.float64).pin_memory()
     out_dev = torch.empty(B, 90, dtype=torch.float64, device=device)
     rate_nb = eng.lif._st["rate"]                     # [N][B]: the readout reads the native layout
+    tables = (torch.from_numpy(o.sens).to(device), torch.from_numpy(o.pr_column.astype(np.int64)).to(device))
     n = min(steps, 100)
 
     def one():
         rad_dev.copy_(rad_host, non_blocking=True)
-        eng.set_photoreceptors(photoreceptor_contrast(cfg, rad_dev))
+        eng.set_photoreceptors(photoreceptor_contrast(cfg, rad_dev, tables))
         eng.step(1)
         out_host.copy_(fcuda.group_means_native(ptr, idx, rate_nb, out_dev), non_blocking=True)
-        torch.cuda.current_stream().synchronize()
 
-    for _ in range(3):
-        one()
-    t0 = time.perf_counter()
-    for _ in range(n):
-        one()
-    dt = time.perf_counter() - t0
+    def timed(fn) -> float:
+        for _ in range(3):
+            fn()
+            torch.cuda.current_stream().synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+            torch.cuda.current_stream().synchronize()       # the host reads this step's readout
+        return time.perf_counter() - t0
+
+    dt_eager = timed(one)
+    # the same calls captured once: a replay copies the pinned radiance in and the readout out
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            one()
+    torch.cuda.current_stream().wait_stream(s)
+    dt = timed(g.replay)
+    del g
     return {"value": eng.n_neurons * B * n / dt, "unit": "neuron-steps/s",
             "h2d_bytes_per_step": int(rad_host.numel() * 4), "d2h_bytes_per_step": int(out_host.numel() * 8),
-            "steps": n}
+            "steps": n, "path": "radiance H2D from pinned memory, photoreceptor contrast, whole-fly step, motor "
+                                "readout D2H to pinned memory, captured once as a CUDA graph; replayed and "
+                                "synchronised every step",
+            "eager": {"value": eng.n_neurons * B * n / dt_eager, "note": "the same calls launched one by one"}}
 
 
 def cpu_port_rate(cfg, batch: int, steps: int, threads: int) -> dict:
