@@ -46,6 +46,9 @@ struct LifK {
   unsigned* spike_n;  // entries appended this step
   long long spike_cap;
   const float* __restrict__ adapt_jump;   // per-neuron adaptation jump, or null (P.jump)
+  const unsigned char* __restrict__ clock_k;  // per-neuron update period, or null (every step)
+  const float* __restrict__ clock_coef;       // [max period + 1][FLYB_CLOCK_NCOEF]
+  long long* clock_acc;                       // [n][batch] input pending until the next update
   LifP P;
 };
 
@@ -580,6 +583,132 @@ __global__ void __launch_bounds__(BLOCK, (DEFER && IPT <= 2) ? 1024 / BLOCK : 1)
 
 __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
 
+// ------------------------------------------------------------------ per-neuron clocks
+// The clocked step (brain.py:899-957): neuron i updates on steps with step % k_i == 0, with the
+// coefficients of a k_i * dt step (row k_i of clock_coef); on other steps it takes row 0 (no
+// decay, no refractory time, no spike, no Poisson). Input arriving at a period-k_i neuron between
+// its updates is summed exactly in clock_acc and applied on the update step, as the reference
+// applies W_k to the spikes accumulated over the period. One item per thread, then the block-wide
+// delivery of the register path.
+template <int BLOCK, bool FIXED>
+__global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
+  using RingT = typename std::conditional<FIXED, long long, int>::type;
+  __shared__ LifSmem<BLOCK> sm;
+  const Clk clk = read_clock(k);
+  const long long W = k.t_end;
+  const long long t = k.t_begin + (long long)blockIdx.x * BLOCK + threadIdx.x;
+  const int rs = slot_after(clk.ring_pos, s, k.R);
+  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
+  const size_t slot = (size_t)k.n * k.batch;
+  const int flags = k.flags;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const LifP& P = k.P;
+  unsigned fired_bit = 0, tx_bit = 0;
+  int iq[1] = {0}, bq[1] = {0};
+  float xq[1] = {0.0f};
+  if (t < W) {
+    const int i = (int)(t / k.batch), b = (int)(t - (long long)i * k.batch);
+    iq[0] = i;
+    bq[0] = b;
+    const bool live = !(flags & FLYB_LIF_EPISODES) || s < k.fly_steps[b];
+    if (live) {
+      RingT* rp = (RingT*)k.ring + (size_t)rs * slot + t;
+      long long due = *rp;
+      if (due) *rp = 0;
+      const long long step = clk.step0 + s;
+      const int period = k.clock_k[i];
+      const bool on = period == 1 || step % period == 0;
+      if (period > 1) {
+        const long long held = k.clock_acc[t], sum = held + due;
+        due = on ? sum : 0;
+        const long long keep = on ? 0 : sum;
+        if (keep != held) k.clock_acc[t] = keep;
+      }
+      const float* cf = k.clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
+      const float act = k.active[i];
+      float g1 = k.g[t] * cf[FLYB_CLOCK_A_S];
+      if (due) {
+        const float inc = FIXED ? __double2float_rn((double)due * (1.0 / 4294967296.0)) : P.w_syn * (float)due;
+        g1 = g1 + inc;
+      }
+      k.g[t] = g1;
+      const float ad = k.adapt[t];
+      float target = P.v_rest + g1;
+      target = target + k.drive[t];
+      target = target - ad;
+      float u = k.v[t] - target;
+      u = u * cf[FLYB_CLOCK_A_M];
+      float v1 = target + u;
+      float r1 = k.refrac[t];
+      if (r1 > 0.0f) v1 = P.v_reset;
+      r1 = r1 - cf[FLYB_CLOCK_DT];
+      if (r1 < 0.0f) r1 = 0.0f;
+      float spike = (v1 >= P.v_th ? 1.0f : 0.0f) * cf[FLYB_CLOCK_U];
+      spike = spike * act;
+      if (flags & FLYB_LIF_POISSON) {
+        const float q = k.poisson_p[t] * cf[FLYB_CLOCK_POIS];
+        if (q > 0.0f) {
+          const float un = (flags & FLYB_LIF_EXT_UNIFORM)
+                               ? k.uniforms[(size_t)s * slot + t]
+                               : philox_uniform(k.seed, clk.step0 + s, (uint32_t)i, (uint32_t)(k.fly0 + b));
+          if (un < q) spike = 1.0f;
+        }
+      }
+      const bool fired = spike > 0.0f;
+      if (fired) { v1 = P.v_reset; r1 = P.t_ref; }
+      k.v[t] = v1;
+      k.refrac[t] = r1;
+      k.spikes[t] = spike;
+      if (flags & FLYB_LIF_ADAPT) {
+        float a1 = ad * cf[FLYB_CLOCK_A_AD];
+        a1 = a1 + spike * (k.adapt_jump ? __ldg(&k.adapt_jump[i]) : P.jump);
+        k.adapt[t] = a1;
+      }
+      float x = spike;
+      if (flags & FLYB_LIF_STD) {
+        float r2 = k.res[t];
+        x = spike * r2;
+        if (fired) { const float keep = 1.0f - k.std_u[i]; r2 = r2 * keep; }
+        float dep = 1.0f - r2;
+        dep = dep * cf[FLYB_CLOCK_A_STD];
+        k.res[t] = 1.0f - dep;
+      }
+      if (flags & FLYB_LIF_COUNTS) k.counts[t] = k.counts[t] + spike;
+      float r3 = k.rate[t] * cf[FLYB_CLOCK_A_R];
+      r3 = r3 + spike * cf[FLYB_CLOCK_RATE_GAIN];
+      k.rate[t] = r3;
+      if (fired) fired_bit = 1u;
+      if (x != 0.0f) { tx_bit = 1u; xq[0] = x; }
+    }
+  }
+  if (k.raster) {
+    const unsigned bits = __ballot_sync(0xffffffffu, fired_bit);
+    const long long wbase = k.t_begin + (long long)blockIdx.x * BLOCK + (long long)warp * 32;
+    if (lane == 0 && wbase < W) {
+      const size_t rslot = k.raster_slots > 0 ? (size_t)slot_after(clk.raster_pos, s, k.raster_slots) : (size_t)s;
+      k.raster[rslot * k.words + (size_t)(wbase >> 5)] = bits;
+    }
+  }
+  deliver<BLOCK, FIXED, 1>(k, sm, tx_bit, iq, bq, xq, ws, slot);
+}
+
+static bool needs_advance(const LifK& k);
+
+template <int BLOCK, bool FIXED>
+static int run_lif_clocked(const LifK& k, cudaStream_t st) {
+  const long long W = (long long)k.t_end - k.t_begin;
+  const unsigned blocks = (unsigned)((W + BLOCK - 1) / BLOCK);
+  for (int s = 0; s < k.nsteps; ++s) {
+    lif_clocked_kernel<BLOCK, FIXED><<<blocks, BLOCK, 0, st>>>(k, s);
+    FLYB_CHECK_LAUNCH();
+  }
+  if (needs_advance(k)) {
+    lif_advance_kernel<<<1, 256, 0, st>>>(k);
+    FLYB_CHECK_LAUNCH();
+  }
+  return 0;
+}
+
 // A run ends by advancing the device clock / episode counters unless the caller does it later.
 static bool needs_advance(const LifK& k) {
   return (k.clock || (k.flags & FLYB_LIF_EPISODES)) && !(k.flags & FLYB_LIF_NO_ADVANCE);
@@ -1061,6 +1190,8 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.events = a->events; k.status = a->status; k.sync = a->sync;
   k.spike_list = nullptr; k.spike_n = nullptr; k.spike_cap = 0;
   k.adapt_jump = a->adapt_jump;
+  k.clock_k = a->clock_k; k.clock_coef = a->clock_coef; k.clock_acc = (long long*)a->clock_acc;
+  if (a->clock_k && (!a->clock_coef || !a->clock_acc || (a->flags & FLYB_LIF_DEFER_DELIVERY))) return FLYB_EINVAL;
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
     if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP || a->staged)
@@ -1091,6 +1222,10 @@ FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   const bool fixed = a->ring_mode == FLYB_RING_FIXED;
   const int block = a->block ? a->block : 256;
+  if (k.clock_k) {
+    if (block != 128 && block != 256 && block != 512) return FLYB_EINVAL;
+    return fixed ? run_lif_clocked<256, true>(k, st) : run_lif_clocked<256, false>(k, st);
+  }
   switch (block) {
     case 128: return fixed ? run_lif<128, true>(k, a->items_per_thread, a->launch, a->grid, a->staged, st)
                      : run_lif<128, false>(k, a->items_per_thread, a->launch, a->grid, a->staged, st);

@@ -95,6 +95,31 @@ def lif_coefficients(p: LIFParams, std_on: bool, adapt_on: bool | None = None) -
     return P
 
 
+def clock_coefficients(p: LIFParams, std_on: bool, max_period: int) -> np.ndarray:
+    """[max_period + 1][CLOCK_NCOEF] float32 phase coefficients of per-neuron clocks (brain.py:
+    627-637): row k those of an update of a period-k neuron (a step of k * dt), row 0 those of a
+    step without update (no decay, no refractory time, no spike, no Poisson). Evaluated with the
+    reference's float32 tensor expressions on the CPU, so they carry its bits."""
+    kt = torch.arange(max_period + 1, dtype=torch.float32)
+    kt[0] = 1.0
+    u = torch.ones(max_period + 1)
+    u[0] = 0.0
+    one = torch.ones_like(u)
+
+    def coef(tau):
+        return torch.where(u > 0, torch.exp(-p.dt * kt / tau), one)
+
+    out = torch.zeros(max_period + 1, _abi.CLOCK_NCOEF)
+    out[:, _abi.CLOCK_A_M], out[:, _abi.CLOCK_A_S], out[:, _abi.CLOCK_A_R] = coef(p.tau_m), coef(p.tau_syn), coef(p.rate_tau)
+    out[:, _abi.CLOCK_A_AD] = coef(p.adapt_tau) if p.adapt_jump > 0 else torch.zeros_like(u)
+    out[:, _abi.CLOCK_A_STD] = coef(p.std_tau) if std_on else one
+    out[:, _abi.CLOCK_DT] = u * kt * p.dt
+    out[:, _abi.CLOCK_RATE_GAIN] = u * (1 - torch.exp(-p.dt * kt / p.rate_tau)) * 1000.0 / (kt * p.dt)
+    out[:, _abi.CLOCK_U] = u
+    out[:, _abi.CLOCK_POIS] = u * kt
+    return out.numpy()
+
+
 def out_edges(W, w_syn: float, prefer: str = "auto", std_on: bool = False):
     """Pre-major (CSC) outgoing synapses of W[post, pre] for the native step.
 
@@ -125,8 +150,6 @@ def _unsupported(p: LIFParams, metal_kernels, cuda_kernels, cuda_sparse) -> None
     if p.surrogate_grad:
         raise NotImplementedError("surrogate_grad (Torch autograd through the LIF) is not part of the native step; "
                                   "the spiking path is left undifferentiated")
-    if p.dt_by_module:
-        raise NotImplementedError("per-module clocks (dt_by_module) are not in the native LIF step")
     if p.receptor_model == "full":
         raise NotImplementedError("the slow receptor term (receptor_model='full') is not in the native LIF step")
     if p.weight_dtype not in ("float32", "float16"):
@@ -201,6 +224,7 @@ class Brain:
         self.t, self.step_count, self.buf_pos = 0.0, 0, 0
         self._rate_np, self._rate_np_key = None, None
         self._weights_version = 0
+        self._kvec = None                       # per-neuron clocks (set_clocks)
         self._W_cpu = W
         self.set_weights(W)
 
@@ -234,6 +258,8 @@ class Brain:
         self._out_ptr = torch.from_numpy(indptr).to(self.device)
         self._out_edge = torch.from_numpy(edges).to(self.device)
         dtype = torch.int32 if mode == _abi.RING_COUNT else torch.int64
+        if getattr(self, "_kvec", None) is not None and had_ring and self.ring.dtype != dtype:
+            self.clock_acc.zero_()          # held input is in the units of the previous ring
         self.ring = torch.zeros(self.R, self.n, self.B, dtype=dtype, device=self.device)
         self._make_args()
         if had_ring and spike_buf is not None:
@@ -268,12 +294,39 @@ class Brain:
         a.ring, a.clock, a.raster = self.ring.data_ptr(), self._clock.data_ptr(), self._hist.data_ptr()
         a.events, a.status, a.sync = self._events.data_ptr(), self._status.data_ptr(), self._sync.data_ptr()
         a.adapt_jump = None if self.adapt_jump_vec is None else self.adapt_jump_vec.data_ptr()
+        if self._kvec is not None:
+            a.clock_k, a.clock_coef = self._clock_k.data_ptr(), self._clock_coef.data_ptr()
+            a.clock_acc = self.clock_acc.data_ptr()
         self._args = a
         self._lists = {}          # deferred-delivery lists per neuron range, sized on first use
 
     def _defer_active(self) -> bool:
         """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step register launches."""
-        return bool(getattr(self, "defer", False)) and self.launch == "step" and not getattr(self, "staged", False)
+        return bool(getattr(self, "defer", False)) and self.launch == "step" and not getattr(self, "staged", False) \
+            and self._kvec is None
+
+    # ------------------------------------------------------------------ per-neuron clocks
+    def set_clocks(self, multiplier) -> None:
+        """Integrate neuron i every multiplier[i] base steps (dt_i = multiplier[i] * dt), the
+        reference's Brain.set_clocks (brain.py:618-640): on other steps a neuron holds its state and
+        the input that reaches it waits for its next update. The native step then runs one launch
+        per step through the clocked kernel. Input already held for a slow neuron stays in the
+        units of the ring it arrived on (it is dropped if set_weights changes the ring mode)."""
+        k = np.asarray(multiplier, dtype=np.int64)
+        if k.shape != (self.n,) or (k < 1).any():
+            raise ValueError("multiplier must be an (N,) array of positive integers")
+        p = self.p
+        if int(k.max()) * p.dt > p.delay + 1e-9:
+            raise ValueError("the slowest clock must not exceed the synaptic delay")
+        if int(k.max()) > 255:
+            raise ValueError("clock periods above 255 steps are not supported")
+        self._kvec = k
+        self.K = int(np.lcm.reduce(np.unique(k)))
+        self._clock_k = torch.from_numpy(k.astype(np.uint8)).to(self.device)
+        self._clock_coef = torch.from_numpy(clock_coefficients(p, self._std_on, int(k.max()))).to(self.device)
+        self.clock_acc = torch.zeros(self.n, self.B, dtype=torch.int64, device=self.device)
+        self._weights_version += 1
+        self._make_args()
 
     def _set_delivery(self, a, n_first: int, n_count: int) -> None:
         """Point the arguments at the spike list of this neuron range (one list per range, so
@@ -404,6 +457,8 @@ class Brain:
         st["res"][:, sel] = 1.0
         self.g_slow[sel] = 0.0
         self.ring[:, :, sel] = 0
+        if self._kvec is not None:
+            self.clock_acc[:, sel] = 0
         if rows is None:
             self._hist.zero_()
         else:
@@ -467,6 +522,8 @@ class Brain:
         out = {k: getattr(self, k).detach().cpu().clone() for k in _STATE}
         out.update(ring=self.ring.cpu().clone(), hist=self._hist.cpu().clone(), clock=self._clock.cpu().clone(),
                    scalars=dict(t=self.t, step_count=self.step_count, buf_pos=self.buf_pos, _poisson_on=self._poisson_on))
+        if self._kvec is not None:
+            out.update(clock_period=self._kvec.copy(), clock_acc=self.clock_acc.cpu().clone())
         return out
 
     def load_state_dict(self, state: dict) -> None:
@@ -477,6 +534,12 @@ class Brain:
         self.ring.copy_(state["ring"].to(self.device))
         self._hist.copy_(state["hist"].to(self.device))
         self._clock.copy_(state["clock"].to(self.device))
+        if "clock_period" in state:
+            if self._kvec is None or not np.array_equal(state["clock_period"], self._kvec):
+                self.set_clocks(state["clock_period"])
+            self.clock_acc.copy_(state["clock_acc"].to(self.device))
+        elif self._kvec is not None:
+            raise ValueError("checkpoint has no per-neuron clocks but this brain runs them")
         for k, v in state["scalars"].items():
             setattr(self, k, v)
         self._rate_np_key = None

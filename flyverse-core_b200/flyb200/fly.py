@@ -55,6 +55,9 @@ class FlyBrain:
                 self.brain.freeze(self.optic.rate_idx)
                 if lp.prune_frozen:
                     self.brain.prune(self.optic.rate_idx)
+        if lp.dt_by_module:             # per-module clocks (fly.py:98-107)
+            from .regions import clock_periods
+            self.brain.set_clocks(clock_periods(c, lp.dt, lp.dt_by_module))
         self._radiance = None
         self._pending_ms = 0.0
         self._base_poisson = torch.zeros_like(self.brain.poisson_p)

@@ -153,7 +153,24 @@ typedef struct flyb_lif_args {
   const float* adapt_jump; /* optional [n]: per-neuron adaptation jump (mV per spike) under
                             FLYB_LIF_ADAPT, the reference's adapt_by_type (brain.py:497-506);
                             null = params[FLYB_P_ADAPT_JUMP] for every neuron             */
+  /* Per-neuron clocks (Brain.set_clocks, brain.py:618-640 and the clocked step :899-957): neuron
+   * i integrates only on steps with step % clock_k[i] == 0, with the coefficients of a step of
+   * clock_k[i] * dt; its synaptic input arriving in between is held in clock_acc and applied on
+   * its next update. Null clock_k: every neuron every step. Runs one launch per step (launch,
+   * items_per_thread, staged are ignored); FLYB_LIF_DEFER_DELIVERY is not allowed with it. */
+  const unsigned char* clock_k; /* [n] update period in steps, 1..255 (device)               */
+  const float* clock_coef; /* [max period + 1][FLYB_CLOCK_NCOEF] (device): row p holds the
+                            coefficients of an update of a period-p neuron, row 0 those of a
+                            step on which a neuron does not update                         */
+  void* clock_acc;       /* [n][batch] int64 (device): pending input of neurons with period
+                            > 1, in ring units (counts, or Q32.32 mV)                       */
 } flyb_lif_args;
+
+/* Columns of flyb_lif_args.clock_coef */
+enum {
+  FLYB_CLOCK_A_M, FLYB_CLOCK_A_S, FLYB_CLOCK_DT, FLYB_CLOCK_A_AD, FLYB_CLOCK_A_STD, FLYB_CLOCK_A_R,
+  FLYB_CLOCK_RATE_GAIN, FLYB_CLOCK_U, FLYB_CLOCK_POIS, FLYB_CLOCK_NCOEF
+};
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);
 

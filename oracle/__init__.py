@@ -110,11 +110,13 @@ class LifState:
 
 
 def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0,
-            uniforms=None, fly_steps=None, raster=False, threads=0, fly0=0, adapt_jump=None):
+            uniforms=None, fly_steps=None, raster=False, threads=0, fly0=0, adapt_jump=None, clocks=None):
     """Advance `state` in place by `nsteps`; returns (raster bits [nsteps][words] or None, events).
     With `fly_steps` (EPISODES), fly b is live for its first fly_steps[b] steps; the array is then
     reduced by the steps taken, as the host layer does after a launch. `adapt_jump` (n,): per-neuron
-    adaptation jumps (the reference's adapt_by_type, brain.py:497-506)."""
+    adaptation jumps (the reference's adapt_by_type, brain.py:497-506). `clocks` = (period (n,),
+    coefficient table [max period + 1][CLOCK_NCOEF]): per-neuron clocks (brain.py:899-957); the
+    pending input of slow neurons lives in `state.clock_acc`."""
     n, B = state.n, state.batch
     words = (n * B + 31) // 32
     r = np.zeros((nsteps, words), np.uint32) if raster else None
@@ -125,6 +127,12 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
     uni = None if uniforms is None else _f32(uniforms)
     fs = None if fly_steps is None else np.ascontiguousarray(fly_steps, np.int32)
     aj = None if adapt_jump is None else _f32(adapt_jump)
+    ck = cc = None
+    if clocks is not None:
+        ck = np.ascontiguousarray(clocks[0], np.uint8)
+        cc = _f32(clocks[1])
+        if getattr(state, "clock_acc", None) is None:
+            state.clock_acc = np.zeros((n, B), np.int64)
     a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
                      ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, step0=state.step, seed=seed, fly0=fly0,
                      out_ptr=_p(out_ptr), out_edge=_p(out_edge), v=_p(state.v), g=_p(state.g),
@@ -132,7 +140,8 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
                      counts=_p(state.counts), spikes=_p(state.spikes), drive=_p(state.drive),
                      poisson_p=_p(state.poisson_p), active=_p(state.active), std_u=_p(state.std_u),
                      params=_p(P), ring=_p(state.ring), uniforms=_p(uni), fly_steps=_p(fs),
-                     raster=_p(r), events=_p(events), adapt_jump=_p(aj))
+                     raster=_p(r), events=_p(events), adapt_jump=_p(aj), clock_k=_p(ck), clock_coef=_p(cc),
+                     clock_acc=_p(getattr(state, "clock_acc", None)) if clocks is not None else None)
     rc = lib().oracle_lif_run(ct.byref(a), threads)
     if rc:
         raise ValueError(f"oracle_lif_run: status {rc}")

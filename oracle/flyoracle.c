@@ -88,17 +88,39 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
   uint64_t events = 0;
   for (int i = 0; i < n; ++i) {
     const size_t t = (size_t)i * B + b;
+    /* per-neuron clocks (brain.py:899-957): the coefficients of this neuron's phase; input that
+     * arrives between its updates waits in clock_acc */
+    float c_m = a_m, c_s = a_s, c_dt = dt, c_ad = a_ad, c_std = a_std, c_r = a_r, c_rg = rg, c_u = 1.0f,
+          c_pois = 1.0f;
+    int period = 1, on = 1;
+    if (a->clock_k) {
+      period = a->clock_k[i];
+      on = step % period == 0;
+      const float* cf = a->clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
+      c_m = cf[FLYB_CLOCK_A_M]; c_s = cf[FLYB_CLOCK_A_S]; c_dt = cf[FLYB_CLOCK_DT]; c_ad = cf[FLYB_CLOCK_A_AD];
+      c_std = cf[FLYB_CLOCK_A_STD]; c_r = cf[FLYB_CLOCK_A_R]; c_rg = cf[FLYB_CLOCK_RATE_GAIN]; c_u = cf[FLYB_CLOCK_U];
+      c_pois = cf[FLYB_CLOCK_POIS];
+    }
     /* 1. synaptic input due now: read and clear the ring slot */
-    float g = a->g[t];
-    g = g * a_s;
+    int64_t due;
     if (a->ring_mode == FLYB_RING_COUNT) {
       int32_t* ring = (int32_t*)a->ring + (size_t)rs * n * B;
-      int32_t c = ring[t]; ring[t] = 0;
-      if (c != 0) { float inc = w_syn * (float)c; g = g + inc; }
+      due = ring[t]; ring[t] = 0;
     } else {
       int64_t* ring = (int64_t*)a->ring + (size_t)rs * n * B;
-      int64_t c = ring[t]; ring[t] = 0;
-      if (c != 0) { float inc = float_of_fixed(c); g = g + inc; }
+      due = ring[t]; ring[t] = 0;
+    }
+    if (period > 1) {   /* the reference's per-period accumulator, applied on the update step */
+      int64_t* acc = (int64_t*)a->clock_acc + t;
+      *acc += due;
+      due = on ? *acc : 0;
+      if (on) *acc = 0;
+    }
+    float g = a->g[t];
+    g = g * c_s;
+    if (due != 0) {
+      float inc = a->ring_mode == FLYB_RING_COUNT ? w_syn * (float)due : float_of_fixed(due);
+      g = g + inc;
     }
     a->g[t] = g;
     /* 2. membrane (brain.py:839-843) */
@@ -106,16 +128,17 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     target = target + a->drive[t];
     target = target - a->adapt[t];
     float v = a->v[t] - target;
-    v = v * a_m;
+    v = v * c_m;
     v = target + v;
     float ref = a->refrac[t];
     if (ref > 0.0f) v = v_reset;
-    ref = ref - dt;
+    ref = ref - c_dt;
     if (ref < 0.0f) ref = 0.0f;
     /* 3. threshold and Poisson forcing (brain.py:845-849) */
-    float spike = (v >= v_th ? 1.0f : 0.0f) * a->active[i];
+    float spike = (v >= v_th ? 1.0f : 0.0f) * c_u;
+    spike = spike * a->active[i];
     if (flags & FLYB_LIF_POISSON) {
-      float p = a->poisson_p[t];
+      float p = a->poisson_p[t] * c_pois;
       if (p > 0.0f) {
         float u = (flags & FLYB_LIF_EXT_UNIFORM) ? a->uniforms[(size_t)k * n * B + t]
                                                  : oracle_uniform(a->seed, (uint64_t)step, (uint32_t)i, (uint32_t)(a->fly0 + b));
@@ -127,7 +150,7 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     a->v[t] = v; a->refrac[t] = ref; a->spikes[t] = spike;
     /* 4. adaptation, depression, counters, rate (brain.py:853-868) */
     if (flags & FLYB_LIF_ADAPT) {
-      float ad = a->adapt[t] * a_ad;
+      float ad = a->adapt[t] * c_ad;
       ad = ad + spike * (a->adapt_jump ? a->adapt_jump[i] : jump);
       a->adapt[t] = ad;
     }
@@ -136,11 +159,11 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
       float res = a->res[t];
       x = spike * res;
       if (fired) { float keep = 1.0f - a->std_u[i]; res = res * keep; }
-      float dep = 1.0f - res; dep = dep * a_std; res = 1.0f - dep;
+      float dep = 1.0f - res; dep = dep * c_std; res = 1.0f - dep;
       a->res[t] = res;
     }
     if (flags & FLYB_LIF_COUNTS) a->counts[t] = a->counts[t] + spike;
-    { float r = a->rate[t] * a_r; r = r + spike * rg; a->rate[t] = r; }
+    { float r = a->rate[t] * c_r; r = r + spike * c_rg; a->rate[t] = r; }
     if (fired_out) fired_out[t] = (unsigned char)fired;
     /* 5. deliver D steps later */
     if (x != 0.0f) {

@@ -15,6 +15,10 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
                   adaptation on: the shaped weights, rasters and final state.
   lif_19cell_adapt_by_type.npz  the same run with per-type adaptation jumps (ADAPT_BY_TYPE, the
                   reference's adapt_by_type): its per-neuron jump vector, rasters and final state.
+  lif_19cell_clocks.npz  the same run with per-neuron clocks (Brain.set_clocks, periods 1/2/3 steps
+                  by neuron index) on the reference's sparse-matmul path, which is where it runs them.
+  lif_c1_clocks.npz  config 1 at 6.5 mV drive with per-neuron clocks of 1, 2 and 4 steps on the
+                  reference's sparse-matmul path: rasters and final state.
   optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
                   of tests/test_optic_hooks.py::hex_graph(), batch 2, three frames.
   optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
@@ -87,6 +91,35 @@ def lif_c1(ref) -> dict:
     return out
 
 
+def lif_c1_clocks(ref) -> dict:
+    """Config 1's drive regime 6.5 mV with per-neuron clocks of 1, 2 and 4 steps (by neuron index),
+    on the reference's sparse-matmul path (where it runs clocks)."""
+    cn, brain = ref["connectome"], ref["brain"]
+    cfg = synthetic.lif_config1(seed=0)
+    c = cfg.c
+    rc = cn.Connectome(c.neurons[["bodyId", "type", "superclass", "nt"]].copy(), c.W.copy(),
+                       pd.Series(np.arange(c.n), index=c.neurons.bodyId.to_numpy()))
+    b = brain.Brain(rc, brain.LIFParams(**cfg.params, event_driven=False), device="cpu", seed=0)
+    period = np.array([1, 2, 4])[np.arange(c.n) % 3]
+    b.set_clocks(period)
+    b.set_poisson(cfg.poisson_idx, cfg.poisson_hz)
+    b.record_activity = True
+    b.set_drive(np.arange(c.n), np.float32(6.5))
+    seed = 1
+    U = uniforms(seed, cfg.steps, (1, c.n))
+    b.gen.manual_seed(seed)
+    ras = np.zeros((cfg.steps, c.n), bool)
+    for s in range(cfg.steps):
+        b.step(1)
+        ras[s] = b.spikes[0].numpy() > 0
+    out = {"raster": np.packbits(ras, axis=1, bitorder="little"), "uniform_sha": np.array(sha(U)),
+           "clock_period": period, "seed": np.int64(seed), "drive": np.float32(6.5)}
+    for key in ("v", "g", "rate", "spike_counts"):
+        out[key] = getattr(b, key)[0].numpy().copy()
+    print(f"lif_c1_clocks: {int(ras.sum())} spikes")
+    return out
+
+
 def _table(n: pd.DataFrame) -> dict:
     return {f"nrn_{col}": n[col].fillna("").astype(str).to_numpy().astype("U") for col in ("type", "superclass", "nt", "class")} | \
         {"nrn_bodyId": n.bodyId.to_numpy().astype(np.int64)}
@@ -95,16 +128,21 @@ def _table(n: pd.DataFrame) -> dict:
 ADAPT_BY_TYPE = {"^ORN_": 3.0, "^JO-": 0.4, "^DNp": 2.5}
 
 
-def lif_19cell(ref, adapt_by_type=None) -> dict:
+def lif_19cell(ref, adapt_by_type=None, clocks=False) -> dict:
     brain = ref["brain"]
     tb = ref["test_bit_identity"]
     c = tb.graph()
     B, steps, seed = 2, 400, 7
-    p = brain.LIFParams(receptor_model=None, event_driven=True, adapt_by_type=adapt_by_type)
+    # per-neuron clocks run on the reference's sparse-matmul path only (brain.py:624-625)
+    p = brain.LIFParams(receptor_model=None, event_driven=not clocks, adapt_by_type=adapt_by_type)
     b = brain.Brain(c, p, device="cpu", seed=seed, batch=B)
     frozen = np.flatnonzero((c.neurons.superclass == "ol_intrinsic").to_numpy())
     b.freeze(frozen)
     b.prune(frozen)
+    period = None
+    if clocks:            # periods 1, 2, 3 steps by neuron (K = 6); 3 x 0.5 ms stays within the delay
+        period = 1 + np.arange(c.n) % 3
+        b.set_clocks(period)
     b.record_activity = True
     orn = c.select(type="ORN_DM1")
     jo = c.select(type="~^JO-")
@@ -125,11 +163,13 @@ def lif_19cell(ref, adapt_by_type=None) -> dict:
                                "steps": np.int64(steps), "batch": np.int64(B)}
     for key in ("v", "g", "refrac", "adapt", "res", "rate", "spike_counts", "spikes"):
         out[f"final_{key}"] = getattr(b, key).numpy().copy()
+    if period is not None:
+        out["clock_period"] = period
     if adapt_by_type:
         out["adapt_jump_vec"] = b.adapt_jump_vec.numpy().copy()
         out["adapt_patterns"] = np.array(list(adapt_by_type), dtype="U")
         out["adapt_values"] = np.array(list(adapt_by_type.values()), np.float32)
-    print(f"lif_19cell (adapt_by_type={adapt_by_type}): {int(ras.sum())} spikes, {W.nnz} shaped entries")
+    print(f"lif_19cell (adapt_by_type={adapt_by_type}, clocks={clocks}): {int(ras.sum())} spikes, {W.nnz} shaped entries")
     return out
 
 
@@ -298,6 +338,8 @@ def main() -> None:
     torch.set_num_threads(1)
     fixtures = {"lif_c1": lambda: lif_c1(ref), "lif_19cell": lambda: lif_19cell(ref),
                 "lif_19cell_adapt_by_type": lambda: lif_19cell(ref, ADAPT_BY_TYPE),
+                "lif_19cell_clocks": lambda: lif_19cell(ref, clocks=True),
+                "lif_c1_clocks": lambda: lif_c1_clocks(ref),
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
                 "tracer": lambda: tracer(ref)}
     for name, make in fixtures.items():

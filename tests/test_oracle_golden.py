@@ -6,7 +6,7 @@ import pytest
 import oracle
 from oracle import frame as oframe
 from flyb200 import _abi, synthetic
-from flyb200.brain import LIFParams, lif_coefficients, out_edges
+from flyb200.brain import LIFParams, clock_coefficients, lif_coefficients, out_edges
 from flyb200.optic import OpticParams, lobe_matrices
 from flyb200.retina import build_retina
 from flyb200.weights import lif_weights, per_type, DEFAULT_STD_U_BY_TYPE
@@ -21,7 +21,7 @@ def test_philox_known_answer_vectors():
         [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1]
 
 
-def _c1_run(regime_seed, drive, ring="auto"):
+def _c1_run(regime_seed, drive, ring="auto", period=None):
     cfg = synthetic.lif_config1(seed=0)
     p = LIFParams(**cfg.params)
     W, _ = lif_weights(cfg.c, p)
@@ -31,9 +31,27 @@ def _c1_run(regime_seed, drive, ring="auto"):
     st.drive[:] = np.float32(drive)
     U = torch_uniforms(regime_seed, cfg.steps, (1, cfg.c.n))
     flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS
+    clocks = None
+    if period is not None:
+        clocks = (period, clock_coefficients(p, False, int(period.max())))
     r, ev = oracle.lif_run(st, ptr, edges, lif_coefficients(p, False), n_delay=18, flags=flags, nsteps=cfg.steps,
-                           uniforms=U.transpose(0, 2, 1), raster=True)
+                           uniforms=U.transpose(0, 2, 1), raster=True, clocks=clocks)
     return cfg, st, unpack(r, cfg.c.n), U, mode
+
+
+def test_lif_config1_clocked_matches_reference():
+    """Config 1 with per-neuron clocks of 1, 2 and 4 steps: the exact count ring against the
+    reference's clocked sparse-matmul step, rasters bit for bit."""
+    z = golden("lif_c1_clocks")
+    cfg, st, ras, U, mode = _c1_run(int(z["seed"]), float(z["drive"]), period=z["clock_period"])
+    assert mode == _abi.RING_COUNT
+    assert sha(U) == str(z["uniform_sha"])
+    ref = np.unpackbits(z["raster"], axis=1, bitorder="little")[:, : cfg.c.n].astype(bool)
+    assert ras.sum() > 500
+    np.testing.assert_array_equal(ras, ref)
+    np.testing.assert_array_equal(st.counts[:, 0], z["spike_counts"])
+    np.testing.assert_allclose(st.v[:, 0], z["v"], rtol=0, atol=2e-5)
+    np.testing.assert_allclose(st.g[:, 0], z["g"], rtol=0, atol=2e-5)
 
 
 @pytest.mark.parametrize("regime", ["poisson", "drive65", "drive72"])
@@ -172,3 +190,35 @@ def test_optic_hex_frames_match_reference():
         np.testing.assert_allclose(st["adapt"].T, z[f"frame{f}_adapt"], rtol=1e-5, atol=1e-6)
         np.testing.assert_allclose(st["delta"].T, z[f"frame{f}_delta_rate"], rtol=1e-5, atol=1e-6)
         np.testing.assert_allclose(drive, z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
+
+
+def test_lif_19cell_clocked_rasters_match_reference():
+    """Per-neuron clocks (periods 1/2/3 steps): the oracle's clocked step against the reference's
+    Brain.set_clocks run (its sparse-matmul path), rasters bit for bit."""
+    z, c, p = _nineteen("lif_19cell_clocks")
+    import scipy.sparse as sp
+    W = sp.csr_matrix((z["shaped_data"], z["shaped_indices"], z["shaped_indptr"]), shape=(c.n, c.n))
+    u = per_type(c, DEFAULT_STD_U_BY_TYPE, p.std_u)
+    ptr, edges, mode = out_edges(W, p.w_syn, "auto", std_on=True)
+    B, T, n = int(z["batch"]), int(z["steps"]), c.n
+    st = oracle.LifState(n, B, 5, mode, p.v_rest)
+    st.active[z["frozen"]] = 0
+    st.std_u[:] = u
+    dtp = np.float32(p.dt / 1000.0)
+    st.poisson_p[z["orn"], 0], st.poisson_p[z["orn"], 1] = np.float32(120.0) * dtp, np.float32(40.0) * dtp
+    st.poisson_p[z["jo"], 0] = np.array([90.0, 10.0], np.float32) * dtp
+    st.poisson_p[z["jo"], 1] = np.array([0.0, 150.0], np.float32) * dtp
+    st.drive[z["dnp01"], 0] = 12.0
+    U = torch_uniforms(int(z["seed"]), T, (B, n))
+    assert sha(U) == str(z["uniform_sha"])
+    flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD | _abi.LIF_SKIP_FROZEN
+    period = z["clock_period"]
+    table = clock_coefficients(p, True, int(period.max()))
+    r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True, True), n_delay=4, flags=flags, nsteps=T,
+                          uniforms=U.transpose(0, 2, 1), raster=True, clocks=(period, table))
+    ras = unpack(r, n * B).reshape(T, n, B).transpose(0, 2, 1)
+    assert ras.sum() > 20
+    np.testing.assert_array_equal(ras, z["raster"])
+    for key, mine in (("v", st.v), ("g", st.g), ("refrac", st.refrac), ("adapt", st.adapt), ("res", st.res),
+                      ("rate", st.rate), ("spike_counts", st.counts)):
+        np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
