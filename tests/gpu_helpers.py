@@ -13,7 +13,8 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
-                   device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False, adapt_jump=None):
+                   device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False, adapt_jump=None,
+                   clocks=None):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -43,6 +44,14 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
                      events=events.data_ptr(), status=status.data_ptr(), sync=sync.data_ptr() if with_sync else None)
     aj = None if adapt_jump is None else torch.from_numpy(np.ascontiguousarray(adapt_jump, np.float32)).to(dev)
     a.adapt_jump = None if aj is None else aj.data_ptr()
+    ck = cc = acc = None
+    if clocks is not None:
+        ck = torch.from_numpy(np.ascontiguousarray(clocks[0], np.uint8)).to(dev)
+        cc = torch.from_numpy(np.ascontiguousarray(clocks[1], np.float32)).to(dev)
+        if getattr(state, "clock_acc", None) is None:
+            state.clock_acc = np.zeros((n, B), np.int64)
+        acc = torch.from_numpy(state.clock_acc).to(dev)
+        a.clock_k, a.clock_coef, a.clock_acc = ck.data_ptr(), cc.data_ptr(), acc.data_ptr()
     if defer:
         a.flags |= _abi.LIF_DEFER_DELIVERY
         cap = int(_abi.lib().flyb_lif_spike_capacity(ct.byref(a)))
@@ -60,6 +69,8 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
     for k in LIF_ARRAYS:
         getattr(state, k)[...] = d[k].cpu().numpy()
     state.ring[...] = ring.cpu().numpy()
+    if acc is not None:
+        state.clock_acc[...] = acc.cpu().numpy()
     state.ring_pos = (state.ring_pos + nsteps) % state.ring_slots
     state.step += nsteps
     if fly_steps is not None:
