@@ -49,6 +49,14 @@ struct LifK {
   const unsigned char* __restrict__ clock_k;  // per-neuron update period, or null (every step)
   const float* __restrict__ clock_coef;       // [max period + 1][FLYB_CLOCK_NCOEF]
   long long* clock_acc;                       // [n][batch] input pending until the next update
+  int slow_classes, slow_mode;                // slow receptor tone (0 classes: none)
+  float slow_norm, slow_clip_lo, slow_clip_hi, slow_th_max;
+  float slow_decay[FLYB_SLOW_MAX_CLASSES];
+  const int* slow_out_ptr[FLYB_SLOW_MAX_CLASSES];
+  const int2* slow_out_edge[FLYB_SLOW_MAX_CLASSES];
+  long long* slow_ring[FLYB_SLOW_MAX_CLASSES];
+  float* slow_g[FLYB_SLOW_MAX_CLASSES];
+  float* g_slow;
   LifP P;
 };
 
@@ -583,15 +591,18 @@ __global__ void __launch_bounds__(BLOCK, (DEFER && IPT <= 2) ? 1024 / BLOCK : 1)
 
 __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
 
-// ------------------------------------------------------------------ per-neuron clocks
+// ------------------------------------------------------------------ clocks and the slow tone
 // The clocked step (brain.py:899-957): neuron i updates on steps with step % k_i == 0, with the
 // coefficients of a k_i * dt step (row k_i of clock_coef); on other steps it takes row 0 (no
 // decay, no refractory time, no spike, no Poisson). Input arriving at a period-k_i neuron between
 // its updates is summed exactly in clock_acc and applied on the update step, as the reference
-// applies W_k to the spikes accumulated over the period. One item per thread, then the block-wide
-// delivery of the register path.
+// applies W_k to the spikes accumulated over the period.
+// The slow tone (brain.py:551-585, 829-845): per class, the tone decays and takes its delayed
+// input from its own exact ring; the summed tone joins the membrane target, scales the fast input
+// or lowers the threshold. Its spikes go out on each class's synapse list after the fast ones.
+// One item per thread, then the block-wide delivery of the register path.
 template <int BLOCK, bool FIXED>
-__global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
+__global__ void __launch_bounds__(BLOCK) lif_ext_kernel(LifK k, int s) {
   using RingT = typename std::conditional<FIXED, long long, int>::type;
   __shared__ LifSmem<BLOCK> sm;
   const Clk clk = read_clock(k);
@@ -615,38 +626,68 @@ __global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
       RingT* rp = (RingT*)k.ring + (size_t)rs * slot + t;
       long long due = *rp;
       if (due) *rp = 0;
-      const long long step = clk.step0 + s;
-      const int period = k.clock_k[i];
-      const bool on = period == 1 || step % period == 0;
-      if (period > 1) {
-        const long long held = k.clock_acc[t], sum = held + due;
-        due = on ? sum : 0;
-        const long long keep = on ? 0 : sum;
-        if (keep != held) k.clock_acc[t] = keep;
+      // this step's coefficients: the neuron's phase row under clocks, else the step's own
+      float c_m = P.a_m, c_s = P.a_s, c_dt = P.dt, c_ad = P.a_ad, c_std = P.a_std, c_r = P.a_r, c_rg = P.rg;
+      float c_u = 1.0f, c_pois = 1.0f;
+      if (k.clock_k) {
+        const long long step = clk.step0 + s;
+        const int period = k.clock_k[i];
+        const bool on = period == 1 || step % period == 0;
+        if (period > 1) {
+          const long long held = k.clock_acc[t], sum = held + due;
+          due = on ? sum : 0;
+          const long long keep = on ? 0 : sum;
+          if (keep != held) k.clock_acc[t] = keep;
+        }
+        const float* cf = k.clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
+        c_m = cf[FLYB_CLOCK_A_M], c_s = cf[FLYB_CLOCK_A_S], c_dt = cf[FLYB_CLOCK_DT], c_ad = cf[FLYB_CLOCK_A_AD];
+        c_std = cf[FLYB_CLOCK_A_STD], c_r = cf[FLYB_CLOCK_A_R], c_rg = cf[FLYB_CLOCK_RATE_GAIN];
+        c_u = cf[FLYB_CLOCK_U], c_pois = cf[FLYB_CLOCK_POIS];
       }
-      const float* cf = k.clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
       const float act = k.active[i];
-      float g1 = k.g[t] * cf[FLYB_CLOCK_A_S];
+      float g1 = k.g[t] * c_s;
       if (due) {
         const float inc = FIXED ? __double2float_rn((double)due * (1.0 / 4294967296.0)) : P.w_syn * (float)due;
         g1 = g1 + inc;
       }
       k.g[t] = g1;
+      // slow tone: each class decays and takes its delayed input; the classes are summed in order
+      float tone = 0.0f;
+      for (int c = 0; c < k.slow_classes; ++c) {
+        long long* sp = k.slow_ring[c] + (size_t)rs * slot + t;
+        const long long sdue = *sp;
+        if (sdue) *sp = 0;
+        float sg = k.slow_g[c][t] * k.slow_decay[c];
+        if (sdue) sg = sg + __double2float_rn((double)sdue * (1.0 / 4294967296.0));
+        k.slow_g[c][t] = sg;
+        tone = tone + sg;
+      }
+      if (k.slow_classes) k.g_slow[t] = tone;
       const float ad = k.adapt[t];
-      float target = P.v_rest + g1;
+      float th = P.v_th;
+      float target;
+      if (k.slow_classes && k.slow_mode == FLYB_SLOW_GAIN) {
+        float f = 1.0f + tone / k.slow_norm;
+        f = fminf(fmaxf(f, k.slow_clip_lo), k.slow_clip_hi);
+        target = P.v_rest + g1 * f;
+      } else {
+        target = P.v_rest + g1;
+      }
       target = target + k.drive[t];
       target = target - ad;
+      if (k.slow_classes && k.slow_mode == FLYB_SLOW_ADDITIVE) target = target + tone;
+      if (k.slow_classes && k.slow_mode == FLYB_SLOW_THRESHOLD) th = -fminf(tone, k.slow_th_max) + P.v_th;
       float u = k.v[t] - target;
-      u = u * cf[FLYB_CLOCK_A_M];
+      u = u * c_m;
       float v1 = target + u;
       float r1 = k.refrac[t];
       if (r1 > 0.0f) v1 = P.v_reset;
-      r1 = r1 - cf[FLYB_CLOCK_DT];
+      r1 = r1 - c_dt;
       if (r1 < 0.0f) r1 = 0.0f;
-      float spike = (v1 >= P.v_th ? 1.0f : 0.0f) * cf[FLYB_CLOCK_U];
+      float spike = (v1 >= th ? 1.0f : 0.0f) * c_u;
       spike = spike * act;
       if (flags & FLYB_LIF_POISSON) {
-        const float q = k.poisson_p[t] * cf[FLYB_CLOCK_POIS];
+        const float q = k.poisson_p[t] * c_pois;
         if (q > 0.0f) {
           const float un = (flags & FLYB_LIF_EXT_UNIFORM)
                                ? k.uniforms[(size_t)s * slot + t]
@@ -660,7 +701,7 @@ __global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
       k.refrac[t] = r1;
       k.spikes[t] = spike;
       if (flags & FLYB_LIF_ADAPT) {
-        float a1 = ad * cf[FLYB_CLOCK_A_AD];
+        float a1 = ad * c_ad;
         a1 = a1 + spike * (k.adapt_jump ? __ldg(&k.adapt_jump[i]) : P.jump);
         k.adapt[t] = a1;
       }
@@ -670,12 +711,12 @@ __global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
         x = spike * r2;
         if (fired) { const float keep = 1.0f - k.std_u[i]; r2 = r2 * keep; }
         float dep = 1.0f - r2;
-        dep = dep * cf[FLYB_CLOCK_A_STD];
+        dep = dep * c_std;
         k.res[t] = 1.0f - dep;
       }
       if (flags & FLYB_LIF_COUNTS) k.counts[t] = k.counts[t] + spike;
-      float r3 = k.rate[t] * cf[FLYB_CLOCK_A_R];
-      r3 = r3 + spike * cf[FLYB_CLOCK_RATE_GAIN];
+      float r3 = k.rate[t] * c_r;
+      r3 = r3 + spike * c_rg;
       k.rate[t] = r3;
       if (fired) fired_bit = 1u;
       if (x != 0.0f) { tx_bit = 1u; xq[0] = x; }
@@ -690,16 +731,24 @@ __global__ void __launch_bounds__(BLOCK) lif_clocked_kernel(LifK k, int s) {
     }
   }
   deliver<BLOCK, FIXED, 1>(k, sm, tx_bit, iq, bq, xq, ws, slot);
+  for (int c = 0; c < k.slow_classes; ++c) {     // the same transmitted amounts onto each slow list
+    LifK ks = k;
+    ks.out_ptr = k.slow_out_ptr[c];
+    ks.out_edge = k.slow_out_edge[c];
+    ks.ring = k.slow_ring[c];
+    ks.events = nullptr;
+    deliver<BLOCK, true, 1>(ks, sm, tx_bit, iq, bq, xq, ws, slot);
+  }
 }
 
 static bool needs_advance(const LifK& k);
 
 template <int BLOCK, bool FIXED>
-static int run_lif_clocked(const LifK& k, cudaStream_t st) {
+static int run_lif_ext(const LifK& k, cudaStream_t st) {
   const long long W = (long long)k.t_end - k.t_begin;
   const unsigned blocks = (unsigned)((W + BLOCK - 1) / BLOCK);
   for (int s = 0; s < k.nsteps; ++s) {
-    lif_clocked_kernel<BLOCK, FIXED><<<blocks, BLOCK, 0, st>>>(k, s);
+    lif_ext_kernel<BLOCK, FIXED><<<blocks, BLOCK, 0, st>>>(k, s);
     FLYB_CHECK_LAUNCH();
   }
   if (needs_advance(k)) {
@@ -1192,6 +1241,25 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.adapt_jump = a->adapt_jump;
   k.clock_k = a->clock_k; k.clock_coef = a->clock_coef; k.clock_acc = (long long*)a->clock_acc;
   if (a->clock_k && (!a->clock_coef || !a->clock_acc || (a->flags & FLYB_LIF_DEFER_DELIVERY))) return FLYB_EINVAL;
+  k.slow_classes = a->slow_classes; k.slow_mode = a->slow_mode;
+  k.slow_norm = a->slow_norm; k.slow_clip_lo = a->slow_clip_lo; k.slow_clip_hi = a->slow_clip_hi;
+  k.slow_th_max = a->slow_th_max; k.g_slow = a->g_slow;
+  if (a->slow_classes < 0 || a->slow_classes > FLYB_SLOW_MAX_CLASSES) return FLYB_EINVAL;
+  if (a->slow_classes) {
+    if (a->clock_k || (a->flags & FLYB_LIF_DEFER_DELIVERY) || !a->g_slow || a->slow_mode < FLYB_SLOW_ADDITIVE ||
+        a->slow_mode > FLYB_SLOW_THRESHOLD || !(a->slow_norm != 0.0f))
+      return FLYB_EINVAL;
+  }
+  for (int c = 0; c < FLYB_SLOW_MAX_CLASSES; ++c) {
+    const bool used = c < a->slow_classes;
+    if (used && (!a->slow_out_ptr[c] || !a->slow_out_edge[c] || !a->slow_ring[c] || !a->slow_g[c]))
+      return FLYB_EINVAL;
+    k.slow_decay[c] = used ? a->slow_decay[c] : 0.0f;
+    k.slow_out_ptr[c] = used ? a->slow_out_ptr[c] : nullptr;
+    k.slow_out_edge[c] = used ? (const int2*)a->slow_out_edge[c] : nullptr;
+    k.slow_ring[c] = used ? (long long*)a->slow_ring[c] : nullptr;
+    k.slow_g[c] = used ? a->slow_g[c] : nullptr;
+  }
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
     if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP || a->staged)
@@ -1222,9 +1290,9 @@ FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {
   cudaStream_t st = (cudaStream_t)stream;
   const bool fixed = a->ring_mode == FLYB_RING_FIXED;
   const int block = a->block ? a->block : 256;
-  if (k.clock_k) {
+  if (k.clock_k || k.slow_classes) {
     if (block != 128 && block != 256 && block != 512) return FLYB_EINVAL;
-    return fixed ? run_lif_clocked<256, true>(k, st) : run_lif_clocked<256, false>(k, st);
+    return fixed ? run_lif_ext<256, true>(k, st) : run_lif_ext<256, false>(k, st);
   }
   switch (block) {
     case 128: return fixed ? run_lif<128, true>(k, a->items_per_thread, a->launch, a->grid, a->staged, st)

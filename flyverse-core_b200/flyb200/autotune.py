@@ -60,9 +60,10 @@ def _time(fn, reps: int) -> float:
 
 def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
     """Install and return the fastest LIF launch choice for this brain; state is left unchanged.
-    A brain with per-neuron clocks has one launch shape (the clocked kernel): nothing to tune."""
-    if getattr(brain, "_kvec", None) is not None:
-        return {"launch": "step", "block": 256, "items_per_thread": 1, "delivery": "clocked", "ms_per_step": None}
+    A brain with per-neuron clocks or the slow receptor tone has one launch shape (the extended
+    kernel): nothing to tune."""
+    if getattr(brain, "_kvec", None) is not None or getattr(brain, "slow", None) is not None:
+        return {"launch": "step", "block": 256, "items_per_thread": 1, "delivery": "extended", "ms_per_step": None}
     key = ("lif", graph_key(brain), brain.B, activity_bucket(brain))
     if key in CACHE:
         _apply(brain, CACHE[key])

@@ -27,7 +27,8 @@ import scipy.sparse as sp
 import torch
 
 from . import _abi
-from .weights import DEFAULT_ADAPT_BY_TYPE, DEFAULT_STD_U_BY_TYPE, integer_counts, lif_weights, per_type
+from .weights import (DEFAULT_ADAPT_BY_TYPE, DEFAULT_STD_U_BY_TYPE, SLOW_THRESHOLD_MAX_FRAC, integer_counts,
+                      lif_weights, per_type, slow_spec, slow_weights)
 
 
 @dataclass
@@ -150,8 +151,6 @@ def _unsupported(p: LIFParams, metal_kernels, cuda_kernels, cuda_sparse) -> None
     if p.surrogate_grad:
         raise NotImplementedError("surrogate_grad (Torch autograd through the LIF) is not part of the native step; "
                                   "the spiking path is left undifferentiated")
-    if p.receptor_model == "full":
-        raise NotImplementedError("the slow receptor term (receptor_model='full') is not in the native LIF step")
     if p.weight_dtype not in ("float32", "float16"):
         raise ValueError("weight_dtype must be float32 or float16")
     if p.event_driven is False:
@@ -209,8 +208,16 @@ class Brain:
         self._st["v"].fill_(p.v_rest)
         self._st["res"].fill_(1.0)
         self.active = torch.ones(N, device=dev)
-        self.g_slow = torch.zeros(B, N, device=dev)
-        self.g_slow_cls = torch.zeros(0, B, N, device=dev)
+        # slow receptor tone (receptor_model "full"): per class [K][N][B] and the sum [N][B], (B, N) views
+        self.slow = slow_spec(p)
+        self.slow_classes = self.slow.classes if self.slow is not None else []
+        K = len(self.slow_classes)
+        self._slow_g = torch.zeros(K, N, B, device=dev)
+        self._g_slow = torch.zeros(N, B, device=dev)
+        self.g_slow = self._g_slow.t()
+        self.g_slow_cls = self._slow_g.transpose(1, 2)
+        self._W_slow_cpu = slow_weights(c, p, receptor, self.slow, self.input_scale) if self.slow is not None else None
+        self._slow_rings = []
         self.gen = torch.Generator(device=dev).manual_seed(seed)
         self.words = (N * B + 31) // 32
         self._hist = torch.zeros(self.n_delay, self.words, dtype=torch.int32, device=dev)   # 1-bit spike history
@@ -252,6 +259,7 @@ class Brain:
         if had_ring and self.step_count and not self._std_on:
             spike_buf = self.spike_buf
         self._W_cpu = sp.csr_matrix(W, dtype=np.float32)
+        self._set_slow_lists()
         self._weights_version += 1
         self.ring_mode = mode
         self.nnz = int(edges.shape[0])
@@ -265,10 +273,29 @@ class Brain:
         if had_ring and spike_buf is not None:
             self.load_spike_buf(spike_buf)
 
+    def _set_slow_lists(self) -> None:
+        """Pre-major synapse lists of the slow classes, and their rings (kept across rebuilds)."""
+        self._slow_lists = []
+        if self._W_slow_cpu is None:
+            return
+        for S in self._W_slow_cpu.values():
+            ptr, edges, _ = out_edges(S, self.p.w_syn, "fixed")
+            self._slow_lists.append((torch.from_numpy(ptr).to(self.device), torch.from_numpy(edges).to(self.device)))
+        if not self._slow_rings:
+            self._slow_rings = [torch.zeros(self.R, self.n, self.B, dtype=torch.int64, device=self.device)
+                                for _ in self._W_slow_cpu]
+
     def prune(self, idx) -> None:
         """Drop every synapse from and onto neurons `idx` (brain.py:602-616)."""
         keep = np.ones(self.n, np.float32)
         keep[np.asarray(idx)] = 0.0
+        if self._W_slow_cpu is not None:
+            S = {}
+            for k, Sk in self._W_slow_cpu.items():
+                Sk = (sp.diags(keep) @ Sk @ sp.diags(keep)).tocsr()
+                Sk.eliminate_zeros()
+                S[k] = Sk
+            self._W_slow_cpu = S
         W = (sp.diags(keep) @ self._W_cpu @ sp.diags(keep)).tocsr()
         W.eliminate_zeros()
         self.set_weights(W)
@@ -297,13 +324,24 @@ class Brain:
         if self._kvec is not None:
             a.clock_k, a.clock_coef = self._clock_k.data_ptr(), self._clock_coef.data_ptr()
             a.clock_acc = self.clock_acc.data_ptr()
+        if self.slow is not None:
+            spec = self.slow
+            a.slow_classes, a.slow_mode = len(self.slow_classes), _abi.SLOW_MODE_CODES[spec.mode]
+            a.slow_norm, a.slow_clip_lo, a.slow_clip_hi = spec.norm_mv, spec.clip[0], spec.clip[1]
+            a.slow_th_max = float(np.float32(SLOW_THRESHOLD_MAX_FRAC * spec.norm_mv))
+            for c, name in enumerate(self.slow_classes):
+                a.slow_decay[c] = math.exp(-self.p.dt / spec.tau[name])
+                a.slow_out_ptr[c] = self._slow_lists[c][0].data_ptr()
+                a.slow_out_edge[c] = self._slow_lists[c][1].data_ptr()
+                a.slow_ring[c], a.slow_g[c] = self._slow_rings[c].data_ptr(), self._slow_g[c].data_ptr()
+            a.g_slow = self._g_slow.data_ptr()
         self._args = a
         self._lists = {}          # deferred-delivery lists per neuron range, sized on first use
 
     def _defer_active(self) -> bool:
         """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step register launches."""
         return bool(getattr(self, "defer", False)) and self.launch == "step" and not getattr(self, "staged", False) \
-            and self._kvec is None
+            and self._kvec is None and self.slow is None
 
     # ------------------------------------------------------------------ per-neuron clocks
     def set_clocks(self, multiplier) -> None:
@@ -320,6 +358,9 @@ class Brain:
             raise ValueError("the slowest clock must not exceed the synaptic delay")
         if int(k.max()) > 255:
             raise ValueError("clock periods above 255 steps are not supported")
+        if self.slow is not None:
+            raise NotImplementedError("per-neuron clocks together with the slow receptor tone are not in the "
+                                      "native step")
         self._kvec = k
         self.K = int(np.lcm.reduce(np.unique(k)))
         self._clock_k = torch.from_numpy(k.astype(np.uint8)).to(self.device)
@@ -456,6 +497,9 @@ class Brain:
             st[k][:, sel] = 0.0
         st["res"][:, sel] = 1.0
         self.g_slow[sel] = 0.0
+        self.g_slow_cls[:, sel] = 0.0
+        for r in self._slow_rings:
+            r[:, :, sel] = 0
         self.ring[:, :, sel] = 0
         if self._kvec is not None:
             self.clock_acc[:, sel] = 0
@@ -524,6 +568,9 @@ class Brain:
                    scalars=dict(t=self.t, step_count=self.step_count, buf_pos=self.buf_pos, _poisson_on=self._poisson_on))
         if self._kvec is not None:
             out.update(clock_period=self._kvec.copy(), clock_acc=self.clock_acc.cpu().clone())
+        if self.slow is not None:
+            out.update(g_slow=self._g_slow.cpu().clone(), g_slow_cls=self._slow_g.cpu().clone(),
+                       slow_rings=[r.cpu().clone() for r in self._slow_rings])
         return out
 
     def load_state_dict(self, state: dict) -> None:
@@ -540,6 +587,13 @@ class Brain:
             self.clock_acc.copy_(state["clock_acc"].to(self.device))
         elif self._kvec is not None:
             raise ValueError("checkpoint has no per-neuron clocks but this brain runs them")
+        if (self.slow is not None) != ("g_slow_cls" in state):
+            raise ValueError("checkpoint and brain disagree on the slow receptor tone")
+        if self.slow is not None:
+            self._g_slow.copy_(state["g_slow"].to(self.device))
+            self._slow_g.copy_(state["g_slow_cls"].to(self.device))
+            for r, saved in zip(self._slow_rings, state["slow_rings"]):
+                r.copy_(saved.to(self.device))
         for k, v in state["scalars"].items():
             setattr(self, k, v)
         self._rate_np_key = None

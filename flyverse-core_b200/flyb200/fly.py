@@ -50,7 +50,7 @@ class FlyBrain:
             self.retina = retina if retina is not None else build_retina(c)
             if self.retina.n_columns:
                 self.optic = OpticLobe(c, self.retina, optic_params, device=self.device, batch=self.B,
-                                       receptor=receptor, launch=launch)
+                                       receptor=receptor, slow=self.brain.slow, launch=launch)
                 self.optic.relax()
                 self.brain.freeze(self.optic.rate_idx)
                 if lp.prune_frozen:

@@ -12,6 +12,7 @@ the reference's; the code is this package's own.
 from __future__ import annotations
 
 import math
+from dataclasses import dataclass
 import re
 
 import numpy as np
@@ -129,6 +130,110 @@ def lif_weights(c, p, receptor=None) -> tuple[sp.csr_matrix, np.ndarray | None]:
     W = W.copy()
     W.data = W.data * np.float32(p.w_syn)
     return W, scale
+
+
+# ------------------------------------------------------------------ the slow receptor tone
+# receptor_model "full" (brain.py:100-147, 176-230, 341-359): a slow tone per neuron and class,
+# driven by the entries whose receptor row has a slow sign. Class names, defaults and modes are the
+# reference's, so the same parameters give the same tone.
+GAIN_CLASSES = ["none", "low", "mid", "high"]
+SLOW_CLASSES = ["none", "metabotropic_classical", "monoamine"]
+SLOW_MODES = ("additive", "gain", "threshold")
+DEFAULT_SLOW_GAIN_BY_CLASS = {"metabotropic_classical": 0.0, "monoamine": None}
+DEFAULT_SLOW_TAU_BY_CLASS = {"metabotropic_classical": 100.0, "monoamine": None}
+SLOW_THRESHOLD_MAX_FRAC = 0.9
+
+
+@dataclass
+class ReceptorSigns:
+    """Per stored entry of W (CSR order): the receptor model's fast and slow signs, gain classes
+    (int8 codes into GAIN_CLASSES), slow class (codes into SLOW_CLASSES) and synapse counts -- the
+    record the reference's connectome.receptor_signs builds (connectome.py:113-170); any object
+    with these fields and methods (the reference's own included) can be passed as `receptor=`."""
+    fast_sign: np.ndarray
+    slow_sign: np.ndarray
+    fast_gain: np.ndarray
+    slow_gain: np.ndarray
+    count: np.ndarray | None = None
+    slow_class: np.ndarray | None = None
+
+    def fast_factor(self, gain: dict | None = None) -> np.ndarray:
+        f = self.fast_sign.astype(np.float32)
+        if gain:
+            g = np.array([float(gain.get(k, 1.0)) for k in GAIN_CLASSES], dtype=np.float32)
+            f = f * g[self.fast_gain]
+        return f
+
+    def slow_factor(self, gain: dict | None = None, slow_class: str | None = None) -> np.ndarray:
+        f = self.slow_sign.astype(np.float32)
+        if gain:
+            g = np.array([float(gain.get(k, 1.0)) for k in GAIN_CLASSES], dtype=np.float32)
+            f = f * g[self.slow_gain]
+        if slow_class is not None:
+            if self.slow_class is None:
+                raise ValueError("this receptor record carries no slow-class codes")
+            f = f * (self.slow_class == SLOW_CLASSES.index(slow_class)).astype(np.float32)
+        return f
+
+
+@dataclass
+class SlowSpec:
+    """The resolved slow tone: mode, per-class scale and time constant (non-zero scales only), the
+    fast synaptic time constant, and the normalisation of the multiplicative modes (v_th - v_rest)."""
+    mode: str
+    gain: dict
+    tau: dict
+    tau_syn: float
+    norm_mv: float
+    clip: tuple = (0.0, 4.0)
+
+    @property
+    def classes(self) -> list:
+        return list(self.gain)
+
+
+def slow_spec(p) -> SlowSpec | None:
+    """None unless receptor_model == "full" and some class has a non-zero scale (brain.py:206-225)."""
+    if p.receptor_model != "full":
+        return None
+    if p.slow_mode not in SLOW_MODES:
+        raise ValueError(f"slow_mode must be one of {SLOW_MODES}")
+    gains = dict(DEFAULT_SLOW_GAIN_BY_CLASS, monoamine=float(p.slow_gain))
+    gains.update({k: float(v) for k, v in (p.slow_gain_by_class or {}).items()})
+    taus = dict(DEFAULT_SLOW_TAU_BY_CLASS, monoamine=float(p.slow_tau_ms))
+    taus.update({k: float(v) for k, v in (p.slow_tau_by_class or {}).items()})
+    bad = (set(gains) | set(taus)) - set(SLOW_CLASSES[1:])
+    if bad:
+        raise ValueError(f"unknown slow classes {sorted(bad)}; use {SLOW_CLASSES[1:]}")
+    for k, tau in taus.items():
+        if not (math.isfinite(tau) and tau > 0):
+            raise ValueError(f"slow tau of class {k!r} must be positive and finite")
+    active = {k: g for k, g in gains.items() if g != 0.0}
+    if not active:
+        return None
+    return SlowSpec(p.slow_mode, active, {k: taus[k] for k in active}, float(p.tau_syn), float(p.v_th - p.v_rest),
+                    tuple(float(x) for x in p.slow_gain_clip))
+
+
+def slow_weights(c, p, receptor, spec: SlowSpec, scale: np.ndarray | None) -> dict:
+    """{class: csr} slow matrices in mV per transmitted spike (brain.py:341-359, 410-429): per entry
+    count x slow sign x gain factor, capped like the fast synapses, entries of other classes
+    dropped; then the fan-in scale of the fast weights and w_syn x the class scale."""
+    if getattr(receptor, "count", None) is None:
+        raise ValueError("the slow tone needs the receptor record's synapse counts")
+    out = {}
+    for cls in spec.classes:
+        S = c.W.tocsr().copy()
+        S.data = receptor.count * receptor.slow_factor(receptor_gain(p), slow_class=cls)
+        if p.conn_cap > 0:
+            S.data = np.sign(S.data) * np.minimum(np.abs(S.data), np.float32(p.conn_cap))
+        S.eliminate_zeros()
+        if scale is not None:
+            S = (sp.diags(scale) @ S).tocsr()
+        S = S.copy()
+        S.data = S.data * np.float32(p.w_syn * spec.gain[cls])
+        out[cls] = S
+    return out
 
 
 def per_type(c, mapping: dict, default: float) -> np.ndarray:

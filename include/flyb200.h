@@ -86,6 +86,8 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
 #define FLYB_LAUNCH_STEP       0   /* one kernel launch per step (the "plain" kernel)        */
 #define FLYB_LAUNCH_PERSISTENT 1   /* one cooperative launch for all steps, grid barrier/step */
 
+#define FLYB_SLOW_MAX_CLASSES 2   /* slow receptor classes: classical metabotropic, monoamine */
+
 /* LIF coefficient vector P[FLYB_LIF_NPARAM] (float32) */
 enum {
   FLYB_P_V_REST = 0, FLYB_P_V_RESET, FLYB_P_V_TH, FLYB_P_A_M, FLYB_P_A_S, FLYB_P_DT,
@@ -164,7 +166,26 @@ typedef struct flyb_lif_args {
                             step on which a neuron does not update                         */
   void* clock_acc;       /* [n][batch] int64 (device): pending input of neurons with period
                             > 1, in ring units (counts, or Q32.32 mV)                       */
+  /* Slow receptor tone (receptor_model "full": brain.py:551-585, the step :829-845): per class c
+   * < slow_classes a tone slow_g[c] (mV) decays by slow_decay[c] per step and takes the delayed
+   * input of its own synapse list (pre-major like out_ptr / out_edge, {post, float bits of w}),
+   * summed exactly on its own Q32.32 ring; g_slow = sum over classes acts by slow_mode: added to
+   * the membrane target, scaling the fast input by clamp(1 + g_slow / slow_norm, slow_clip_lo,
+   * slow_clip_hi), or lowering the threshold by min(g_slow, slow_th_max). Runs one launch per step
+   * like the clocks (which it cannot be combined with). slow_classes 0: no tone. */
+  int slow_classes;      /* 0..FLYB_SLOW_MAX_CLASSES                                      */
+  int slow_mode;         /* FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN or FLYB_SLOW_THRESHOLD      */
+  float slow_norm, slow_clip_lo, slow_clip_hi, slow_th_max;
+  float slow_decay[FLYB_SLOW_MAX_CLASSES];
+  const int* slow_out_ptr[FLYB_SLOW_MAX_CLASSES];   /* [n+1] per class (device)          */
+  const int* slow_out_edge[FLYB_SLOW_MAX_CLASSES];  /* [nnz][2] per class (device)       */
+  void* slow_ring[FLYB_SLOW_MAX_CLASSES];           /* [R][n][batch] int64 per class     */
+  float* slow_g[FLYB_SLOW_MAX_CLASSES];             /* [n][batch] tone per class (mV)    */
+  float* g_slow;                                    /* [n][batch] summed tone (mV)       */
 } flyb_lif_args;
+
+/* flyb_lif_args.slow_mode */
+enum { FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN, FLYB_SLOW_THRESHOLD };
 
 /* Columns of flyb_lif_args.clock_coef */
 enum {

@@ -110,13 +110,17 @@ class LifState:
 
 
 def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0,
-            uniforms=None, fly_steps=None, raster=False, threads=0, fly0=0, adapt_jump=None, clocks=None):
+            uniforms=None, fly_steps=None, raster=False, threads=0, fly0=0, adapt_jump=None, clocks=None,
+            slow=None):
     """Advance `state` in place by `nsteps`; returns (raster bits [nsteps][words] or None, events).
     With `fly_steps` (EPISODES), fly b is live for its first fly_steps[b] steps; the array is then
     reduced by the steps taken, as the host layer does after a launch. `adapt_jump` (n,): per-neuron
     adaptation jumps (the reference's adapt_by_type, brain.py:497-506). `clocks` = (period (n,),
     coefficient table [max period + 1][CLOCK_NCOEF]): per-neuron clocks (brain.py:899-957); the
-    pending input of slow neurons lives in `state.clock_acc`."""
+    pending input of slow neurons lives in `state.clock_acc`. `slow` = {"mode", "norm", "clip",
+    "th_max", "classes": [(out_ptr, out_edge, decay), ...]}: the slow receptor tone (brain.py:551-585);
+    its rings, per-class tones and summed tone live in `state.slow_ring`, `state.slow_g`,
+    `state.g_slow`."""
     n, B = state.n, state.batch
     words = (n * B + 31) // 32
     r = np.zeros((nsteps, words), np.uint32) if raster else None
@@ -133,6 +137,13 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
         cc = _f32(clocks[1])
         if getattr(state, "clock_acc", None) is None:
             state.clock_acc = np.zeros((n, B), np.int64)
+    keep = []
+    if slow is not None:
+        K = len(slow["classes"])
+        if getattr(state, "slow_ring", None) is None:
+            state.slow_ring = np.zeros((K, state.ring_slots, n, B), np.int64)
+            state.slow_g = np.zeros((K, n, B), np.float32)
+            state.g_slow = np.zeros((n, B), np.float32)
     a = _abi.LifArgs(n=n, batch=B, n_delay=n_delay, ring_slots=state.ring_slots, ring_mode=state.ring_mode,
                      ring_pos=state.ring_pos, flags=flags, nsteps=nsteps, step0=state.step, seed=seed, fly0=fly0,
                      out_ptr=_p(out_ptr), out_edge=_p(out_edge), v=_p(state.v), g=_p(state.g),
@@ -142,6 +153,17 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
                      params=_p(P), ring=_p(state.ring), uniforms=_p(uni), fly_steps=_p(fs),
                      raster=_p(r), events=_p(events), adapt_jump=_p(aj), clock_k=_p(ck), clock_coef=_p(cc),
                      clock_acc=_p(getattr(state, "clock_acc", None)) if clocks is not None else None)
+    if slow is not None:
+        a.slow_classes, a.slow_mode = len(slow["classes"]), _abi.SLOW_MODE_CODES[slow["mode"]]
+        a.slow_norm, a.slow_th_max = slow["norm"], slow["th_max"]
+        a.slow_clip_lo, a.slow_clip_hi = slow["clip"]
+        for c, (sp_, se_, decay) in enumerate(slow["classes"]):
+            sp_, se_ = np.ascontiguousarray(sp_, np.int32), np.ascontiguousarray(se_, np.int32)
+            keep += [sp_, se_]
+            a.slow_out_ptr[c], a.slow_out_edge[c] = _p(sp_), _p(se_)
+            a.slow_ring[c], a.slow_g[c] = state.slow_ring[c].ctypes.data, state.slow_g[c].ctypes.data
+            a.slow_decay[c] = decay
+        a.g_slow = _p(state.g_slow)
     rc = lib().oracle_lif_run(ct.byref(a), threads)
     if rc:
         raise ValueError(f"oracle_lif_run: status {rc}")

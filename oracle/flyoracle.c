@@ -123,10 +123,35 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
       g = g + inc;
     }
     a->g[t] = g;
-    /* 2. membrane (brain.py:839-843) */
-    float target = v_rest + g;
+    /* the slow tone (brain.py:551-557, 834-837): per class decay plus its delayed input */
+    float tone = 0.0f;
+    for (int c = 0; c < a->slow_classes; ++c) {
+      int64_t* sring = (int64_t*)a->slow_ring[c] + (size_t)rs * n * B;
+      int64_t sdue = sring[t]; sring[t] = 0;
+      float sg = a->slow_g[c][t] * a->slow_decay[c];
+      if (sdue != 0) { float inc = float_of_fixed(sdue); sg = sg + inc; }
+      a->slow_g[c][t] = sg;
+      tone = tone + sg;
+    }
+    if (a->slow_classes) a->g_slow[t] = tone;
+    /* 2. membrane (brain.py:568-577, 839-843) */
+    float th = v_th;
+    float target;
+    if (a->slow_classes && a->slow_mode == FLYB_SLOW_GAIN) {
+      float f = 1.0f + tone / a->slow_norm;
+      if (f < a->slow_clip_lo) f = a->slow_clip_lo;
+      if (f > a->slow_clip_hi) f = a->slow_clip_hi;
+      target = v_rest + g * f;
+    } else {
+      target = v_rest + g;
+    }
     target = target + a->drive[t];
     target = target - a->adapt[t];
+    if (a->slow_classes && a->slow_mode == FLYB_SLOW_ADDITIVE) target = target + tone;
+    if (a->slow_classes && a->slow_mode == FLYB_SLOW_THRESHOLD) {
+      float m = tone < a->slow_th_max ? tone : a->slow_th_max;
+      th = -m + v_th;
+    }
     float v = a->v[t] - target;
     v = v * c_m;
     v = target + v;
@@ -135,7 +160,7 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     ref = ref - c_dt;
     if (ref < 0.0f) ref = 0.0f;
     /* 3. threshold and Poisson forcing (brain.py:845-849) */
-    float spike = (v >= v_th ? 1.0f : 0.0f) * c_u;
+    float spike = (v >= th ? 1.0f : 0.0f) * c_u;
     spike = spike * a->active[i];
     if (flags & FLYB_LIF_POISSON) {
       float p = a->poisson_p[t] * c_pois;
@@ -169,6 +194,15 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     if (x != 0.0f) {
       const int e0 = a->out_ptr[i], e1 = a->out_ptr[i + 1];
       events += (uint64_t)(e1 - e0);
+      for (int c = 0; c < a->slow_classes; ++c) {   /* the slow lists carry the same amounts */
+        int64_t* sring = (int64_t*)a->slow_ring[c] + (size_t)ws * n * B;
+        const int* sp = a->slow_out_ptr[c];
+        const int* se = a->slow_out_edge[c];
+        for (int e = sp[i]; e < sp[i + 1]; ++e) {
+          float w; memcpy(&w, &se[2 * e + 1], sizeof w);
+          sring[(size_t)se[2 * e] * B + b] += fixed_of(w, x);
+        }
+      }
       if (a->ring_mode == FLYB_RING_COUNT) {
         int32_t* ring = (int32_t*)a->ring + (size_t)ws * n * B;
         for (int e = e0; e < e1; ++e) ring[(size_t)a->out_edge[2 * e] * B + b] += a->out_edge[2 * e + 1];

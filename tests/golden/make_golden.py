@@ -17,6 +17,9 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
                   reference's adapt_by_type): its per-neuron jump vector, rasters and final state.
   lif_19cell_clocks.npz  the same run with per-neuron clocks (Brain.set_clocks, periods 1/2/3 steps
                   by neuron index) on the reference's sparse-matmul path, which is where it runs them.
+  lif_19cell_slow_{additive,gain,threshold}.npz  the 19-cell run with the slow receptor tone
+                  (receptor_model="full", classical class at scale 0.5) in each slow_mode, with the
+                  per-entry receptor arrays (connectome.receptor_signs) it was built from.
   lif_c1_clocks.npz  config 1 at 6.5 mV drive with per-neuron clocks of 1, 2 and 4 steps on the
                   reference's sparse-matmul path: rasters and final state.
   optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
@@ -88,6 +91,51 @@ def lif_c1(ref) -> dict:
         out[f"{name}_drive"] = np.float32(drive)
         out[f"{name}_seed"] = np.int64(k)
         print(f"lif_c1 {name}: {int(ras.sum())} spikes")
+    return out
+
+
+def lif_19cell_slow(ref, mode: str) -> dict:
+    """The 19-cell run with the receptor model's slow tone (receptor_model="full", classical class
+    at scale 0.5) in one slow_mode: the per-entry receptor arrays the model read, the shaped fast
+    and slow matrices, rasters, final state and tone."""
+    brain, cn = ref["brain"], ref["connectome"]
+    tb = ref["test_bit_identity"]
+    c = tb.graph()
+    B, steps, seed = 2, 400, 7
+    p = brain.LIFParams(receptor_model="full", event_driven=True, slow_gain_by_class={"metabotropic_classical": 0.5},
+                        slow_mode=mode)
+    rec = cn.receptor_signs(c, net_rule=p.receptor_net_rule, with_counts=True)
+    b = brain.Brain(c, p, device="cpu", seed=seed, batch=B, receptor=rec)
+    frozen = np.flatnonzero((c.neurons.superclass == "ol_intrinsic").to_numpy())
+    b.freeze(frozen)
+    b.prune(frozen)
+    b.record_activity = True
+    orn, jo, dnp = c.select(type="ORN_DM1"), c.select(type="~^JO-"), c.select(type="DNp01")
+    b.set_poisson(orn, torch.tensor([[120.0], [40.0]]))
+    b.set_poisson(jo, torch.tensor([[90.0, 10.0], [0.0, 150.0]]))
+    b.set_drive(dnp, torch.tensor([[12.0], [0.0]]))
+    gen = torch.Generator().manual_seed(seed)
+    U = np.stack([torch.rand((B, c.n), generator=gen).numpy() for _ in range(steps)])
+    ras = np.zeros((steps, B, c.n), bool)
+    for s in range(steps):
+        b.step(1)
+        ras[s] = b.spikes.numpy() > 0
+    W = b._W_cpu.tocsr()
+    out = _table(c.neurons) | {"W_data": c.W.data, "W_indices": c.W.indices, "W_indptr": c.W.indptr,
+                               "shaped_data": W.data, "shaped_indices": W.indices, "shaped_indptr": W.indptr,
+                               "frozen": frozen, "orn": orn, "jo": jo, "dnp01": dnp, "raster": ras,
+                               "uniform_sha": np.array(sha(U)), "seed": np.int64(seed), "steps": np.int64(steps),
+                               "batch": np.int64(B), "slow_mode": np.array(mode), "slow_classes": np.array(b.slow_classes),
+                               "rec_fast_sign": rec.fast_sign, "rec_slow_sign": rec.slow_sign,
+                               "rec_fast_gain": rec.fast_gain, "rec_slow_gain": rec.slow_gain,
+                               "rec_slow_class": rec.slow_class, "rec_count": rec.count}
+    for k, S in b._W_slow_cpu.items():
+        S = S.tocsr()
+        out[f"slow_{k}_data"], out[f"slow_{k}_indices"], out[f"slow_{k}_indptr"] = S.data, S.indices, S.indptr
+    for key in ("v", "g", "refrac", "adapt", "res", "rate", "spike_counts", "spikes", "g_slow"):
+        out[f"final_{key}"] = getattr(b, key).numpy().copy()
+    print(f"lif_19cell_slow ({mode}): {int(ras.sum())} spikes, slow entries "
+          f"{[(k, S.nnz) for k, S in b._W_slow_cpu.items()]}, max tone {float(b.g_slow.abs().max()):.3f} mV")
     return out
 
 
@@ -340,6 +388,7 @@ def main() -> None:
                 "lif_19cell_adapt_by_type": lambda: lif_19cell(ref, ADAPT_BY_TYPE),
                 "lif_19cell_clocks": lambda: lif_19cell(ref, clocks=True),
                 "lif_c1_clocks": lambda: lif_c1_clocks(ref),
+                **{f"lif_19cell_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m)) for m in ("additive", "gain", "threshold")},
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
                 "tracer": lambda: tracer(ref)}
     for name, make in fixtures.items():

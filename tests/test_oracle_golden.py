@@ -222,3 +222,71 @@ def test_lif_19cell_clocked_rasters_match_reference():
     for key, mine in (("v", st.v), ("g", st.g), ("refrac", st.refrac), ("adapt", st.adapt), ("res", st.res),
                       ("rate", st.rate), ("spike_counts", st.counts)):
         np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
+
+
+def slow_case(mode):
+    """The 19-cell slow-tone fixture: connectome, parameters, the receptor record it was built
+    from, and the shaped fast and slow matrices the reference held after pruning."""
+    import scipy.sparse as sp
+    from flyb200.weights import ReceptorSigns
+    z = golden(f"lif_19cell_slow_{mode}")
+    c = connectome_from_fixture(z)
+    p = LIFParams(receptor_model="full", slow_gain_by_class={"metabotropic_classical": 0.5}, slow_mode=mode)
+    rec = ReceptorSigns(fast_sign=z["rec_fast_sign"], slow_sign=z["rec_slow_sign"], fast_gain=z["rec_fast_gain"],
+                        slow_gain=z["rec_slow_gain"], count=z["rec_count"], slow_class=z["rec_slow_class"])
+    W = sp.csr_matrix((z["shaped_data"], z["shaped_indices"], z["shaped_indptr"]), shape=(c.n, c.n))
+    S = {k: sp.csr_matrix((z[f"slow_{k}_data"], z[f"slow_{k}_indices"], z[f"slow_{k}_indptr"]), shape=(c.n, c.n))
+         for k in z["slow_classes"].tolist()}
+    return z, c, p, rec, W, S
+
+
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+def test_lif_19cell_slow_tone_matches_reference(mode):
+    """receptor_model="full": the shaped fast and slow matrices are the reference's bit for bit, and
+    the oracle's step with the slow tone reproduces its rasters in every slow_mode."""
+    import math
+    import scipy.sparse as sp
+    from flyb200.weights import slow_spec, slow_weights
+    z, c, p, rec, W_ref, S_ref = slow_case(mode)
+    W, scale = lif_weights(c, p, rec)
+    keep = np.ones(c.n, np.float32)
+    keep[z["frozen"]] = 0
+    W = (sp.diags(keep) @ W @ sp.diags(keep)).tocsr()
+    W.eliminate_zeros()
+    np.testing.assert_array_equal(W.data, W_ref.data)
+    spec = slow_spec(p)
+    S = slow_weights(c, p, rec, spec, scale)
+    assert list(S) == list(S_ref) == spec.classes
+    for k in S:
+        Sk = (sp.diags(keep) @ S[k] @ sp.diags(keep)).tocsr()
+        Sk.eliminate_zeros()
+        np.testing.assert_array_equal(Sk.toarray(), S_ref[k].toarray(), err_msg=k)
+    assert sum(Sk.nnz for Sk in S_ref.values()) > 0
+    u = per_type(c, DEFAULT_STD_U_BY_TYPE, p.std_u)
+    ptr, edges, mode_r = out_edges(W_ref, p.w_syn, "auto", std_on=True)
+    B, T, n = int(z["batch"]), int(z["steps"]), c.n
+    st = oracle.LifState(n, B, 5, mode_r, p.v_rest)
+    st.active[z["frozen"]] = 0
+    st.std_u[:] = u
+    dtp = np.float32(p.dt / 1000.0)
+    st.poisson_p[z["orn"], 0], st.poisson_p[z["orn"], 1] = np.float32(120.0) * dtp, np.float32(40.0) * dtp
+    st.poisson_p[z["jo"], 0] = np.array([90.0, 10.0], np.float32) * dtp
+    st.poisson_p[z["jo"], 1] = np.array([0.0, 150.0], np.float32) * dtp
+    st.drive[z["dnp01"], 0] = 12.0
+    U = torch_uniforms(int(z["seed"]), T, (B, n))
+    assert sha(U) == str(z["uniform_sha"])
+    classes = []
+    for k, Sk in S_ref.items():
+        sptr, sedges, smode = out_edges(Sk, p.w_syn, "fixed")
+        classes.append((sptr, sedges, math.exp(-p.dt / spec.tau[k])))
+    slow = {"mode": mode, "norm": spec.norm_mv, "clip": spec.clip, "th_max": float(np.float32(0.9 * spec.norm_mv)),
+            "classes": classes}
+    flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD | _abi.LIF_SKIP_FROZEN
+    r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True, True), n_delay=4, flags=flags, nsteps=T,
+                          uniforms=U.transpose(0, 2, 1), raster=True, slow=slow)
+    ras = unpack(r, n * B).reshape(T, n, B).transpose(0, 2, 1)
+    np.testing.assert_array_equal(ras, z["raster"])
+    for key, mine in (("v", st.v), ("g", st.g), ("adapt", st.adapt), ("res", st.res), ("rate", st.rate),
+                      ("spike_counts", st.counts), ("g_slow", st.g_slow)):
+        np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
+    assert np.abs(st.g_slow).max() > 1.0
