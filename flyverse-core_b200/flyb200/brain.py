@@ -280,6 +280,8 @@ class Brain:
             return
         for S in self._W_slow_cpu.values():
             ptr, edges, _ = out_edges(S, self.p.w_syn, "fixed")
+            if not len(edges):                  # a class without synapses still needs an address
+                edges = np.zeros((1, 2), np.int32)
             self._slow_lists.append((torch.from_numpy(ptr).to(self.device), torch.from_numpy(edges).to(self.device)))
         if not self._slow_rings:
             self._slow_rings = [torch.zeros(self.R, self.n, self.B, dtype=torch.int64, device=self.device)

@@ -14,7 +14,7 @@ LIF_ARRAYS = ("v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "d
 def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, seed=0, uniforms=None,
                    fly_steps=None, raster=False, launch=_abi.LAUNCH_PERSISTENT, block=256, grid=0, fly0=0,
                    device="cuda", items_per_thread=0, with_sync=True, staged=0, defer=False, adapt_jump=None,
-                   clocks=None):
+                   clocks=None, slow=None):
     """Same contract as oracle.lif_run, executed by flyb_lif_run on the device."""
     dev = torch.device(device)
     n, B = state.n, state.batch
@@ -52,6 +52,27 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
             state.clock_acc = np.zeros((n, B), np.int64)
         acc = torch.from_numpy(state.clock_acc).to(dev)
         a.clock_k, a.clock_coef, a.clock_acc = ck.data_ptr(), cc.data_ptr(), acc.data_ptr()
+    held = []
+    if slow is not None:
+        K = len(slow["classes"])
+        if getattr(state, "slow_ring", None) is None:
+            state.slow_ring = np.zeros((K, state.ring_slots, n, B), np.int64)
+            state.slow_g = np.zeros((K, n, B), np.float32)
+            state.g_slow = np.zeros((n, B), np.float32)
+        srings = torch.from_numpy(state.slow_ring).to(dev)
+        sg = torch.from_numpy(state.slow_g).to(dev)
+        gs = torch.from_numpy(state.g_slow).to(dev)
+        a.slow_classes, a.slow_mode = K, _abi.SLOW_MODE_CODES[slow["mode"]]
+        a.slow_norm, a.slow_th_max = slow["norm"], slow["th_max"]
+        a.slow_clip_lo, a.slow_clip_hi = slow["clip"]
+        for c, (sp_, se_, decay) in enumerate(slow["classes"]):
+            tp = torch.from_numpy(np.ascontiguousarray(sp_, np.int32)).to(dev)
+            te = torch.from_numpy(np.ascontiguousarray(se_, np.int32)).to(dev)
+            held += [tp, te]
+            a.slow_out_ptr[c], a.slow_out_edge[c] = tp.data_ptr(), te.data_ptr()
+            a.slow_ring[c], a.slow_g[c] = srings[c].data_ptr(), sg[c].data_ptr()
+            a.slow_decay[c] = decay
+        a.g_slow = gs.data_ptr()
     if defer:
         a.flags |= _abi.LIF_DEFER_DELIVERY
         cap = int(_abi.lib().flyb_lif_spike_capacity(ct.byref(a)))
@@ -71,6 +92,10 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
     state.ring[...] = ring.cpu().numpy()
     if acc is not None:
         state.clock_acc[...] = acc.cpu().numpy()
+    if slow is not None:
+        state.slow_ring[...] = srings.cpu().numpy()
+        state.slow_g[...] = sg.cpu().numpy()
+        state.g_slow[...] = gs.cpu().numpy()
     state.ring_pos = (state.ring_pos + nsteps) % state.ring_slots
     state.step += nsteps
     if fly_steps is not None:

@@ -1,0 +1,93 @@
+"""The slow receptor tone (receptor_model "full") on the GPU: the extended LIF kernel against the
+oracle bit for bit (state, rings, per-class and summed tone, rasters) on a random graph in every
+slow_mode, and the Brain drop-in against the reference's rasters."""
+import math
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import torch
+
+import oracle
+from flyb200 import _abi
+from flyb200.brain import Brain, LIFParams, out_edges
+from gpu_helpers import LIF_ARRAYS, native_lif_run
+from helpers import torch_uniforms, unpack
+from test_gpu_lif import case_random
+from test_oracle_golden import slow_case
+
+pytestmark = pytest.mark.gpu
+
+
+def random_slow(n, mode, seed=5, entries=40_000):
+    """Two slow classes over random synapses (signed, 0.01-0.2 mV per spike), decays of 100 and
+    200 ms at dt 0.1 ms, the reference's normalisation and clip."""
+    rng = np.random.default_rng(seed)
+    classes = []
+    for c, tau in enumerate((100.0, 200.0)):
+        pre, post = rng.integers(0, n, entries), rng.integers(0, n, entries)
+        w = (rng.uniform(0.01, 0.2, entries) * np.where(rng.random(entries) < 0.7, 1, -1)).astype(np.float32)
+        S = sp.csr_matrix((w, (post, pre)), shape=(n, n))
+        ptr, edges, _ = out_edges(S, 0.275, "fixed")
+        classes.append((ptr, edges, math.exp(-0.1 / tau)))
+    return {"mode": mode, "norm": 7.0, "clip": (0.0, 4.0), "th_max": float(np.float32(0.9 * 7.0)), "classes": classes}
+
+
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+@pytest.mark.parametrize("kind", ["count", "fixed-std"])
+def test_slow_tone_kernel_equals_oracle(mode, kind):
+    case = case_random(batch=8, n=3000, edges=60_000, steps=100, fixed=kind == "fixed-std", std=kind == "fixed-std")
+    slow = random_slow(3000, mode)
+    s_ref, s_gpu = case["state"].copy(), case["state"].copy()
+    for chunk in (40, 60):
+        kw = dict(n_delay=case["n_delay"], flags=case["flags"], nsteps=chunk, seed=case["seed"], raster=True,
+                  slow=slow)
+        r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], **kw)
+        r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], launch=_abi.LAUNCH_PERSISTENT,
+                                       **kw)
+        np.testing.assert_array_equal(r_gpu, r_ref)
+        for k in LIF_ARRAYS:
+            np.testing.assert_array_equal(getattr(s_gpu, k), getattr(s_ref, k), err_msg=k)
+        np.testing.assert_array_equal(s_gpu.ring, s_ref.ring)
+        np.testing.assert_array_equal(s_gpu.slow_ring, s_ref.slow_ring)
+        np.testing.assert_array_equal(s_gpu.slow_g, s_ref.slow_g)
+        np.testing.assert_array_equal(s_gpu.g_slow, s_ref.g_slow)
+        assert ev_gpu == ev_ref
+    assert unpack(r_ref, s_ref.n * s_ref.batch).sum() > 0
+    assert np.abs(s_ref.g_slow).max() > 0.1
+
+
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+def test_brain_slow_tone_drop_in_equals_reference_golden(mode):
+    z, c, p, rec, W_ref, S_ref = slow_case(mode)
+    B, T = int(z["batch"]), int(z["steps"])
+    b = Brain(c, p, device="cuda", seed=int(z["seed"]), batch=B, launch="step", receptor=rec)
+    b.freeze(z["frozen"])
+    b.prune(z["frozen"])
+    np.testing.assert_array_equal(b._W_cpu.data, z["shaped_data"])
+    for k, Sk in S_ref.items():
+        np.testing.assert_array_equal(b._W_slow_cpu[k].toarray(), Sk.toarray(), err_msg=k)
+    b.record_activity = True
+    b.set_poisson(z["orn"], torch.tensor([[120.0], [40.0]]))
+    b.set_poisson(z["jo"], torch.tensor([[90.0, 10.0], [0.0, 150.0]]))
+    b.set_drive(z["dnp01"], torch.tensor([[12.0], [0.0]]))
+    U = torch.from_numpy(torch_uniforms(int(z["seed"]), T, (B, c.n))).cuda()
+    ras = []
+    for s in range(T):
+        b.step(1, uniforms=U[s:s + 1])
+        ras.append((b.spikes > 0).cpu().numpy())
+    np.testing.assert_array_equal(np.stack(ras), z["raster"])
+    for key in ("v", "g", "adapt", "res", "rate", "spike_counts", "g_slow"):
+        np.testing.assert_allclose(getattr(b, key).cpu().numpy(), z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
+    # checkpoint round trip and a row reset with the tone
+    saved = b.state_dict()
+    b.step(20)
+    after = {k: getattr(b, k).clone() for k in ("v", "g_slow", "rate")}
+    b.load_state_dict(saved)
+    b.step(20)
+    for k, v in after.items():
+        assert torch.equal(getattr(b, k), v), k
+    b.reset([1])
+    assert float(b.g_slow[1].abs().sum()) == 0.0 and float(b.g_slow_cls[:, 1].abs().sum()) == 0.0
+    with pytest.raises(NotImplementedError):
+        b.set_clocks(np.ones(c.n, np.int64))
