@@ -841,7 +841,7 @@ __device__ __forceinline__ void staged_issue_stores(const LifK& k, unsigned char
   bulk_commit();
 }
 
-template <int BLOCK, bool FIXED, int IPT>
+template <int BLOCK, bool FIXED, int IPT, bool DEFER = false>
 __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
   using L = StagedLayout<BLOCK, FIXED, IPT>;
   using RingT = typename L::RingT;
@@ -954,24 +954,29 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
     __syncthreads();
     if (threadIdx.x == 0) staged_issue_stores<BLOCK, FIXED, IPT>(k, stage, base, W);
     // block-wide delivery: the edges of a chunk's spikers are spread over all its threads (a
-    // warp-local delivery leaves one warp with a high out-degree spiker's whole edge list)
-    deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
+    // warp-local delivery leaves one warp with a high out-degree spiker's whole edge list); or,
+    // deferred, list entries for the scatter kernel of the step
+    if constexpr (DEFER)
+      append_spikes<IPT>(k, s, tx_bits, iq, bq, xq);
+    else
+      deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
     __syncthreads();
   }
   if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // Shared memory of the staged kernel, opted in once per instantiation (above the 48 KB default).
-template <int BLOCK, bool FIXED, int IPT>
+template <int BLOCK, bool FIXED, int IPT, bool DEFER>
 static int staged_prepare(int* blocks_per_sm) {
   using L = StagedLayout<BLOCK, FIXED, IPT>;
   static int per_sm = -1;
   if (per_sm < 0) {
-    cudaError_t e = cudaFuncSetAttribute(lif_staged_kernel<BLOCK, FIXED, IPT>,
+    cudaError_t e = cudaFuncSetAttribute(lif_staged_kernel<BLOCK, FIXED, IPT, DEFER>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES);
     if (e != cudaSuccess) return (int)e;
     int b = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_staged_kernel<BLOCK, FIXED, IPT>, BLOCK, L::BYTES);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, lif_staged_kernel<BLOCK, FIXED, IPT, DEFER>, BLOCK,
+                                                      L::BYTES);
     if (e != cudaSuccess) return (int)e;
     per_sm = b;
   }
@@ -989,12 +994,12 @@ static bool stageable(const LifK& k) {
   return true;
 }
 
-template <int BLOCK, bool FIXED, int IPT>
-static int run_lif_staged(const LifK& k, int grid_cap, cudaStream_t st) {
+template <int BLOCK, bool FIXED, int IPT, bool DEFER>
+static int run_lif_staged_as(const LifK& k, int grid_cap, cudaStream_t st) {
   using L = StagedLayout<BLOCK, FIXED, IPT>;
   if constexpr (L::BYTES > 227 * 1024) return FLYB_EINVAL;   // beyond one block's shared memory
   int per_sm = 0;
-  int rc = staged_prepare<BLOCK, FIXED, IPT>(&per_sm);
+  int rc = staged_prepare<BLOCK, FIXED, IPT, DEFER>(&per_sm);
   if (rc) return rc;
   if (per_sm < 1) return FLYB_ECOOP;
   int dev = 0, sms = 0;
@@ -1005,7 +1010,15 @@ static int run_lif_staged(const LifK& k, int grid_cap, cudaStream_t st) {
   if (grid > chunks) grid = chunks;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
   for (int s = 0; s < k.nsteps; ++s) {
-    lif_staged_kernel<BLOCK, FIXED, IPT><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
+    if constexpr (DEFER) {   // staged update + list, then the balanced scatter
+      cudaError_t e = cudaMemsetAsync(k.spike_n, 0, sizeof(unsigned), st);
+      if (e != cudaSuccess) return (int)e;
+      lif_staged_kernel<BLOCK, FIXED, IPT, true><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
+      FLYB_CHECK_LAUNCH();
+      lif_scatter_kernel<FIXED><<<sms * 8, 256, 0, st>>>(k, s);
+    } else {
+      lif_staged_kernel<BLOCK, FIXED, IPT><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
+    }
     FLYB_CHECK_LAUNCH();
   }
   if (needs_advance(k)) {
@@ -1013,6 +1026,12 @@ static int run_lif_staged(const LifK& k, int grid_cap, cudaStream_t st) {
     FLYB_CHECK_LAUNCH();
   }
   return 0;
+}
+
+template <int BLOCK, bool FIXED, int IPT>
+static int run_lif_staged(const LifK& k, int grid_cap, cudaStream_t st) {
+  return k.spike_list ? run_lif_staged_as<BLOCK, FIXED, IPT, true>(k, grid_cap, st)
+                      : run_lif_staged_as<BLOCK, FIXED, IPT, false>(k, grid_cap, st);
 }
 
 template <int BLOCK, bool FIXED, int IPT>
@@ -1262,8 +1281,7 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   }
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
-    if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP || a->staged)
-      return FLYB_EINVAL;
+    if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP) return FLYB_EINVAL;
     k.spike_list = (int4*)a->spike_list; k.spike_n = a->spike_n; k.spike_cap = a->spike_cap;
   }
   const float* P = a->params;

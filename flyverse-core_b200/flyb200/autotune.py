@@ -20,11 +20,12 @@ CACHE: dict = {}
 OPTIC_VARIANTS = 6          # flyb_optic_args.variant values; a batch width has a subset of them
 # (launch, block, items per thread, delivery): "fused" delivers spikes inside the update kernel,
 # "staged" runs per-step launches through the bulk-copy kernel, "defer" lists the spikers and
-# delivers them from a second, load-balanced kernel
+# delivers them from a second, load-balanced kernel, "staged-defer" does both
 LIF_CANDIDATES = (("step", 256, 4, "fused"), ("step", 256, 2, "fused"), ("step", 256, 1, "fused"),
                   ("step", 256, 2, "staged"), ("step", 512, 2, "staged"), ("step", 256, 4, "staged"),
                   ("step", 256, 2, "defer"), ("step", 256, 1, "defer"), ("step", 128, 2, "defer"),
-                  ("step", 256, 4, "defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"))
+                  ("step", 256, 4, "defer"), ("step", 256, 2, "staged-defer"), ("step", 512, 2, "staged-defer"),
+                  ("step", 256, 4, "staged-defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"))
 
 
 def graph_key(brain) -> str:
@@ -88,7 +89,7 @@ def _apply(brain, choice: dict) -> None:
     brain.launch, brain.block = choice["launch"], choice["block"]
     brain.items_per_thread = choice.get("items_per_thread", 0)
     delivery = choice.get("delivery", "fused")
-    brain.staged, brain.defer = delivery == "staged", delivery == "defer"
+    brain.staged, brain.defer = delivery in ("staged", "staged-defer"), delivery in ("defer", "staged-defer")
     brain._make_args()
 
 

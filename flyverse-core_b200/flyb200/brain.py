@@ -341,9 +341,10 @@ class Brain:
         self._lists = {}          # deferred-delivery lists per neuron range, sized on first use
 
     def _defer_active(self) -> bool:
-        """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step register launches."""
-        return bool(getattr(self, "defer", False)) and self.launch == "step" and not getattr(self, "staged", False) \
-            and self._kvec is None and self.slow is None
+        """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step launches (register or staged
+        path) without clocks or the slow tone."""
+        return bool(getattr(self, "defer", False)) and self.launch == "step" and self._kvec is None \
+            and self.slow is None
 
     # ------------------------------------------------------------------ per-neuron clocks
     def set_clocks(self, multiplier) -> None:

@@ -70,10 +70,11 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
 #define FLYB_LIF_EXT_UNIFORM  16   /* Poisson uniforms from `uniforms` instead of Philox      */
 #define FLYB_LIF_SKIP_FROZEN  32   /* frozen cells at rest are left untouched                 */
 #define FLYB_LIF_EPISODES     64   /* per-fly remaining-step counters gate the update         */
-#define FLYB_LIF_DEFER_DELIVERY 256 /* per-step register launches: the update kernel lists the
-                                      transmitting items (one entry per 1024 out-edges) in
-                                      `spike_list` and a second kernel delivers them, one block
-                                      per entry; needs spike_list / spike_n / spike_cap       */
+#define FLYB_LIF_DEFER_DELIVERY 256 /* per-step launches (register or staged path): the update
+                                      kernel lists the transmitting items (one entry per 1024
+                                      out-edges) in `spike_list` and a second kernel delivers
+                                      them, one block per entry; needs spike_list / spike_n /
+                                      spike_cap                                                */
 #define FLYB_LIF_NO_ADVANCE   128  /* leave `clock` and `fly_steps` as they are: other launches of
                                       the same steps cover the other neurons; flyb_lif_advance
                                       moves them on once all have run                           */

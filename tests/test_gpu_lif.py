@@ -153,6 +153,15 @@ def test_deferred_delivery_equals_oracle(block, ipt, kind):
     _compare(case, STEP, block, ipt=ipt, defer=True)
 
 
+@pytest.mark.parametrize("block,ipt", [(256, 2), (512, 2), (256, 4)])
+@pytest.mark.parametrize("kind", ["count", "fixed", "episodes"])
+def test_staged_deferred_delivery_equals_oracle(block, ipt, kind):
+    """The staged (bulk-copy) update listing its spikers for the scatter kernel: every state bit,
+    ring, raster and event count equal the oracle."""
+    case = case_random(batch=20, n=2999, steps=80, fixed=kind == "fixed", episodes=kind == "episodes")
+    _compare(case, STEP, block, ipt=ipt, staged=1, defer=True)
+
+
 def test_deferred_delivery_splits_high_out_degree_spikers():
     """A hub with more out-edges than one list entry covers (and uneven batch 3) still delivers
     every edge once."""

@@ -19,7 +19,7 @@ def small_fly():
 
 
 @pytest.mark.parametrize("overlap,capped,defer", [(True, False, False), (False, False, False), (True, True, False),
-                                                  (True, False, True)])
+                                                  (True, False, True), (True, False, "staged")])
 def test_whole_fly_matches_oracle_step_order(overlap, capped, defer):
     """Bit-identical spikes every step whether the undriven LIF neurons update concurrently with
     the optic chain (overlap) or after it, also with a capped persistent optic grid beside capped
@@ -31,7 +31,10 @@ def test_whole_fly_matches_oracle_step_order(overlap, capped, defer):
         eng.optic.launch, eng.optic.grid = "persistent", 20
         eng.lif.staged, eng.lif.grid = True, 7
         eng.lif._make_args()
-    eng.lif.defer = defer
+    eng.lif.defer = bool(defer)
+    if defer == "staged":
+        eng.lif.staged = True
+        eng.lif._make_args()
     assert eng.overlapping == overlap
     a_pr = torch.from_numpy((np.random.default_rng(0).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
     eng.set_photoreceptors(a_pr)
