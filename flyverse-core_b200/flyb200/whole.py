@@ -108,11 +108,13 @@ class WholeFly:
         self.a_pr.copy_(a_pr)
         spmm(self.W_rp, self.a_pr, self.optic.pr_in, alpha=self.cfg.optic.gain_in)
 
-    def step(self, n: int = 1) -> None:
+    def step(self, n: int = 1, before=None, after=None) -> None:
         """Advance every fly n steps. Each optic substep reuses the dr the previous one wrote. Under
         CUDA-graph capture the recorded steps end with that dr in the buffer they started from, so
         the graph replays back to back; a graph replay assumes nothing else wrote the optic state
-        since the capture (a write is seen at capture time only)."""
+        since the capture (a write is seen at capture time only). `before(k)` / `after(k)` run on
+        the current stream around step k (new inputs, a readout), inside the same call, so n steps
+        with per-step inputs and outputs stay one call."""
         o = self.cfg.optic
         lif_rate = self.lif._st["rate"]
         drive = self.lif._st["drive"]
@@ -120,7 +122,9 @@ class WholeFly:
         overlap = self.overlapping
         main = torch.cuda.current_stream(self.device)
         hi, side = self._fork
-        for _ in range(int(n)):
+        for k in range(int(n)):
+            if before is not None:
+                before(k)
             spmm(self.W_rs, lif_rate, self.optic.spk_in, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=o.gain_fb,
                  y_index=self.rs_rows)
             if overlap:
@@ -138,6 +142,8 @@ class WholeFly:
             else:
                 self._optic_and_drive(drive)
                 self.lif.step(1)
+            if after is not None:
+                after(k)
         if torch.cuda.is_current_stream_capturing():
             self.optic.pin_dr(cur0)
         self.steps_taken += int(n)

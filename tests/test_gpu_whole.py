@@ -162,3 +162,25 @@ def test_fly_shards_equal_one_batch_after_argument_rebuilds():
         assert whole.spike_counts.sum().item() > 0
         assert torch.equal(part.spike_counts, whole.spike_counts[lo:lo + 4])
         assert torch.equal(part._st["v"], whole._st["v"][:, lo:lo + 4])
+
+
+def test_per_step_inputs_and_readouts_in_one_call():
+    """step(n, before, after) installs each step's photoreceptor input and reads each step's rates
+    exactly as n separate calls do."""
+    cfg = small_fly()
+    B = 4
+    rng = np.random.default_rng(9)
+    frames = torch.from_numpy((rng.standard_normal((5, cfg.optic.n_pr, B)) * 0.4).astype(np.float32)).cuda()
+    a, b = (WholeFly(cfg, B, device="cuda", seed=4, launch="step") for _ in range(2))
+    seen_a, seen_b = [], []
+    a.step(5, before=lambda k: a.set_photoreceptors(frames[k]), after=lambda k: seen_a.append(a.lif.rate.clone()))
+    for k in range(5):
+        b.set_photoreceptors(frames[k])
+        b.step(1)
+        seen_b.append(b.lif.rate.clone())
+    torch.cuda.synchronize()
+    for x, y in zip(seen_a, seen_b):
+        assert torch.equal(x, y)
+    for k in ("v", "g", "rate", "spike_counts"):
+        assert torch.equal(a.lif._st[k], b.lif._st[k]), k
+    assert torch.equal(a.optic.v_s, b.optic.v_s)
