@@ -698,3 +698,75 @@ FLYB_API int launch_csr(void** p, int rows, int cols, int batch, int half, void*
   }
   return (int)cudaGetLastError();
 }
+
+// ------------------------------------------------------------------ the slow tone's unit update
+namespace flyb {
+struct OpticSlowK {
+  int m, batch, classes, mode;
+  float ga, aad, norm, lo, hi;
+  float scale[FLYB_SLOW_MAX_CLASSES], decay[FLYB_SLOW_MAX_CLASSES];
+  float *v, *adapt, *g_slow;
+  float* g_cls[FLYB_SLOW_MAX_CLASSES];
+  const float* held[FLYB_SLOW_MAX_CLASSES];
+  const float* rec_slow[FLYB_SLOW_MAX_CLASSES];
+  const float *rec, *pr, *spk, *dr, *a;
+};
+
+// One thread per (unit, fly), the reference's operation order (optic.py:534-551).
+__global__ void __launch_bounds__(256) optic_slow_kernel(OpticSlowK k) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)k.m * k.batch) return;
+  const int i = (int)(t / k.batch);
+  float tone = 0.0f;
+  for (int c = 0; c < k.classes; ++c) {
+    float target = k.held[c] ? k.held[c][t] : 0.0f;
+    if (k.rec_slow[c]) target = target + k.rec_slow[c][t];
+    const float ts = target * k.scale[c];
+    const float gk = ts + (k.g_cls[c][t] - ts) * k.decay[c];
+    k.g_cls[c][t] = gk;
+    tone = tone + gk;
+  }
+  k.g_slow[t] = tone;
+  const float syn = (k.rec[t] + k.pr[t]) + k.spk[t];
+  const float ad = k.adapt[t];
+  float inp;
+  if (k.mode == FLYB_SLOW_GAIN) {
+    float f = 1.0f + tone / k.norm;
+    f = fminf(fmaxf(f, k.lo), k.hi);
+    inp = syn * f - k.ga * ad;
+  } else {
+    inp = syn - k.ga * ad;
+    if (k.mode == FLYB_SLOW_ADDITIVE) inp = inp + tone;
+  }
+  const float v = k.v[t];
+  k.v[t] = inp + (v - inp) * k.a[i];
+  const float dr = k.dr[t];
+  k.adapt[t] = dr + (ad - dr) * k.aad;
+}
+}  // namespace flyb
+
+FLYB_API int flyb_optic_slow_step(const flyb_optic_slow_args* a, void* stream) {
+  using namespace flyb;
+  if (!a || a->m <= 0 || a->batch <= 0 || a->classes < 1 || a->classes > FLYB_SLOW_MAX_CLASSES ||
+      a->mode < FLYB_SLOW_ADDITIVE || a->mode > FLYB_SLOW_THRESHOLD || !a->v || !a->adapt || !a->g_slow || !a->rec ||
+      !a->pr || !a->spk || !a->dr || !a->a || !(a->norm != 0.0f))
+    return FLYB_EINVAL;
+  const long long total = (long long)a->m * a->batch;
+  if (total >= (1ll << 31)) return FLYB_ETOOBIG;
+  OpticSlowK k;
+  k.m = a->m; k.batch = a->batch; k.classes = a->classes; k.mode = a->mode;
+  k.ga = a->adapt_gain; k.aad = a->a_ad; k.norm = a->norm; k.lo = a->clip_lo; k.hi = a->clip_hi;
+  for (int c = 0; c < FLYB_SLOW_MAX_CLASSES; ++c) {
+    const bool used = c < a->classes;
+    if (used && !a->g_cls[c]) return FLYB_EINVAL;
+    k.scale[c] = used ? a->scale[c] : 0.0f;
+    k.decay[c] = used ? a->decay[c] : 0.0f;
+    k.g_cls[c] = used ? a->g_cls[c] : nullptr;
+    k.held[c] = used ? a->held[c] : nullptr;
+    k.rec_slow[c] = used ? a->rec_slow[c] : nullptr;
+  }
+  k.v = a->v; k.adapt = a->adapt; k.g_slow = a->g_slow;
+  k.rec = a->rec; k.pr = a->pr; k.spk = a->spk; k.dr = a->dr; k.a = a->a;
+  optic_slow_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(k);
+  return (int)cudaGetLastError();
+}

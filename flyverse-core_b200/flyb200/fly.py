@@ -25,11 +25,12 @@ from .brain import Brain, LIFParams
 from .connectome import PHOTORECEPTOR_TYPES
 from .optic import OpticLobe, OpticParams
 from .retina import build_retina
+from .weights import receptor_gain
 
 
 class FlyBrain:
     BRAIN_TENSORS = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
-    OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate")
+    OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate", "g_slow", "g_slow_cls", "_slow_in_s")
 
     def __init__(self, c, *, batch: int = 1, device=None, seed: int = 0, lif_params: LIFParams | None = None,
                  optic_params: OpticParams | None = None, cuda_graphs: bool = False, retina=None,
@@ -50,7 +51,8 @@ class FlyBrain:
             self.retina = retina if retina is not None else build_retina(c)
             if self.retina.n_columns:
                 self.optic = OpticLobe(c, self.retina, optic_params, device=self.device, batch=self.B,
-                                       receptor=receptor, slow=self.brain.slow, launch=launch)
+                                       receptor=receptor, receptor_gain=receptor_gain(lp), slow=self.brain.slow,
+                                       launch=launch)
                 self.optic.relax()
                 self.brain.freeze(self.optic.rate_idx)
                 if lp.prune_frozen:
@@ -321,7 +323,8 @@ class FlyBrain:
         o = self.optic
         if o is not None:
             for k in self.OPTIC_TENSORS:
-                getattr(o, k).copy_(state["optic"][k].to(self.device))
+                if k in state["optic"]:          # the slow tone's state is absent from older checkpoints
+                    getattr(o, k).copy_(state["optic"][k].to(self.device))
             o._fresh_u8.copy_(state["optic_fresh"].to(self.device))
             o._pending_ms = state["optic_pending_ms"]
             o.r0 = o.b_vec[None].clone()

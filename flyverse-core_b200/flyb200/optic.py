@@ -362,6 +362,30 @@ def lobe_matrices(c, retina, p: OpticParams, receptor=None, receptor_gain=None) 
                         np.asarray(retina.pr_column, np.int64), np.asarray(retina.pr_sens, np.float32).reshape(-1, 4))
 
 
+def slow_blocks(c, rate_idx, spk_idx, p: OpticParams, receptor, receptor_gain, spec) -> tuple[list, float]:
+    """The optic lobe's slow-tone blocks (optic.py:285-309): per active class of `spec` the
+    spiking -> rate and rate -> rate matrices (count x slow sign x gain class, normalised by the same
+    denominators as the fast blocks; None where empty), the relaxation scale gain tau / tau_syn and
+    factor exp(-dt / tau); and the tone's normalisation 1 - baseline."""
+    if getattr(receptor, "count", None) is None:
+        raise ValueError("the optic lobe's slow term needs the receptor record's synapse counts")
+    denom = c.neurons.in_syn_l2.to_numpy() if p.norm == "l2" else c.neurons.in_syn.to_numpy()
+    out = []
+    for cls in spec.classes:
+        S = c.W.tocsr().copy()
+        S.data = receptor.count * receptor.slow_factor(receptor_gain, slow_class=cls)
+        S.eliminate_zeros()
+        Sn = (sp.diags(1.0 / np.maximum(denom, 1.0)) @ S).tocsr()
+        rs = Sn[rate_idx][:, spk_idx].tocsr()
+        rr = Sn[rate_idx][:, rate_idx].tocsr()
+        out.append((rs if rs.nnz else None, rr if rr.nnz else None, float(spec.gain[cls] * spec.tau[cls] / spec.tau_syn),
+                    float(np.exp(-p.dt_ms / spec.tau[cls]))))
+    norm = float(1.0 - p.baseline)
+    if norm <= 0:
+        raise ValueError("the optic slow term needs baseline < 1")
+    return out, norm
+
+
 class OpticLobe:
     def __init__(self, c, retina, params: OpticParams | None = None, device=None, batch: int = 1,
                  metal_kernels=None, cuda_kernels=None, cuda_sparse: str = "torch", receptor=None,
@@ -377,8 +401,6 @@ class OpticLobe:
             raise NotImplementedError("use flyb200.adjoint (hand-written optic adjoint) for gradients")
         if p.stream_rectify or p.stream_adapt or p.spatial_suppress:
             raise NotImplementedError("the per-stream hooks are Torch-only in the reference and not provided")
-        if slow is not None and receptor is not None and getattr(slow, "gain", None):
-            raise NotImplementedError("the slow receptor term is Torch-only in the reference and not provided")
         if not np.isfinite(p.dt_ms) or p.dt_ms <= 0:
             raise ValueError("optic dt_ms must be positive and finite")
         self.device = torch.device(device) if device is not None else torch.device("cuda")
@@ -387,7 +409,9 @@ class OpticLobe:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.B = int(batch)
-        self.receptor, self.slow, self.surrogate_grad = receptor, None, False
+        # the slow receptor tone (optic.py:203, 285-309) is active with a receptor record and a scale
+        self.slow = slow if (slow is not None and receptor is not None and getattr(slow, "gain", None)) else None
+        self.receptor, self.surrogate_grad = receptor, False
         self._pending_ms = 0.0
         L = lobe_matrices(c, retina, p, receptor, receptor_gain)
         self.L = L
@@ -419,9 +443,16 @@ class OpticLobe:
         self._a_pr = torch.zeros(self.n_pr, B, device=dev)
         self._delta = torch.zeros(self.n_rate, B, device=dev)
         self._drive = torch.zeros(c.n, B, device=dev)
-        self.g_slow_cls = torch.zeros(0, B, self.n_rate, device=dev)
-        self.g_slow = torch.zeros(B, self.n_rate, device=dev)
-        self._slow_in_s = torch.zeros(0, B, self.n_rate, device=dev)
+        self.slow_classes = list(self.slow.classes) if self.slow is not None else []
+        K = len(self.slow_classes)
+        self._g_cls_s = torch.zeros(K, self.n_rate, B, device=dev)        # [K][m][B] storage
+        self._g_slow_s = torch.zeros(self.n_rate, B, device=dev)
+        self._held_s = torch.zeros(K, self.n_rate, B, device=dev)
+        self.g_slow_cls = self._g_cls_s.transpose(1, 2)                   # (K, B, m) views
+        self.g_slow = self._g_slow_s.t()
+        self._slow_in_s = self._held_s.transpose(1, 2)
+        if self.slow is not None:
+            self._setup_slow(c, receptor, receptor_gain)
         self.stream_adapt_state = torch.zeros(0, B, self.n_rate, device=dev)
         self.r0 = None
         self.last = {}
@@ -477,8 +508,60 @@ class OpticLobe:
             raise RuntimeError(f"flyb_photoreceptor: error {rc}")
         return self._a_pr.t()
 
+    # ------------------------------------------------------------------ the slow receptor tone
+    def _setup_slow(self, c, receptor, receptor_gain) -> None:
+        """Device copies of the slow-tone blocks (`slow_blocks`) and the products' buffers."""
+        p, dev = self.p, self.device
+        blocks, self._slow_norm = slow_blocks(c, self.rate_idx, self.spk_idx, p, receptor, receptor_gain, self.slow)
+        self._slow_rs = [DeviceCSR(rs, dev) if rs is not None else None for rs, _, _, _ in blocks]
+        self._slow_rr = [DeviceCSR(rr, dev) if rr is not None else None for _, rr, _, _ in blocks]
+        self._slow_scale = [scale for _, _, scale, _ in blocks]
+        self._a_slow = [decay for _, _, _, decay in blocks]
+        self.slow_entries = {cls: {"spiking_to_rate": 0 if rs is None else int(rs.nnz),
+                                   "rate_to_rate": 0 if rr is None else int(rr.nnz)}
+                             for cls, (rs, rr, _, _) in zip(self.slow_classes, blocks)}
+        self._W_rr_plain = DeviceCSR(self.M_rr, dev)
+        m, B = self.n_rate, self.B
+        self._rec = torch.zeros(m, B, device=dev)
+        self._rec_slow = [torch.zeros(m, B, device=dev) if W is not None else None for W in self._slow_rr]
+        self._dr_slow = torch.zeros(m, B, device=dev)
+
+    def _slow_substeps(self, steps: int) -> None:
+        """The substeps with the slow tone (optic.py:526-551): dr (shifted by the tone in the
+        threshold mode), the recurrent and slow products, then the native unit update."""
+        p = self.p
+        core = self.core
+        b = self.b_vec[:, None]
+        mode = _abi.SLOW_MODE_CODES[self.slow.mode]
+        args = _abi.OpticSlowArgs(m=self.n_rate, batch=self.B, classes=len(self.slow_classes), mode=mode,
+                                  adapt_gain=p.adapt_gain, a_ad=self._a_ad, norm=self._slow_norm,
+                                  clip_lo=self.slow.clip[0], clip_hi=self.slow.clip[1], v=core.v_s.data_ptr(),
+                                  adapt=core.adapt_s.data_ptr(), g_slow=self._g_slow_s.data_ptr(),
+                                  rec=self._rec.data_ptr(), pr=core.pr_in.data_ptr(), spk=core.spk_in.data_ptr(),
+                                  dr=self._dr_slow.data_ptr(), a=self.core.a.data_ptr())
+        for c in range(len(self.slow_classes)):
+            args.scale[c], args.decay[c] = self._slow_scale[c], self._a_slow[c]
+            args.g_cls[c] = self._g_cls_s[c].data_ptr()
+            args.held[c] = self._held_s[c].data_ptr() if self._slow_rs[c] is not None else None
+            args.rec_slow[c] = self._rec_slow[c].data_ptr() if self._rec_slow[c] is not None else None
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        for _ in range(steps):
+            r = core.v_s + b
+            if self.slow.mode == "threshold":
+                r = r + self._g_slow_s.clamp(max=0.9 * self._slow_norm)
+            torch.sub(r.clamp(0.0, 1.0), b, out=self._dr_slow)
+            spmm(self._W_rr_plain, self._dr_slow, self._rec, alpha=p.gain_rr)
+            for W, y in zip(self._slow_rr, self._rec_slow):
+                if W is not None:
+                    spmm(W, self._dr_slow, y, alpha=p.gain_rr)
+            rc = _abi.lib().flyb_optic_slow_step(ct.byref(args), stream)
+            if rc:
+                raise RuntimeError(f"flyb_optic_slow_step: error {rc}")
+
     # ------------------------------------------------------------------ rate dynamics
     def rates(self) -> torch.Tensor:
+        if self.slow is not None and self.slow.mode == "threshold":
+            return (self.v + self.b_vec[None] + self.g_slow.clamp(max=0.9 * self._slow_norm)).clamp(0.0, 1.0)
         return (self.v + self.b_vec[None]).clamp(0.0, 1.0)
 
     def relax(self, ms: float = 0.0) -> None:
@@ -511,7 +594,13 @@ class OpticLobe:
             spmm(self.W_rp, self._fly_minor(a_pr), self.core.pr_in, alpha=p.gain_in)
             spmm(self.W_rs, rates_s, self.core.spk_in, x_index=self._spk_idx32, x_div=100.0, x_lo=0.0, x_hi=3.0,
                  alpha=p.gain_fb)
-            self.core.substeps(steps)
+            if self.slow is None:
+                self.core.substeps(steps)
+            else:                       # the spiking part of the slow input, held for the frame too
+                for W, h in zip(self._slow_rs, self._held_s):
+                    if W is not None:
+                        spmm(W, rates_s, h, x_index=self._spk_idx32, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=p.gain_fb)
+                self._slow_substeps(steps)
         torch.sub(self.rates(), self.r0, out=self.delta_rate)
         drive = out if out is not None else self._drive
         drive.zero_()
@@ -525,10 +614,16 @@ class OpticLobe:
             self._fresh_u8.fill_(1)
             self.core.v_s.zero_()
             self.core.adapt_s.zero_()
+            self._g_slow_s.zero_()
+            self._g_cls_s.zero_()
+            self._held_s.zero_()
             self._pending_ms = 0.0
         else:
             sel = torch.as_tensor(np.asarray(rows), device=self.device, dtype=torch.long)
             self._fresh_u8[sel] = 1
             self.core.v_s[:, sel] = 0.0
             self.core.adapt_s[:, sel] = 0.0
+            self._g_slow_s[:, sel] = 0.0
+            self._g_cls_s[:, :, sel] = 0.0
+            self._held_s[:, :, sel] = 0.0
 

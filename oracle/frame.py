@@ -38,8 +38,53 @@ def photoreceptor(L, st: dict, rad: np.ndarray, dt_ms: float, p) -> np.ndarray:
     return np.ascontiguousarray(con[:, L.pr_cell].T)                           # [n_pr][B]
 
 
-def frame(L, st: dict, rad: np.ndarray, spk_rate: np.ndarray, frame_ms: float, p) -> np.ndarray:
-    """Advance one frame in place; returns the drive (B, N) in mV. spk_rate: (B, N) Hz."""
+def _csr_mv(M, x, alpha):
+    """alpha x (M @ x) for x [cols][B], rows summed in CSR order in float32 (the reference's
+    sparse product), through the C restatement."""
+    M = M.tocsr()
+    return spmm(M.indptr, M.indices, M.data, x, x.shape[1], rows=M.shape[0], alpha=alpha)
+
+
+def slow_substeps(L, st: dict, pr, spk, steps: int, p, slow: dict) -> None:
+    """The substeps with the slow receptor tone (optic.py:526-551), FP32 in the reference order:
+    slow = {"mode", "norm", "clip", "classes": [(rs, rr, scale, decay)]}; state st["g_cls"]
+    [K][m][B], st["g_slow"] [m][B], st["held"] [K][m][B]."""
+    f32 = np.float32
+    b = L.b[:, None].astype(f32)
+    a = L.a[:, None].astype(f32)
+    norm = f32(slow["norm"])
+    for _ in range(steps):
+        r = (st["v"] + b).astype(f32)
+        if slow["mode"] == "threshold":
+            r = (r + np.minimum(st["g_slow"], f32(0.9 * slow["norm"]))).astype(f32)
+        dr = (np.clip(r, f32(0), f32(1)) - b).astype(f32)
+        rec = _csr_mv(L.M_rr, dr, p.gain_rr)
+        tone = np.zeros_like(dr)
+        for k, (rs, rr, scale, decay) in enumerate(slow["classes"]):
+            target = st["held"][k].copy()
+            if rr is not None:
+                target = (target + _csr_mv(rr, dr, p.gain_rr)).astype(f32)
+            ts = (target * f32(scale)).astype(f32)
+            gk = (ts + (st["g_cls"][k] - ts) * f32(decay)).astype(f32)
+            st["g_cls"][k] = gk
+            tone = (tone + gk).astype(f32)
+        st["g_slow"] = tone
+        syn = ((rec + pr).astype(f32) + spk).astype(f32)
+        ad = (f32(p.adapt_gain) * st["adapt"]).astype(f32)
+        if slow["mode"] == "gain":
+            fac = np.clip((f32(1) + tone / norm).astype(f32), f32(slow["clip"][0]), f32(slow["clip"][1]))
+            inp = ((syn * fac).astype(f32) - ad).astype(f32)
+        else:
+            inp = (syn - ad).astype(f32)
+            if slow["mode"] == "additive":
+                inp = (inp + tone).astype(f32)
+        st["v"] = (inp + (st["v"] - inp) * a).astype(f32)
+        st["adapt"] = (dr + (st["adapt"] - dr) * f32(L.aad)).astype(f32)
+
+
+def frame(L, st: dict, rad: np.ndarray, spk_rate: np.ndarray, frame_ms: float, p, slow: dict | None = None) -> np.ndarray:
+    """Advance one frame in place; returns the drive (B, N) in mV. spk_rate: (B, N) Hz. `slow`: the
+    slow receptor tone (see slow_substeps)."""
     B = rad.shape[0]
     a_pr = photoreceptor(L, st, rad, frame_ms, p)
     total = st["pending"] + frame_ms
@@ -52,11 +97,23 @@ def frame(L, st: dict, rad: np.ndarray, spk_rate: np.ndarray, frame_ms: float, p
         M = L.M_rs.tocsr()
         spk = spmm(M.indptr, M.indices, M.data, rates, B, rows=M.shape[0], x_index=L.spk_idx, x_div=100.0,
                    x_lo=0.0, x_hi=3.0, alpha=p.gain_fb)
-        M = L.M_rr.tocsr()
-        optic_run(st["v"], st["adapt"], M.indptr, M.indices, M.data, pr, spk, L.a, L.b, p.gain_rr, p.adapt_gain,
-                  L.aad, steps)
+        if slow is None:
+            M = L.M_rr.tocsr()
+            optic_run(st["v"], st["adapt"], M.indptr, M.indices, M.data, pr, spk, L.a, L.b, p.gain_rr, p.adapt_gain,
+                      L.aad, steps)
+        else:
+            for k, (rs, rr, scale, decay) in enumerate(slow["classes"]):
+                st["held"][k] = 0.0
+                if rs is not None:
+                    rs = rs.tocsr()
+                    st["held"][k] = spmm(rs.indptr, rs.indices, rs.data, rates, B, rows=rs.shape[0], x_index=L.spk_idx,
+                                         x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=p.gain_fb)
+            slow_substeps(L, st, pr, spk, steps, p, slow)
     b = L.b[:, None].astype(np.float32)
-    delta = (np.clip(st["v"] + b, 0.0, 1.0) - b).astype(np.float32)
+    r = (st["v"] + b).astype(np.float32)
+    if slow is not None and slow["mode"] == "threshold":
+        r = (r + np.minimum(st["g_slow"], np.float32(0.9 * slow["norm"]))).astype(np.float32)
+    delta = (np.clip(r, 0.0, 1.0) - b).astype(np.float32)
     st["delta"] = delta
     M = L.M_sr.tocsr()
     n = spk_rate.shape[1]

@@ -24,6 +24,9 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
                   reference's sparse-matmul path: rasters and final state.
   optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
                   of tests/test_optic_hooks.py::hex_graph(), batch 2, three frames.
+  optic_hex_slow_{additive,gain,threshold}.npz  the hex patch's OpticLobe with the receptor model's
+                  slow tone (classical class at scale 2) in each slow_mode, three frames from a displaced start, with the
+                  receptor record it was built from.
   optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
                   synthetic 3,000-unit lobe from flyb200.synthetic.optic_config3, 60 substeps.
   tracer.npz      flyverse.world / flyverse.batch_world (CPU): the reference tests' rays in
@@ -247,6 +250,41 @@ def optic_hex(ref) -> dict:
     return out
 
 
+def optic_hex_slow(ref, mode: str) -> dict:
+    """The hex patch's optic lobe under the receptor model's slow tone (classical class at scale 2,
+    built from connectome.receptor_signs) in one slow_mode, batch 2, three frames from a displaced
+    start."""
+    optic, rt, brain, cn = ref["optic"], ref["retina"], ref["brain"], ref["connectome"]
+    th = ref["test_optic_hooks"]
+    c = th.hex_graph()
+    r = rt.build_retina(c)
+    p = brain.LIFParams(receptor_model="full", slow_gain_by_class={"metabotropic_classical": 2.0}, slow_mode=mode)
+    rec = cn.receptor_signs(c, net_rule=p.receptor_net_rule, with_counts=True)
+    B = 2
+    ol = optic.OpticLobe(c, r, optic.OpticParams(), device="cpu", batch=B, receptor=rec,
+                         receptor_gain=brain._receptor_gain(p), slow=brain._slow_spec(p))
+    ol.relax()
+    gen = torch.Generator().manual_seed(4)
+    # the receptor model silences the patch's histamine photoreceptor synapses, so the lobe starts
+    # from a displaced state (public state, as a caller may set it) whose decay drives the tone
+    v0 = torch.rand(B, ol.n_rate, generator=gen) * 0.8 - 0.3
+    ol.v.copy_(v0)
+    out = {"rec_fast_sign": rec.fast_sign, "rec_slow_sign": rec.slow_sign, "rec_fast_gain": rec.fast_gain,
+           "rec_slow_gain": rec.slow_gain, "rec_slow_class": rec.slow_class, "rec_count": rec.count,
+           "slow_mode": np.array(mode), "slow_entries": np.array(repr(ol.slow_entries)), "v0": v0.numpy()}
+    for f in range(3):
+        rad = torch.rand(B, r.n_columns, 4, generator=gen)
+        spk = torch.rand(B, c.n, generator=gen) * 80.0
+        drive = ol.step_frame(rad, spk, 10.0)
+        out[f"frame{f}_rad"], out[f"frame{f}_spk"] = rad.numpy(), spk.numpy()
+        for key in ("v", "adapt", "delta_rate", "g_slow"):
+            out[f"frame{f}_{key}"] = getattr(ol, key).numpy().copy()
+        out[f"frame{f}_g_slow_cls"] = ol.g_slow_cls.numpy().copy()
+        out[f"frame{f}_drive"] = drive.numpy().copy()
+    print(f"optic_hex_slow ({mode}): slow entries {ol.slow_entries}, max tone {float(ol.g_slow.abs().max()):.4f}")
+    return out
+
+
 def optic_synth(ref) -> dict:
     """The reference's substep expressions on a synthetic lobe, called on the reference class."""
     optic = ref["optic"]
@@ -390,7 +428,8 @@ def main() -> None:
                 "lif_c1_clocks": lambda: lif_c1_clocks(ref),
                 **{f"lif_19cell_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m)) for m in ("additive", "gain", "threshold")},
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
-                "tracer": lambda: tracer(ref)}
+                "tracer": lambda: tracer(ref),
+                **{f"optic_hex_slow_{m}": (lambda m=m: optic_hex_slow(ref, m)) for m in ("additive", "gain", "threshold")}}
     for name, make in fixtures.items():
         if args.only in (None, name):
             np.savez_compressed(HERE / f"{name}.npz", **make())

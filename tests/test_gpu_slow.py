@@ -91,3 +91,49 @@ def test_brain_slow_tone_drop_in_equals_reference_golden(mode):
     assert float(b.g_slow[1].abs().sum()) == 0.0 and float(b.g_slow_cls[:, 1].abs().sum()) == 0.0
     with pytest.raises(NotImplementedError):
         b.set_clocks(np.ones(c.n, np.int64))
+
+
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+def test_optic_slow_tone_equals_reference_golden(mode):
+    """OpticLobe with the slow receptor tone (the unit update kernel after the recurrent and slow
+    products) against the reference's frames, and the state survives a FlyBrain-style checkpoint
+    of its tensors."""
+    from flyb200.optic import OpticLobe
+    from flyb200.weights import receptor_gain, slow_spec
+    from test_oracle_golden import optic_slow_case
+    z, c, r, rec, lp, p, L, slow = optic_slow_case(mode)
+    ol = OpticLobe(c, r, p, device="cuda", batch=2, receptor=rec, receptor_gain=receptor_gain(lp), slow=slow_spec(lp),
+                   launch="step")
+    ol.relax()
+    ol.v = torch.from_numpy(z["v0"]).cuda()
+    for f in range(3):
+        drive = ol.step_frame(torch.from_numpy(z[f"frame{f}_rad"]), torch.from_numpy(z[f"frame{f}_spk"]).cuda(), 10.0)
+        for key in ("v", "adapt", "g_slow", "delta_rate"):
+            np.testing.assert_allclose(getattr(ol, key).cpu().numpy(), z[f"frame{f}_{key}"], rtol=1e-5, atol=1e-6,
+                                       err_msg=f"{key} frame {f}")
+        np.testing.assert_allclose(ol.g_slow_cls.cpu().numpy(), z[f"frame{f}_g_slow_cls"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(drive.cpu().numpy(), z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
+    assert float(ol.g_slow.abs().max()) > 0.5
+    ol.reset([1])
+    assert float(ol.g_slow[1].abs().sum()) == 0.0 and float(ol.g_slow_cls[:, 1].abs().sum()) == 0.0
+
+
+def test_flybrain_full_receptor_model_runs_both_tones():
+    """FlyBrain under receptor_model="full": the brain and the optic lobe both carry the tone, and a
+    checkpoint restores it."""
+    from flyb200.fly import FlyBrain
+    from test_oracle_golden import optic_slow_case
+    z, c, r, rec, lp, p, L, slow = optic_slow_case("additive")
+    lp = LIFParams(receptor_model="full", slow_gain_by_class={"metabotropic_classical": 2.0}, dt=0.5)
+    fb = FlyBrain(c, batch=2, device="cuda", seed=3, retina=r, lif_params=lp, optic_params=p, receptor=rec)
+    assert fb.brain.slow is not None and fb.optic.slow is not None
+    fb.optic.v = torch.from_numpy(z["v0"]).cuda()
+    fb.vision(z["frame0_rad"][0])
+    fb.step(10.0)
+    saved = fb.state_dict()
+    fb.step(10.0)
+    after = (fb.optic.g_slow.clone(), fb.optic.v.clone(), fb.brain.v.clone())
+    fb.load_state_dict(saved)
+    fb.step(10.0)
+    assert torch.equal(fb.optic.g_slow, after[0]) and torch.equal(fb.optic.v, after[1]) and torch.equal(fb.brain.v, after[2])
+    assert float(fb.optic.g_slow.abs().max()) > 0

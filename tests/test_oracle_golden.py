@@ -290,3 +290,42 @@ def test_lif_19cell_slow_tone_matches_reference(mode):
                       ("spike_counts", st.counts), ("g_slow", st.g_slow)):
         np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
     assert np.abs(st.g_slow).max() > 1.0
+
+
+def optic_slow_case(mode):
+    """The hex patch under the slow receptor tone: fixture, lobe matrices with the receptor record,
+    the slow description for the oracle and its initial state."""
+    from flyb200.optic import slow_blocks
+    from flyb200.weights import ReceptorSigns, receptor_gain, slow_spec
+    _, c, r = hex_lobe()
+    z = golden(f"optic_hex_slow_{mode}")
+    rec = ReceptorSigns(fast_sign=z["rec_fast_sign"], slow_sign=z["rec_slow_sign"], fast_gain=z["rec_fast_gain"],
+                        slow_gain=z["rec_slow_gain"], count=z["rec_count"], slow_class=z["rec_slow_class"])
+    lp = LIFParams(receptor_model="full", slow_gain_by_class={"metabotropic_classical": 2.0}, slow_mode=mode)
+    p = OpticParams()
+    L = lobe_matrices(c, r, p, rec, receptor_gain(lp))
+    spec = slow_spec(lp)
+    blocks, norm = slow_blocks(c, L.rate_idx, L.spk_idx, p, rec, receptor_gain(lp), spec)
+    slow = {"mode": mode, "norm": norm, "clip": spec.clip, "classes": blocks}
+    return z, c, r, rec, lp, p, L, slow
+
+
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+def test_optic_slow_tone_frames_match_reference(mode):
+    """The optic lobe's slow receptor tone (optic.py:526-551): three frames from a displaced start,
+    every state within 1e-5 of the reference's OpticLobe."""
+    z, c, r, rec, lp, p, L, slow = optic_slow_case(mode)
+    B, m, K = 2, len(L.rate_idx), len(slow["classes"])
+    st = {"v": np.ascontiguousarray(z["v0"].T), "adapt": np.zeros((m, B), np.float32),
+          "I_lp": np.zeros((B, r.n_columns * 5), np.float32), "I_mean": np.zeros((B, r.n_columns * 5), np.float32),
+          "fresh": np.ones(B, bool), "pending": 0.0, "g_cls": np.zeros((K, m, B), np.float32),
+          "g_slow": np.zeros((m, B), np.float32), "held": np.zeros((K, m, B), np.float32)}
+    for f in range(3):
+        drive = oframe.frame(L, st, z[f"frame{f}_rad"], z[f"frame{f}_spk"], 10.0, p, slow=slow)
+        np.testing.assert_allclose(st["v"].T, z[f"frame{f}_v"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["adapt"].T, z[f"frame{f}_adapt"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["g_slow"].T, z[f"frame{f}_g_slow"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["g_cls"].transpose(0, 2, 1), z[f"frame{f}_g_slow_cls"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["delta"].T, z[f"frame{f}_delta_rate"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(drive, z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
+    assert np.abs(st["g_slow"]).max() > 0.5
