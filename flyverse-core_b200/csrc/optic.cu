@@ -699,9 +699,9 @@ FLYB_API int launch_csr(void** p, int rows, int cols, int batch, int half, void*
   return (int)cudaGetLastError();
 }
 
-// ------------------------------------------------------------------ the slow tone's unit update
+// ------------------------------------------------------------------ the unit update of the extended substep
 namespace flyb {
-struct OpticSlowK {
+struct OpticUnitK {
   int m, batch, classes, mode;
   float ga, aad, norm, lo, hi;
   float scale[FLYB_SLOW_MAX_CLASSES], decay[FLYB_SLOW_MAX_CLASSES];
@@ -713,7 +713,7 @@ struct OpticSlowK {
 };
 
 // One thread per (unit, fly), the reference's operation order (optic.py:534-551).
-__global__ void __launch_bounds__(256) optic_slow_kernel(OpticSlowK k) {
+__global__ void __launch_bounds__(256) optic_unit_kernel(OpticUnitK k) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long long)k.m * k.batch) return;
   const int i = (int)(t / k.batch);
@@ -726,15 +726,20 @@ __global__ void __launch_bounds__(256) optic_slow_kernel(OpticSlowK k) {
     k.g_cls[c][t] = gk;
     tone = tone + gk;
   }
-  k.g_slow[t] = tone;
-  const float syn = (k.rec[t] + k.pr[t]) + k.spk[t];
   const float ad = k.adapt[t];
   float inp;
-  if (k.mode == FLYB_SLOW_GAIN) {
+  if (!k.classes) {                     // the plain order (optic.py:530-532)
+    inp = (k.rec[t] + k.pr[t]) - k.ga * ad;
+    inp = inp + k.spk[t];
+  } else if (k.mode == FLYB_SLOW_GAIN) {
+    k.g_slow[t] = tone;
+    const float syn = (k.rec[t] + k.pr[t]) + k.spk[t];
     float f = 1.0f + tone / k.norm;
     f = fminf(fmaxf(f, k.lo), k.hi);
     inp = syn * f - k.ga * ad;
   } else {
+    k.g_slow[t] = tone;
+    const float syn = (k.rec[t] + k.pr[t]) + k.spk[t];
     inp = syn - k.ga * ad;
     if (k.mode == FLYB_SLOW_ADDITIVE) inp = inp + tone;
   }
@@ -745,15 +750,17 @@ __global__ void __launch_bounds__(256) optic_slow_kernel(OpticSlowK k) {
 }
 }  // namespace flyb
 
-FLYB_API int flyb_optic_slow_step(const flyb_optic_slow_args* a, void* stream) {
+FLYB_API int flyb_optic_unit_step(const flyb_optic_unit_args* a, void* stream) {
   using namespace flyb;
-  if (!a || a->m <= 0 || a->batch <= 0 || a->classes < 1 || a->classes > FLYB_SLOW_MAX_CLASSES ||
-      a->mode < FLYB_SLOW_ADDITIVE || a->mode > FLYB_SLOW_THRESHOLD || !a->v || !a->adapt || !a->g_slow || !a->rec ||
-      !a->pr || !a->spk || !a->dr || !a->a || !(a->norm != 0.0f))
+  if (!a || a->m <= 0 || a->batch <= 0 || a->classes < 0 || a->classes > FLYB_SLOW_MAX_CLASSES || !a->v ||
+      !a->adapt || !a->rec || !a->pr || !a->spk || !a->dr || !a->a)
+    return FLYB_EINVAL;
+  if (a->classes && (a->mode < FLYB_SLOW_ADDITIVE || a->mode > FLYB_SLOW_THRESHOLD || !a->g_slow ||
+                     !(a->norm != 0.0f)))
     return FLYB_EINVAL;
   const long long total = (long long)a->m * a->batch;
   if (total >= (1ll << 31)) return FLYB_ETOOBIG;
-  OpticSlowK k;
+  OpticUnitK k;
   k.m = a->m; k.batch = a->batch; k.classes = a->classes; k.mode = a->mode;
   k.ga = a->adapt_gain; k.aad = a->a_ad; k.norm = a->norm; k.lo = a->clip_lo; k.hi = a->clip_hi;
   for (int c = 0; c < FLYB_SLOW_MAX_CLASSES; ++c) {
@@ -767,6 +774,6 @@ FLYB_API int flyb_optic_slow_step(const flyb_optic_slow_args* a, void* stream) {
   }
   k.v = a->v; k.adapt = a->adapt; k.g_slow = a->g_slow;
   k.rec = a->rec; k.pr = a->pr; k.spk = a->spk; k.dr = a->dr; k.a = a->a;
-  optic_slow_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(k);
+  optic_unit_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(k);
   return (int)cudaGetLastError();
 }

@@ -196,7 +196,7 @@ FLYB_API const char* flyb_version(void) { return "flyb200 0.1.0 (sm_100a)"; }
 FLYB_API int flyb_abi_sizes(int* sizes, int n) {
   const int s[7] = {(int)sizeof(flyb_lif_args),     (int)sizeof(flyb_optic_args), (int)sizeof(flyb_spmm_args),
                     (int)sizeof(flyb_adjoint_args), (int)sizeof(flyb_photo_args), (int)sizeof(flyb_trace_args),
-                    (int)sizeof(flyb_optic_slow_args)};
+                    (int)sizeof(flyb_optic_unit_args)};
   int k = 0;
   for (; k < n && k < 7; ++k) sizes[k] = s[k];
   return k;

@@ -102,7 +102,7 @@ class TraceArgs(ct.Structure):
                 ("out", _VP)]
 
 
-class OpticSlowArgs(ct.Structure):
+class OpticUnitArgs(ct.Structure):
     _fields_ = [("m", _I), ("batch", _I), ("classes", _I), ("mode", _I), ("adapt_gain", ct.c_float),
                 ("a_ad", ct.c_float), ("norm", ct.c_float), ("clip_lo", ct.c_float), ("clip_hi", ct.c_float),
                 ("scale", ct.c_float * 2), ("decay", ct.c_float * 2), ("v", _VP), ("adapt", _VP), ("g_slow", _VP),
@@ -110,7 +110,7 @@ class OpticSlowArgs(ct.Structure):
                 ("dr", _VP), ("a", _VP)]
 
 
-STRUCTS = (LifArgs, OpticArgs, SpmmArgs, AdjointArgs, PhotoArgs, TraceArgs, OpticSlowArgs)
+STRUCTS = (LifArgs, OpticArgs, SpmmArgs, AdjointArgs, PhotoArgs, TraceArgs, OpticUnitArgs)
 
 # Every symbol include/flyb200.h declares, with its ctypes signature.
 _P = ct.POINTER(ct.c_void_p)
@@ -133,7 +133,7 @@ SIGNATURES = {
     "flyb_group_means": [_VP, _VP, _VP, _VP, _I, _I, _VP],
     "flyb_trace_scene_floats": [_I, _I, _I],
     "flyb_trace": [ct.POINTER(TraceArgs), _VP],
-    "flyb_optic_slow_step": [ct.POINTER(OpticSlowArgs), _VP],
+    "flyb_optic_unit_step": [ct.POINTER(OpticUnitArgs), _VP],
     "flyb_occupancy": [_I, _I, ct.POINTER(_I), ct.POINTER(_I)],
     "flyb_selftest_wait": [_VP, _VP, ct.c_longlong, _VP],
     "flyb_gather_probe": [_VP, _I, _VP, _I, _VP, _I, _VP],

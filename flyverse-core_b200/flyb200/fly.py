@@ -30,7 +30,8 @@ from .weights import receptor_gain
 
 class FlyBrain:
     BRAIN_TENSORS = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
-    OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate", "g_slow", "g_slow_cls", "_slow_in_s")
+    OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate", "g_slow", "g_slow_cls", "_slow_in_s",
+                     "stream_adapt_state")
 
     def __init__(self, c, *, batch: int = 1, device=None, seed: int = 0, lif_params: LIFParams | None = None,
                  optic_params: OpticParams | None = None, cuda_graphs: bool = False, retina=None,

@@ -362,6 +362,130 @@ def lobe_matrices(c, retina, p: OpticParams, receptor=None, receptor_gain=None) 
                         np.asarray(retina.pr_column, np.int64), np.asarray(retina.pr_sens, np.float32).reshape(-1, 4))
 
 
+def _adopt_strongest(W: sp.csr_matrix, cells, known: np.ndarray, out: np.ndarray) -> None:
+    """For each i of `cells`, visited in order: out[i] = known[j] of the input j of row i of W with the
+    largest weight among the inputs whose known[j] >= 0 (the first of equal ones); a row with no such
+    input keeps out[i]. With out = known a later cell sees the result of an earlier one."""
+    for i in cells:
+        lo, hi = W.indptr[i], W.indptr[i + 1]
+        pre = W.indices[lo:hi]
+        good = known[pre] >= 0
+        if good.any():
+            out[i] = known[pre[good][np.argmax(W.data[lo:hi][good])]]
+
+
+def column_of_cells(c, retina, rate_idx) -> np.ndarray:
+    """Retinal column of every cell (-1: none), as the reference assigns it for spatial suppression
+    (interp/trace.py:945-971): a rate cell from its hex annotation; three passes then give an
+    unannotated rate cell the column of its strongest rate input, and a last pass does the same for
+    every cell still without one, spiking cells included."""
+    lookup = {(str(side), int(h[0]), int(h[1])): k for k, (side, h) in enumerate(zip(retina.col_side, retina.col_hex))}
+    ridx = np.asarray(rate_idx)
+    ann = c.neurons.iloc[ridx]
+
+    def annotated(side, h1, h2) -> int:
+        return -1 if (h1 != h1 or h2 != h2) else lookup.get((str(side), int(h1), int(h2)), -1)
+
+    col_rate = np.fromiter((annotated(*t) for t in zip(ann["hex_side"].fillna("").to_numpy(), ann["hex1"].to_numpy(),
+                                                        ann["hex2"].to_numpy())), np.int64, len(ridx))
+    absW = sp.csr_matrix(abs(c.W))
+    rate_in = absW[ridx][:, ridx].tocsr()
+    for _ in range(3):
+        _adopt_strongest(rate_in, np.flatnonzero(col_rate < 0), col_rate, col_rate)
+    col = np.full(c.n, -1, np.int64)
+    col[ridx] = col_rate
+    _adopt_strongest(absW[:, ridx].tocsr(), np.flatnonzero(col < 0), col_rate, col)
+    return col
+
+
+def _csr_select(C: sp.csr_matrix, keep: np.ndarray) -> sp.csr_matrix:
+    """The entries of C flagged by `keep`, in C's order (each row sums its survivors in C's order)."""
+    C = C.tocsr()
+    rows = np.repeat(np.arange(C.shape[0]), np.diff(C.indptr))
+    indptr = np.concatenate([[0], np.cumsum(np.bincount(rows[keep], minlength=C.shape[0]))])
+    return sp.csr_matrix((C.data[keep], C.indices[keep], indptr), shape=C.shape)
+
+
+def _first_rule(n: int, holds: list) -> np.ndarray:
+    """Per item, the index of the first rule that holds for it (`holds`: one boolean mask per rule), -1 for none."""
+    owner = np.full(n, -1, np.int64)
+    for k in range(len(holds) - 1, -1, -1):
+        owner[holds[k]] = k
+    return owner
+
+
+@dataclass
+class StreamHooks:
+    """The per-stream hooks (optic.py:50-70, 378-451): W_rr and W_sr split into the rest and one
+    block per (rectify entry, adapt entry) stream, each block multiplying its stream's signal
+    x = rectify(u - gain A), u = dr - G dr (G: the spatial suppression operator, or None)."""
+    rest_rr: sp.csr_matrix
+    rest_sr: sp.csr_matrix
+    streams: list          # [{"mode": None|"pos"|"neg"|"abs", "adapt_id": int, "W_rr": csr|None, "W_sr": csr|None}]
+    adapt_decay: list      # exp(-dt / tau) per stream_adapt entry
+    adapt_gain: list
+    G: sp.csr_matrix | None
+
+    def matched(self, which: str) -> int:
+        """Entries of W_rr ("rr") or W_sr ("sr") that belong to a stream."""
+        return sum(s[f"W_{which}"].nnz for s in self.streams if s[f"W_{which}"] is not None)
+
+
+def stream_hooks(c, retina, rate_idx, spk_idx, p: OpticParams, M_rr, M_sr) -> StreamHooks | None:
+    """The blocks of OpticParams.stream_rectify / stream_adapt / spatial_suppress, or None when all
+    three are off. An entry of W belongs to the first rectify and the first adapt rule whose pre and
+    post patterns full-match its cells' types; it is in a stream when either rule, or a suppression
+    rule on its presynaptic cell, matched. Streams are ordered by (rectify rule, adapt rule)."""
+    rect, adapt, supp = list(p.stream_rectify or []), list(p.stream_adapt or []), list(p.spatial_suppress or [])
+    if not (rect or adapt or supp):
+        return None
+    for k, rule in enumerate(rect):
+        if rule[2] not in ("pos", "neg", "abs"):
+            raise ValueError(f"stream_rectify[{k}]: mode must be pos, neg or abs, got {rule[2]!r}")
+    for k, rule in enumerate(adapt):
+        if not (np.isfinite(rule[2]) and rule[2] > 0):
+            raise ValueError(f"stream_adapt[{k}]: tau_ms must be positive and finite")
+    types = c.neurons.type.fillna("").to_numpy()
+    rate_t, spk_t = types[rate_idx], types[spk_idx]
+    n_rate = len(rate_idx)
+    supp_of = _first_rule(n_rate, [_full_mask(rule[0], rate_t) for rule in supp])
+
+    def blocks_of(M, post_t):
+        C = M.tocsr()
+        post, pre = np.repeat(np.arange(C.shape[0]), np.diff(C.indptr)), C.indices
+        rect_of = _first_rule(C.nnz, [_full_mask(r[0], rate_t)[pre] & _full_mask(r[1], post_t)[post] for r in rect])
+        adapt_of = _first_rule(C.nnz, [_full_mask(r[0], rate_t)[pre] & _full_mask(r[1], post_t)[post] for r in adapt])
+        hooked = (rect_of >= 0) | (adapt_of >= 0) | (supp_of[pre] >= 0)
+        keys = sorted(set(zip(rect_of[hooked].tolist(), adapt_of[hooked].tolist())))
+        return ({k: _csr_select(C, hooked & (rect_of == k[0]) & (adapt_of == k[1])) for k in keys},
+                _csr_select(C, ~hooked))
+
+    blk_rr, rest_rr = blocks_of(M_rr, rate_t)
+    blk_sr, rest_sr = blocks_of(M_sr, spk_t)
+    streams = [{"mode": rect[k[0]][2] if k[0] >= 0 else None, "adapt_id": k[1], "W_rr": blk_rr.get(k),
+                "W_sr": blk_sr.get(k)} for k in sorted(set(blk_rr) | set(blk_sr))]
+    G = None
+    if supp:
+        # G[j, j'] = k / n_j over the n_j cells j' of j's type whose column lies within the rule's
+        # radius of j's column (j itself included): u = dr - G dr is dr less k x the local type mean.
+        col = column_of_cells(c, retina, rate_idx)[rate_idx]
+        cd = np.asarray(retina.col_dir, dtype=np.float64)
+        cos_cc = np.clip(cd @ cd.T, -1.0, 1.0)
+        ii, jj, vv = [np.zeros(0, np.int64)], [np.zeros(0, np.int64)], [np.zeros(0)]
+        for k, (_, strength, radius) in enumerate(supp):
+            near_cc = cos_cc >= np.cos(np.radians(float(radius)))
+            cells = np.flatnonzero((supp_of == k) & (col >= 0))
+            for t in np.unique(rate_t[cells]):
+                ct = cells[rate_t[cells] == t]
+                near = near_cc[np.ix_(col[ct], col[ct])]
+                r_, c_ = np.nonzero(near)
+                ii.append(ct[r_]), jj.append(ct[c_]), vv.append(float(strength) / near.sum(1)[r_])
+        G = sp.csr_matrix((np.concatenate(vv).astype(np.float32), (np.concatenate(ii), np.concatenate(jj))),
+                          shape=(n_rate, n_rate))
+    return StreamHooks(rest_rr, rest_sr, streams, [float(np.exp(-p.dt_ms / float(r[2]))) for r in adapt],
+                       [float(r[3]) for r in adapt], G)
+
+
 def slow_blocks(c, rate_idx, spk_idx, p: OpticParams, receptor, receptor_gain, spec) -> tuple[list, float]:
     """The optic lobe's slow-tone blocks (optic.py:285-309): per active class of `spec` the
     spiking -> rate and rate -> rate matrices (count x slow sign x gain class, normalised by the same
@@ -399,8 +523,6 @@ class OpticLobe:
             raise ValueError("flyb200 has no Torch path: cuda_kernels=False is not available")
         if surrogate_grad:
             raise NotImplementedError("use flyb200.adjoint (hand-written optic adjoint) for gradients")
-        if p.stream_rectify or p.stream_adapt or p.spatial_suppress:
-            raise NotImplementedError("the per-stream hooks are Torch-only in the reference and not provided")
         if not np.isfinite(p.dt_ms) or p.dt_ms <= 0:
             raise ValueError("optic dt_ms must be positive and finite")
         self.device = torch.device(device) if device is not None else torch.device("cuda")
@@ -451,9 +573,12 @@ class OpticLobe:
         self.g_slow_cls = self._g_cls_s.transpose(1, 2)                   # (K, B, m) views
         self.g_slow = self._g_slow_s.t()
         self._slow_in_s = self._held_s.transpose(1, 2)
-        if self.slow is not None:
-            self._setup_slow(c, receptor, receptor_gain)
-        self.stream_adapt_state = torch.zeros(0, B, self.n_rate, device=dev)
+        K_a = len(p.stream_adapt or [])
+        self._stream_A_s = torch.zeros(K_a, self.n_rate, B, device=dev)     # [K_a][m][B] storage
+        self.stream_adapt_state = self._stream_A_s.transpose(1, 2)
+        self.hooks = stream_hooks(c, retina, self.rate_idx, self.spk_idx, p, self.M_rr, self.M_sr)
+        if self.slow is not None or self.hooks is not None:
+            self._setup_ext(c, receptor, receptor_gain)
         self.r0 = None
         self.last = {}
         self.diagnostics = False
@@ -509,9 +634,26 @@ class OpticLobe:
         return self._a_pr.t()
 
     # ------------------------------------------------------------------ the slow receptor tone
-    def _setup_slow(self, c, receptor, receptor_gain) -> None:
-        """Device copies of the slow-tone blocks (`slow_blocks`) and the products' buffers."""
+    def _setup_ext(self, c, receptor, receptor_gain) -> None:
+        """Device copies of the slow-tone blocks (`slow_blocks`), the hook blocks (`stream_hooks`)
+        and the buffers of the extended substep."""
         p, dev = self.p, self.device
+        m, B = self.n_rate, self.B
+        self._rec = torch.zeros(m, B, device=dev)
+        self._dr_ext = torch.zeros(m, B, device=dev)
+        self._slow_rs, self._slow_rr, self._rec_slow = [], [], []
+        h = self.hooks
+        if h is not None:
+            self._h_rest_rr, self._h_rest_sr = DeviceCSR(h.rest_rr, dev), DeviceCSR(h.rest_sr, dev)
+            self._h_rr = [DeviceCSR(s_["W_rr"], dev) if s_["W_rr"] is not None else None for s_ in h.streams]
+            self._h_sr = [DeviceCSR(s_["W_sr"], dev) if s_["W_sr"] is not None else None for s_ in h.streams]
+            self._h_G = DeviceCSR(h.G, dev) if h.G is not None else None
+            self._h_tmp = torch.zeros(m, B, device=dev)
+            self._h_out = torch.zeros(len(self.spk_idx), B, device=dev)
+        else:
+            self._W_rr_plain = DeviceCSR(self.M_rr, dev)
+        if self.slow is None:
+            return
         blocks, self._slow_norm = slow_blocks(c, self.rate_idx, self.spk_idx, p, receptor, receptor_gain, self.slow)
         self._slow_rs = [DeviceCSR(rs, dev) if rs is not None else None for rs, _, _, _ in blocks]
         self._slow_rr = [DeviceCSR(rr, dev) if rr is not None else None for _, rr, _, _ in blocks]
@@ -520,26 +662,55 @@ class OpticLobe:
         self.slow_entries = {cls: {"spiking_to_rate": 0 if rs is None else int(rs.nnz),
                                    "rate_to_rate": 0 if rr is None else int(rr.nnz)}
                              for cls, (rs, rr, _, _) in zip(self.slow_classes, blocks)}
-        self._W_rr_plain = DeviceCSR(self.M_rr, dev)
-        m, B = self.n_rate, self.B
-        self._rec = torch.zeros(m, B, device=dev)
         self._rec_slow = [torch.zeros(m, B, device=dev) if W is not None else None for W in self._slow_rr]
-        self._dr_slow = torch.zeros(m, B, device=dev)
 
-    def _slow_substeps(self, steps: int) -> None:
-        """The substeps with the slow tone (optic.py:526-551): dr (shifted by the tone in the
-        threshold mode), the recurrent and slow products, then the native unit update."""
+    def _stream_signals(self, dr: torch.Tensor, update: bool) -> list:
+        """x per hook stream from dr [m][B] (optic.py:453-472): u = dr - G dr, y = u - gain A,
+        x = rectify(y); with `update` each adaptation state then relaxes towards u."""
+        h = self.hooks
+        u = dr
+        if self._h_G is not None:
+            spmm(self._h_G, dr, self._h_tmp)
+            u = dr - self._h_tmp
+        xs = []
+        for s_ in h.streams:
+            a_id = s_["adapt_id"]
+            y = u if a_id < 0 else u - h.adapt_gain[a_id] * self._stream_A_s[a_id]
+            mode = s_["mode"]
+            xs.append(y if mode is None else (y.clamp(min=0.0) if mode == "pos" else
+                                              ((-y).clamp(min=0.0) if mode == "neg" else y.abs())))
+        if update:
+            for k, decay in enumerate(h.adapt_decay):
+                torch.add(u, (self._stream_A_s[k] - u) * decay, out=self._stream_A_s[k])
+        return xs
+
+    def _hook_output(self, dr: torch.Tensor) -> torch.Tensor:
+        """W_sr dr through the hook blocks (optic.py:485-495), [n_spk][B]."""
+        xs = self._stream_signals(dr, False)
+        spmm(self._h_rest_sr, dr, self._h_out)
+        for W, x in zip(self._h_sr, xs):
+            if W is not None:
+                spmm(W, x, self._h_out, accumulate=True)
+        return self._h_out
+
+    def _ext_substeps(self, steps: int) -> None:
+        """The substeps with the slow tone and / or the per-stream hooks (optic.py:526-551): dr
+        (shifted by the tone in the threshold mode), the recurrent product (with the hooks, the rest
+        block on dr plus each stream block on its signal), the slow products, then the native unit
+        update."""
         p = self.p
         core = self.core
         b = self.b_vec[:, None]
-        mode = _abi.SLOW_MODE_CODES[self.slow.mode]
-        args = _abi.OpticSlowArgs(m=self.n_rate, batch=self.B, classes=len(self.slow_classes), mode=mode,
-                                  adapt_gain=p.adapt_gain, a_ad=self._a_ad, norm=self._slow_norm,
-                                  clip_lo=self.slow.clip[0], clip_hi=self.slow.clip[1], v=core.v_s.data_ptr(),
-                                  adapt=core.adapt_s.data_ptr(), g_slow=self._g_slow_s.data_ptr(),
-                                  rec=self._rec.data_ptr(), pr=core.pr_in.data_ptr(), spk=core.spk_in.data_ptr(),
-                                  dr=self._dr_slow.data_ptr(), a=self.core.a.data_ptr())
-        for c in range(len(self.slow_classes)):
+        K = len(self.slow_classes)
+        args = _abi.OpticUnitArgs(m=self.n_rate, batch=self.B, classes=K,
+                                  mode=_abi.SLOW_MODE_CODES[self.slow.mode] if K else 0, adapt_gain=p.adapt_gain,
+                                  a_ad=self._a_ad, norm=self._slow_norm if K else 1.0,
+                                  clip_lo=self.slow.clip[0] if K else 0.0, clip_hi=self.slow.clip[1] if K else 0.0,
+                                  v=core.v_s.data_ptr(), adapt=core.adapt_s.data_ptr(),
+                                  g_slow=self._g_slow_s.data_ptr() if K else None, rec=self._rec.data_ptr(),
+                                  pr=core.pr_in.data_ptr(), spk=core.spk_in.data_ptr(), dr=self._dr_ext.data_ptr(),
+                                  a=self.core.a.data_ptr())
+        for c in range(K):
             args.scale[c], args.decay[c] = self._slow_scale[c], self._a_slow[c]
             args.g_cls[c] = self._g_cls_s[c].data_ptr()
             args.held[c] = self._held_s[c].data_ptr() if self._slow_rs[c] is not None else None
@@ -547,16 +718,24 @@ class OpticLobe:
         stream = torch.cuda.current_stream(self.device).cuda_stream
         for _ in range(steps):
             r = core.v_s + b
-            if self.slow.mode == "threshold":
+            if K and self.slow.mode == "threshold":
                 r = r + self._g_slow_s.clamp(max=0.9 * self._slow_norm)
-            torch.sub(r.clamp(0.0, 1.0), b, out=self._dr_slow)
-            spmm(self._W_rr_plain, self._dr_slow, self._rec, alpha=p.gain_rr)
+            torch.sub(r.clamp(0.0, 1.0), b, out=self._dr_ext)
+            if self.hooks is None:
+                spmm(self._W_rr_plain, self._dr_ext, self._rec, alpha=p.gain_rr)
+            else:
+                xs = self._stream_signals(self._dr_ext, True)
+                spmm(self._h_rest_rr, self._dr_ext, self._h_tmp)
+                for W, x in zip(self._h_rr, xs):        # acc + (W x), the reference's rounding
+                    if W is not None:
+                        spmm(W, x, self._h_tmp, accumulate=True)
+                torch.mul(self._h_tmp, p.gain_rr, out=self._rec)
             for W, y in zip(self._slow_rr, self._rec_slow):
                 if W is not None:
-                    spmm(W, self._dr_slow, y, alpha=p.gain_rr)
-            rc = _abi.lib().flyb_optic_slow_step(ct.byref(args), stream)
+                    spmm(W, self._dr_ext, y, alpha=p.gain_rr)
+            rc = _abi.lib().flyb_optic_unit_step(ct.byref(args), stream)
             if rc:
-                raise RuntimeError(f"flyb_optic_slow_step: error {rc}")
+                raise RuntimeError(f"flyb_optic_unit_step: error {rc}")
 
     # ------------------------------------------------------------------ rate dynamics
     def rates(self) -> torch.Tensor:
@@ -594,18 +773,22 @@ class OpticLobe:
             spmm(self.W_rp, self._fly_minor(a_pr), self.core.pr_in, alpha=p.gain_in)
             spmm(self.W_rs, rates_s, self.core.spk_in, x_index=self._spk_idx32, x_div=100.0, x_lo=0.0, x_hi=3.0,
                  alpha=p.gain_fb)
-            if self.slow is None:
+            if self.slow is None and self.hooks is None:
                 self.core.substeps(steps)
             else:                       # the spiking part of the slow input, held for the frame too
                 for W, h in zip(self._slow_rs, self._held_s):
                     if W is not None:
                         spmm(W, rates_s, h, x_index=self._spk_idx32, x_div=100.0, x_lo=0.0, x_hi=3.0, alpha=p.gain_fb)
-                self._slow_substeps(steps)
+                self._ext_substeps(steps)
         torch.sub(self.rates(), self.r0, out=self.delta_rate)
         drive = out if out is not None else self._drive
         drive.zero_()
-        spmm(self.W_sr, self._delta, drive, y_index=self._spk_idx32, alpha=p.gain_out_mv, y_lo=-p.drive_clip_mv,
-             y_hi=p.drive_clip_mv)
+        if self.hooks is None:
+            spmm(self.W_sr, self._delta, drive, y_index=self._spk_idx32, alpha=p.gain_out_mv, y_lo=-p.drive_clip_mv,
+                 y_hi=p.drive_clip_mv)
+        else:                           # the drive through the hook blocks (optic.py:602)
+            acc = self._hook_output(self._delta)
+            drive[self.spk_idx_t] = (p.gain_out_mv * acc).clamp(-p.drive_clip_mv, p.drive_clip_mv)
         self.last["dr"] = self.delta_rate
         return drive.t() if out is not None else drive.t().clone()
 
@@ -617,6 +800,7 @@ class OpticLobe:
             self._g_slow_s.zero_()
             self._g_cls_s.zero_()
             self._held_s.zero_()
+            self._stream_A_s.zero_()
             self._pending_ms = 0.0
         else:
             sel = torch.as_tensor(np.asarray(rows), device=self.device, dtype=torch.long)
@@ -626,4 +810,5 @@ class OpticLobe:
             self._g_slow_s[:, sel] = 0.0
             self._g_cls_s[:, :, sel] = 0.0
             self._held_s[:, :, sel] = 0.0
+            self._stream_A_s[:, :, sel] = 0.0
 

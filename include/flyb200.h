@@ -267,25 +267,29 @@ int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream);
  * a correctly rounded division, as torch's `rate / 100.0` at flyverse/optic.py:572)
  * and the result row i written at y[ymap(i)]. accumulate != 0 adds into y.
  * x and y use the stated fly-minor layout with `x_rows` / `y_rows` leading rows. */
-/* The optic lobe's slow receptor tone (receptor_model "full": the substep of flyverse/optic.py:
- * 526-551), the update after a substep's products: per class c the tone relaxes towards scale[c] x
- * (held[c] + rec_slow[c]) with factor decay[c]; g_slow = sum over classes; the unit input is
- * (rec + pr) + spk, with the tone added (FLYB_SLOW_ADDITIVE), multiplying it by
- * clamp(1 + g_slow / norm, clip_lo, clip_hi) (FLYB_SLOW_GAIN), or left as is (FLYB_SLOW_THRESHOLD,
- * where the caller shifts dr by min(g_slow, 0.9 norm) before the products); then v and adapt are
- * advanced as in the plain substep. rec = gain_rr W_rr dr, rec_slow[c] = gain_rr W_slow_rr[c] dr
- * (or null), held[c] = gain_fb W_slow_rs[c] s for the frame (or null). State [m][batch]. */
-typedef struct flyb_optic_slow_args {
+/* The optic substep's unit update after its products, for the configurations that are not the
+ * fused substep: the slow receptor tone (receptor_model "full") and the per-stream hooks (the
+ * substep of flyverse/optic.py:526-551). rec = gain_rr x the recurrent product (with the hooks, of
+ * the rest block on dr plus each stream block on its transformed signal). classes 0: the plain
+ * order, inp = ((rec + pr) - adapt_gain adapt) + spk. classes 1..FLYB_SLOW_MAX_CLASSES: per class c
+ * the tone relaxes towards scale[c] x (held[c] + rec_slow[c]) with factor decay[c]; g_slow = the
+ * sum over classes; inp = (rec + pr) + spk with the tone added (FLYB_SLOW_ADDITIVE), multiplying it
+ * by clamp(1 + g_slow / norm, clip_lo, clip_hi) (FLYB_SLOW_GAIN), or left as is
+ * (FLYB_SLOW_THRESHOLD, where the caller shifts dr by min(g_slow, 0.9 norm) before the products),
+ * minus adapt_gain adapt. Then v <- inp + (v - inp) a and adapt <- dr + (adapt - dr) a_ad.
+ * rec_slow[c] = gain_rr W_slow_rr[c] dr (or null), held[c] = gain_fb W_slow_rs[c] s for the frame
+ * (or null). State [m][batch]. */
+typedef struct flyb_optic_unit_args {
   int m;
   int batch;
-  int classes;           /* 1..FLYB_SLOW_MAX_CLASSES */
-  int mode;              /* FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN or FLYB_SLOW_THRESHOLD */
+  int classes;           /* 0..FLYB_SLOW_MAX_CLASSES */
+  int mode;              /* with classes > 0: FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN or FLYB_SLOW_THRESHOLD */
   float adapt_gain, a_ad, norm, clip_lo, clip_hi;
   float scale[FLYB_SLOW_MAX_CLASSES];
   float decay[FLYB_SLOW_MAX_CLASSES];
   float* v;
   float* adapt;
-  float* g_slow;
+  float* g_slow;         /* with classes > 0 */
   float* g_cls[FLYB_SLOW_MAX_CLASSES];
   const float* held[FLYB_SLOW_MAX_CLASSES];
   const float* rec_slow[FLYB_SLOW_MAX_CLASSES];
@@ -294,9 +298,9 @@ typedef struct flyb_optic_slow_args {
   const float* spk;
   const float* dr;
   const float* a;        /* [m] per-unit membrane factor */
-} flyb_optic_slow_args;
+} flyb_optic_unit_args;
 
-int flyb_optic_slow_step(const flyb_optic_slow_args* a, void* stream);
+int flyb_optic_unit_step(const flyb_optic_unit_args* a, void* stream);
 
 typedef struct flyb_spmm_args {
   int rows, cols, batch;

@@ -27,6 +27,9 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
   optic_hex_slow_{additive,gain,threshold}.npz  the hex patch's OpticLobe with the receptor model's
                   slow tone (classical class at scale 2) in each slow_mode, three frames from a displaced start, with the
                   receptor record it was built from.
+  optic_hex_hooks_{rectify,adapt,suppress,all}.npz  the hex patch's OpticLobe with the per-stream
+                  hooks of HOOK_CASES (rectified, adapting and spatially suppressed Mi1 streams),
+                  three frames.
   optic_synth.npz the reference's own `OpticLobe._substep` (optic.py:525-551), run on a
                   synthetic 3,000-unit lobe from flyb200.synthetic.optic_config3, 60 substeps.
   tracer.npz      flyverse.world / flyverse.batch_world (CPU): the reference tests' rays in
@@ -285,6 +288,39 @@ def optic_hex_slow(ref, mode: str) -> dict:
     return out
 
 
+HOOK_CASES = {
+    "rectify": dict(stream_rectify=[("Mi1", "T3", "pos"), ("Mi1", "Pm1", "abs")]),
+    "adapt": dict(stream_adapt=[("Mi1", "T3|Pm1", 15.0, 0.8)]),
+    "suppress": dict(spatial_suppress=[("Mi1", 0.6, 6.0)]),
+    "all": dict(stream_rectify=[("Mi1", "T3", "neg"), ("T3", "LC11", "abs")], stream_adapt=[("Mi1", ".*", 25.0, 0.5)],
+                spatial_suppress=[("Mi1", 0.4, 6.0)]),
+}
+
+
+def optic_hex_hooks(ref, case: str) -> dict:
+    """The hex patch's OpticLobe with the per-stream hooks of HOOK_CASES[case], batch 2, three frames."""
+    optic, rt = ref["optic"], ref["retina"]
+    th = ref["test_optic_hooks"]
+    c = th.hex_graph()
+    r = rt.build_retina(c)
+    B = 2
+    ol = optic.OpticLobe(c, r, optic.OpticParams(**HOOK_CASES[case]), device="cpu", batch=B)
+    ol.relax()
+    gen = torch.Generator().manual_seed(6)
+    out = {"case": np.array(case), "hook_info": np.array(repr(ol.hook_info))}
+    for f in range(3):
+        rad = torch.rand(B, r.n_columns, 4, generator=gen)
+        spk = torch.rand(B, c.n, generator=gen) * 80.0
+        drive = ol.step_frame(rad, spk, 10.0)
+        out[f"frame{f}_rad"], out[f"frame{f}_spk"] = rad.numpy(), spk.numpy()
+        for key in ("v", "adapt", "delta_rate", "stream_adapt_state"):
+            out[f"frame{f}_{key}"] = getattr(ol, key).numpy().copy()
+        out[f"frame{f}_drive"] = drive.numpy().copy()
+    print(f"optic_hex_hooks ({case}): {ol.hook_info.get('entries_rr_matched')} rr / "
+          f"{ol.hook_info.get('entries_sr_matched')} sr entries in streams, |v| max {float(ol.v.abs().max()):.4f}")
+    return out
+
+
 def optic_synth(ref) -> dict:
     """The reference's substep expressions on a synthetic lobe, called on the reference class."""
     optic = ref["optic"]
@@ -429,7 +465,8 @@ def main() -> None:
                 **{f"lif_19cell_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m)) for m in ("additive", "gain", "threshold")},
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
                 "tracer": lambda: tracer(ref),
-                **{f"optic_hex_slow_{m}": (lambda m=m: optic_hex_slow(ref, m)) for m in ("additive", "gain", "threshold")}}
+                **{f"optic_hex_slow_{m}": (lambda m=m: optic_hex_slow(ref, m)) for m in ("additive", "gain", "threshold")},
+                **{f"optic_hex_hooks_{k}": (lambda k=k: optic_hex_hooks(ref, k)) for k in HOOK_CASES}}
     for name, make in fixtures.items():
         if args.only in (None, name):
             np.savez_compressed(HERE / f"{name}.npz", **make())

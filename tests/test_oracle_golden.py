@@ -329,3 +329,77 @@ def test_optic_slow_tone_frames_match_reference(mode):
         np.testing.assert_allclose(st["delta"].T, z[f"frame{f}_delta_rate"], rtol=1e-5, atol=1e-6)
         np.testing.assert_allclose(drive, z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
     assert np.abs(st["g_slow"]).max() > 0.5
+
+
+HOOK_CASES = {      # the OpticParams of tests/golden/make_golden.py's optic_hex_hooks_{case} fixtures
+    "rectify": dict(stream_rectify=[("Mi1", "T3", "pos"), ("Mi1", "Pm1", "abs")]),
+    "adapt": dict(stream_adapt=[("Mi1", "T3|Pm1", 15.0, 0.8)]),
+    "suppress": dict(spatial_suppress=[("Mi1", 0.6, 6.0)]),
+    "all": dict(stream_rectify=[("Mi1", "T3", "neg"), ("T3", "LC11", "abs")], stream_adapt=[("Mi1", ".*", 25.0, 0.5)],
+                spatial_suppress=[("Mi1", 0.4, 6.0)]),
+}
+
+
+def optic_hooks_case(case):
+    """The hex patch with the per-stream hooks of HOOK_CASES[case]: fixture, lobe matrices, hook blocks."""
+    from flyb200.optic import stream_hooks
+    _, c, r = hex_lobe()
+    z = golden(f"optic_hex_hooks_{case}")
+    p = OpticParams(**HOOK_CASES[case])
+    L = lobe_matrices(c, r, p)
+    return z, c, r, p, L, stream_hooks(c, r, L.rate_idx, L.spk_idx, p, L.M_rr, L.M_sr)
+
+
+@pytest.mark.parametrize("case", list(HOOK_CASES))
+def test_optic_hook_blocks_match_reference(case):
+    """The stream split and the spatial operator: per stream the rule pair and its entry counts, the
+    rest blocks and G's entries, against the reference lobe's own hook record."""
+    z, c, r, p, L, h = optic_hooks_case(case)
+    info = eval(str(z["hook_info"]), {"__builtins__": {}}, {"True": True, "False": False, "None": None})
+    assert len(h.streams) == len(info["streams"])
+    rect, adapt = p.stream_rectify or [], p.stream_adapt or []
+    for s, ref in zip(h.streams, info["streams"]):
+        assert s["mode"] == (ref["rect"][2] if ref["rect"] else None)
+        assert (list(adapt[s["adapt_id"]]) if s["adapt_id"] >= 0 else None) == ref["adapt"]
+        for which, key in (("W_rr", "rate_to_rate"), ("W_sr", "rate_to_spiking")):
+            assert (s[which].nnz if s[which] is not None else None) == (ref[key]["entries"] if ref[key] else None)
+            if s[which] is not None:
+                assert abs(float(np.abs(s[which].data).sum()) - ref[key]["syn_eq"]) < 1e-5
+    assert (h.matched("rr"), h.rest_rr.nnz) == (info["entries_rr_matched"], info["entries_rr_rest"])
+    assert (h.matched("sr"), h.rest_sr.nnz) == (info["entries_sr_matched"], info["entries_sr_rest"])
+    if "spatial" in info:
+        assert h.G.nnz == info["spatial"]["G_nnz"]
+        assert [(e["pre"], e["k"], e["radius_deg"]) for e in info["spatial"]["entries"]] == \
+            [tuple(x) for x in p.spatial_suppress]
+    else:
+        assert h.G is None
+    assert {tuple(x["rect"]) for x in info["streams"] if x["rect"]} <= {tuple(x) for x in rect}
+
+
+@pytest.mark.parametrize("case", list(HOOK_CASES))
+def test_optic_hook_frames_match_reference(case):
+    """The per-stream hooks (optic.py:453-495, 526-551): three frames of the hex patch, every state
+    within 1e-5 of the reference's OpticLobe, the drive within 1e-4 mV."""
+    z, c, r, p, L, h = optic_hooks_case(case)
+    B, m = 2, len(L.rate_idx)
+    st = {"v": np.zeros((m, B), np.float32), "adapt": np.zeros((m, B), np.float32),
+          "I_lp": np.zeros((B, r.n_columns * 5), np.float32), "I_mean": np.zeros((B, r.n_columns * 5), np.float32),
+          "fresh": np.ones(B, bool), "pending": 0.0, "A": np.zeros((len(p.stream_adapt or []), m, B), np.float32)}
+    for f in range(3):
+        drive = oframe.frame(L, st, z[f"frame{f}_rad"], z[f"frame{f}_spk"], 10.0, p, hooks=h)
+        np.testing.assert_allclose(st["v"].T, z[f"frame{f}_v"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["adapt"].T, z[f"frame{f}_adapt"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["A"].transpose(0, 2, 1), z[f"frame{f}_stream_adapt_state"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(st["delta"].T, z[f"frame{f}_delta_rate"], rtol=1e-5, atol=1e-6)
+        np.testing.assert_allclose(drive, z[f"frame{f}_drive"], rtol=1e-5, atol=1e-4)
+    assert np.abs(z["frame2_drive"]).max() > 0
+
+
+def test_optic_hooks_reject_bad_rules():
+    from flyb200.optic import stream_hooks
+    _, c, r = hex_lobe()
+    for kw in (dict(stream_rectify=[("Mi1", "T3", "half")]), dict(stream_adapt=[("Mi1", "T3", 0.0, 1.0)])):
+        p = OpticParams(**kw)
+        L = lobe_matrices(c, r, p)
+        with pytest.raises(ValueError):
+            stream_hooks(c, r, L.rate_idx, L.spk_idx, p, L.M_rr, L.M_sr)
