@@ -49,6 +49,7 @@ struct LifK {
   const unsigned char* __restrict__ clock_k;  // per-neuron update period, or null (every step)
   const float* __restrict__ clock_coef;       // [max period + 1][FLYB_CLOCK_NCOEF]
   long long* clock_acc;                       // [n][batch] input pending until the next update
+  long long* slow_clock_acc[FLYB_SLOW_MAX_CLASSES];  // the same per slow class (clocks + tone)
   int slow_classes, slow_mode;                // slow receptor tone (0 classes: none)
   float slow_norm, slow_clip_lo, slow_clip_hi, slow_th_max;
   float slow_decay[FLYB_SLOW_MAX_CLASSES];
@@ -600,7 +601,18 @@ __global__ void lif_advance_kernel(LifK k) { advance_clock(k, read_clock(k)); }
 // The slow tone (brain.py:551-585, 829-845): per class, the tone decays and takes its delayed
 // input from its own exact ring; the summed tone joins the membrane target, scales the fast input
 // or lowers the threshold. Its spikes go out on each class's synapse list after the fast ones.
+// Under clocks a class decays by its column of the phase row and its input to a period-k neuron
+// waits for the update like the fast input (brain.py:905-917).
 // One item per thread, then the block-wide delivery of the register path.
+// Input reaching a neuron that updates every `period` > 1 steps: summed exactly in *acc while the
+// neuron holds, returned whole (with this step's) on its update step.
+__device__ __forceinline__ long long hold_until_update(long long* acc, long long due, bool on) {
+  const long long held = *acc, sum = held + due;
+  const long long keep = on ? 0 : sum;
+  if (keep != held) *acc = keep;
+  return on ? sum : 0;
+}
+
 template <int BLOCK, bool FIXED>
 __global__ void __launch_bounds__(BLOCK) lif_ext_kernel(LifK k, int s) {
   using RingT = typename std::conditional<FIXED, long long, int>::type;
@@ -629,17 +641,15 @@ __global__ void __launch_bounds__(BLOCK) lif_ext_kernel(LifK k, int s) {
       // this step's coefficients: the neuron's phase row under clocks, else the step's own
       float c_m = P.a_m, c_s = P.a_s, c_dt = P.dt, c_ad = P.a_ad, c_std = P.a_std, c_r = P.a_r, c_rg = P.rg;
       float c_u = 1.0f, c_pois = 1.0f;
+      const float* cf = nullptr;   // the phase row under clocks
+      int period = 1;
+      bool on = true;
       if (k.clock_k) {
         const long long step = clk.step0 + s;
-        const int period = k.clock_k[i];
-        const bool on = period == 1 || step % period == 0;
-        if (period > 1) {
-          const long long held = k.clock_acc[t], sum = held + due;
-          due = on ? sum : 0;
-          const long long keep = on ? 0 : sum;
-          if (keep != held) k.clock_acc[t] = keep;
-        }
-        const float* cf = k.clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
+        period = k.clock_k[i];
+        on = period == 1 || step % period == 0;
+        if (period > 1) due = hold_until_update(k.clock_acc + t, due, on);
+        cf = k.clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
         c_m = cf[FLYB_CLOCK_A_M], c_s = cf[FLYB_CLOCK_A_S], c_dt = cf[FLYB_CLOCK_DT], c_ad = cf[FLYB_CLOCK_A_AD];
         c_std = cf[FLYB_CLOCK_A_STD], c_r = cf[FLYB_CLOCK_A_R], c_rg = cf[FLYB_CLOCK_RATE_GAIN];
         c_u = cf[FLYB_CLOCK_U], c_pois = cf[FLYB_CLOCK_POIS];
@@ -655,9 +665,10 @@ __global__ void __launch_bounds__(BLOCK) lif_ext_kernel(LifK k, int s) {
       float tone = 0.0f;
       for (int c = 0; c < k.slow_classes; ++c) {
         long long* sp = k.slow_ring[c] + (size_t)rs * slot + t;
-        const long long sdue = *sp;
+        long long sdue = *sp;
         if (sdue) *sp = 0;
-        float sg = k.slow_g[c][t] * k.slow_decay[c];
+        if (period > 1) sdue = hold_until_update(k.slow_clock_acc[c] + t, sdue, on);
+        float sg = k.slow_g[c][t] * (cf ? cf[FLYB_CLOCK_A_SLOW0 + c] : k.slow_decay[c]);
         if (sdue) sg = sg + __double2float_rn((double)sdue * (1.0 / 4294967296.0));
         k.slow_g[c][t] = sg;
         tone = tone + sg;
@@ -1265,14 +1276,16 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.slow_th_max = a->slow_th_max; k.g_slow = a->g_slow;
   if (a->slow_classes < 0 || a->slow_classes > FLYB_SLOW_MAX_CLASSES) return FLYB_EINVAL;
   if (a->slow_classes) {
-    if (a->clock_k || (a->flags & FLYB_LIF_DEFER_DELIVERY) || !a->g_slow || a->slow_mode < FLYB_SLOW_ADDITIVE ||
+    if ((a->flags & FLYB_LIF_DEFER_DELIVERY) || !a->g_slow || a->slow_mode < FLYB_SLOW_ADDITIVE ||
         a->slow_mode > FLYB_SLOW_THRESHOLD || !(a->slow_norm != 0.0f))
       return FLYB_EINVAL;
   }
   for (int c = 0; c < FLYB_SLOW_MAX_CLASSES; ++c) {
     const bool used = c < a->slow_classes;
-    if (used && (!a->slow_out_ptr[c] || !a->slow_out_edge[c] || !a->slow_ring[c] || !a->slow_g[c]))
+    if (used && (!a->slow_out_ptr[c] || !a->slow_out_edge[c] || !a->slow_ring[c] || !a->slow_g[c] ||
+                 (a->clock_k && !a->slow_clock_acc[c])))
       return FLYB_EINVAL;
+    k.slow_clock_acc[c] = used && a->clock_k ? (long long*)a->slow_clock_acc[c] : nullptr;
     k.slow_decay[c] = used ? a->slow_decay[c] : 0.0f;
     k.slow_out_ptr[c] = used ? a->slow_out_ptr[c] : nullptr;
     k.slow_out_edge[c] = used ? (const int2*)a->slow_out_edge[c] : nullptr;

@@ -31,7 +31,7 @@ OPTIC_HISTORY, OPTIC_DR_VALID = 1, 2
 SLOW_MAX_CLASSES = 2
 SLOW_MODE_CODES = {"additive": 0, "gain": 1, "threshold": 2}
 (CLOCK_A_M, CLOCK_A_S, CLOCK_DT, CLOCK_A_AD, CLOCK_A_STD, CLOCK_A_R, CLOCK_RATE_GAIN, CLOCK_U, CLOCK_POIS,
- CLOCK_NCOEF) = range(10)
+ CLOCK_A_SLOW0, CLOCK_A_SLOW1, CLOCK_NCOEF) = range(12)
 
 _VP = ct.c_void_p
 _I = ct.c_int
@@ -50,6 +50,7 @@ class LifArgs(ct.Structure):
                 ("fly_steps", _VP), ("clock", _VP), ("raster", _VP), ("events", _VP), ("status", _VP),
                 ("sync", _VP), ("spike_list", _VP), ("spike_n", _VP), ("spike_cap", ct.c_longlong),
                 ("adapt_jump", _VP), ("clock_k", _VP), ("clock_coef", _VP), ("clock_acc", _VP),
+                ("slow_clock_acc", _VP * 2),
                 ("slow_classes", _I), ("slow_mode", _I), ("slow_norm", ct.c_float), ("slow_clip_lo", ct.c_float),
                 ("slow_clip_hi", ct.c_float), ("slow_th_max", ct.c_float), ("slow_decay", ct.c_float * 2),
                 ("slow_out_ptr", _VP * 2), ("slow_out_edge", _VP * 2), ("slow_ring", _VP * 2), ("slow_g", _VP * 2),

@@ -96,11 +96,12 @@ def lif_coefficients(p: LIFParams, std_on: bool, adapt_on: bool | None = None) -
     return P
 
 
-def clock_coefficients(p: LIFParams, std_on: bool, max_period: int) -> np.ndarray:
+def clock_coefficients(p: LIFParams, std_on: bool, max_period: int, slow_tau=()) -> np.ndarray:
     """[max_period + 1][CLOCK_NCOEF] float32 phase coefficients of per-neuron clocks (brain.py:
     627-637): row k those of an update of a period-k neuron (a step of k * dt), row 0 those of a
-    step without update (no decay, no refractory time, no spike, no Poisson). Evaluated with the
-    reference's float32 tensor expressions on the CPU, so they carry its bits."""
+    step without update (no decay, no refractory time, no spike, no Poisson). `slow_tau`: the time
+    constants of the slow tone's classes, in class order (their decays fill CLOCK_A_SLOW0 on).
+    Evaluated with the reference's float32 tensor expressions on the CPU, so they carry its bits."""
     kt = torch.arange(max_period + 1, dtype=torch.float32)
     kt[0] = 1.0
     u = torch.ones(max_period + 1)
@@ -118,6 +119,11 @@ def clock_coefficients(p: LIFParams, std_on: bool, max_period: int) -> np.ndarra
     out[:, _abi.CLOCK_RATE_GAIN] = u * (1 - torch.exp(-p.dt * kt / p.rate_tau)) * 1000.0 / (kt * p.dt)
     out[:, _abi.CLOCK_U] = u
     out[:, _abi.CLOCK_POIS] = u * kt
+    if len(slow_tau) > _abi.SLOW_MAX_CLASSES:
+        raise ValueError("more slow classes than the native step holds")
+    out[:, _abi.CLOCK_A_SLOW0:_abi.CLOCK_A_SLOW0 + _abi.SLOW_MAX_CLASSES] = 1.0
+    for c, tau in enumerate(slow_tau):
+        out[:, _abi.CLOCK_A_SLOW0 + c] = coef(tau)
     return out.numpy()
 
 
@@ -326,6 +332,9 @@ class Brain:
         if self._kvec is not None:
             a.clock_k, a.clock_coef = self._clock_k.data_ptr(), self._clock_coef.data_ptr()
             a.clock_acc = self.clock_acc.data_ptr()
+            if self.slow is not None:
+                for c in range(len(self.slow_classes)):
+                    a.slow_clock_acc[c] = self.slow_clock_acc[c].data_ptr()
         if self.slow is not None:
             spec = self.slow
             a.slow_classes, a.slow_mode = len(self.slow_classes), _abi.SLOW_MODE_CODES[spec.mode]
@@ -352,7 +361,9 @@ class Brain:
         reference's Brain.set_clocks (brain.py:618-640): on other steps a neuron holds its state and
         the input that reaches it waits for its next update. The native step then runs one launch
         per step through the clocked kernel. Input already held for a slow neuron stays in the
-        units of the ring it arrived on (it is dropped if set_weights changes the ring mode)."""
+        units of the ring it arrived on (it is dropped if set_weights changes the ring mode). With
+        the slow receptor tone each class decays by its phase coefficient and its input waits
+        for the update too (brain.py:905-917)."""
         k = np.asarray(multiplier, dtype=np.int64)
         if k.shape != (self.n,) or (k < 1).any():
             raise ValueError("multiplier must be an (N,) array of positive integers")
@@ -361,14 +372,13 @@ class Brain:
             raise ValueError("the slowest clock must not exceed the synaptic delay")
         if int(k.max()) > 255:
             raise ValueError("clock periods above 255 steps are not supported")
-        if self.slow is not None:
-            raise NotImplementedError("per-neuron clocks together with the slow receptor tone are not in the "
-                                      "native step")
         self._kvec = k
         self.K = int(np.lcm.reduce(np.unique(k)))
         self._clock_k = torch.from_numpy(k.astype(np.uint8)).to(self.device)
-        self._clock_coef = torch.from_numpy(clock_coefficients(p, self._std_on, int(k.max()))).to(self.device)
+        slow_tau = [self.slow.tau[name] for name in self.slow_classes] if self.slow is not None else []
+        self._clock_coef = torch.from_numpy(clock_coefficients(p, self._std_on, int(k.max()), slow_tau)).to(self.device)
         self.clock_acc = torch.zeros(self.n, self.B, dtype=torch.int64, device=self.device)
+        self.slow_clock_acc = torch.zeros(len(slow_tau), self.n, self.B, dtype=torch.int64, device=self.device)
         self._weights_version += 1
         self._make_args()
 
@@ -506,6 +516,7 @@ class Brain:
         self.ring[:, :, sel] = 0
         if self._kvec is not None:
             self.clock_acc[:, sel] = 0
+            self.slow_clock_acc[:, :, sel] = 0
         if rows is None:
             self._hist.zero_()
         else:
@@ -570,7 +581,8 @@ class Brain:
         out.update(ring=self.ring.cpu().clone(), hist=self._hist.cpu().clone(), clock=self._clock.cpu().clone(),
                    scalars=dict(t=self.t, step_count=self.step_count, buf_pos=self.buf_pos, _poisson_on=self._poisson_on))
         if self._kvec is not None:
-            out.update(clock_period=self._kvec.copy(), clock_acc=self.clock_acc.cpu().clone())
+            out.update(clock_period=self._kvec.copy(), clock_acc=self.clock_acc.cpu().clone(),
+                       slow_clock_acc=self.slow_clock_acc.cpu().clone())
         if self.slow is not None:
             out.update(g_slow=self._g_slow.cpu().clone(), g_slow_cls=self._slow_g.cpu().clone(),
                        slow_rings=[r.cpu().clone() for r in self._slow_rings])
@@ -588,6 +600,8 @@ class Brain:
             if self._kvec is None or not np.array_equal(state["clock_period"], self._kvec):
                 self.set_clocks(state["clock_period"])
             self.clock_acc.copy_(state["clock_acc"].to(self.device))
+            if "slow_clock_acc" in state:
+                self.slow_clock_acc.copy_(state["slow_clock_acc"].to(self.device))
         elif self._kvec is not None:
             raise ValueError("checkpoint has no per-neuron clocks but this brain runs them")
         if (self.slow is not None) != ("g_slow_cls" in state):

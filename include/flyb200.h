@@ -167,13 +167,17 @@ typedef struct flyb_lif_args {
                             step on which a neuron does not update                         */
   void* clock_acc;       /* [n][batch] int64 (device): pending input of neurons with period
                             > 1, in ring units (counts, or Q32.32 mV)                       */
+  void* slow_clock_acc[FLYB_SLOW_MAX_CLASSES]; /* clocks with the slow tone: [n][batch] int64
+                            Q32.32 per class (device), slow input pending at period > 1       */
   /* Slow receptor tone (receptor_model "full": brain.py:551-585, the step :829-845): per class c
    * < slow_classes a tone slow_g[c] (mV) decays by slow_decay[c] per step and takes the delayed
    * input of its own synapse list (pre-major like out_ptr / out_edge, {post, float bits of w}),
    * summed exactly on its own Q32.32 ring; g_slow = sum over classes acts by slow_mode: added to
    * the membrane target, scaling the fast input by clamp(1 + g_slow / slow_norm, slow_clip_lo,
    * slow_clip_hi), or lowering the threshold by min(g_slow, slow_th_max). Runs one launch per step
-   * like the clocks (which it cannot be combined with). slow_classes 0: no tone. */
+   * like the clocks. With clocks (the reference's clocked step) a class decays by column
+   * FLYB_CLOCK_A_SLOW0 + c of the neuron's phase row instead of slow_decay[c], and its input to a
+   * neuron with period > 1 waits in slow_clock_acc[c] for the update. slow_classes 0: no tone. */
   int slow_classes;      /* 0..FLYB_SLOW_MAX_CLASSES                                      */
   int slow_mode;         /* FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN or FLYB_SLOW_THRESHOLD      */
   float slow_norm, slow_clip_lo, slow_clip_hi, slow_th_max;
@@ -191,7 +195,8 @@ enum { FLYB_SLOW_ADDITIVE, FLYB_SLOW_GAIN, FLYB_SLOW_THRESHOLD };
 /* Columns of flyb_lif_args.clock_coef */
 enum {
   FLYB_CLOCK_A_M, FLYB_CLOCK_A_S, FLYB_CLOCK_DT, FLYB_CLOCK_A_AD, FLYB_CLOCK_A_STD, FLYB_CLOCK_A_R,
-  FLYB_CLOCK_RATE_GAIN, FLYB_CLOCK_U, FLYB_CLOCK_POIS, FLYB_CLOCK_NCOEF
+  FLYB_CLOCK_RATE_GAIN, FLYB_CLOCK_U, FLYB_CLOCK_POIS, FLYB_CLOCK_A_SLOW0, FLYB_CLOCK_A_SLOW1,
+  FLYB_CLOCK_NCOEF
 };
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);

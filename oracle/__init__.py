@@ -117,7 +117,8 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
     reduced by the steps taken, as the host layer does after a launch. `adapt_jump` (n,): per-neuron
     adaptation jumps (the reference's adapt_by_type, brain.py:497-506). `clocks` = (period (n,),
     coefficient table [max period + 1][CLOCK_NCOEF]): per-neuron clocks (brain.py:899-957); the
-    pending input of slow neurons lives in `state.clock_acc`. `slow` = {"mode", "norm", "clip",
+    pending input of slow neurons lives in `state.clock_acc` (and, with the slow tone, per class in
+    `state.slow_clock_acc`). `slow` = {"mode", "norm", "clip",
     "th_max", "classes": [(out_ptr, out_edge, decay), ...]}: the slow receptor tone (brain.py:551-585);
     its rings, per-class tones and summed tone live in `state.slow_ring`, `state.slow_g`,
     `state.g_slow`."""
@@ -164,6 +165,11 @@ def lif_run(state: LifState, out_ptr, out_edge, params, *, n_delay, flags, nstep
             a.slow_ring[c], a.slow_g[c] = state.slow_ring[c].ctypes.data, state.slow_g[c].ctypes.data
             a.slow_decay[c] = decay
         a.g_slow = _p(state.g_slow)
+        if clocks is not None:           # the slow input pending at clocked neurons, per class
+            if getattr(state, "slow_clock_acc", None) is None:
+                state.slow_clock_acc = np.zeros((K, n, B), np.int64)
+            for c in range(K):
+                a.slow_clock_acc[c] = state.slow_clock_acc[c].ctypes.data
     rc = lib().oracle_lif_run(ct.byref(a), threads)
     if rc:
         raise ValueError(f"oracle_lif_run: status {rc}")

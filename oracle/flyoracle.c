@@ -93,10 +93,11 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
     float c_m = a_m, c_s = a_s, c_dt = dt, c_ad = a_ad, c_std = a_std, c_r = a_r, c_rg = rg, c_u = 1.0f,
           c_pois = 1.0f;
     int period = 1, on = 1;
+    const float* cf = NULL;
     if (a->clock_k) {
       period = a->clock_k[i];
       on = step % period == 0;
-      const float* cf = a->clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
+      cf = a->clock_coef + FLYB_CLOCK_NCOEF * (on ? period : 0);
       c_m = cf[FLYB_CLOCK_A_M]; c_s = cf[FLYB_CLOCK_A_S]; c_dt = cf[FLYB_CLOCK_DT]; c_ad = cf[FLYB_CLOCK_A_AD];
       c_std = cf[FLYB_CLOCK_A_STD]; c_r = cf[FLYB_CLOCK_A_R]; c_rg = cf[FLYB_CLOCK_RATE_GAIN]; c_u = cf[FLYB_CLOCK_U];
       c_pois = cf[FLYB_CLOCK_POIS];
@@ -123,12 +124,19 @@ static uint64_t lif_fly_step(const flyb_lif_args* a, int b, int k, const float* 
       g = g + inc;
     }
     a->g[t] = g;
-    /* the slow tone (brain.py:551-557, 834-837): per class decay plus its delayed input */
+    /* the slow tone (brain.py:551-557, 834-837): per class decay plus its delayed input; under
+     * clocks the phase's decay and the per-period accumulator of the class (brain.py:905-917) */
     float tone = 0.0f;
     for (int c = 0; c < a->slow_classes; ++c) {
       int64_t* sring = (int64_t*)a->slow_ring[c] + (size_t)rs * n * B;
       int64_t sdue = sring[t]; sring[t] = 0;
-      float sg = a->slow_g[c][t] * a->slow_decay[c];
+      if (period > 1) {
+        int64_t* acc = (int64_t*)a->slow_clock_acc[c] + t;
+        *acc += sdue;
+        sdue = on ? *acc : 0;
+        if (on) *acc = 0;
+      }
+      float sg = a->slow_g[c][t] * (cf ? cf[FLYB_CLOCK_A_SLOW0 + c] : a->slow_decay[c]);
       if (sdue != 0) { float inc = float_of_fixed(sdue); sg = sg + inc; }
       a->slow_g[c][t] = sg;
       tone = tone + sg;

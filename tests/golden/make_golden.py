@@ -20,6 +20,8 @@ regenerate; the fixtures store the reference's outputs and hashes of the inputs.
   lif_19cell_slow_{additive,gain,threshold}.npz  the 19-cell run with the slow receptor tone
                   (receptor_model="full", classical class at scale 0.5) in each slow_mode, with the
                   per-entry receptor arrays (connectome.receptor_signs) it was built from.
+  lif_19cell_clocks_slow_{additive,gain,threshold}.npz  the same slow-tone runs with the clocks of
+                  lif_19cell_clocks (the reference's clocked step, sparse-matmul path).
   lif_c1_clocks.npz  config 1 at 6.5 mV drive with per-neuron clocks of 1, 2 and 4 steps on the
                   reference's sparse-matmul path: rasters and final state.
   optic_hex.npz   flyverse.optic.OpticLobe (CPU) with default parameters on the 7-column hex patch
@@ -100,21 +102,26 @@ def lif_c1(ref) -> dict:
     return out
 
 
-def lif_19cell_slow(ref, mode: str) -> dict:
+def lif_19cell_slow(ref, mode: str, clocks: bool = False) -> dict:
     """The 19-cell run with the receptor model's slow tone (receptor_model="full", classical class
     at scale 0.5) in one slow_mode: the per-entry receptor arrays the model read, the shaped fast
-    and slow matrices, rasters, final state and tone."""
+    and slow matrices, rasters, final state and tone. With `clocks`, periods 1, 2, 3 steps by
+    neuron on the reference's sparse-matmul path (its clocked step carries the tone too)."""
     brain, cn = ref["brain"], ref["connectome"]
     tb = ref["test_bit_identity"]
     c = tb.graph()
     B, steps, seed = 2, 400, 7
-    p = brain.LIFParams(receptor_model="full", event_driven=True, slow_gain_by_class={"metabotropic_classical": 0.5},
-                        slow_mode=mode)
+    p = brain.LIFParams(receptor_model="full", event_driven=not clocks,
+                        slow_gain_by_class={"metabotropic_classical": 0.5}, slow_mode=mode)
     rec = cn.receptor_signs(c, net_rule=p.receptor_net_rule, with_counts=True)
     b = brain.Brain(c, p, device="cpu", seed=seed, batch=B, receptor=rec)
     frozen = np.flatnonzero((c.neurons.superclass == "ol_intrinsic").to_numpy())
     b.freeze(frozen)
     b.prune(frozen)
+    period = None
+    if clocks:
+        period = 1 + np.arange(c.n) % 3
+        b.set_clocks(period)
     b.record_activity = True
     orn, jo, dnp = c.select(type="ORN_DM1"), c.select(type="~^JO-"), c.select(type="DNp01")
     b.set_poisson(orn, torch.tensor([[120.0], [40.0]]))
@@ -140,7 +147,9 @@ def lif_19cell_slow(ref, mode: str) -> dict:
         out[f"slow_{k}_data"], out[f"slow_{k}_indices"], out[f"slow_{k}_indptr"] = S.data, S.indices, S.indptr
     for key in ("v", "g", "refrac", "adapt", "res", "rate", "spike_counts", "spikes", "g_slow"):
         out[f"final_{key}"] = getattr(b, key).numpy().copy()
-    print(f"lif_19cell_slow ({mode}): {int(ras.sum())} spikes, slow entries "
+    if period is not None:
+        out["clock_period"] = period
+    print(f"lif_19cell_slow ({mode}, clocks={clocks}): {int(ras.sum())} spikes, slow entries "
           f"{[(k, S.nnz) for k, S in b._W_slow_cpu.items()]}, max tone {float(b.g_slow.abs().max()):.3f} mV")
     return out
 
@@ -463,6 +472,8 @@ def main() -> None:
                 "lif_19cell_clocks": lambda: lif_19cell(ref, clocks=True),
                 "lif_c1_clocks": lambda: lif_c1_clocks(ref),
                 **{f"lif_19cell_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m)) for m in ("additive", "gain", "threshold")},
+                **{f"lif_19cell_clocks_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m, clocks=True))
+                   for m in ("additive", "gain", "threshold")},
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
                 "tracer": lambda: tracer(ref),
                 **{f"optic_hex_slow_{m}": (lambda m=m: optic_hex_slow(ref, m)) for m in ("additive", "gain", "threshold")},

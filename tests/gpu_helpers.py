@@ -73,6 +73,13 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
             a.slow_ring[c], a.slow_g[c] = srings[c].data_ptr(), sg[c].data_ptr()
             a.slow_decay[c] = decay
         a.g_slow = gs.data_ptr()
+        sacc = None
+        if clocks is not None:
+            if getattr(state, "slow_clock_acc", None) is None:
+                state.slow_clock_acc = np.zeros((K, n, B), np.int64)
+            sacc = torch.from_numpy(state.slow_clock_acc).to(dev)
+            for c in range(K):
+                a.slow_clock_acc[c] = sacc[c].data_ptr()
     if defer:
         a.flags |= _abi.LIF_DEFER_DELIVERY
         cap = int(_abi.lib().flyb_lif_spike_capacity(ct.byref(a)))
@@ -96,6 +103,8 @@ def native_lif_run(state, out_ptr, out_edge, params, *, n_delay, flags, nsteps, 
         state.slow_ring[...] = srings.cpu().numpy()
         state.slow_g[...] = sg.cpu().numpy()
         state.g_slow[...] = gs.cpu().numpy()
+        if sacc is not None:
+            state.slow_clock_acc[...] = sacc.cpu().numpy()
     state.ring_pos = (state.ring_pos + nsteps) % state.ring_slots
     state.step += nsteps
     if fly_steps is not None:

@@ -58,12 +58,42 @@ def test_slow_tone_kernel_equals_oracle(mode, kind):
 
 
 @pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
-def test_brain_slow_tone_drop_in_equals_reference_golden(mode):
-    z, c, p, rec, W_ref, S_ref = slow_case(mode)
+@pytest.mark.parametrize("kind", ["count", "fixed-std"])
+def test_clocked_slow_tone_kernel_equals_oracle(mode, kind):
+    """Clocks and the slow tone together: per-class phase decays and per-class pending input, bit
+    for bit against the oracle over two calls (the held slow input carries over)."""
+    from flyb200.brain import clock_coefficients
+    case = case_random(batch=8, n=3000, edges=60_000, steps=100, fixed=kind == "fixed-std", std=kind == "fixed-std")
+    slow = random_slow(3000, mode)
+    p = LIFParams(adapt_jump=1.5, dt=0.1)
+    period = np.random.default_rng(3).choice([1, 2, 3, 6], 3000).astype(np.int64)
+    clocks = (period, clock_coefficients(p, kind == "fixed-std", 6, (100.0, 200.0)))
+    s_ref, s_gpu = case["state"].copy(), case["state"].copy()
+    for chunk in (41, 59):
+        kw = dict(n_delay=case["n_delay"], flags=case["flags"], nsteps=chunk, seed=case["seed"], raster=True,
+                  slow=slow, clocks=clocks)
+        r_ref, ev_ref = oracle.lif_run(s_ref, case["ptr"], case["edges"], case["P"], **kw)
+        r_gpu, ev_gpu = native_lif_run(s_gpu, case["ptr"], case["edges"], case["P"], launch=_abi.LAUNCH_STEP, **kw)
+        np.testing.assert_array_equal(r_gpu, r_ref)
+        for k in LIF_ARRAYS:
+            np.testing.assert_array_equal(getattr(s_gpu, k), getattr(s_ref, k), err_msg=k)
+        for k in ("ring", "clock_acc", "slow_ring", "slow_g", "g_slow", "slow_clock_acc"):
+            np.testing.assert_array_equal(getattr(s_gpu, k), getattr(s_ref, k), err_msg=k)
+        assert ev_gpu == ev_ref
+    assert np.abs(s_ref.slow_clock_acc).sum() > 0        # slow input held between updates
+    assert np.abs(s_ref.g_slow).max() > 0.1
+
+
+@pytest.mark.parametrize("clocks", [False, True], ids=["plain", "clocked"])
+@pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
+def test_brain_slow_tone_drop_in_equals_reference_golden(mode, clocks):
+    z, c, p, rec, W_ref, S_ref = slow_case(mode, clocks)
     B, T = int(z["batch"]), int(z["steps"])
     b = Brain(c, p, device="cuda", seed=int(z["seed"]), batch=B, launch="step", receptor=rec)
     b.freeze(z["frozen"])
     b.prune(z["frozen"])
+    if clocks:
+        b.set_clocks(z["clock_period"])
     np.testing.assert_array_equal(b._W_cpu.data, z["shaped_data"])
     for k, Sk in S_ref.items():
         np.testing.assert_array_equal(b._W_slow_cpu[k].toarray(), Sk.toarray(), err_msg=k)
@@ -87,10 +117,12 @@ def test_brain_slow_tone_drop_in_equals_reference_golden(mode):
     b.step(20)
     for k, v in after.items():
         assert torch.equal(getattr(b, k), v), k
+    if clocks:
+        assert "slow_clock_acc" in saved
     b.reset([1])
     assert float(b.g_slow[1].abs().sum()) == 0.0 and float(b.g_slow_cls[:, 1].abs().sum()) == 0.0
-    with pytest.raises(NotImplementedError):
-        b.set_clocks(np.ones(c.n, np.int64))
+    if clocks:
+        assert int(b.slow_clock_acc[:, :, 1].abs().sum()) == 0
 
 
 @pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])

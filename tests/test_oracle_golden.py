@@ -224,12 +224,13 @@ def test_lif_19cell_clocked_rasters_match_reference():
         np.testing.assert_allclose(mine.T, z[f"final_{key}"], rtol=1e-5, atol=1e-4, err_msg=key)
 
 
-def slow_case(mode):
-    """The 19-cell slow-tone fixture: connectome, parameters, the receptor record it was built
-    from, and the shaped fast and slow matrices the reference held after pruning."""
+def slow_case(mode, clocks=False):
+    """The 19-cell slow-tone fixture (with `clocks`, the clocked one): connectome, parameters, the
+    receptor record it was built from, and the shaped fast and slow matrices the reference held
+    after pruning."""
     import scipy.sparse as sp
     from flyb200.weights import ReceptorSigns
-    z = golden(f"lif_19cell_slow_{mode}")
+    z = golden(f"lif_19cell_clocks_slow_{mode}" if clocks else f"lif_19cell_slow_{mode}")
     c = connectome_from_fixture(z)
     p = LIFParams(receptor_model="full", slow_gain_by_class={"metabotropic_classical": 0.5}, slow_mode=mode)
     rec = ReceptorSigns(fast_sign=z["rec_fast_sign"], slow_sign=z["rec_slow_sign"], fast_gain=z["rec_fast_gain"],
@@ -240,14 +241,16 @@ def slow_case(mode):
     return z, c, p, rec, W, S
 
 
+@pytest.mark.parametrize("clocks", [False, True], ids=["plain", "clocked"])
 @pytest.mark.parametrize("mode", ["additive", "gain", "threshold"])
-def test_lif_19cell_slow_tone_matches_reference(mode):
+def test_lif_19cell_slow_tone_matches_reference(mode, clocks):
     """receptor_model="full": the shaped fast and slow matrices are the reference's bit for bit, and
-    the oracle's step with the slow tone reproduces its rasters in every slow_mode."""
+    the oracle's step with the slow tone reproduces its rasters in every slow_mode, also under
+    per-neuron clocks of 1, 2 and 3 steps (the reference's clocked step, brain.py:898-957)."""
     import math
     import scipy.sparse as sp
     from flyb200.weights import slow_spec, slow_weights
-    z, c, p, rec, W_ref, S_ref = slow_case(mode)
+    z, c, p, rec, W_ref, S_ref = slow_case(mode, clocks)
     W, scale = lif_weights(c, p, rec)
     keep = np.ones(c.n, np.float32)
     keep[z["frozen"]] = 0
@@ -282,8 +285,12 @@ def test_lif_19cell_slow_tone_matches_reference(mode):
     slow = {"mode": mode, "norm": spec.norm_mv, "clip": spec.clip, "th_max": float(np.float32(0.9 * spec.norm_mv)),
             "classes": classes}
     flags = _abi.LIF_POISSON | _abi.LIF_EXT_UNIFORM | _abi.LIF_COUNTS | _abi.LIF_ADAPT | _abi.LIF_STD | _abi.LIF_SKIP_FROZEN
+    ck = None
+    if clocks:
+        period = z["clock_period"]
+        ck = (period, clock_coefficients(p, True, int(period.max()), [spec.tau[k] for k in S_ref]))
     r, _ = oracle.lif_run(st, ptr, edges, lif_coefficients(p, True, True), n_delay=4, flags=flags, nsteps=T,
-                          uniforms=U.transpose(0, 2, 1), raster=True, slow=slow)
+                          uniforms=U.transpose(0, 2, 1), raster=True, slow=slow, clocks=ck)
     ras = unpack(r, n * B).reshape(T, n, B).transpose(0, 2, 1)
     np.testing.assert_array_equal(ras, z["raster"])
     for key, mine in (("v", st.v), ("g", st.g), ("adapt", st.adapt), ("res", st.res), ("rate", st.rate),
