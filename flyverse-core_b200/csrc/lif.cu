@@ -58,6 +58,10 @@ struct LifK {
   long long* slow_ring[FLYB_SLOW_MAX_CLASSES];
   float* slow_g[FLYB_SLOW_MAX_CLASSES];
   float* g_slow;
+  const int* __restrict__ pull_ptr;            // pull delivery: first 32-entry input chunk per row
+  const int* __restrict__ pull_pre;            // [chunks][32] presynaptic neuron (-1: padding)
+  const unsigned* __restrict__ pull_planes;    // [chunks][pull_nplanes] count bit planes
+  int pull_nplanes;
   LifP P;
 };
 
@@ -405,6 +409,170 @@ __global__ void __launch_bounds__(256) lif_scatter_kernel(LifK k, int s) {
   if (k.events && threadIdx.x == 0 && edges) atomicAdd(k.events, edges);
 }
 
+// 32 x 32 bit transpose across a warp: lane r holds row r (bit c = column c) on entry and
+// column r (bit c = row c) on return. Five exchanges: at distance j a lane keeps the half of each
+// 2j-bit group on its own side and takes the partner's other half, rotated into place.
+__device__ __forceinline__ unsigned warp_transpose32(unsigned x, int lane) {
+  constexpr unsigned M[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const int j = 16 >> q;
+    const bool hi = lane & j;
+    const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
+    const unsigned t = __funnelshift_l(y, y, hi ? 32 - j : j);
+    const unsigned keep = hi ? ~M[q] : M[q];
+    x = (x & keep) | (t & ~keep);
+  }
+  return x;
+}
+
+// Pull delivery (FLYB_LIF_PULL_DELIVERY): one warp per postsynaptic row, 32 inputs per pass. Each
+// lane reads its input's spike words (one per 32 flies) from the raster of step `s`; the warp
+// transposes them so that lane f holds, for fly f of the group, the mask of the 32 inputs that
+// spiked; the chunk's counts arrive as P bit planes, so the row's input for fly f is
+// sum_p 2^p popc(mask & plane_p), the top plane weighted -2^(P-1) (two's complement). Integer and
+// exact: the ring slot ends with the sums the scatter's atomics give. Rows are added into the
+// write slot with coalesced 128-byte accesses per group of 32 flies.
+template <int G>
+__device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, int pre, unsigned (&w)[G]) {
+  if (pre < 0) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) w[g] = 0u;
+    return;
+  }
+  const unsigned* src = bits + (size_t)pre * G;
+  if constexpr (G == 1) {
+    w[0] = __ldg(src);
+  } else if constexpr (G == 2) {
+    const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
+    w[0] = v.x; w[1] = v.y;
+  } else {
+#pragma unroll
+    for (int g = 0; g < G; g += 4) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + g));
+      w[g] = v.x; w[g + 1] = v.y; w[g + 2] = v.z; w[g + 3] = v.w;
+    }
+  }
+}
+
+template <int P>
+__device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes, long long c, unsigned (&pl)[P]) {
+  const uint4* src = reinterpret_cast<const uint4*>(planes + (size_t)c * P);
+#pragma unroll
+  for (int q = 0; q < P; q += 4) {
+    const uint4 v = __ldg(src + q / 4);
+    pl[q] = v.x; pl[q + 1] = v.y; pl[q + 2] = v.z; pl[q + 3] = v.w;
+  }
+}
+
+// Pull delivery (FLYB_LIF_PULL_DELIVERY): each warp owns a contiguous block of postsynaptic rows
+// and walks their 32-input chunks as one stream. Per chunk a lane reads its input's spike words
+// (one per 32 flies) from the raster of step `s`; the warp transposes them so that lane f holds,
+// for fly f of the group, the mask of the 32 inputs that spiked; the counts arrive as P bit
+// planes, so the chunk adds sum_p 2^p popc(mask & plane_p) for fly f, the top plane weighted
+// -2^(P-1) (two's complement). Integer and exact: the ring slot ends with the sums the scatter's
+// atomics give. The stream is software-pipelined: the spike words and planes of the next chunk
+// and the inputs of the one after are in flight while a chunk is summed. A finished row is added
+// into the write slot with coalesced 128-byte accesses per group of 32 flies.
+template <int G, int P>
+__global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
+  const Clk clk = read_clock(k);
+  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
+  const int rsl = k.raster_slots > 0 ? slot_after(clk.raster_pos, s, k.raster_slots) : s;
+  const unsigned* __restrict__ bits = k.raster + (size_t)rsl * k.words;
+  int* ring = (int*)k.ring + (size_t)ws * k.n * k.batch;
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int per = (int)((k.n + warps - 1) / warps);
+  const int r0 = (int)(wid * per < k.n ? wid * per : k.n);
+  const int r1 = r0 + per < k.n ? r0 + per : k.n;
+  unsigned long long ev = 0;
+  if (r0 < r1) {
+    const int ce = __ldg(&k.pull_ptr[r1]);
+    int c = __ldg(&k.pull_ptr[r0]);
+    int row = r0, bound = __ldg(&k.pull_ptr[r0 + 1]);
+    int acc[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) acc[g] = 0;
+    // pipeline: words + planes of chunk c, inputs of chunk c + 1
+    unsigned w[G], pl[P];
+    int pre_next = -1;
+    if (c < ce) {
+      pull_words<G>(bits, __ldg(&k.pull_pre[(size_t)c * 32 + lane]), w);
+      pull_planes<P>(k.pull_planes, c, pl);
+      if (c + 1 < ce) pre_next = __ldg(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
+    }
+    for (; c < ce; ++c) {
+      unsigned wn[G], pn[P];
+      int pre_after = -1;
+      if (c + 1 < ce) {
+        pull_words<G>(bits, pre_next, wn);
+        pull_planes<P>(k.pull_planes, c + 1, pn);
+        if (c + 2 < ce) pre_after = __ldg(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
+      }
+      while (c >= bound) {                 // chunk c starts a later row: the current one is done
+        int* dst = ring + (size_t)row * k.batch + lane;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (acc[g]) dst[g * 32] += acc[g];
+          acc[g] = 0;
+        }
+        ++row;
+        bound = __ldg(&k.pull_ptr[row + 1]);
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        ev += (unsigned)__popc(w[g]);
+        const unsigned m = warp_transpose32(w[g], lane);
+        int sum = 0;
+#pragma unroll
+        for (int q = 0; q < P - 1; ++q) sum += __popc(m & pl[q]) << q;
+        sum -= __popc(m & pl[P - 1]) << (P - 1);
+        acc[g] += sum;
+      }
+#pragma unroll
+      for (int g = 0; g < G; ++g) w[g] = wn[g];
+#pragma unroll
+      for (int q = 0; q < P; ++q) pl[q] = pn[q];
+      pre_next = pre_after;
+    }
+    int* dst = ring + (size_t)row * k.batch + lane;      // the last row with inputs
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (acc[g]) dst[g * 32] += acc[g];
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
+  if (k.events && lane == 0 && ev) atomicAdd(k.events, ev);
+}
+
+template <int G>
+static int launch_pull_g(const LifK& k, int s, int grid, cudaStream_t st) {
+  if (k.pull_nplanes == 8) lif_pull_kernel<G, 8><<<grid, 256, 0, st>>>(k, s);
+  else lif_pull_kernel<G, 16><<<grid, 256, 0, st>>>(k, s);
+  return (int)cudaGetLastError();
+}
+
+static int launch_pull(const LifK& k, int s, cudaStream_t st) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = sms * 8;
+  switch (k.batch / 32) {
+    case 1: return launch_pull_g<1>(k, s, grid, st);
+    case 2: return launch_pull_g<2>(k, s, grid, st);
+    case 4: return launch_pull_g<4>(k, s, grid, st);
+    case 8: return launch_pull_g<8>(k, s, grid, st);
+    default: return FLYB_EINVAL;
+  }
+}
+
+// Whether the launch pulls each step itself: pull delivery over all neurons.
+static bool pulls_itself(const LifK& k) {
+  return (k.flags & FLYB_LIF_PULL_DELIVERY) && k.t_begin == 0 && k.t_end == (long long)k.n * k.batch;
+}
+
 // One block processes work items [base, base + BLOCK*IPT) of local step `s`: update, then deliver.
 // Thread j owns the IPT consecutive items base + j*IPT + q (neuron-major, fly-minor order), loads
 // every state array as one vector and keeps all loads in flight before computing.
@@ -577,7 +745,7 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
   }
   if constexpr (DEFER)
     append_spikes<IPT>(k, s, tx_bits, iq, bq, xq);
-  else
+  else if (!(k.flags & FLYB_LIF_PULL_DELIVERY))
     deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
 }
 
@@ -969,7 +1137,7 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
     // deferred, list entries for the scatter kernel of the step
     if constexpr (DEFER)
       append_spikes<IPT>(k, s, tx_bits, iq, bq, xq);
-    else
+    else if (!(k.flags & FLYB_LIF_PULL_DELIVERY))
       deliver<BLOCK, FIXED, IPT>(k, sm, tx_bits, iq, bq, xq, ws, slot);
     __syncthreads();
   }
@@ -1029,6 +1197,11 @@ static int run_lif_staged_as(const LifK& k, int grid_cap, cudaStream_t st) {
       lif_scatter_kernel<FIXED><<<sms * 8, 256, 0, st>>>(k, s);
     } else {
       lif_staged_kernel<BLOCK, FIXED, IPT><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
+      FLYB_CHECK_LAUNCH();
+      if (pulls_itself(k)) {
+        const int rc = launch_pull(k, s, st);
+        if (rc) return rc;
+      }
     }
     FLYB_CHECK_LAUNCH();
   }
@@ -1066,6 +1239,11 @@ static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st)
         lif_scatter_kernel<FIXED><<<scatter_grid, 256, 0, st>>>(k, s);
       } else {
         lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
+        FLYB_CHECK_LAUNCH();
+        if (pulls_itself(k)) {
+          const int rc = launch_pull(k, s, st);
+          if (rc) return rc;
+        }
       }
       FLYB_CHECK_LAUNCH();
     }
@@ -1292,6 +1470,17 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
     k.slow_ring[c] = used ? (long long*)a->slow_ring[c] : nullptr;
     k.slow_g[c] = used ? a->slow_g[c] : nullptr;
   }
+  k.pull_ptr = a->pull_ptr; k.pull_pre = a->pull_pre; k.pull_planes = a->pull_planes;
+  k.pull_nplanes = a->pull_nplanes;
+  if (a->flags & FLYB_LIF_PULL_DELIVERY) {
+    const int g = a->batch / 32;
+    if (a->batch % 32 || (g != 1 && g != 2 && g != 4 && g != 8) || a->ring_mode != FLYB_RING_COUNT ||
+        a->launch != FLYB_LAUNCH_STEP || (a->flags & (FLYB_LIF_DEFER_DELIVERY | FLYB_LIF_STD)) || a->clock_k ||
+        a->slow_classes || !a->raster || !a->pull_ptr || !a->pull_pre || !a->pull_planes ||
+        (a->pull_nplanes != 8 && a->pull_nplanes != 16) || (reinterpret_cast<uintptr_t>(a->raster) & 15) ||
+        (reinterpret_cast<uintptr_t>(a->pull_planes) & 15))
+      return FLYB_EINVAL;
+  }
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
     if (!a->spike_list || !a->spike_n || a->spike_cap <= 0 || a->launch != FLYB_LAUNCH_STEP) return FLYB_EINVAL;
@@ -1311,6 +1500,14 @@ FLYB_API int flyb_lif_advance(const flyb_lif_args* a, void* stream) {
   if (a->nsteps == 0 || !(k.clock || (k.flags & FLYB_LIF_EPISODES))) return 0;
   lif_advance_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(k);
   return (int)cudaGetLastError();
+}
+
+FLYB_API int flyb_lif_pull(const flyb_lif_args* a, void* stream) {
+  LifK k;
+  const int rc = make_lif_k(a, k);
+  if (rc) return rc;
+  if (!(k.flags & FLYB_LIF_PULL_DELIVERY)) return FLYB_EINVAL;
+  return launch_pull(k, 0, (cudaStream_t)stream);
 }
 
 FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {

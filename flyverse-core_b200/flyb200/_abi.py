@@ -21,6 +21,7 @@ _LIB = None
 OK, EINVAL, EBARRIER, ECOOP, ETOOBIG = 0, 1001, 1002, 1003, 1004
 LIF_POISSON, LIF_STD, LIF_COUNTS, LIF_ADAPT = 1, 2, 4, 8
 LIF_EXT_UNIFORM, LIF_SKIP_FROZEN, LIF_EPISODES, LIF_NO_ADVANCE, LIF_DEFER_DELIVERY = 16, 32, 64, 128, 256
+LIF_PULL_DELIVERY = 512
 RING_COUNT, RING_FIXED = 0, 1
 LAUNCH_STEP, LAUNCH_PERSISTENT = 0, 1
 LAUNCHES_BY_NAME = {"step": LAUNCH_STEP, "persistent": LAUNCH_PERSISTENT}
@@ -54,7 +55,7 @@ class LifArgs(ct.Structure):
                 ("slow_classes", _I), ("slow_mode", _I), ("slow_norm", ct.c_float), ("slow_clip_lo", ct.c_float),
                 ("slow_clip_hi", ct.c_float), ("slow_th_max", ct.c_float), ("slow_decay", ct.c_float * 2),
                 ("slow_out_ptr", _VP * 2), ("slow_out_edge", _VP * 2), ("slow_ring", _VP * 2), ("slow_g", _VP * 2),
-                ("g_slow", _VP)]
+                ("g_slow", _VP), ("pull_ptr", _VP), ("pull_pre", _VP), ("pull_planes", _VP), ("pull_nplanes", _I)]
 
 
 class OpticArgs(ct.Structure):
@@ -124,6 +125,7 @@ SIGNATURES = {
     "launch_means": [_P, _I, _I, _I, _I, _VP],
     "flyb_lif_run": [ct.POINTER(LifArgs), _VP],
     "flyb_lif_advance": [ct.POINTER(LifArgs), _VP],
+    "flyb_lif_pull": [ct.POINTER(LifArgs), _VP],
     "flyb_lif_spike_capacity": [ct.POINTER(LifArgs)],
     "flyb_ring_deposit": [_I, _I, _I, _VP, _VP, _VP, _VP, _VP],
     "flyb_optic_run": [ct.POINTER(OpticArgs), _VP],

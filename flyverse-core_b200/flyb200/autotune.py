@@ -25,7 +25,9 @@ LIF_CANDIDATES = (("step", 256, 4, "fused"), ("step", 256, 2, "fused"), ("step",
                   ("step", 256, 2, "staged"), ("step", 512, 2, "staged"), ("step", 256, 4, "staged"),
                   ("step", 256, 2, "defer"), ("step", 256, 1, "defer"), ("step", 128, 2, "defer"),
                   ("step", 256, 4, "defer"), ("step", 256, 2, "staged-defer"), ("step", 512, 2, "staged-defer"),
-                  ("step", 256, 4, "staged-defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"))
+                  ("step", 256, 4, "staged-defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"),
+                  ("step", 256, 2, "pull"), ("step", 256, 1, "pull"), ("step", 256, 2, "staged-pull"),
+                  ("step", 512, 2, "staged-pull"))
 
 
 def graph_key(brain) -> str:
@@ -71,6 +73,8 @@ def tune_lif(brain, steps: int = 10, candidates=LIF_CANDIDATES) -> dict:
         return CACHE[key]
     saved = brain.state_dict()
     results = {}
+    if not brain.can_pull():             # pull delivery: count ring and 32-fly groups only
+        candidates = [c for c in candidates if "pull" not in c[3]]
     for launch, block, ipt, delivery in candidates:
         _apply(brain, {"launch": launch, "block": block, "items_per_thread": ipt, "delivery": delivery})
         brain.step(2)
@@ -89,7 +93,9 @@ def _apply(brain, choice: dict) -> None:
     brain.launch, brain.block = choice["launch"], choice["block"]
     brain.items_per_thread = choice.get("items_per_thread", 0)
     delivery = choice.get("delivery", "fused")
-    brain.staged, brain.defer = delivery in ("staged", "staged-defer"), delivery in ("defer", "staged-defer")
+    brain.staged = delivery in ("staged", "staged-defer", "staged-pull")
+    brain.defer = delivery in ("defer", "staged-defer")
+    brain.pull = delivery in ("pull", "staged-pull")
     brain._make_args()
 
 

@@ -127,6 +127,39 @@ def clock_coefficients(p: LIFParams, std_on: bool, max_period: int, slow_tau=())
     return out.numpy()
 
 
+def pull_inputs(W, w_syn: float):
+    """The inputs of every neuron for FLYB_LIF_PULL_DELIVERY, from W[post, pre] = w_syn x signed
+    integer counts: (pull_ptr int32 [N+1] in 32-entry chunks, pull_pre int32 [chunks * 32] with -1
+    padding the last chunk of a row, pull_planes uint32 [chunks * P] where bit l of plane p is bit
+    p of entry l's count in P-bit two's complement, P = 8 or 16), or None when the weights are not
+    such counts or a count needs more than 16 bits."""
+    Wr = sp.csr_matrix(W, dtype=np.float32)
+    Wr.sum_duplicates()
+    Wr.sort_indices()
+    counts = integer_counts(Wr, w_syn)
+    if counts is None:
+        return None
+    counts = counts.astype(np.int64)
+    lo, hi = (int(counts.min()), int(counts.max())) if counts.size else (0, 0)
+    P = 8 if -128 <= lo and hi <= 127 else (16 if -32768 <= lo and hi <= 32767 else 0)
+    if not P:
+        return None
+    n = Wr.shape[0]
+    deg = np.diff(Wr.indptr).astype(np.int64)
+    ptr = np.concatenate([[0], np.cumsum((deg + 31) // 32)])
+    chunks = int(ptr[-1])
+    row = np.repeat(np.arange(n), deg)
+    pos = ptr[row] * 32 + (np.arange(Wr.nnz) - np.repeat(Wr.indptr[:-1].astype(np.int64), deg))
+    pre = np.full(chunks * 32, -1, np.int32)
+    pre[pos] = Wr.indices
+    u = np.zeros(chunks * 32, np.uint64)
+    u[pos] = (counts & ((1 << P) - 1)).astype(np.uint64)
+    u = u.reshape(chunks, 32)
+    lanes = np.arange(32, dtype=np.uint64)
+    planes = np.stack([(((u >> np.uint64(q)) & np.uint64(1)) << lanes).sum(axis=1) for q in range(P)], axis=1)
+    return ptr.astype(np.int32), pre, planes.astype(np.uint32).ravel(), P
+
+
 def out_edges(W, w_syn: float, prefer: str = "auto", std_on: bool = False):
     """Pre-major (CSC) outgoing synapses of W[post, pre] for the native step.
 
@@ -353,7 +386,34 @@ class Brain:
         """Deferred delivery (FLYB_LIF_DEFER_DELIVERY) applies to per-step launches (register or staged
         path) without clocks or the slow tone."""
         return bool(getattr(self, "defer", False)) and self.launch == "step" and self._kvec is None \
-            and self.slow is None
+            and self.slow is None and not self._pull_active()
+
+    def can_pull(self) -> bool:
+        """Whether pull delivery (FLYB_LIF_PULL_DELIVERY) fits this brain: the int32 count ring (no
+        depression), 32, 64, 128 or 256 flies, no clocks or slow tone."""
+        return self.ring_mode == _abi.RING_COUNT and self.B in (32, 64, 128, 256) and self._kvec is None \
+            and self.slow is None and not self._std_on
+
+    def _pull_active(self) -> bool:
+        """Pull delivery runs: requested (`pull`), per-step launches, and `can_pull`."""
+        return bool(getattr(self, "pull", False)) and self.launch == "step" and self.can_pull()
+
+    def _set_pull(self, a) -> None:
+        """Point the arguments at the pull tables (built from the shaped weights on first use)."""
+        if not self._pull_active():
+            a.pull_ptr = a.pull_pre = a.pull_planes = None
+            a.pull_nplanes = 0
+            return
+        key = self._weights_version
+        if getattr(self, "_pull_key", None) != key:
+            t = pull_inputs(self._W_cpu, self.p.w_syn)
+            if t is None:
+                raise ValueError("pull delivery needs weights of w_syn x counts within 16 bits")
+            ptr, pre, planes, P = t
+            self._pull_t = tuple(torch.from_numpy(x).to(self.device) for x in (ptr, pre, planes.view(np.int32)))
+            self._pull_planes_n, self._pull_key = P, key
+        a.pull_ptr, a.pull_pre, a.pull_planes = (x.data_ptr() for x in self._pull_t)
+        a.pull_nplanes = self._pull_planes_n
 
     # ------------------------------------------------------------------ per-neuron clocks
     def set_clocks(self, multiplier) -> None:
@@ -404,6 +464,8 @@ class Brain:
         f = 0
         if self._defer_active():
             f |= _abi.LIF_DEFER_DELIVERY
+        if self._pull_active():
+            f |= _abi.LIF_PULL_DELIVERY
         if self._poisson_on:
             f |= _abi.LIF_POISSON
         if self._std_on:
@@ -433,6 +495,7 @@ class Brain:
         a.nsteps = n_steps
         a.uniforms = ext.data_ptr() if ext is not None else None
         self._set_delivery(a, 0, 0)
+        self._set_pull(a)
         a.n_first, a.n_count = 0, 0
         stream = torch.cuda.current_stream(self.device).cuda_stream
         with torch.cuda.device(self.device):
@@ -452,6 +515,7 @@ class Brain:
         a.flags = self._flags(False) | _abi.LIF_NO_ADVANCE
         a.nsteps, a.uniforms = 1, None
         self._set_delivery(a, n_first, n_count)
+        self._set_pull(a)
         a.n_first, a.n_count = int(n_first), int(n_count)
         try:
             with torch.cuda.device(self.device):
@@ -467,8 +531,17 @@ class Brain:
         a = self._args
         a.flags = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY
         a.nsteps = int(n_steps)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        if self._pull_active():          # the ranges recorded their spikes: deliver them, then advance
+            if n_steps != 1:
+                raise ValueError("with pull delivery, ranges advance one step at a time")
+            self._set_pull(a)
+            with torch.cuda.device(self.device):
+                rc = self._lib.flyb_lif_pull(ct.byref(a), stream)
+            if rc:
+                raise RuntimeError(f"flyb_lif_pull: error {rc}")
         with torch.cuda.device(self.device):
-            rc = self._lib.flyb_lif_advance(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
+            rc = self._lib.flyb_lif_advance(ct.byref(a), stream)
         if rc:
             raise RuntimeError(f"flyb_lif_advance: error {rc}")
         self.buf_pos = (self.buf_pos + n_steps) % self.R

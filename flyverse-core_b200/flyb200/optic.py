@@ -296,6 +296,73 @@ class LobeMatrices:
     sens: np.ndarray
 
 
+def photoreceptor_cells(pr_column, pr_family, n_col: int):
+    """The column x family cells of the photoreceptor stage (optic.py:343-348): which cells have
+    members (n_col, 5), the averaging matrix (n_col * 5, n_pr) with 1 / members per entry, and each
+    photoreceptor's cell (column * 5 + family)."""
+    pr_column, pr_family = np.asarray(pr_column, np.int64), np.asarray(pr_family, np.int64)
+    has = np.zeros((n_col, 5), bool)
+    np.add.at(has, (pr_column, pr_family), True)
+    cnt = np.zeros((n_col, 5), np.float32)
+    np.add.at(cnt, (pr_column, pr_family), 1.0)
+    cell = pr_column * 5 + pr_family
+    avg = sp.csr_matrix((1.0 / cnt[pr_column, pr_family], (cell, np.arange(len(cell)))), shape=(n_col * 5, len(cell)))
+    return has, avg, cell
+
+
+class PhotoreceptorStage:
+    """The photoreceptor stage on the device (optic.py:496-517, `flyb_photoreceptor`): per fly and
+    column x family cell the channel-weighted intensity averaged over the cell's photoreceptors, its
+    low-pass (tau_lp_ms) and adaptation (tau_adapt_ms) states, the clipped contrast, gathered back
+    to the photoreceptors as a_pr [n_pr][B]. The first frame after construction or `reset` starts
+    both states at the frame's intensity. State: I_lp, I_mean, contrast (B, n_col * 5), fresh (B)."""
+
+    def __init__(self, pr_column, pr_family, sens, n_col: int, batch: int, device, p: OpticParams | None = None):
+        self.p = p or OpticParams()
+        dev = torch.device(device)
+        self.device, self.B, self.n_col = dev, int(batch), int(n_col)
+        self.has, avg, cell = photoreceptor_cells(pr_column, pr_family, n_col)
+        self.n_pr = len(cell)
+        self.avg = DeviceCSR(avg, dev)
+        self.sens = torch.from_numpy(np.ascontiguousarray(sens, np.float32).reshape(-1, 4)).to(dev)
+        self.pr_column_t = torch.as_tensor(np.asarray(pr_column, np.int32), device=dev)
+        self.pr_cell_t = torch.as_tensor(cell.astype(np.int32), device=dev)
+        self.has_t = torch.from_numpy(self.has.reshape(-1).astype(np.uint8)).to(dev)
+        self.I_lp = torch.zeros(self.B, n_col * 5, device=dev)
+        self.I_mean = torch.zeros(self.B, n_col * 5, device=dev)
+        self.contrast = torch.zeros(self.B, n_col * 5, device=dev)
+        self.fresh_u8 = torch.ones(self.B, dtype=torch.uint8, device=dev)
+        self.a_pr = torch.zeros(self.n_pr, self.B, device=dev)
+
+    def reset(self, rows=None) -> None:
+        sel = slice(None) if rows is None else torch.as_tensor(rows, device=self.device)
+        for t in (self.I_lp, self.I_mean, self.contrast):
+            t[sel] = 0.0
+        self.fresh_u8[sel] = 1
+
+    def __call__(self, rad: torch.Tensor, dt_ms: float, out: torch.Tensor | None = None) -> torch.Tensor:
+        """rad: contiguous float32 (B, n_col, 4) on the device -> a_pr [n_pr][B] (`out` or the
+        stage's own buffer), on the current stream."""
+        if rad.dtype != torch.float32 or not rad.is_contiguous() or tuple(rad.shape) != (self.B, self.n_col, 4):
+            raise ValueError("radiance must be a contiguous float32 (batch, columns, 4) tensor")
+        out = self.a_pr if out is None else out
+        if out.dtype != torch.float32 or not out.is_contiguous() or tuple(out.shape) != (self.n_pr, self.B):
+            raise ValueError("out must be a contiguous float32 [n_pr][batch] tensor")
+        p = self.p
+        a_lp, a_ad = float(np.exp(-dt_ms / p.tau_lp_ms)), float(np.exp(-dt_ms / p.tau_adapt_ms))
+        args = _abi.PhotoArgs(n_pr=self.n_pr, n_col=self.n_col, batch=self.B, rad=rad.data_ptr(),
+                              pr_column=self.pr_column_t.data_ptr(), sens=self.sens.data_ptr(),
+                              avg_ptr=self.avg.ptr.data_ptr(), avg_idx=self.avg.col.data_ptr(), avg_w=self.avg.w.data_ptr(),
+                              pr_cell=self.pr_cell_t.data_ptr(), has=self.has_t.data_ptr(), I_lp=self.I_lp.data_ptr(),
+                              I_mean=self.I_mean.data_ptr(), contrast=self.contrast.data_ptr(),
+                              fresh=self.fresh_u8.data_ptr(), a_lp=a_lp, c_lp=1 - a_lp, a_ad=a_ad, c_ad=1 - a_ad,
+                              eps=p.eps, clip_hi=p.contrast_clip, a_pr=out.data_ptr())
+        rc = _abi.lib().flyb_photoreceptor(ct.byref(args), torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError(f"flyb_photoreceptor: error {rc}")
+        return out
+
+
 def lobe_matrices(c, retina, p: OpticParams, receptor=None, receptor_gain=None) -> LobeMatrices:
     """The reference's optic-lobe construction (optic.py:229-348): unit selection, normalised and
     gain-shaped blocks, per-type constants and the photoreceptor averaging matrix."""
@@ -349,14 +416,7 @@ def lobe_matrices(c, retina, p: OpticParams, receptor=None, receptor_gain=None) 
     bl_map = DEFAULT_BASELINE_BY_TYPE if p.baseline_by_type is None else p.baseline_by_type
     b = np.array([bl_map.get(t, p.baseline) for t in rt], dtype=np.float32)
     pr_family = np.array([FAMILY_OF_TYPE[t] for t in types[pr_idx]], dtype=np.int64)
-    n_col = retina.n_columns
-    has = np.zeros((n_col, 5), bool)
-    np.add.at(has, (retina.pr_column, pr_family), True)
-    cnt = np.zeros((n_col, 5), np.float32)
-    np.add.at(cnt, (retina.pr_column, pr_family), 1.0)
-    rows = np.asarray(retina.pr_column) * 5 + pr_family
-    avg = sp.csr_matrix((1.0 / cnt[retina.pr_column, pr_family], (rows, np.arange(len(pr_idx)))),
-                        shape=(n_col * 5, len(pr_idx)))
+    has, avg, rows = photoreceptor_cells(retina.pr_column, pr_family, retina.n_columns)
     return LobeMatrices(rate_idx, pr_idx, spk_idx, M_rr, M_rp, M_rs, M_sr, a.astype(np.float32), b,
                         float(np.exp(-p.dt_ms / p.adapt_tau_ms)), pr_family, has, avg, rows,
                         np.asarray(retina.pr_column, np.int64), np.asarray(retina.pr_sens, np.float32).reshape(-1, 4))
@@ -550,19 +610,13 @@ class OpticLobe:
         self.spk_idx_t = torch.as_tensor(self.spk_idx, device=dev)
         self._spk_idx32 = self.spk_idx_t.to(torch.int32)
         self._a, self.b_vec = self.core.a, self.core.b
-        self.pr_family, self.has = L.pr_family, L.has
-        n_col = retina.n_columns
-        self.avg = DeviceCSR(L.avg, dev)
-        self.sens = torch.from_numpy(np.ascontiguousarray(retina.pr_sens, np.float32)).to(dev)
-        self.pr_column_t = torch.as_tensor(np.asarray(retina.pr_column, np.int32), device=dev)
-        self.pr_cell_t = torch.as_tensor(L.pr_cell.astype(np.int32), device=dev)
-        self.has_t = torch.from_numpy(self.has.reshape(-1).astype(np.uint8)).to(dev)
+        self.pr_family = L.pr_family
+        self.photo = PhotoreceptorStage(retina.pr_column, L.pr_family, retina.pr_sens, retina.n_columns, self.B, dev, p)
+        self.has = self.photo.has
+        # the stage's state tensors, under the reference's names (FlyBrain checkpoints them)
+        self.I_lp, self.I_mean, self.contrast = self.photo.I_lp, self.photo.I_mean, self.photo.contrast
+        self._fresh_u8, self._a_pr = self.photo.fresh_u8, self.photo.a_pr
         B = self.B
-        self.I_lp = torch.zeros(B, n_col * 5, device=dev)
-        self.I_mean = torch.zeros(B, n_col * 5, device=dev)
-        self.contrast = torch.zeros(B, n_col * 5, device=dev)
-        self._fresh_u8 = torch.ones(B, dtype=torch.uint8, device=dev)
-        self._a_pr = torch.zeros(self.n_pr, B, device=dev)
         self._delta = torch.zeros(self.n_rate, B, device=dev)
         self._drive = torch.zeros(c.n, B, device=dev)
         self.slow_classes = list(self.slow.classes) if self.slow is not None else []
@@ -614,23 +668,10 @@ class OpticLobe:
         """(B, n_col, 4) radiance -> (B, n_pr) contrast activity (a view of [n_pr][B] storage)."""
         if intensity is not None:
             raise NotImplementedError("an intensity override is an extension-module input, not provided here")
-        p = self.p
         rad = torch.as_tensor(col_radiance, dtype=torch.float32, device=self.device)
         if rad.dim() == 2:
             rad = rad[None]
-        rad = rad.expand(self.B, -1, -1).contiguous()
-        a_lp = float(np.exp(-dt_ms / p.tau_lp_ms))
-        a_ad = float(np.exp(-dt_ms / p.tau_adapt_ms))
-        args = _abi.PhotoArgs(n_pr=self.n_pr, n_col=self.r.n_columns, batch=self.B, rad=rad.data_ptr(),
-                              pr_column=self.pr_column_t.data_ptr(), sens=self.sens.data_ptr(),
-                              avg_ptr=self.avg.ptr.data_ptr(), avg_idx=self.avg.col.data_ptr(), avg_w=self.avg.w.data_ptr(),
-                              pr_cell=self.pr_cell_t.data_ptr(), has=self.has_t.data_ptr(), I_lp=self.I_lp.data_ptr(),
-                              I_mean=self.I_mean.data_ptr(), contrast=self.contrast.data_ptr(),
-                              fresh=self._fresh_u8.data_ptr(), a_lp=a_lp, c_lp=1 - a_lp, a_ad=a_ad, c_ad=1 - a_ad,
-                              eps=p.eps, clip_hi=p.contrast_clip, a_pr=self._a_pr.data_ptr())
-        rc = _abi.lib().flyb_photoreceptor(ct.byref(args), torch.cuda.current_stream(self.device).cuda_stream)
-        if rc:
-            raise RuntimeError(f"flyb_photoreceptor: error {rc}")
+        self.photo(rad.expand(self.B, -1, -1).contiguous(), dt_ms)
         return self._a_pr.t()
 
     # ------------------------------------------------------------------ the slow receptor tone

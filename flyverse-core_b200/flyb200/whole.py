@@ -27,7 +27,7 @@ import torch
 
 from . import _abi
 from .brain import Brain, LIFParams
-from .optic import DeviceCSR, OpticCore, spmm
+from .optic import DeviceCSR, OpticCore, PhotoreceptorStage, spmm
 from .synthetic import WholeFlyConfig
 
 
@@ -70,8 +70,10 @@ class WholeFly:
         self.W_sr_host = o.W_sr.tocsr()[self.lif_order]                # rows in stored LIF order
         self.W_rs, self.rs_rows = self._rows_with_entries(self.W_rs_host, dev)
         self.W_sr, self.sr_rows = self._rows_with_entries(self.W_sr_host, dev)
-        self.W_rp = DeviceCSR(o.W_rp, dev)
-        self.a_pr = torch.zeros(o.n_pr, self.B, device=dev)
+        # pr_in has input on the lamina rows alone: the product writes those and the rest stay zero
+        self.W_rp, self.rp_rows = self._rows_with_entries(o.W_rp, dev)
+        self.photo = PhotoreceptorStage(o.pr_column, o.pr_family, o.sens, o.n_col, self.B, dev)
+        self.a_pr = self.photo.a_pr                       # [n_pr][B]: the stage's output
         self.steps_taken = 0
         self._fork = (torch.cuda.Stream(self.device, priority=-1), torch.cuda.Stream(self.device))
 
@@ -79,10 +81,13 @@ class WholeFly:
     def launches_per_step(self) -> int:
         """Kernels launched by one step once running: two coupling products, the optic substep (its
         dr carried over), the LIF update (two ranges when overlapped; each followed by its scatter
-        under deferred delivery) and the device-clock advance (or one persistent launch)."""
+        under deferred delivery, or one pull kernel after both under pull delivery) and the
+        device-clock advance (or one persistent launch)."""
         n = 6 if self.overlapping else (5 if self.lif.launch == "step" else 4)
         if self.lif._defer_active():
             n += 2 if self.overlapping else 1          # the scatter kernel of each LIF launch
+        if self.lif._pull_active():
+            n += 1
         return n
 
     @property
@@ -104,9 +109,19 @@ class WholeFly:
         return self.cfg.n_rate + self.cfg.n_spiking
 
     def set_photoreceptors(self, a_pr: torch.Tensor) -> None:
-        """Photoreceptor activity [n_pr][B] -> held pr_in = gain_in * W_rp a_pr (a frame's input)."""
-        self.a_pr.copy_(a_pr)
-        spmm(self.W_rp, self.a_pr, self.optic.pr_in, alpha=self.cfg.optic.gain_in)
+        """Photoreceptor activity [n_pr][B] (contiguous, on the device) -> held pr_in =
+        gain_in * W_rp a_pr (a frame's input), read from `a_pr` where it lies."""
+        spmm(self.W_rp, a_pr, self.optic.pr_in, alpha=self.cfg.optic.gain_in, y_index=self.rp_rows)
+
+    def set_radiance(self, rad: torch.Tensor, frame_ms: float, a_pr: torch.Tensor | None = None) -> None:
+        """A radiance frame (B, n_col, 4) on the device -> the photoreceptor stage (optic.py:496-517,
+        its low-pass and adaptation advanced by frame_ms) -> held pr_in (optic.py:575). With `a_pr`
+        the stage's output lands there (for instance a per-frame buffer on an input stream) and only
+        the stage runs; `set_photoreceptors(a_pr)` installs it later."""
+        if a_pr is not None:
+            self.photo(rad, frame_ms, out=a_pr)
+            return
+        self.set_photoreceptors(self.photo(rad, frame_ms))
 
     def step(self, n: int = 1, before=None, after=None) -> None:
         """Advance every fly n steps. Each optic substep reuses the dr the previous one wrote. Under
@@ -157,9 +172,15 @@ class WholeFly:
     # ------------------------------------------------------------------ algorithmic bytes (roofline)
     def lif_bytes_per_step(self) -> int:
         """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate, counts
-        read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active."""
+        read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active.
+        Under pull delivery also its input tables once (presynaptic index per input slot, the
+        count bit planes per 32 slots) and the write slot read + written."""
         per = 4 * (5 * 2 + 4 + 1)
-        return self.cfg.n_spiking * (self.B * per + 4)
+        total = self.cfg.n_spiking * (self.B * per + 4)
+        if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
+            ptr, pre, planes = self.lif._pull_t
+            total += pre.numel() * 4 + planes.numel() * 4 + self.cfg.n_spiking * self.B * 4 * 2
+        return total
 
     def optic_bytes_per_step(self) -> int:
         """CSR once (idx + w) + row pointers, per unit-fly v, adapt r+w, pr, spk, dr in / out."""

@@ -78,6 +78,14 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
 #define FLYB_LIF_NO_ADVANCE   128  /* leave `clock` and `fly_steps` as they are: other launches of
                                       the same steps cover the other neurons; flyb_lif_advance
                                       moves them on once all have run                           */
+#define FLYB_LIF_PULL_DELIVERY 512 /* per-step launches (register or staged path), count ring,
+                                      batch a multiple of 32 (at most 256), raster on: the
+                                      update kernels only record the step's spikes in the raster,
+                                      then each postsynaptic row sums count x spike over its
+                                      inputs (pull_ptr / pull_pre / pull_planes) into the write
+                                      slot, the same exact integers the scatter adds. A launch
+                                      over all neurons pulls after every step; launches over
+                                      neuron ranges leave it to flyb_lif_pull                    */
 
 /* Delay-ring element types */
 #define FLYB_RING_COUNT  0   /* int32 signed synapse counts; g += w_syn * count (exact sum)     */
@@ -187,6 +195,15 @@ typedef struct flyb_lif_args {
   void* slow_ring[FLYB_SLOW_MAX_CLASSES];           /* [R][n][batch] int64 per class     */
   float* slow_g[FLYB_SLOW_MAX_CLASSES];             /* [n][batch] tone per class (mV)    */
   float* g_slow;                                    /* [n][batch] summed tone (mV)       */
+  /* FLYB_LIF_PULL_DELIVERY: the inputs of each neuron (rows of W[post, pre]) in chunks of 32
+   * entries, a row's last chunk padded with pre = -1: pull_ptr [n+1] first chunk of each row,
+   * pull_pre [chunks][32] presynaptic neuron, pull_planes [chunks][pull_nplanes] the chunk's signed
+   * synapse counts as bit planes (bit l of plane p = bit p of entry l's count in pull_nplanes-bit
+   * two's complement; pull_nplanes 8 or 16). */
+  const int* pull_ptr;
+  const int* pull_pre;
+  const unsigned* pull_planes;
+  int pull_nplanes;
 } flyb_lif_args;
 
 /* flyb_lif_args.slow_mode */
@@ -200,6 +217,11 @@ enum {
 };
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);
+
+/* FLYB_LIF_PULL_DELIVERY over neuron ranges: after every range of a step ran (each with
+ * FLYB_LIF_NO_ADVANCE and nsteps 1), delivers that step's spikes from the raster into the write
+ * slot; then flyb_lif_advance. The arguments are those of the launches (any range). */
+int flyb_lif_pull(const flyb_lif_args* a, void* stream);
 
 /* Entries a FLYB_LIF_DEFER_DELIVERY step of these arguments can write when every item of the
  * neuron range fires (n_count * batch + batch * out-edges of the range / 1024); reads two row

@@ -19,23 +19,27 @@ def small_fly():
 
 
 @pytest.mark.parametrize("overlap,capped,defer", [(True, False, False), (False, False, False), (True, True, False),
-                                                  (True, False, True), (True, False, "staged")])
+                                                  (True, False, True), (True, False, "staged"), (True, False, "pull"),
+                                                  (False, False, "pull"), (True, False, "staged-pull")])
 def test_whole_fly_matches_oracle_step_order(overlap, capped, defer):
     """Bit-identical spikes every step whether the undriven LIF neurons update concurrently with
     the optic chain (overlap) or after it, also with a capped persistent optic grid beside capped
-    staged LIF blocks; the oracle runs the stages serially on the engine's stored neuron order."""
+    staged LIF blocks, and with pull delivery (32 flies, the ranges' spikes pulled once per step);
+    the oracle runs the stages serially on the engine's stored neuron order."""
     cfg = small_fly()
-    B, T = 4, 120
+    pull = isinstance(defer, str) and "pull" in defer
+    B, T = (32, 120) if pull else (4, 120)
     eng = WholeFly(cfg, B, device="cuda", seed=1, launch="step", overlap=overlap)
     if capped:
         eng.optic.launch, eng.optic.grid = "persistent", 20
         eng.lif.staged, eng.lif.grid = True, 7
         eng.lif._make_args()
-    eng.lif.defer = bool(defer)
-    if defer == "staged":
+    eng.lif.defer = bool(defer) and not pull
+    eng.lif.pull = pull
+    if defer in ("staged", "staged-pull"):
         eng.lif.staged = True
-        eng.lif._make_args()
-    assert eng.overlapping == overlap
+    eng.lif._make_args()
+    assert eng.overlapping == overlap and eng.lif._pull_active() == pull
     a_pr = torch.from_numpy((np.random.default_rng(0).standard_normal((cfg.optic.n_pr, B)) * 0.5).astype(np.float32)).cuda()
     eng.set_photoreceptors(a_pr)
     pr = eng.optic.pr_in.cpu().numpy()
@@ -68,6 +72,8 @@ def test_whole_fly_matches_oracle_step_order(overlap, capped, defer):
         ocounts.append(float(st.counts.sum()))
     assert ocounts[-1] > 0
     np.testing.assert_array_equal(np.array(counts), np.array(ocounts))          # same spikes every step
+    if pull:
+        assert eng.lif.synaptic_events > 0
     np.testing.assert_array_equal(eng.lif.spike_counts.t().cpu().numpy(), st.counts)
     np.testing.assert_allclose(eng.optic.v_s.cpu().numpy(), v, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(eng.lif._st["v"].cpu().numpy(), st.v, rtol=0, atol=1e-4)
@@ -184,3 +190,66 @@ def test_per_step_inputs_and_readouts_in_one_call():
     for k in ("v", "g", "rate", "spike_counts"):
         assert torch.equal(a.lif._st[k], b.lif._st[k]), k
     assert torch.equal(a.optic.v_s, b.optic.v_s)
+
+
+def test_set_radiance_equals_oracle_photoreceptor_stage():
+    """WholeFly.set_radiance: the native photoreceptor stage (its low-pass and adaptation states
+    carried frame to frame, the first frame fresh) and the lamina-row product into pr_in, against
+    the oracle's stage and a full-matrix product; pr_in stays zero off the lamina rows."""
+    from types import SimpleNamespace
+    from oracle import frame as oframe
+    from flyb200.optic import OpticParams, photoreceptor_cells
+    cfg = small_fly()
+    o, B = cfg.optic, 4
+    eng = WholeFly(cfg, B, device="cuda", seed=7, launch="step")
+    has, avg, cell = photoreceptor_cells(o.pr_column, o.pr_family, o.n_col)
+    L = SimpleNamespace(sens=o.sens, pr_column=o.pr_column, avg=avg, has=has, pr_cell=cell)
+    st = {"I_lp": np.zeros((B, o.n_col * 5), np.float32), "I_mean": np.zeros((B, o.n_col * 5), np.float32),
+          "fresh": np.ones(B, bool)}
+    M = o.W_rp.tocsr()
+    for f in range(4):
+        rad = o.grating(7.0 * f, B, seed=f)
+        eng.set_radiance(torch.from_numpy(rad).cuda(), 2.0)
+        want = oframe.photoreceptor(L, st, rad, 2.0, OpticParams())
+        np.testing.assert_allclose(eng.photo.a_pr.cpu().numpy(), want, rtol=1e-5, atol=1e-6)
+        pr = oracle.spmm(M.indptr, M.indices, M.data, want, B, rows=M.shape[0], alpha=o.gain_in)
+        np.testing.assert_allclose(eng.optic.pr_in.cpu().numpy(), pr, rtol=1e-5, atol=1e-6)
+    assert np.abs(want).max() > 0.01
+    assert not eng.optic.pr_in[np.flatnonzero(np.diff(M.indptr) == 0)].any()
+    # a per-frame buffer leaves the installed input alone until set_photoreceptors
+    held = eng.optic.pr_in.clone()
+    buf = torch.empty(o.n_pr, B, device="cuda")
+    eng.set_radiance(torch.from_numpy(o.grating(40.0, B, seed=9)).cuda(), 2.0, a_pr=buf)
+    assert torch.equal(eng.optic.pr_in, held)
+    eng.set_photoreceptors(buf)
+    assert not torch.equal(eng.optic.pr_in, held)
+
+
+@pytest.mark.parametrize("B", [32, 64, 128, 256])
+@pytest.mark.parametrize("staged", [False, True])
+def test_pull_delivery_equals_scatter_at_high_activity(B, staged):
+    """Pull delivery against the scatter, bit for bit (state, ring, rasters, synaptic event count),
+    on a graph driven into dense firing, at every supported batch width."""
+    from flyb200.brain import Brain
+    cfg = synthetic.lif_config2(seed=4, n=4000, edges=600_000, n_poisson=800, poisson_hz=400.0)
+    p = LIFParams(**cfg.params)
+    brains = []
+    for pull in (False, True):
+        b = Brain(cfg.c, p, device="cuda", seed=3, batch=B, launch="step")
+        b.set_poisson(cfg.poisson_idx, 400.0)
+        b.set_drive(np.arange(cfg.c.n), 5.0)
+        b.record_activity = True
+        b.pull, b.staged = pull, staged
+        b._make_args()
+        assert b._pull_active() == pull
+        brains.append(b)
+    push, pull = brains
+    for chunk in (1, 7, 40):
+        push.step(chunk)
+        pull.step(chunk)
+        torch.cuda.synchronize()
+        for k in ("v", "g", "refrac", "rate", "spike_counts", "spikes"):
+            assert torch.equal(getattr(push, k), getattr(pull, k)), k
+        assert torch.equal(push.ring, pull.ring)
+        assert push.synaptic_events == pull.synaptic_events
+    assert float(pull.spike_counts.sum()) / (48 * B * cfg.c.n) > 0.005     # dense firing
