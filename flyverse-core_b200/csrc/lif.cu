@@ -61,7 +61,8 @@ struct LifK {
   const int* __restrict__ pull_ptr;            // pull delivery: first 32-entry input chunk per row
   const int* __restrict__ pull_pre;            // [chunks][32] presynaptic neuron (-1: padding)
   const unsigned* __restrict__ pull_planes;    // [chunks][pull_nplanes] count bit planes
-  int pull_nplanes;
+  int pull_nplanes;                            // plane stride per chunk (8 or 16)
+  const int* __restrict__ pull_meta;           // per chunk: base count << 5 | planes used
   LifP P;
 };
 
@@ -465,15 +466,45 @@ __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes,
   }
 }
 
+// sum_{p < planes} 2^p popc(m & pl[p]) for a warp-uniform plane count (a uniform branch, no
+// predicated-off work).
+template <int P>
+__device__ __forceinline__ int plane_sum(unsigned m, const unsigned (&pl)[P], int planes) {
+  int sum = 0;
+#define FLYB_PLANE(q) case q + 1: sum += __popc(m & pl[q]) << q; [[fallthrough]];
+  if constexpr (P > 8) {
+    if (planes > 8) {
+      switch (planes) {
+        FLYB_PLANE(15) FLYB_PLANE(14) FLYB_PLANE(13) FLYB_PLANE(12)
+        FLYB_PLANE(11) FLYB_PLANE(10) FLYB_PLANE(9) FLYB_PLANE(8)
+        default: break;
+      }
+      planes = 8;
+    }
+  }
+  switch (planes) {
+    FLYB_PLANE(7) FLYB_PLANE(6) FLYB_PLANE(5) FLYB_PLANE(4) FLYB_PLANE(3) FLYB_PLANE(2) FLYB_PLANE(1)
+    FLYB_PLANE(0)
+    default: break;
+  }
+#undef FLYB_PLANE
+  return sum;
+}
+
 // Pull delivery (FLYB_LIF_PULL_DELIVERY): each warp owns a contiguous block of postsynaptic rows
 // and walks their 32-input chunks as one stream. Per chunk a lane reads its input's spike words
 // (one per 32 flies) from the raster of step `s`; the warp transposes them so that lane f holds,
-// for fly f of the group, the mask of the 32 inputs that spiked; the counts arrive as P bit
-// planes, so the chunk adds sum_p 2^p popc(mask & plane_p) for fly f, the top plane weighted
-// -2^(P-1) (two's complement). Integer and exact: the ring slot ends with the sums the scatter's
-// atomics give. The stream is software-pipelined: the spike words and planes of the next chunk
-// and the inputs of the one after are in flight while a chunk is summed. A finished row is added
-// into the write slot with coalesced 128-byte accesses per group of 32 flies.
+// for fly f of the group, the mask of the 32 inputs that spiked. A row's inputs are sorted by
+// count, and a chunk stores its smallest count as a base and the excess of each entry in as few
+// bit planes as its range needs, so fly f gains base x popc(mask) + sum_p 2^p popc(mask &
+// plane_p). Integer and exact: the ring slot ends with the sums the scatter's atomics give. The
+// stream is software-pipelined: the spike words and planes of the next chunk and the inputs of
+// the one after are in flight while a chunk is summed. A finished row is added into the write
+// slot with coalesced 128-byte accesses per group of 32 flies. The synaptic events (out-degree x
+// flies spiking, per presynaptic neuron) are counted over the same block of neuron indices. Each
+// input is one random 8-byte gather (64 flies) from the step's raster, a 32-byte sector through
+// L1/L2: at the whole fly's 19 M inputs that sector stream bounds the kernel (~150 us at 64 flies,
+// L1TEX 67 % busy, DRAM 11 %); at 256 flies the same sectors carry four times the flies.
 template <int G, int P>
 __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
   const Clk clk = read_clock(k);
@@ -497,18 +528,20 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
     for (int g = 0; g < G; ++g) acc[g] = 0;
     // pipeline: words + planes of chunk c, inputs of chunk c + 1
     unsigned w[G], pl[P];
-    int pre_next = -1;
+    int meta = 0, pre_next = -1;
     if (c < ce) {
       pull_words<G>(bits, __ldg(&k.pull_pre[(size_t)c * 32 + lane]), w);
       pull_planes<P>(k.pull_planes, c, pl);
+      meta = __ldg(&k.pull_meta[c]);
       if (c + 1 < ce) pre_next = __ldg(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
     }
     for (; c < ce; ++c) {
       unsigned wn[G], pn[P];
-      int pre_after = -1;
+      int meta_next = 0, pre_after = -1;
       if (c + 1 < ce) {
         pull_words<G>(bits, pre_next, wn);
         pull_planes<P>(k.pull_planes, c + 1, pn);
+        meta_next = __ldg(&k.pull_meta[c + 1]);
         if (c + 2 < ce) pre_after = __ldg(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
       }
       while (c >= bound) {                 // chunk c starts a later row: the current one is done
@@ -521,36 +554,55 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
         ++row;
         bound = __ldg(&k.pull_ptr[row + 1]);
       }
+      const int base = meta >> 5, planes = meta & 31;
 #pragma unroll
       for (int g = 0; g < G; ++g) {
-        ev += (unsigned)__popc(w[g]);
         const unsigned m = warp_transpose32(w[g], lane);
-        int sum = 0;
-#pragma unroll
-        for (int q = 0; q < P - 1; ++q) sum += __popc(m & pl[q]) << q;
-        sum -= __popc(m & pl[P - 1]) << (P - 1);
-        acc[g] += sum;
+        acc[g] += base * __popc(m) + plane_sum<P>(m, pl, planes);
       }
 #pragma unroll
       for (int g = 0; g < G; ++g) w[g] = wn[g];
 #pragma unroll
       for (int q = 0; q < P; ++q) pl[q] = pn[q];
+      meta = meta_next;
       pre_next = pre_after;
     }
     int* dst = ring + (size_t)row * k.batch + lane;      // the last row with inputs
 #pragma unroll
     for (int g = 0; g < G; ++g)
       if (acc[g]) dst[g * 32] += acc[g];
+    if (k.events) {                                      // events of presynaptic neurons r0 .. r1
+      for (int j = r0 + lane; j < r1; j += 32) {
+        unsigned wj[G];
+        pull_words<G>(bits, j, wj);
+        int fl = 0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) fl += __popc(wj[g]);
+        if (fl) ev += (unsigned long long)fl * (unsigned)(__ldg(&k.out_ptr[j + 1]) - __ldg(&k.out_ptr[j]));
+      }
+    }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
   if (k.events && lane == 0 && ev) atomicAdd(k.events, ev);
 }
 
+// The pull kernel uses no shared memory: it asks for the largest L1, where part of the step's
+// raster (the spike words its gathers read, 8 B per neuron at 64 flies) stays resident.
+template <int G, int P>
+static void launch_pull_gp(const LifK& k, int s, int grid, cudaStream_t st) {
+  static bool carved = false;
+  if (!carved) {
+    cudaFuncSetAttribute(lif_pull_kernel<G, P>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    carved = true;
+  }
+  lif_pull_kernel<G, P><<<grid, 256, 0, st>>>(k, s);
+}
+
 template <int G>
 static int launch_pull_g(const LifK& k, int s, int grid, cudaStream_t st) {
-  if (k.pull_nplanes == 8) lif_pull_kernel<G, 8><<<grid, 256, 0, st>>>(k, s);
-  else lif_pull_kernel<G, 16><<<grid, 256, 0, st>>>(k, s);
+  if (k.pull_nplanes == 8) launch_pull_gp<G, 8>(k, s, grid, st);
+  else launch_pull_gp<G, 16>(k, s, grid, st);
   return (int)cudaGetLastError();
 }
 
@@ -1471,12 +1523,12 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
     k.slow_g[c] = used ? a->slow_g[c] : nullptr;
   }
   k.pull_ptr = a->pull_ptr; k.pull_pre = a->pull_pre; k.pull_planes = a->pull_planes;
-  k.pull_nplanes = a->pull_nplanes;
+  k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta;
   if (a->flags & FLYB_LIF_PULL_DELIVERY) {
     const int g = a->batch / 32;
     if (a->batch % 32 || (g != 1 && g != 2 && g != 4 && g != 8) || a->ring_mode != FLYB_RING_COUNT ||
         a->launch != FLYB_LAUNCH_STEP || (a->flags & (FLYB_LIF_DEFER_DELIVERY | FLYB_LIF_STD)) || a->clock_k ||
-        a->slow_classes || !a->raster || !a->pull_ptr || !a->pull_pre || !a->pull_planes ||
+        a->slow_classes || !a->raster || !a->pull_ptr || !a->pull_pre || !a->pull_planes || !a->pull_meta ||
         (a->pull_nplanes != 8 && a->pull_nplanes != 16) || (reinterpret_cast<uintptr_t>(a->raster) & 15) ||
         (reinterpret_cast<uintptr_t>(a->pull_planes) & 15))
       return FLYB_EINVAL;

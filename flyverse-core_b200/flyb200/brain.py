@@ -130,9 +130,12 @@ def clock_coefficients(p: LIFParams, std_on: bool, max_period: int, slow_tau=())
 def pull_inputs(W, w_syn: float):
     """The inputs of every neuron for FLYB_LIF_PULL_DELIVERY, from W[post, pre] = w_syn x signed
     integer counts: (pull_ptr int32 [N+1] in 32-entry chunks, pull_pre int32 [chunks * 32] with -1
-    padding the last chunk of a row, pull_planes uint32 [chunks * P] where bit l of plane p is bit
-    p of entry l's count in P-bit two's complement, P = 8 or 16), or None when the weights are not
-    such counts or a count needs more than 16 bits."""
+    padding the last chunk of a row, pull_planes uint32 [chunks * S], pull_meta int32 [chunks], S).
+    A row's inputs are sorted by count, so a chunk's counts lie close together: it stores its
+    smallest count as the base and each entry's excess over it in as few bit planes as that range
+    needs (meta = base << 5 | planes; bit l of plane p = bit p of entry l's excess); S, the plane
+    stride, is 8 or 16. None when the weights are not such counts or a chunk's range needs more
+    than 16 bits."""
     Wr = sp.csr_matrix(W, dtype=np.float32)
     Wr.sum_duplicates()
     Wr.sort_indices()
@@ -140,24 +143,38 @@ def pull_inputs(W, w_syn: float):
     if counts is None:
         return None
     counts = counts.astype(np.int64)
-    lo, hi = (int(counts.min()), int(counts.max())) if counts.size else (0, 0)
-    P = 8 if -128 <= lo and hi <= 127 else (16 if -32768 <= lo and hi <= 32767 else 0)
-    if not P:
-        return None
     n = Wr.shape[0]
     deg = np.diff(Wr.indptr).astype(np.int64)
+    row = np.repeat(np.arange(n), deg)
+    order = np.lexsort((counts, row))                 # by row, then by count
+    pre_sorted, cnt_sorted = Wr.indices[order], counts[order]
     ptr = np.concatenate([[0], np.cumsum((deg + 31) // 32)])
     chunks = int(ptr[-1])
-    row = np.repeat(np.arange(n), deg)
     pos = ptr[row] * 32 + (np.arange(Wr.nnz) - np.repeat(Wr.indptr[:-1].astype(np.int64), deg))
+    chunk_of = pos // 32
     pre = np.full(chunks * 32, -1, np.int32)
-    pre[pos] = Wr.indices
-    u = np.zeros(chunks * 32, np.uint64)
-    u[pos] = (counts & ((1 << P) - 1)).astype(np.uint64)
-    u = u.reshape(chunks, 32)
+    pre[pos] = pre_sorted
+    base = np.zeros(chunks, np.int64)
+    if Wr.nnz:
+        base_min = np.full(chunks, np.iinfo(np.int64).max)
+        np.minimum.at(base_min, chunk_of, cnt_sorted)
+        base = np.where(base_min == np.iinfo(np.int64).max, 0, base_min)
+    excess = np.zeros(chunks * 32, np.int64)
+    excess[pos] = cnt_sorted - base[chunk_of]
+    top = excess.reshape(chunks, 32).max(axis=1) if chunks else np.zeros(0, np.int64)
+    planes_needed = np.array([int(t).bit_length() for t in top], np.int64)
+    if planes_needed.size and planes_needed.max() > 16:
+        return None
+    if base.size and (base.min() < -(1 << 26) or base.max() >= (1 << 26)):
+        return None
+    S = 8 if not planes_needed.size or planes_needed.max() <= 8 else 16
+    u = excess.astype(np.uint64).reshape(chunks, 32)
     lanes = np.arange(32, dtype=np.uint64)
-    planes = np.stack([(((u >> np.uint64(q)) & np.uint64(1)) << lanes).sum(axis=1) for q in range(P)], axis=1)
-    return ptr.astype(np.int32), pre, planes.astype(np.uint32).ravel(), P
+    planes = np.zeros((chunks, S), np.uint64)
+    for q in range(S):
+        planes[:, q] = (((u >> np.uint64(q)) & np.uint64(1)) << lanes).sum(axis=1)
+    meta = ((base << 5) | planes_needed).astype(np.int32)
+    return ptr.astype(np.int32), pre, planes.astype(np.uint32).ravel(), meta, S
 
 
 def out_edges(W, w_syn: float, prefer: str = "auto", std_on: bool = False):
@@ -401,7 +418,7 @@ class Brain:
     def _set_pull(self, a) -> None:
         """Point the arguments at the pull tables (built from the shaped weights on first use)."""
         if not self._pull_active():
-            a.pull_ptr = a.pull_pre = a.pull_planes = None
+            a.pull_ptr = a.pull_pre = a.pull_planes = a.pull_meta = None
             a.pull_nplanes = 0
             return
         key = self._weights_version
@@ -409,10 +426,10 @@ class Brain:
             t = pull_inputs(self._W_cpu, self.p.w_syn)
             if t is None:
                 raise ValueError("pull delivery needs weights of w_syn x counts within 16 bits")
-            ptr, pre, planes, P = t
-            self._pull_t = tuple(torch.from_numpy(x).to(self.device) for x in (ptr, pre, planes.view(np.int32)))
-            self._pull_planes_n, self._pull_key = P, key
-        a.pull_ptr, a.pull_pre, a.pull_planes = (x.data_ptr() for x in self._pull_t)
+            ptr, pre, planes, meta, S = t
+            self._pull_t = tuple(torch.from_numpy(x).to(self.device) for x in (ptr, pre, planes.view(np.int32), meta))
+            self._pull_planes_n, self._pull_key = S, key
+        a.pull_ptr, a.pull_pre, a.pull_planes, a.pull_meta = (x.data_ptr() for x in self._pull_t)
         a.pull_nplanes = self._pull_planes_n
 
     # ------------------------------------------------------------------ per-neuron clocks

@@ -1,14 +1,17 @@
 """A short, eager run of the whole-fly step for profilers (every kernel launched separately).
 
-    python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic|tracer]
+    python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic|tracer|pull]
                               [--lif-block 256] [--lif-ipt 0|1|2|4] [--lif-staged] [--lif-defer] [--lif-grid 0]
+                              [--lif-pull] [--density 0.024]
                               [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
                               [--no-overlap]
     python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
 `--steps` steps of the chosen part. Used for the launch list and the per-kernel captures whose
-summaries live in profiles/. `--breakdown` instead times each stage of the step on its own with
+summaries live in profiles/. `--part pull` fills the LIF spike history with random spikes at
+`--density` (per neuron and fly; 0.024 is the whole fly's steady firing at 64 flies) and runs the
+pull delivery of one step `--steps` times. `--breakdown` instead times each stage of the step on its own with
 CUDA events (stream-ordered, warm L2) and prints one JSON line of microseconds per stage.
 """
 from __future__ import annotations
@@ -99,12 +102,38 @@ def trace_eyes(args) -> None:
           f"{float(out.mean()):.4f}")
 
 
+def pull_steps(eng, steps: int, density: float) -> None:
+    """The pull delivery of one LIF step, `steps` times, from a spike history filled at `density`."""
+    import ctypes as ct
+    from . import _abi
+    b = eng.lif
+    if not b._pull_active():
+        raise ValueError("pull delivery needs 32, 64, 128 or 256 flies and the count ring")
+    g = torch.Generator(device=b.device).manual_seed(1)
+    bits = (torch.rand(*b._hist.shape, 32, device=b.device, generator=g) < density).to(torch.int64)
+    words = (bits << torch.arange(32, device=b.device)).sum(-1)
+    b._hist.copy_(torch.where(words >= 2**31, words - 2**32, words).to(torch.int32))
+    del bits, words
+    a = b._args
+    a.flags, a.nsteps, a.n_first, a.n_count = b._flags(False), 1, 0, 0
+    b._set_pull(a)
+    stream = torch.cuda.current_stream(b.device).cuda_stream
+    for _ in range(steps):
+        rc = _abi.lib().flyb_lif_pull(ct.byref(a), stream)
+        if rc:
+            raise RuntimeError(f"flyb_lif_pull: error {rc}")
+    torch.cuda.synchronize()
+    print(f"pulled {steps} steps at batch {b.B}, density {density}: {int(b._pull_t[1].numel()) // 32:,} chunks")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--batch", type=int, default=64)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=2)
-    ap.add_argument("--part", default="whole", choices=["whole", "lif", "optic", "tracer"])
+    ap.add_argument("--part", default="whole", choices=["whole", "lif", "optic", "tracer", "pull"])
+    ap.add_argument("--lif-pull", action="store_true", help="LIF spikes delivered by the pull kernel")
+    ap.add_argument("--density", type=float, default=0.024, help="spike density for --part pull")
     ap.add_argument("--breakdown", action="store_true")
     ap.add_argument("--lif-block", type=int, default=256)
     ap.add_argument("--lif-ipt", type=int, default=0, help="LIF items per thread (0: automatic)")
@@ -123,6 +152,7 @@ def main() -> None:
     eng = WholeFly(cfg, args.batch, device="cuda", seed=1, launch="step", overlap=not args.no_overlap)
     eng.lif.block, eng.lif.items_per_thread, eng.lif.staged = args.lif_block, args.lif_ipt, args.lif_staged
     eng.lif.grid, eng.lif.defer = args.lif_grid, args.lif_defer
+    eng.lif.pull = args.lif_pull or args.part == "pull"
     eng.optic.launch, eng.optic.variant, eng.optic.grid = args.optic_launch, args.optic_variant, args.optic_grid
     eng.lif._make_args()
     eng.optic.pr_in.normal_(0.0, 0.2)
@@ -132,6 +162,9 @@ def main() -> None:
         res = breakdown(eng, max(10, args.steps))
         eng.lif.check()
         print(json.dumps({"batch": args.batch, "us": res}))
+        return
+    if args.part == "pull":
+        pull_steps(eng, args.steps, args.density)
         return
     for _ in range(args.steps):
         if args.part == "whole":

@@ -178,8 +178,8 @@ class WholeFly:
         per = 4 * (5 * 2 + 4 + 1)
         total = self.cfg.n_spiking * (self.B * per + 4)
         if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
-            ptr, pre, planes = self.lif._pull_t
-            total += pre.numel() * 4 + planes.numel() * 4 + self.cfg.n_spiking * self.B * 4 * 2
+            ptr, pre, planes, meta = self.lif._pull_t
+            total += pre.numel() * 4 + planes.numel() * 4 + meta.numel() * 4 + self.cfg.n_spiking * self.B * 4 * 2
         return total
 
     def optic_bytes_per_step(self) -> int:

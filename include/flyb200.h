@@ -197,13 +197,15 @@ typedef struct flyb_lif_args {
   float* g_slow;                                    /* [n][batch] summed tone (mV)       */
   /* FLYB_LIF_PULL_DELIVERY: the inputs of each neuron (rows of W[post, pre]) in chunks of 32
    * entries, a row's last chunk padded with pre = -1: pull_ptr [n+1] first chunk of each row,
-   * pull_pre [chunks][32] presynaptic neuron, pull_planes [chunks][pull_nplanes] the chunk's signed
-   * synapse counts as bit planes (bit l of plane p = bit p of entry l's count in pull_nplanes-bit
-   * two's complement; pull_nplanes 8 or 16). */
+   * pull_pre [chunks][32] presynaptic neuron, pull_meta [chunks] = (base << 5) | planes: entry l
+   * of the chunk carries count base + d_l, 0 <= d_l < 2^planes, planes <= pull_nplanes;
+   * pull_planes [chunks][pull_nplanes] the d_l as bit planes (bit l of plane p = bit p of d_l);
+   * pull_nplanes (the plane stride) 8 or 16. */
   const int* pull_ptr;
   const int* pull_pre;
   const unsigned* pull_planes;
   int pull_nplanes;
+  const int* pull_meta;
 } flyb_lif_args;
 
 /* flyb_lif_args.slow_mode */
