@@ -468,10 +468,17 @@ __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes,
 
 // sum_{p < planes} 2^p popc(m & pl[p]) for a warp-uniform plane count (a uniform branch, no
 // predicated-off work).
-template <int P>
-__device__ __forceinline__ int plane_sum(unsigned m, const unsigned (&pl)[P], int planes) {
-  int sum = 0;
-#define FLYB_PLANE(q) case q + 1: sum += __popc(m & pl[q]) << q; [[fallthrough]];
+template <int G, int P, int Q>
+__device__ __forceinline__ void add_plane(const unsigned (&m)[G], const unsigned (&pl)[P], int (&sum)[G]) {
+#pragma unroll
+  for (int g = 0; g < G; ++g) sum[g] += __popc(m[g] & pl[Q]) << Q;
+}
+
+// sum[g] += sum_{p < planes} 2^p popc(m[g] & pl[p]) for every group, dispatched once on the
+// warp-uniform plane count (a uniform branch, no predicated-off work).
+template <int G, int P>
+__device__ __forceinline__ void plane_sums(const unsigned (&m)[G], const unsigned (&pl)[P], int planes, int (&sum)[G]) {
+#define FLYB_PLANE(q) case q + 1: add_plane<G, P, q>(m, pl, sum); [[fallthrough]];
   if constexpr (P > 8) {
     if (planes > 8) {
       switch (planes) {
@@ -488,7 +495,6 @@ __device__ __forceinline__ int plane_sum(unsigned m, const unsigned (&pl)[P], in
     default: break;
   }
 #undef FLYB_PLANE
-  return sum;
 }
 
 // Pull delivery (FLYB_LIF_PULL_DELIVERY): each warp owns a contiguous block of postsynaptic rows
@@ -554,12 +560,17 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
         ++row;
         bound = __ldg(&k.pull_ptr[row + 1]);
       }
-      const int base = meta >> 5, planes = meta & 31;
+      const int base = meta >> 5;
+      unsigned m[G];
+      int add[G];
 #pragma unroll
       for (int g = 0; g < G; ++g) {
-        const unsigned m = warp_transpose32(w[g], lane);
-        acc[g] += base * __popc(m) + plane_sum<P>(m, pl, planes);
+        m[g] = warp_transpose32(w[g], lane);
+        add[g] = base * __popc(m[g]);
       }
+      plane_sums<G, P>(m, pl, meta & 31, add);
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[g] += add[g];
 #pragma unroll
       for (int g = 0; g < G; ++g) w[g] = wn[g];
 #pragma unroll
