@@ -63,6 +63,7 @@ struct LifK {
   const unsigned* __restrict__ pull_planes;    // [chunks][pull_nplanes] count bit planes
   int pull_nplanes;                            // plane stride per chunk (8 or 16)
   const int* __restrict__ pull_meta;           // per chunk: base count << 5 | planes used
+  int pull_lag;                                // flyb_lif_pull: steps before the device clock
   LifP P;
 };
 
@@ -515,7 +516,8 @@ template <int G, int P>
 __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
   const Clk clk = read_clock(k);
   const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
-  const int rsl = k.raster_slots > 0 ? slot_after(clk.raster_pos, s, k.raster_slots) : s;
+  // s < 0 (pull_lag): a step before the device clock; its raster slot wraps backwards
+  const int rsl = k.raster_slots > 0 ? slot_after(clk.raster_pos, s >= 0 ? s : k.raster_slots + s, k.raster_slots) : s;
   const unsigned* __restrict__ bits = k.raster + (size_t)rsl * k.words;
   int* ring = (int*)k.ring + (size_t)ws * k.n * k.batch;
   const int lane = threadIdx.x & 31;
@@ -1534,7 +1536,9 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
     k.slow_g[c] = used ? a->slow_g[c] : nullptr;
   }
   k.pull_ptr = a->pull_ptr; k.pull_pre = a->pull_pre; k.pull_planes = a->pull_planes;
-  k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta;
+  k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta; k.pull_lag = a->pull_lag;
+  if (a->pull_lag < 0 || a->pull_lag > 1 || (a->pull_lag && (a->raster_slots <= 0 || a->n_delay < 2)))
+    return FLYB_EINVAL;
   if (a->flags & FLYB_LIF_PULL_DELIVERY) {
     const int g = a->batch / 32;
     if (a->batch % 32 || (g != 1 && g != 2 && g != 4 && g != 8) || a->ring_mode != FLYB_RING_COUNT ||
@@ -1570,7 +1574,7 @@ FLYB_API int flyb_lif_pull(const flyb_lif_args* a, void* stream) {
   const int rc = make_lif_k(a, k);
   if (rc) return rc;
   if (!(k.flags & FLYB_LIF_PULL_DELIVERY)) return FLYB_EINVAL;
-  return launch_pull(k, 0, (cudaStream_t)stream);
+  return launch_pull(k, -k.pull_lag, (cudaStream_t)stream);
 }
 
 FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {

@@ -542,14 +542,30 @@ class Brain:
         if rc:
             raise RuntimeError(f"flyb_lif_run: error {rc}")
 
-    def advance(self, n_steps: int = 1) -> None:
+    def pull_previous(self) -> None:
+        """Pull delivery of the step before the device clock (after `advance(1, pull=False)`), on
+        the current stream: it may run beside the next step's ranges and must end before the next
+        `advance`."""
+        a = self._args
+        a.flags, a.nsteps, a.pull_lag = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY, 1, 1
+        self._set_pull(a)
+        try:
+            with torch.cuda.device(self.device):
+                rc = self._lib.flyb_lif_pull(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
+        finally:
+            a.pull_lag = 0
+        if rc:
+            raise RuntimeError(f"flyb_lif_pull: error {rc}")
+
+    def advance(self, n_steps: int = 1, *, pull: bool = True) -> None:
         """End `n_steps` steps run by ranges: move the device clock (ring and history positions,
-        Philox step) on, as the end of `step` does."""
+        Philox step) on, as the end of `step` does. Under pull delivery the step's spikes are
+        pulled first, unless `pull` is False (then `pull_previous` delivers them)."""
         a = self._args
         a.flags = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY
         a.nsteps = int(n_steps)
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        if self._pull_active():          # the ranges recorded their spikes: deliver them, then advance
+        if self._pull_active() and pull:  # the ranges recorded their spikes: deliver them, then advance
             if n_steps != 1:
                 raise ValueError("with pull delivery, ranges advance one step at a time")
             self._set_pull(a)

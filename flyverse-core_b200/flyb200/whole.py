@@ -76,6 +76,7 @@ class WholeFly:
         self.a_pr = self.photo.a_pr                       # [n_pr][B]: the stage's output
         self.steps_taken = 0
         self._fork = (torch.cuda.Stream(self.device, priority=-1), torch.cuda.Stream(self.device))
+        self._pull_stream = torch.cuda.Stream(self.device)
 
     @property
     def launches_per_step(self) -> int:
@@ -137,6 +138,10 @@ class WholeFly:
         overlap = self.overlapping
         main = torch.cuda.current_stream(self.device)
         hi, side = self._fork
+        # under pull delivery a step's pull runs on its own stream beside the next step and joins
+        # before that step's clock advance (it reads the clock of the step it delivers)
+        lag = overlap and self.lif._pull_active() and self.lif.n_delay >= 2
+        pulling = False
         for k in range(int(n)):
             if before is not None:
                 before(k)
@@ -153,12 +158,23 @@ class WholeFly:
                     self.lif.step_range(self.split, self.cfg.n_spiking - self.split)
                 main.wait_stream(hi)
                 main.wait_stream(side)
-                self.lif.advance(1)
+                if lag:
+                    if pulling:
+                        main.wait_stream(self._pull_stream)
+                    self.lif.advance(1, pull=False)
+                    self._pull_stream.wait_stream(main)
+                    with torch.cuda.stream(self._pull_stream):
+                        self.lif.pull_previous()
+                    pulling = True
+                else:
+                    self.lif.advance(1)
             else:
                 self._optic_and_drive(drive)
                 self.lif.step(1)
             if after is not None:
                 after(k)
+        if pulling:
+            main.wait_stream(self._pull_stream)
         if torch.cuda.is_current_stream_capturing():
             self.optic.pin_dr(cur0)
         self.steps_taken += int(n)

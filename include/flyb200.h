@@ -206,6 +206,9 @@ typedef struct flyb_lif_args {
   const unsigned* pull_planes;
   int pull_nplanes;
   const int* pull_meta;
+  int pull_lag;          /* flyb_lif_pull: 0 delivers the step the device clock is at (before
+                            flyb_lif_advance), 1 the step before it (after the advance; needs
+                            raster_slots > 0 and n_delay >= 2) */
 } flyb_lif_args;
 
 /* flyb_lif_args.slow_mode */
@@ -222,7 +225,10 @@ int flyb_lif_run(const flyb_lif_args* a, void* stream);
 
 /* FLYB_LIF_PULL_DELIVERY over neuron ranges: after every range of a step ran (each with
  * FLYB_LIF_NO_ADVANCE and nsteps 1), delivers that step's spikes from the raster into the write
- * slot; then flyb_lif_advance. The arguments are those of the launches (any range). */
+ * slot; then flyb_lif_advance. With pull_lag 1 it delivers the step before the clock instead, so
+ * it may run after the advance, beside the next step's updates (which touch neither that step's
+ * raster slot nor its write slot), as long as it completes before the next advance. The
+ * arguments are those of the launches (any range). */
 int flyb_lif_pull(const flyb_lif_args* a, void* stream);
 
 /* Entries a FLYB_LIF_DEFER_DELIVERY step of these arguments can write when every item of the

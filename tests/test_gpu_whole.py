@@ -253,3 +253,43 @@ def test_pull_delivery_equals_scatter_at_high_activity(B, staged):
         assert torch.equal(push.ring, pull.ring)
         assert push.synaptic_events == pull.synaptic_events
     assert float(pull.spike_counts.sum()) / (48 * B * cfg.c.n) > 0.005     # dense firing
+
+
+def test_lagged_pull_beside_the_next_step_equals_one_step_per_call():
+    """Under pull delivery the whole-fly step delivers each step's spikes on a side stream beside
+    the next step (joined before that step's clock advance): ten steps per call, eager or from a
+    captured graph, end bit-identical to one step per call (each call joins its last pull)."""
+    cfg = small_fly()
+    B = 32
+    a_pr = torch.from_numpy((np.random.default_rng(2).standard_normal((cfg.optic.n_pr, B)) * 0.5)
+                            .astype(np.float32)).cuda()
+    engs = []
+    for _ in range(3):
+        eng = WholeFly(cfg, B, device="cuda", seed=3, launch="step")
+        eng.lif.pull, eng.lif.staged = True, True
+        eng.lif._make_args()
+        eng.set_photoreceptors(a_pr)
+        engs.append(eng)
+    single, batched, graphed = engs
+    for _ in range(40):
+        single.step(1)
+    for _ in range(4):
+        batched.step(10)
+    graphed.step(2)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            graphed.step(19)
+    torch.cuda.current_stream().wait_stream(s)
+    g.replay()
+    graphed.step(19)
+    torch.cuda.synchronize()
+    for eng in (batched, graphed):
+        for k in ("v", "g", "rate", "spike_counts", "refrac"):
+            assert torch.equal(getattr(single.lif, k), getattr(eng.lif, k)), k
+        assert torch.equal(single.lif.ring, eng.lif.ring)
+        assert torch.equal(single.optic.v_s, eng.optic.v_s)
+    assert single.lif.synaptic_events == batched.lif.synaptic_events > 0
+    del g
