@@ -457,12 +457,14 @@ __device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, in
   }
 }
 
+// The input tables stream through once per step (cache-streaming loads), leaving L1 to the
+// raster words the gathers reuse.
 template <int P>
 __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes, long long c, unsigned (&pl)[P]) {
   const uint4* src = reinterpret_cast<const uint4*>(planes + (size_t)c * P);
 #pragma unroll
   for (int q = 0; q < P; q += 4) {
-    const uint4 v = __ldg(src + q / 4);
+    const uint4 v = __ldcs(src + q / 4);
     pl[q] = v.x; pl[q + 1] = v.y; pl[q + 2] = v.z; pl[q + 3] = v.w;
   }
 }
@@ -538,10 +540,10 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
     unsigned w[G], pl[P];
     int meta = 0, pre_next = -1;
     if (c < ce) {
-      pull_words<G>(bits, __ldg(&k.pull_pre[(size_t)c * 32 + lane]), w);
+      pull_words<G>(bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), w);
       pull_planes<P>(k.pull_planes, c, pl);
-      meta = __ldg(&k.pull_meta[c]);
-      if (c + 1 < ce) pre_next = __ldg(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
+      meta = __ldcs(&k.pull_meta[c]);
+      if (c + 1 < ce) pre_next = __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
     }
     for (; c < ce; ++c) {
       unsigned wn[G], pn[P];
@@ -549,8 +551,8 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
       if (c + 1 < ce) {
         pull_words<G>(bits, pre_next, wn);
         pull_planes<P>(k.pull_planes, c + 1, pn);
-        meta_next = __ldg(&k.pull_meta[c + 1]);
-        if (c + 2 < ce) pre_after = __ldg(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
+        meta_next = __ldcs(&k.pull_meta[c + 1]);
+        if (c + 2 < ce) pre_after = __ldcs(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
       }
       while (c >= bound) {                 // chunk c starts a later row: the current one is done
         int* dst = ring + (size_t)row * k.batch + lane;
