@@ -609,7 +609,9 @@ def arm_config(world: int) -> dict:
     return {"workload": "whole fly 167,106 neurons (89,390 optic + 71,618 LIF + 6,098 sensory), 25.6M edges, "
                         "dt 0.1 ms, optic<->LIF coupling every step", "batch_per_gpu": BATCH,
             "flies_total": BATCH * world, "l2": "state of 64 flies > 126 MB L2; no flush needed",
-            "parallelism": f"fly shards x{world}, no per-step collective"}
+            "parallelism": f"fly shards x{world}, no per-step collective",
+            "state": f"our arm: steady firing after {SETTLE_STEPS} settling steps (onset from rest reported "
+                     f"under 'onset'); reference arm: a sample of the first steps from rest"}
 
 
 def reference_arm(args) -> None:
