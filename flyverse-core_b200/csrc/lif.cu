@@ -603,21 +603,23 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
 }
 
 // The pull kernel uses no shared memory: it asks for the largest L1, where part of the step's
-// raster (the spike words its gathers read, 8 B per neuron at 64 flies) stays resident.
+// raster (the spike words its gathers read, 8 B per neuron at 64 flies) stays resident, and runs
+// as one wave of resident blocks.
 template <int G, int P>
-static void launch_pull_gp(const LifK& k, int s, int grid, cudaStream_t st) {
-  static bool carved = false;
-  if (!carved) {
+static void launch_pull_gp(const LifK& k, int s, int sms, cudaStream_t st) {
+  static int per_sm = 0;                 // resident blocks: one wave, each warp a longer row stream
+  if (!per_sm) {
     cudaFuncSetAttribute(lif_pull_kernel<G, P>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    carved = true;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, P>, 256, 0);
+    if (per_sm < 1) per_sm = 1;
   }
-  lif_pull_kernel<G, P><<<grid, 256, 0, st>>>(k, s);
+  lif_pull_kernel<G, P><<<sms * per_sm, 256, 0, st>>>(k, s);
 }
 
 template <int G>
-static int launch_pull_g(const LifK& k, int s, int grid, cudaStream_t st) {
-  if (k.pull_nplanes == 8) launch_pull_gp<G, 8>(k, s, grid, st);
-  else launch_pull_gp<G, 16>(k, s, grid, st);
+static int launch_pull_g(const LifK& k, int s, int sms, cudaStream_t st) {
+  if (k.pull_nplanes == 8) launch_pull_gp<G, 8>(k, s, sms, st);
+  else launch_pull_gp<G, 16>(k, s, sms, st);
   return (int)cudaGetLastError();
 }
 
@@ -625,12 +627,11 @@ static int launch_pull(const LifK& k, int s, cudaStream_t st) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = sms * 8;
   switch (k.batch / 32) {
-    case 1: return launch_pull_g<1>(k, s, grid, st);
-    case 2: return launch_pull_g<2>(k, s, grid, st);
-    case 4: return launch_pull_g<4>(k, s, grid, st);
-    case 8: return launch_pull_g<8>(k, s, grid, st);
+    case 1: return launch_pull_g<1>(k, s, sms, st);
+    case 2: return launch_pull_g<2>(k, s, sms, st);
+    case 4: return launch_pull_g<4>(k, s, sms, st);
+    case 8: return launch_pull_g<8>(k, s, sms, st);
     default: return FLYB_EINVAL;
   }
 }
