@@ -38,15 +38,18 @@ def test_pull_delivery_arguments_are_validated_before_any_launch():
     32, 64, 128 or 256 flies, the fixed-point ring, depression, persistent launches, missing tables,
     a lag without a history ring) with FLYB_EINVAL, before touching the device."""
     import ctypes as ct
+    import numpy as np
     lib = _abi.lib()
-    fake = 4096                                   # never dereferenced: validation fails first
+    fake = 4096                # device pointers are never dereferenced: validation fails first
+    params = np.zeros(64, np.float32)             # the one host array the validation reads
 
     def args(**kw):
         a = _abi.LifArgs(n=256, batch=64, n_delay=18, ring_slots=19, ring_mode=_abi.RING_COUNT, nsteps=1,
                          flags=_abi.LIF_PULL_DELIVERY, launch=_abi.LAUNCH_STEP, raster_slots=18)
         for f in ("out_ptr", "v", "g", "refrac", "adapt", "res", "rate", "counts", "spikes", "drive", "poisson_p",
-                  "active", "params", "ring", "raster", "pull_ptr", "pull_pre", "pull_planes", "pull_meta"):
+                  "active", "ring", "raster", "pull_ptr", "pull_pre", "pull_planes", "pull_meta"):
             setattr(a, f, fake)
+        a.params = params.ctypes.data
         a.pull_nplanes = 8
         for k, v in kw.items():
             setattr(a, k, v)
