@@ -739,7 +739,7 @@ def main() -> None:
         "cpu_baseline": cpu,
         "e2e": e2e,
         "autotune": {k: {kk: vv for kk, vv in v.items()} for k, v in eng.tuned.items()},
-        "gpu_launches": eng.launches_per_step * timed_steps,
+        "gpu_launches": eng.launches(chunk) * reps,
         "clocks": clocks,
     }
     print(json.dumps(line))

@@ -63,7 +63,10 @@ struct LifK {
   const unsigned* __restrict__ pull_planes;    // [chunks][pull_nplanes] count bit planes
   int pull_nplanes;                            // plane stride per chunk (8 or 16)
   const int* __restrict__ pull_meta;           // per chunk: base count << 5 | planes used
-  int pull_lag;                                // flyb_lif_pull: steps before the device clock
+  int pull_group;                              // L: steps a pull delivers together
+  int pull_phase;                              // runs that pull themselves: first step's index mod L
+  unsigned* pull_bits;                         // [2][words][L] spike words of the last two groups
+  long long* pull_state;                       // {first undelivered step, its ring position, counter}
   LifP P;
 };
 
@@ -413,52 +416,63 @@ __global__ void __launch_bounds__(256) lif_scatter_kernel(LifK k, int s) {
 
 // 32 x 32 bit transpose across a warp: lane r holds row r (bit c = column c) on entry and
 // column r (bit c = row c) on return. Five exchanges: at distance j a lane keeps the half of each
-// 2j-bit group on its own side and takes the partner's other half, rotated into place.
-__device__ __forceinline__ unsigned warp_transpose32(unsigned x, int lane) {
-  constexpr unsigned M[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+// 2j-bit group on its own side and takes the partner's other half, rotated into place. The
+// rotation and the kept bits depend only on the lane's side of each exchange, so they are
+// computed once per thread.
+struct Transpose32 {
+  int lane;
+  __device__ __forceinline__ explicit Transpose32(int l) : lane(l) {}
+  __device__ __forceinline__ unsigned operator()(unsigned x) const {
+    constexpr unsigned M[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
 #pragma unroll
-  for (int q = 0; q < 5; ++q) {
-    const int j = 16 >> q;
-    const bool hi = lane & j;
-    const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
-    const unsigned t = __funnelshift_l(y, y, hi ? 32 - j : j);
-    const unsigned keep = hi ? ~M[q] : M[q];
-    x = (x & keep) | (t & ~keep);
+    for (int q = 0; q < 5; ++q) {
+      const int j = 16 >> q;
+      const bool hi = lane & j;
+      const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
+      const unsigned t = __funnelshift_l(y, y, hi ? 32 - j : j);
+      const unsigned keep = hi ? ~M[q] : M[q];
+      x = (x & keep) | (t & ~keep);
+    }
+    return x;
   }
-  return x;
+};
+
+// Pull delivery (FLYB_LIF_PULL_DELIVERY) reads spike words from `pull_bits`, which the update
+// kernels fill beside the spike history: the words of the last two groups of L consecutive steps,
+// laid out [group parity][word][L], so one neuron's words of a whole group (G words per step, G =
+// batch / 32) are G * L adjacent words. L = 8 / G makes that one 32-byte sector: the gather of an
+// input then fetches every step of the group at once, where a per-step pull fetched a whole
+// sector for G words of one step.
+__device__ __forceinline__ size_t pull_word_index(const LifK& k, long long step, long long word) {
+  const long long L = k.pull_group;
+  return (size_t)(((step / L) & 1) * k.words + word) * (size_t)L + (size_t)(step % L);
 }
 
-// Pull delivery (FLYB_LIF_PULL_DELIVERY): one warp per postsynaptic row, 32 inputs per pass. Each
-// lane reads its input's spike words (one per 32 flies) from the raster of step `s`; the warp
-// transposes them so that lane f holds, for fly f of the group, the mask of the 32 inputs that
-// spiked; the chunk's counts arrive as P bit planes, so the row's input for fly f is
-// sum_p 2^p popc(mask & plane_p), the top plane weighted -2^(P-1) (two's complement). Integer and
-// exact: the ring slot ends with the sums the scatter's atomics give. Rows are added into the
-// write slot with coalesced 128-byte accesses per group of 32 flies.
-template <int G>
-__device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, int pre, unsigned (&w)[G]) {
+// One input's words of a group: NW = G * L adjacent words (16-byte aligned for NW >= 4).
+template <int NW>
+__device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, int pre, unsigned (&w)[NW]) {
   if (pre < 0) {
 #pragma unroll
-    for (int g = 0; g < G; ++g) w[g] = 0u;
+    for (int i = 0; i < NW; ++i) w[i] = 0u;
     return;
   }
-  const unsigned* src = bits + (size_t)pre * G;
-  if constexpr (G == 1) {
+  const unsigned* src = bits + (size_t)pre * NW;
+  if constexpr (NW == 1) {
     w[0] = __ldg(src);
-  } else if constexpr (G == 2) {
+  } else if constexpr (NW == 2) {
     const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
     w[0] = v.x; w[1] = v.y;
   } else {
 #pragma unroll
-    for (int g = 0; g < G; g += 4) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + g));
-      w[g] = v.x; w[g + 1] = v.y; w[g + 2] = v.z; w[g + 3] = v.w;
+    for (int i = 0; i < NW; i += 4) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src + i));
+      w[i] = v.x; w[i + 1] = v.y; w[i + 2] = v.z; w[i + 3] = v.w;
     }
   }
 }
 
-// The input tables stream through once per step (cache-streaming loads), leaving L1 to the
-// raster words the gathers reuse.
+// The input tables stream through once per pull (cache-streaming loads), leaving L1 to the spike
+// words the gathers reuse.
 template <int P>
 __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes, long long c, unsigned (&pl)[P]) {
   const uint4* src = reinterpret_cast<const uint4*>(planes + (size_t)c * P);
@@ -469,8 +483,7 @@ __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes,
   }
 }
 
-// sum_{p < planes} 2^p popc(m & pl[p]) for a warp-uniform plane count (a uniform branch, no
-// predicated-off work).
+// sum[g] += 2^Q popc(m[g] & pl[Q]) for every fly group.
 template <int G, int P, int Q>
 __device__ __forceinline__ void add_plane(const unsigned (&m)[G], const unsigned (&pl)[P], int (&sum)[G]) {
 #pragma unroll
@@ -500,99 +513,129 @@ __device__ __forceinline__ void plane_sums(const unsigned (&m)[G], const unsigne
 #undef FLYB_PLANE
 }
 
-// Pull delivery (FLYB_LIF_PULL_DELIVERY): each warp owns a contiguous block of postsynaptic rows
-// and walks their 32-input chunks as one stream. Per chunk a lane reads its input's spike words
-// (one per 32 flies) from the raster of step `s`; the warp transposes them so that lane f holds,
-// for fly f of the group, the mask of the 32 inputs that spiked. A row's inputs are sorted by
-// count, and a chunk stores its smallest count as a base and the excess of each entry in as few
-// bit planes as its range needs, so fly f gains base x popc(mask) + sum_p 2^p popc(mask &
-// plane_p). Integer and exact: the ring slot ends with the sums the scatter's atomics give. The
-// stream is software-pipelined: the spike words and planes of the next chunk and the inputs of
-// the one after are in flight while a chunk is summed. A finished row is added into the write
-// slot with coalesced 128-byte accesses per group of 32 flies. The synaptic events (out-degree x
-// flies spiking, per presynaptic neuron) are counted over the same block of neuron indices. Each
-// input is one random 8-byte gather (64 flies) from the step's raster, a 32-byte sector through
-// L1/L2: at the whole fly's 19 M inputs that sector stream bounds the kernel (~150 us at 64 flies,
-// L1TEX 67 % busy, DRAM 11 %); at 256 flies the same sectors carry four times the flies.
-template <int G, int P>
-__global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
-  const Clk clk = read_clock(k);
-  const int ws = slot_after(clk.ring_pos, s + k.n_delay, k.R);
-  // s < 0 (pull_lag): a step before the device clock; its raster slot wraps backwards
-  const int rsl = k.raster_slots > 0 ? slot_after(clk.raster_pos, s >= 0 ? s : k.raster_slots + s, k.raster_slots) : s;
-  const unsigned* __restrict__ bits = k.raster + (size_t)rsl * k.words;
-  int* ring = (int*)k.ring + (size_t)ws * k.n * k.batch;
+// a mod m in [0, m) for any sign of a (m > 0).
+__device__ __forceinline__ int pos_mod(long long a, int m) {
+  const long long r = a % m;
+  return (int)(r < 0 ? r + m : r);
+}
+
+// Pull delivery of `nsteps` (1..L) undelivered steps, starting at pull_state[0] (its ring position
+// pull_state[1]). Each warp owns a contiguous block of postsynaptic rows and walks their 32-input
+// chunks as one stream, once per group of L steps the range touches (one group when the pulls
+// follow the group ends, two when a range straddles a group end). Per chunk a lane gathers its
+// input's G * L spike words of the group (one 32-byte sector); for each step of the range the warp
+// transposes the step's G words so that lane f holds, for fly f of a group of 32, the mask of the
+// chunk's inputs that spiked, and adds base x popc(mask) + sum_p 2^p popc(mask & plane_p) (a row's
+// inputs are sorted by count; a chunk stores its smallest count as the base and the excess of each
+// entry in as few bit planes as its range needs). Integer and exact: each step's write slot ends
+// with the sums the scatter's atomics give. The chunk tables (inputs, planes, base) are read once
+// per group instead of once per step. The stream is software-pipelined (the next chunk's words and
+// planes and the inputs of the one after are in flight while a chunk is summed); a finished row is
+// added into each step's write slot with coalesced 128-byte accesses per group of 32 flies. The
+// synaptic events of presynaptic neurons in the warp's row block are counted from the same words.
+// The last block to finish moves pull_state on by nsteps (every block has read it by then).
+template <int G, int L, int P>
+__global__ void __launch_bounds__(256, 3) lif_pull_kernel(LifK k, int nsteps) {
+  constexpr int NW = G * L;
+  const long long done = k.pull_state[0];
+  const int rp_done = (int)k.pull_state[1];
   const int lane = threadIdx.x & 31;
+  const Transpose32 transpose(lane);
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int per = (int)((k.n + warps - 1) / warps);
   const int r0 = (int)(wid * per < k.n ? wid * per : k.n);
   const int r1 = r0 + per < k.n ? r0 + per : k.n;
+  const size_t slot = (size_t)k.n * k.batch;
   unsigned long long ev = 0;
-  if (r0 < r1) {
+  const long long end = done + nsteps;
+  for (long long grp = done / L; grp * L < end; ++grp) {
+    const int lo = (int)((done > grp * L ? done : grp * L) - grp * L);          // steps [lo, hi) of the group
+    const int hi = (int)((end < (grp + 1) * L ? end : (grp + 1) * L) - grp * L);
+    const unsigned* __restrict__ bits = k.pull_bits + (size_t)(grp & 1) * k.words * L;
+    // write slot of step grp * L + u: D slots after its read slot (consecutive steps, consecutive slots)
+    const int ws0 = pos_mod(rp_done + (grp * L - done) + k.n_delay, k.R);
+    if (r0 >= r1) continue;
     const int ce = __ldg(&k.pull_ptr[r1]);
     int c = __ldg(&k.pull_ptr[r0]);
     int row = r0, bound = __ldg(&k.pull_ptr[r0 + 1]);
-    int acc[G];
+    int acc[L][G];
 #pragma unroll
-    for (int g = 0; g < G; ++g) acc[g] = 0;
-    // pipeline: words + planes of chunk c, inputs of chunk c + 1
-    unsigned w[G], pl[P];
+    for (int u = 0; u < L; ++u)
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[u][g] = 0;
+    unsigned w[NW], pl[P];
     int meta = 0, pre_next = -1;
     if (c < ce) {
-      pull_words<G>(bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), w);
+      pull_words<NW>(bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), w);
       pull_planes<P>(k.pull_planes, c, pl);
       meta = __ldcs(&k.pull_meta[c]);
       if (c + 1 < ce) pre_next = __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
     }
     for (; c < ce; ++c) {
-      unsigned wn[G], pn[P];
+      unsigned wn[NW], pn[P];
       int meta_next = 0, pre_after = -1;
       if (c + 1 < ce) {
-        pull_words<G>(bits, pre_next, wn);
+        pull_words<NW>(bits, pre_next, wn);
         pull_planes<P>(k.pull_planes, c + 1, pn);
         meta_next = __ldcs(&k.pull_meta[c + 1]);
         if (c + 2 < ce) pre_after = __ldcs(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
       }
       while (c >= bound) {                 // chunk c starts a later row: the current one is done
-        int* dst = ring + (size_t)row * k.batch + lane;
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-          if (acc[g]) dst[g * 32] += acc[g];
-          acc[g] = 0;
+        for (int u = 0; u < L; ++u) {
+          if (u < lo || u >= hi) continue;
+          int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            if (acc[u][g]) dst[g * 32] += acc[u][g];
+            acc[u][g] = 0;
+          }
         }
         ++row;
         bound = __ldg(&k.pull_ptr[row + 1]);
       }
-      const int base = meta >> 5;
-      unsigned m[G];
-      int add[G];
+      const int base = meta >> 5, planes = meta & 31;
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
-        m[g] = warp_transpose32(w[g], lane);
-        add[g] = base * __popc(m[g]);
+      for (int u = 0; u < L; ++u) {
+        if (u < lo || u >= hi) continue;   // kernel-uniform: no divergence
+        unsigned m[G];
+        int add[G];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          m[g] = transpose(w[g * L + u]);
+          add[g] = base * __popc(m[g]);
+        }
+        plane_sums<G, P>(m, pl, planes, add);
+#pragma unroll
+        for (int g = 0; g < G; ++g) acc[u][g] += add[g];
       }
-      plane_sums<G, P>(m, pl, meta & 31, add);
 #pragma unroll
-      for (int g = 0; g < G; ++g) acc[g] += add[g];
-#pragma unroll
-      for (int g = 0; g < G; ++g) w[g] = wn[g];
+      for (int i = 0; i < NW; ++i) w[i] = wn[i];
 #pragma unroll
       for (int q = 0; q < P; ++q) pl[q] = pn[q];
       meta = meta_next;
       pre_next = pre_after;
     }
-    int* dst = ring + (size_t)row * k.batch + lane;      // the last row with inputs
 #pragma unroll
-    for (int g = 0; g < G; ++g)
-      if (acc[g]) dst[g * 32] += acc[g];
-    if (k.events) {                                      // events of presynaptic neurons r0 .. r1
+    for (int u = 0; u < L; ++u) {            // the last row with inputs
+      if (u < lo || u >= hi) continue;
+      int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (acc[u][g]) dst[g * 32] += acc[u][g];
+    }
+    if (k.events) {                          // events of presynaptic neurons r0 .. r1 in these steps
       for (int j = r0 + lane; j < r1; j += 32) {
-        unsigned wj[G];
-        pull_words<G>(bits, j, wj);
+        unsigned wj[NW];
+        pull_words<NW>(bits, j, wj);
         int fl = 0;
 #pragma unroll
-        for (int g = 0; g < G; ++g) fl += __popc(wj[g]);
+        for (int u = 0; u < L; ++u) {
+          if (u < lo || u >= hi) continue;
+#pragma unroll
+          for (int g = 0; g < G; ++g) fl += __popc(wj[g * L + u]);
+        }
         if (fl) ev += (unsigned long long)fl * (unsigned)(__ldg(&k.out_ptr[j + 1]) - __ldg(&k.out_ptr[j]));
       }
     }
@@ -600,45 +643,76 @@ __global__ void __launch_bounds__(256) lif_pull_kernel(LifK k, int s) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) ev += __shfl_xor_sync(0xffffffffu, ev, o);
   if (k.events && lane == 0 && ev) atomicAdd(k.events, ev);
+  // the last block to finish moves the undelivered range on (every block read it at its start)
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned long long prev = atomicAdd(reinterpret_cast<unsigned long long*>(k.pull_state + 2), 1ull);
+    if (prev == (unsigned long long)gridDim.x - 1) {
+      k.pull_state[0] = end;
+      k.pull_state[1] = pos_mod(rp_done + nsteps, k.R);
+      k.pull_state[2] = 0;
+      __threadfence();
+    }
+  }
 }
 
-// The pull kernel uses no shared memory: it asks for the largest L1, where part of the step's
-// raster (the spike words its gathers read, 8 B per neuron at 64 flies) stays resident, and runs
-// as one wave of resident blocks.
-template <int G, int P>
-static void launch_pull_gp(const LifK& k, int s, int sms, cudaStream_t st) {
+// The pull kernel uses no shared memory: it asks for the largest L1, where part of the spike words
+// its gathers read stays resident, and runs as one wave of resident blocks.
+template <int G, int L, int P>
+static void launch_pull_glp(const LifK& k, int nsteps, int sms, cudaStream_t st) {
   static int per_sm = 0;                 // resident blocks: one wave, each warp a longer row stream
   if (!per_sm) {
-    cudaFuncSetAttribute(lif_pull_kernel<G, P>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, P>, 256, 0);
+    cudaFuncSetAttribute(lif_pull_kernel<G, L, P>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, L, P>, 256, 0);
     if (per_sm < 1) per_sm = 1;
   }
-  lif_pull_kernel<G, P><<<sms * per_sm, 256, 0, st>>>(k, s);
+  lif_pull_kernel<G, L, P><<<sms * per_sm, 256, 0, st>>>(k, nsteps);
 }
 
-template <int G>
-static int launch_pull_g(const LifK& k, int s, int sms, cudaStream_t st) {
-  if (k.pull_nplanes == 8) launch_pull_gp<G, 8>(k, s, sms, st);
-  else launch_pull_gp<G, 16>(k, s, sms, st);
-  return (int)cudaGetLastError();
+template <int G, int L>
+static void launch_pull_gl(const LifK& k, int nsteps, int sms, cudaStream_t st) {
+  if (k.pull_nplanes == 8) launch_pull_glp<G, L, 8>(k, nsteps, sms, st);
+  else launch_pull_glp<G, L, 16>(k, nsteps, sms, st);
 }
 
-static int launch_pull(const LifK& k, int s, cudaStream_t st) {
+// Steps per group a batch width allows: 8 / G (one sector per input and group), or 1.
+static bool pull_group_ok(int batch, int L) {
+  const int g = batch / 32;
+  return L == 1 || L == 8 / g;
+}
+
+static int launch_pull(const LifK& k, int nsteps, cudaStream_t st) {
+  if (nsteps < 1 || nsteps > k.pull_group) return FLYB_EINVAL;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const bool grouped = k.pull_group > 1;
   switch (k.batch / 32) {
-    case 1: return launch_pull_g<1>(k, s, sms, st);
-    case 2: return launch_pull_g<2>(k, s, sms, st);
-    case 4: return launch_pull_g<4>(k, s, sms, st);
-    case 8: return launch_pull_g<8>(k, s, sms, st);
+    case 1: grouped ? launch_pull_gl<1, 8>(k, nsteps, sms, st) : launch_pull_gl<1, 1>(k, nsteps, sms, st); break;
+    case 2: grouped ? launch_pull_gl<2, 4>(k, nsteps, sms, st) : launch_pull_gl<2, 1>(k, nsteps, sms, st); break;
+    case 4: grouped ? launch_pull_gl<4, 2>(k, nsteps, sms, st) : launch_pull_gl<4, 1>(k, nsteps, sms, st); break;
+    case 8: launch_pull_gl<8, 1>(k, nsteps, sms, st); break;
     default: return FLYB_EINVAL;
   }
+  return (int)cudaGetLastError();
 }
 
-// Whether the launch pulls each step itself: pull delivery over all neurons.
+// Whether the launch pulls its steps itself: pull delivery over all neurons.
 static bool pulls_itself(const LifK& k) {
   return (k.flags & FLYB_LIF_PULL_DELIVERY) && k.t_begin == 0 && k.t_end == (long long)k.n * k.batch;
+}
+
+// A run that pulls itself delivers at every group end (local step s ends a group when the step
+// index, pull_phase + s + 1 counted from a group start, is a multiple of L) and after its last
+// step, so it ends with nothing pending. `pending` counts the steps since the last pull.
+static int pull_after_step(const LifK& k, int s, int& pending, cudaStream_t st) {
+  if (!pulls_itself(k)) return 0;
+  ++pending;
+  if ((k.pull_phase + s + 1) % k.pull_group != 0 && s != k.nsteps - 1) return 0;
+  const int rc = launch_pull(k, pending, st);
+  pending = 0;
+  return rc;
 }
 
 // One block processes work items [base, base + BLOCK*IPT) of local step `s`: update, then deliver.
@@ -809,6 +883,7 @@ __device__ __forceinline__ void lif_chunk(const LifK& k, const Clk& clk, int s, 
     if (lane % LPW == 0 && wbase + (long long)(lane / LPW) * 32 < W) {
       const size_t rslot = k.raster_slots > 0 ? (size_t)slot_after(clk.raster_pos, s, k.raster_slots) : (size_t)s;
       k.raster[rslot * k.words + (size_t)((wbase >> 5) + lane / LPW)] = v;
+      if (k.pull_bits) k.pull_bits[pull_word_index(k, clk.step0 + s, (wbase >> 5) + lane / LPW)] = v;
     }
   }
   if constexpr (DEFER)
@@ -1194,6 +1269,7 @@ __global__ void __launch_bounds__(BLOCK) lif_staged_kernel(LifK k, int s) {
         if (lane == 0 && wfirst < W) {
           const size_t rslot = k.raster_slots > 0 ? (size_t)slot_after(clk.raster_pos, s, k.raster_slots) : (size_t)s;
           k.raster[rslot * k.words + (size_t)(wfirst >> 5)] = word;
+          if (k.pull_bits) k.pull_bits[pull_word_index(k, clk.step0 + s, wfirst >> 5)] = word;
         }
       }
     }
@@ -1256,6 +1332,7 @@ static int run_lif_staged_as(const LifK& k, int grid_cap, cudaStream_t st) {
   const long long chunks = ((long long)k.t_end - k.t_begin + L::CH - 1) / L::CH;
   if (grid > chunks) grid = chunks;
   if (grid_cap > 0 && grid > grid_cap) grid = grid_cap;
+  int pending = 0;
   for (int s = 0; s < k.nsteps; ++s) {
     if constexpr (DEFER) {   // staged update + list, then the balanced scatter
       cudaError_t e = cudaMemsetAsync(k.spike_n, 0, sizeof(unsigned), st);
@@ -1266,10 +1343,8 @@ static int run_lif_staged_as(const LifK& k, int grid_cap, cudaStream_t st) {
     } else {
       lif_staged_kernel<BLOCK, FIXED, IPT><<<(unsigned)grid, BLOCK, L::BYTES, st>>>(k, s);
       FLYB_CHECK_LAUNCH();
-      if (pulls_itself(k)) {
-        const int rc = launch_pull(k, s, st);
-        if (rc) return rc;
-      }
+      const int rc = pull_after_step(k, s, pending, st);
+      if (rc) return rc;
     }
     FLYB_CHECK_LAUNCH();
   }
@@ -1298,6 +1373,7 @@ static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st)
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
       scatter_grid = sms * 8;
     }
+    int pending = 0;
     for (int s = 0; s < k.nsteps; ++s) {
       if (k.spike_list) {   // deferred delivery: update + list, then the balanced scatter
         cudaError_t e = cudaMemsetAsync(k.spike_n, 0, sizeof(unsigned), st);
@@ -1308,10 +1384,8 @@ static int run_lif_ipt(const LifK& k, int launch, int grid_cap, cudaStream_t st)
       } else {
         lif_step_kernel<BLOCK, FIXED, IPT><<<(unsigned)chunks, BLOCK, 0, st>>>(k, s);
         FLYB_CHECK_LAUNCH();
-        if (pulls_itself(k)) {
-          const int rc = launch_pull(k, s, st);
-          if (rc) return rc;
-        }
+        const int rc = pull_after_step(k, s, pending, st);
+        if (rc) return rc;
       }
       FLYB_CHECK_LAUNCH();
     }
@@ -1539,17 +1613,21 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
     k.slow_g[c] = used ? a->slow_g[c] : nullptr;
   }
   k.pull_ptr = a->pull_ptr; k.pull_pre = a->pull_pre; k.pull_planes = a->pull_planes;
-  k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta; k.pull_lag = a->pull_lag;
-  if (a->pull_lag < 0 || a->pull_lag > 1 || (a->pull_lag && (a->raster_slots <= 0 || a->n_delay < 2)))
-    return FLYB_EINVAL;
+  k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta;
+  k.pull_group = a->pull_group; k.pull_phase = a->pull_phase; k.pull_bits = nullptr; k.pull_state = nullptr;
   if (a->flags & FLYB_LIF_PULL_DELIVERY) {
     const int g = a->batch / 32;
+    // a group's pull may run beside the next group's updates and must end before the steps after
+    // them: its earliest write slot is read n_delay steps after its first step, so 2 L <= n_delay
     if (a->batch % 32 || (g != 1 && g != 2 && g != 4 && g != 8) || a->ring_mode != FLYB_RING_COUNT ||
         a->launch != FLYB_LAUNCH_STEP || (a->flags & (FLYB_LIF_DEFER_DELIVERY | FLYB_LIF_STD)) || a->clock_k ||
-        a->slow_classes || !a->raster || !a->pull_ptr || !a->pull_pre || !a->pull_planes || !a->pull_meta ||
-        (a->pull_nplanes != 8 && a->pull_nplanes != 16) || (reinterpret_cast<uintptr_t>(a->raster) & 15) ||
-        (reinterpret_cast<uintptr_t>(a->pull_planes) & 15))
+        a->slow_classes || !a->pull_ptr || !a->pull_pre || !a->pull_planes || !a->pull_meta ||
+        (a->pull_nplanes != 8 && a->pull_nplanes != 16) || (reinterpret_cast<uintptr_t>(a->pull_planes) & 15) ||
+        !a->pull_bits || !a->pull_state || (reinterpret_cast<uintptr_t>(a->pull_bits) & 31) ||
+        !pull_group_ok(a->batch, a->pull_group) || (a->pull_group > 1 && 2 * a->pull_group > a->n_delay) ||
+        a->pull_phase < 0 || a->pull_phase >= a->pull_group)
       return FLYB_EINVAL;
+    k.pull_bits = a->pull_bits; k.pull_state = a->pull_state;
   }
   if (a->flags & FLYB_LIF_DEFER_DELIVERY) {
     // per-step launches of the register path only; the list must hold every entry a step can make
@@ -1576,8 +1654,8 @@ FLYB_API int flyb_lif_pull(const flyb_lif_args* a, void* stream) {
   LifK k;
   const int rc = make_lif_k(a, k);
   if (rc) return rc;
-  if (!(k.flags & FLYB_LIF_PULL_DELIVERY)) return FLYB_EINVAL;
-  return launch_pull(k, -k.pull_lag, (cudaStream_t)stream);
+  if (!(k.flags & FLYB_LIF_PULL_DELIVERY) || a->pull_steps < 1 || a->pull_steps > k.pull_group) return FLYB_EINVAL;
+  return launch_pull(k, a->pull_steps, (cudaStream_t)stream);
 }
 
 FLYB_API int flyb_lif_run(const flyb_lif_args* a, void* stream) {

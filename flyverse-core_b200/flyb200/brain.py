@@ -278,6 +278,11 @@ class Brain:
         self.words = (N * B + 31) // 32
         self._hist = torch.zeros(self.n_delay, self.words, dtype=torch.int32, device=dev)   # 1-bit spike history
         self._clock = torch.zeros(3, dtype=torch.int64, device=dev)        # {step, ring_pos, hist_pos}
+        # pull delivery: {first undelivered step, its ring position, block counter}; equal to the
+        # clock's first two words whenever nothing is pending (between calls)
+        self._pull_state = torch.zeros(3, dtype=torch.int64, device=dev)
+        self._pull_pending = 0                  # steps updated but not yet pulled (host count)
+        self._pull_bits = None
         self._status = torch.zeros(4, dtype=torch.int32, device=dev)
         self._sync = torch.zeros(_abi.LIF_SYNC_WORDS, dtype=torch.int32, device=dev)
         self._events = torch.zeros(1, dtype=torch.int64, device=dev)
@@ -431,6 +436,19 @@ class Brain:
             self._pull_planes_n, self._pull_key = S, key
         a.pull_ptr, a.pull_pre, a.pull_planes, a.pull_meta = (x.data_ptr() for x in self._pull_t)
         a.pull_nplanes = self._pull_planes_n
+        L = self.pull_group
+        if self._pull_bits is None or self._pull_bits.numel() != 2 * L * self.words:
+            self._pull_bits = torch.zeros(2 * L * self.words, dtype=torch.int32, device=self.device)
+        a.pull_group, a.pull_bits, a.pull_state = L, self._pull_bits.data_ptr(), self._pull_state.data_ptr()
+        a.pull_phase = self.step_count % L
+
+    @property
+    def pull_group(self) -> int:
+        """Steps a pull delivers together (flyb_lif_args.pull_group): 8 / (B / 32), so that one
+        gather per input fetches a 32-byte sector of spike words, when the delay allows a group's
+        pull to run beside the next group (2 L <= n_delay); else 1."""
+        L = 8 // max(1, self.B // 32)
+        return L if 2 * L <= self.n_delay else 1
 
     # ------------------------------------------------------------------ per-neuron clocks
     def set_clocks(self, multiplier) -> None:
@@ -542,37 +560,42 @@ class Brain:
         if rc:
             raise RuntimeError(f"flyb_lif_run: error {rc}")
 
-    def pull_previous(self) -> None:
-        """Pull delivery of the step before the device clock (after `advance(1, pull=False)`), on
-        the current stream: it may run beside the next step's ranges and must end before the next
-        `advance`."""
+    def deliver(self, steps: int | None = None) -> None:
+        """Pull delivery of the first `steps` (default: all) steps updated but not yet delivered
+        (after `advance(n, pull=False)`), on the current stream, in launches that end at group
+        boundaries. A delivery may run on another stream beside the updates of the next group of
+        steps; the caller orders it before the next delivery and before the updates of the group
+        after that (their spike words reuse its half of the pull buffer)."""
+        left = self._pull_pending if steps is None else int(steps)
+        if left <= 0:
+            return
+        if left > self._pull_pending:
+            raise ValueError(f"only {self._pull_pending} steps are pending")
         a = self._args
-        a.flags, a.nsteps, a.pull_lag = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY, 1, 1
+        a.flags, a.nsteps = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY, 1
         self._set_pull(a)
-        try:
-            with torch.cuda.device(self.device):
-                rc = self._lib.flyb_lif_pull(ct.byref(a), torch.cuda.current_stream(self.device).cuda_stream)
-        finally:
-            a.pull_lag = 0
-        if rc:
-            raise RuntimeError(f"flyb_lif_pull: error {rc}")
-
-    def advance(self, n_steps: int = 1, *, pull: bool = True) -> None:
-        """End `n_steps` steps run by ranges: move the device clock (ring and history positions,
-        Philox step) on, as the end of `step` does. Under pull delivery the step's spikes are
-        pulled first, unless `pull` is False (then `pull_previous` delivers them)."""
-        a = self._args
-        a.flags = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY
-        a.nsteps = int(n_steps)
+        L = self.pull_group
+        first = self.step_count - self._pull_pending            # the first undelivered step
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        if self._pull_active() and pull:  # the ranges recorded their spikes: deliver them, then advance
-            if n_steps != 1:
-                raise ValueError("with pull delivery, ranges advance one step at a time")
-            self._set_pull(a)
+        while left:
+            a.pull_steps = min(left, L - first % L)
             with torch.cuda.device(self.device):
                 rc = self._lib.flyb_lif_pull(ct.byref(a), stream)
             if rc:
                 raise RuntimeError(f"flyb_lif_pull: error {rc}")
+            first += a.pull_steps
+            left -= a.pull_steps
+            self._pull_pending -= a.pull_steps
+
+    def advance(self, n_steps: int = 1, *, pull: bool = True) -> None:
+        """End `n_steps` steps run by ranges: move the device clock (ring and history positions,
+        Philox step) on, as the end of `step` does. Under pull delivery the steps become pending;
+        with `pull` they are delivered at once, else `deliver` delivers them later (at most a
+        group's worth may be pending)."""
+        a = self._args
+        a.flags = self._flags(False) & ~_abi.LIF_DEFER_DELIVERY
+        a.nsteps = int(n_steps)
+        stream = torch.cuda.current_stream(self.device).cuda_stream
         with torch.cuda.device(self.device):
             rc = self._lib.flyb_lif_advance(ct.byref(a), stream)
         if rc:
@@ -580,6 +603,19 @@ class Brain:
         self.buf_pos = (self.buf_pos + n_steps) % self.R
         self.t += n_steps * self.p.dt
         self.step_count += n_steps
+        if self._pull_active():
+            self._pull_pending += int(n_steps)
+            if self._pull_pending > self.pull_group and not pull:
+                raise ValueError("more than one group of steps is waiting for its pull")
+            if pull:
+                self.deliver()
+
+    def restart_clock(self) -> None:
+        """Step counter, ring and history positions back to 0 (a full reset), nothing pending."""
+        self._clock.zero_()
+        self._pull_state.zero_()
+        self._pull_pending = 0
+        self.t, self.step_count, self.buf_pos = 0.0, 0, 0
 
     def run_ms(self, ms: float) -> None:
         self.step(int(round(ms / self.p.dt)))
@@ -702,6 +738,9 @@ class Brain:
         self.ring.copy_(state["ring"].to(self.device))
         self._hist.copy_(state["hist"].to(self.device))
         self._clock.copy_(state["clock"].to(self.device))
+        self._pull_state[:2].copy_(self._clock[:2])         # a checkpoint has nothing pending
+        self._pull_state[2] = 0
+        self._pull_pending = 0
         if "clock_period" in state:
             if self._kvec is None or not np.array_equal(state["clock_period"], self._kvec):
                 self.set_clocks(state["clock_period"])

@@ -11,6 +11,7 @@ connectome.py:870-895); compiling the raw MaleCNS feather tables is not part of 
 from __future__ import annotations
 
 import json
+import re
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -36,10 +37,12 @@ class Connectome:
 
     def __post_init__(self):
         self.W = sp.csr_matrix(self.W, dtype=np.float32)
-        if "in_syn" not in self.neurons:
-            self.neurons["in_syn"] = np.asarray(abs(self.W).sum(axis=1)).ravel()
-        if "in_syn_l2" not in self.neurons:
-            self.neurons["in_syn_l2"] = np.sqrt(np.asarray(self.W.multiply(self.W).sum(axis=1)).ravel())
+        missing = [k for k in ("in_syn", "in_syn_l2") if k not in self.neurons]
+        if missing:
+            l1, l2 = row_norms(self.W)
+            fill = {"in_syn": l1, "in_syn_l2": l2}
+            for k in missing:
+                self.neurons[k] = fill[k]
 
     @property
     def n(self) -> int:
@@ -62,33 +65,37 @@ class Connectome:
         return self.body_to_index.loc[np.asarray(body_ids)].to_numpy()
 
     def indices(self, selection) -> np.ndarray:
-        """Validate a row-index selection, boolean mask or select() criteria (connectome.py:453-467)."""
+        """Row numbers of a selection (connectome.py:453-467): a dict of `select` criteria, a boolean
+        mask with one entry per neuron, or distinct in-range integer rows in the caller's order.
+        Anything else raises ValueError."""
         if isinstance(selection, dict):
             return self.select(**selection)
-        idx = np.asarray(selection)
-        if idx.dtype == bool:
-            if idx.shape != (self.n,):
-                raise ValueError(f"mask must have shape ({self.n},)")
-            return np.flatnonzero(idx)
-        if idx.ndim != 1 or (idx.size and not np.issubdtype(idx.dtype, np.integer)):
-            raise ValueError("selection must be a one-dimensional integer index array")
-        idx = idx.astype(np.int64)
-        if np.any((idx < 0) | (idx >= self.n)) or len(np.unique(idx)) != len(idx):
-            raise ValueError("indices must be unique and within the connectome")
-        return idx
+        arr = np.asarray(selection)
+        if arr.dtype == np.bool_:
+            if arr.shape != (self.n,):
+                raise ValueError(f"a boolean selection needs shape ({self.n},), got {arr.shape}")
+            return np.nonzero(arr)[0]
+        if arr.ndim != 1:
+            raise ValueError(f"a row selection must be one-dimensional, got {arr.ndim} dimensions")
+        if arr.size == 0:
+            return np.zeros(0, np.int64)
+        if not np.issubdtype(arr.dtype, np.integer):
+            raise ValueError(f"row numbers must be integers, got {arr.dtype}")
+        rows = arr.astype(np.int64)
+        if rows.min() < 0 or rows.max() >= self.n:
+            raise ValueError(f"row numbers must lie in [0, {self.n})")
+        if np.unique(rows).size != rows.size:
+            raise ValueError("row numbers must not repeat")
+        return rows
 
     def select(self, **criteria) -> np.ndarray:
-        """Rows matching every criterion; a string starting with '~' is a regex (connectome.py:604-616)."""
-        m = np.ones(self.n, dtype=bool)
-        for col, val in criteria.items():
-            s = self.neurons[col]
-            if isinstance(val, str) and val.startswith("~"):
-                m &= s.fillna("").astype(str).str.contains(val[1:], regex=True).to_numpy()
-            elif isinstance(val, (list, tuple, set, np.ndarray)):
-                m &= s.isin(list(val)).to_numpy()
-            else:
-                m &= (s == val).to_numpy()
-        return np.flatnonzero(m)
+        """Rows meeting every criterion column=value (connectome.py:604-616): a list, tuple, set or
+        array is a set of accepted values, a string starting with '~' a regular expression searched
+        in the column's text (missing values read as ''), anything else an exact value."""
+        keep = np.ones(self.n, dtype=bool)
+        for column, wanted in criteria.items():
+            keep &= _column_matches(self.neurons[column], wanted)
+        return np.nonzero(keep)[0]
 
     def subset(self, selection) -> "Connectome":
         """Induced subgraph in selection order; normalisation keeps reading the original graph."""
@@ -100,6 +107,28 @@ class Connectome:
     def describe(self, idx) -> pd.DataFrame:
         cols = [c for c in ("bodyId", "type", "instance", "superclass", "somaSide", "nt") if c in self.neurons]
         return self.neurons.iloc[np.asarray(idx)][cols]
+
+
+def row_norms(W: sp.csr_matrix) -> tuple[np.ndarray, np.ndarray]:
+    """Per postsynaptic row the L1 norm (sum |w|) and the L2 norm of W, as float32: the in-degree
+    totals `in_syn` / `in_syn_l2` that the fan-in scale and the optic normalisation read. Summed
+    in float64 (exact for integer synapse counts), then rounded once to float32."""
+    W = sp.csr_matrix(W)
+    row = np.repeat(np.arange(W.shape[0]), np.diff(W.indptr))
+    w = W.data.astype(np.float64)
+    l1 = np.bincount(row, weights=np.abs(w), minlength=W.shape[0])
+    sq = np.bincount(row, weights=w * w, minlength=W.shape[0])
+    return l1.astype(np.float32), np.sqrt(sq).astype(np.float32)
+
+
+def _column_matches(column: pd.Series, wanted) -> np.ndarray:
+    if isinstance(wanted, str) and wanted[:1] == "~":
+        pattern = re.compile(wanted[1:])
+        text = column.fillna("").astype(str)
+        return np.fromiter((pattern.search(t) is not None for t in text), dtype=bool, count=len(text))
+    if isinstance(wanted, (list, tuple, set, np.ndarray)):
+        return column.isin(list(wanted)).to_numpy()
+    return (column == wanted).to_numpy()
 
 
 def from_arrays(neurons: pd.DataFrame, W) -> Connectome:

@@ -28,6 +28,69 @@ from .retina import build_retina
 from .weights import receptor_gain
 
 
+class PoissonSchedule:
+    """The Poisson forcing of a FlyBrain (fly.py:312-396): held inputs, set by name and kept until
+    replaced, and timed pulses. The forcing a step sees is, per (fly, neuron), the larger of the
+    held probability and that of every pulse still running; a pulse of `ms` runs for whole LIF steps
+    (ceil(ms / dt) of them) and ends when the clock reaches its end time (1e-9 ms tolerance).
+    Probabilities per step are float32 rate x (dt / 1000), as the brain's `set_poisson`."""
+
+    EPS_MS = 1e-9
+
+    def __init__(self, brain: Brain):
+        self.brain = brain
+        self.held = torch.zeros_like(brain.poisson_p)       # (B, N)
+        self.held_on: dict[str, bool] = {}                  # input name -> any positive rate
+        self.pulses: list = []                              # [rows (k,), rates (B, k) Hz float32, end ms]
+
+    def per_step(self, hz) -> torch.Tensor:
+        return torch.as_tensor(hz, dtype=torch.float32, device=self.brain.device) * (self.brain.p.dt / 1000)
+
+    def hold(self, name: str, idx, hz) -> None:
+        cols = self.brain._idx(idx)
+        prob = self.per_step(np.asarray(hz, dtype=np.float32))
+        self.held[:, cols] = prob
+        self.held_on[name] = bool(np.any(np.asarray(hz) > 0))
+        if self.pulses:
+            self.apply()
+            return
+        self.brain.poisson_p[:, cols] = prob          # no pulse can sit above the held rates
+        self.brain._poisson_on = any(self.held_on.values())
+
+    def add_pulse(self, rows: np.ndarray, hz: np.ndarray, end_ms: float) -> None:
+        self.pulses.append((rows.copy(), hz, end_ms))
+        self.apply()
+
+    def next_end(self) -> float | None:
+        return min(end for _, _, end in self.pulses) if self.pulses else None
+
+    def ends_before(self, t_ms: float) -> bool:
+        return any(end < t_ms - self.EPS_MS for _, _, end in self.pulses)
+
+    def apply(self) -> None:
+        """Write held and running pulses into the brain's forcing at the brain's current time."""
+        now = self.brain.t
+        self.pulses = [pl for pl in self.pulses if pl[2] > now + self.EPS_MS]
+        forcing = self.brain.poisson_p
+        forcing.copy_(self.held)
+        for rows, hz, _ in self.pulses:
+            cols = self.brain._idx(rows)
+            forcing[:, cols] = torch.maximum(forcing[:, cols], self.per_step(hz))
+        self.brain._poisson_on = any(self.held_on.values()) or any(bool((hz > 0).any()) for _, hz, _ in self.pulses)
+
+    def clear(self, rows=None) -> None:
+        """Forget the held inputs and pulses of fly rows `rows` (all flies, and the input names,
+        when None); the forcing itself is rewritten by the next `apply`."""
+        if rows is None:
+            self.held.zero_()
+            self.held_on.clear()
+            self.pulses.clear()
+            return
+        self.held[self.brain._idx(rows)] = 0
+        for _, hz, _ in self.pulses:
+            hz[rows] = 0
+
+
 class FlyBrain:
     BRAIN_TENSORS = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
     OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate", "g_slow", "g_slow_cls", "_slow_in_s",
@@ -63,9 +126,7 @@ class FlyBrain:
             self.brain.set_clocks(clock_periods(c, lp.dt, lp.dt_by_module))
         self._radiance = None
         self._pending_ms = 0.0
-        self._base_poisson = torch.zeros_like(self.brain.poisson_p)
-        self._inputs_on = {}
-        self._pulses = []
+        self.poisson = PoissonSchedule(self.brain)
         self._activity_ms = np.zeros(self.B)
         self._motor = None                # (names, ptr, idx, device means, pinned means, event)
         self._motor_fresh = False
@@ -76,20 +137,22 @@ class FlyBrain:
 
     # ------------------------------------------------------------------ inputs
     def vision(self, radiance) -> None:
-        """(columns, 4) or (B, columns, 4) radiance [UV, B, G, R], held until the next call."""
+        """Hold a radiance frame [UV, B, G, R] until the next call: (columns, 4), the same for every
+        fly, or (B, columns, 4); values must be finite and nonnegative (fly.py:298-309)."""
         if self.optic is None:
-            raise ValueError("vision is absent from this connectome subset")
-        value = torch.as_tensor(radiance, dtype=torch.float32, device=self.device)
-        if value.ndim == 2:
-            value = value[None].expand(self.B, -1, -1)
-        if value.shape != (self.B, self.retina.n_columns, 4):
-            raise ValueError(f"radiance must have shape ({self.B}, {self.retina.n_columns}, 4) or ({self.retina.n_columns}, 4)")
-        if not bool(torch.isfinite(value).all() & (value >= 0).all()):
-            raise ValueError("radiance must be finite and nonnegative")
+            raise ValueError("this connectome subset has no eye: vision is unavailable")
+        cols = self.retina.n_columns
+        frame = torch.as_tensor(radiance, dtype=torch.float32, device=self.device)
+        if tuple(frame.shape) == (cols, 4):
+            frame = frame.expand(self.B, cols, 4)
+        elif tuple(frame.shape) != (self.B, cols, 4):
+            raise ValueError(f"radiance of shape {tuple(frame.shape)}: expected ({self.B}, {cols}, 4) or ({cols}, 4)")
+        if bool((~torch.isfinite(frame) | (frame < 0)).any()):
+            raise ValueError("radiance values must be finite and nonnegative")
         if self._radiance is None:
-            self._radiance = value.clone()
+            self._radiance = frame.clone()
         else:
-            self._radiance.copy_(value)
+            self._radiance.copy_(frame)
 
     def look(self, world, eye, forward, left, up) -> None:
         """Trace every fly's eye in its own scene of `world` (a BatchWorld, one scene per fly) from
@@ -106,37 +169,24 @@ class FlyBrain:
         world.column_radiance(eye, forward, left, up, out=self._radiance)
 
     def set_input(self, name: str, idx, hz) -> None:
-        """A held sensory Poisson input (the reference's `_input`, fly.py:312-324)."""
-        ti = self.brain._idx(idx)
-        prob = torch.as_tensor(np.asarray(hz, dtype=np.float32), device=self.device) * (self.brain.p.dt / 1000)
-        self.brain.poisson_p[:, ti] = prob
-        self._base_poisson[:, ti] = prob
-        self._inputs_on[name] = bool(np.any(np.asarray(hz) > 0))
-        if self._pulses:
-            self._refresh_poisson()
-        else:
-            self.brain._poisson_on = any(self._inputs_on.values())
+        """Hold a named sensory Poisson input: rates `hz` (Hz; scalar, per neuron or (B, k)) on
+        neurons `idx` until the input is set again (the reference's `_input`, fly.py:312-324)."""
+        self.poisson.hold(name, idx, hz)
 
     def stimulate(self, selection, hz, ms) -> None:
-        """A Poisson pulse combined with the held inputs by maximum, ending on a LIF boundary."""
-        if not math.isfinite(ms) or ms <= 0:
-            raise ValueError("pulse duration must be positive and finite")
-        idx = self.c.indices(selection)
-        value = np.broadcast_to(np.asarray(hz, dtype=np.float32), (self.B, len(idx))).copy()
-        if not np.isfinite(value).all() or np.any((value < 0) | (value * self.brain.p.dt > 1000)):
-            raise ValueError("pulse rates must be finite and between 0 and 1000/dt Hz")
-        duration = math.ceil(ms / self.brain.p.dt) * self.brain.p.dt
-        self._pulses.append((idx.copy(), value, self.t + duration))
-        self._refresh_poisson()
+        """A Poisson pulse of `hz` on the selected neurons for `ms` (rounded up to whole LIF steps),
+        combined with the held inputs by maximum (fly.py:375-385)."""
+        if not (math.isfinite(ms) and ms > 0):
+            raise ValueError(f"a pulse lasts a positive finite time, not {ms} ms")
+        rows = self.c.indices(selection)
+        rates = np.array(np.broadcast_to(np.asarray(hz, dtype=np.float32), (self.B, len(rows))))
+        dt = self.brain.p.dt
+        if not np.isfinite(rates).all() or rates.min(initial=0.0) < 0 or (rates * dt).max(initial=0.0) > 1000:
+            raise ValueError(f"pulse rates must be finite, in [0, {1000 / dt:g}] Hz")
+        self.poisson.add_pulse(rows, rates, self.t + math.ceil(ms / dt) * dt)
 
     def _refresh_poisson(self) -> None:
-        self.brain.poisson_p.copy_(self._base_poisson)
-        self._pulses = [p for p in self._pulses if p[2] > self.t + 1e-9]
-        for idx, hz, _ in self._pulses:
-            ti = self.brain._idx(idx)
-            prob = torch.as_tensor(hz, device=self.device) * (self.brain.p.dt / 1000)
-            self.brain.poisson_p[:, ti] = torch.maximum(self.brain.poisson_p[:, ti], prob)
-        self.brain._poisson_on = any(self._inputs_on.values()) or any(np.any(p[1] > 0) for p in self._pulses)
+        self.poisson.apply()
 
     # ------------------------------------------------------------------ stepping (fly.py:398-610)
     def step(self, ms: float = 10.0) -> float:
@@ -149,24 +199,24 @@ class FlyBrain:
         self._pending_ms = max(0.0, total - elapsed)
         if not steps:
             return 0.0
-        if self.cuda_graphs and not any(p[2] < self.t + elapsed - 1e-9 for p in self._pulses):
+        if self.cuda_graphs and not self.poisson.ends_before(self.t + elapsed):
             self._graph_frame(steps)
             self._mark_readout()
-            if self._pulses:
-                self._refresh_poisson()
+            if self.poisson.pulses:
+                self.poisson.apply()
             self._activity_ms += elapsed
             return elapsed
         self._vision_frame(elapsed)
         remaining = steps
         while remaining:
             count = remaining
-            if self._pulses:
-                until = min(p[2] for p in self._pulses) - self.t
-                count = min(count, max(1, int(round(until / self.brain.p.dt))))
+            end = self.poisson.next_end()
+            if end is not None:            # stop at the next pulse end (a LIF step boundary)
+                count = min(count, max(1, int(round((end - self.t) / self.brain.p.dt))))
             self.brain.step(count)
             remaining -= count
-            if self._pulses:
-                self._refresh_poisson()
+            if self.poisson.pulses:
+                self.poisson.apply()
         self._readout()
         self._mark_readout()
         self._activity_ms += elapsed
@@ -279,26 +329,28 @@ class FlyBrain:
         return {k: means[:, n] for n, k in enumerate(names)}
 
     def reset(self, rows=None) -> None:
+        """Return flies `rows` (every fly when None) to rest: brain, optic lobe, their held inputs and
+        pulses, activity time (fly.py:682-707). A full reset also restarts the clock, drops the held
+        radiance and the captured frames."""
         self._motor_fresh = False
         self.brain.reset(rows)
         if self.optic is not None:
             self.optic.reset(rows)
-        sel = slice(None) if rows is None else self.brain._idx(rows)
-        self._base_poisson[sel] = 0
         if rows is None:
-            self._pulses.clear()
-            self._inputs_on.clear()
-            self._pending_ms = 0.0
-            self._activity_ms[:] = 0.0
-            self._graphs.clear()
-            self._radiance = None
-            self.brain.t, self.brain.step_count, self.brain.buf_pos = 0.0, 0, 0
-            self.brain._clock.zero_()
+            self._restart()
         else:
-            self._activity_ms[np.asarray(rows)] = 0.0
-            for _, hz, _ in self._pulses:
-                hz[np.asarray(rows)] = 0
-        self._refresh_poisson()
+            rows = np.asarray(rows)
+            self.poisson.clear(rows)
+            self._activity_ms[rows] = 0.0
+        self.poisson.apply()
+
+    def _restart(self) -> None:
+        self.poisson.clear()
+        self._pending_ms = 0.0
+        self._activity_ms[:] = 0.0
+        self._graphs.clear()
+        self._radiance = None
+        self.brain.restart_clock()
 
     def state_dict(self) -> dict:
         o = self.optic
@@ -309,8 +361,8 @@ class FlyBrain:
                 "optic_fresh": o._fresh_u8.cpu().clone() if o is not None else None,
                 "optic_pending_ms": o._pending_ms if o is not None else 0.0,
                 "radiance": self._radiance.detach().cpu().clone() if self._radiance is not None else None,
-                "base_poisson": self._base_poisson.cpu().clone(), "inputs_on": dict(self._inputs_on),
-                "pulses": [(i.copy(), h.copy(), e) for i, h, e in self._pulses], "pending_ms": self._pending_ms,
+                "base_poisson": self.poisson.held.cpu().clone(), "inputs_on": dict(self.poisson.held_on),
+                "pulses": [(i.copy(), h.copy(), e) for i, h, e in self.poisson.pulses], "pending_ms": self._pending_ms,
                 "activity_ms": self._activity_ms.copy()}
 
     def load_state_dict(self, state: dict) -> None:
@@ -330,7 +382,7 @@ class FlyBrain:
             o._pending_ms = state["optic_pending_ms"]
             o.r0 = o.b_vec[None].clone()
         self._radiance = state["radiance"].to(self.device).clone() if state["radiance"] is not None else None
-        self._base_poisson.copy_(state["base_poisson"].to(self.device))
-        self._inputs_on = dict(state["inputs_on"])
-        self._pulses = [(i.copy(), h.copy(), e) for i, h, e in state["pulses"]]
+        self.poisson.held.copy_(state["base_poisson"].to(self.device))
+        self.poisson.held_on = dict(state["inputs_on"])
+        self.poisson.pulses = [(i.copy(), h.copy(), e) for i, h, e in state["pulses"]]
         self._pending_ms, self._activity_ms = state["pending_ms"], state["activity_ms"].copy()

@@ -9,9 +9,9 @@
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
 `--steps` steps of the chosen part. Used for the launch list and the per-kernel captures whose
-summaries live in profiles/. `--part pull` fills the LIF spike history with random spikes at
-`--density` (per neuron and fly; 0.024 is the whole fly's steady firing at 64 flies) and runs the
-pull delivery of one step `--steps` times. `--breakdown` instead times each stage of the step on its own with
+summaries live in profiles/. `--part pull` fills the LIF pull buffer with random spikes at
+`--density` (per neuron, fly and step; 0.024 is the whole fly's steady firing at 64 flies) and
+runs the pull delivery of one group of steps (Brain.pull_group: 4 at 64 flies) `--steps` times. `--breakdown` instead times each stage of the step on its own with
 CUDA events (stream-ordered, warm L2) and prints one JSON line of microseconds per stage.
 """
 from __future__ import annotations
@@ -103,27 +103,33 @@ def trace_eyes(args) -> None:
 
 
 def pull_steps(eng, steps: int, density: float) -> None:
-    """The pull delivery of one LIF step, `steps` times, from a spike history filled at `density`."""
+    """Pull delivery of whole groups of LIF steps (Brain.pull_group), `steps` groups, from spike
+    words filled at `density` per (neuron, fly, step)."""
     import ctypes as ct
     from . import _abi
     b = eng.lif
     if not b._pull_active():
         raise ValueError("pull delivery needs 32, 64, 128 or 256 flies and the count ring")
-    g = torch.Generator(device=b.device).manual_seed(1)
-    bits = (torch.rand(*b._hist.shape, 32, device=b.device, generator=g) < density).to(torch.int64)
-    words = (bits << torch.arange(32, device=b.device)).sum(-1)
-    b._hist.copy_(torch.where(words >= 2**31, words - 2**32, words).to(torch.int32))
-    del bits, words
     a = b._args
     a.flags, a.nsteps, a.n_first, a.n_count = b._flags(False), 1, 0, 0
     b._set_pull(a)
+    g = torch.Generator(device=b.device).manual_seed(1)
+    bits = (torch.rand(b._pull_bits.numel(), 32, device=b.device, generator=g) < density).to(torch.int64)
+    words = (bits << torch.arange(32, device=b.device)).sum(-1)
+    b._pull_bits.copy_(torch.where(words >= 2**31, words - 2**32, words).to(torch.int32))
+    del bits, words
+    L = b.pull_group
+    a.pull_steps = L
+    b._pull_state.zero_()
     stream = torch.cuda.current_stream(b.device).cuda_stream
     for _ in range(steps):
         rc = _abi.lib().flyb_lif_pull(ct.byref(a), stream)
         if rc:
             raise RuntimeError(f"flyb_lif_pull: error {rc}")
     torch.cuda.synchronize()
-    print(f"pulled {steps} steps at batch {b.B}, density {density}: {int(b._pull_t[1].numel()) // 32:,} chunks")
+    b._pull_state[:2].copy_(b._clock[:2])
+    print(f"pulled {steps} groups of {L} steps at batch {b.B}, density {density}: "
+          f"{int(b._pull_t[1].numel()) // 32:,} chunks")
 
 
 def main() -> None:

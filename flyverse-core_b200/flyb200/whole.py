@@ -78,18 +78,21 @@ class WholeFly:
         self._fork = (torch.cuda.Stream(self.device, priority=-1), torch.cuda.Stream(self.device))
         self._pull_stream = torch.cuda.Stream(self.device)
 
-    @property
-    def launches_per_step(self) -> int:
-        """Kernels launched by one step once running: two coupling products, the optic substep (its
-        dr carried over), the LIF update (two ranges when overlapped; each followed by its scatter
-        under deferred delivery, or one pull kernel after both under pull delivery) and the
-        device-clock advance (or one persistent launch)."""
+    def launches(self, steps: int) -> int:
+        """Kernels launched by `steps` steps in one call once running: per step two coupling
+        products, the optic substep (its dr carried over), the LIF update (two ranges when
+        overlapped; each followed by its scatter under deferred delivery) and the device-clock
+        advance (or one persistent launch); under pull delivery one pull per group of
+        `pull_group` steps (one per step without the overlap) and one for a group the call ends
+        inside."""
         n = 6 if self.overlapping else (5 if self.lif.launch == "step" else 4)
         if self.lif._defer_active():
             n += 2 if self.overlapping else 1          # the scatter kernel of each LIF launch
+        total = n * steps
         if self.lif._pull_active():
-            n += 1
-        return n
+            L = self.lif.pull_group if self.overlapping else 1
+            total += -(-steps // L)
+        return total
 
     @property
     def overlapping(self) -> bool:
@@ -138,9 +141,12 @@ class WholeFly:
         overlap = self.overlapping
         main = torch.cuda.current_stream(self.device)
         hi, side = self._fork
-        # under pull delivery a step's pull runs on its own stream beside the next step and joins
-        # before that step's clock advance (it reads the clock of the step it delivers)
+        # under pull delivery each group of L steps (Brain.pull_group) is pulled on its own stream
+        # beside the next group's steps; the main stream joins it before the next group's pull
+        # (and so before the updates of the group after, whose spike words reuse its half of the
+        # pull buffer), and the call ends with the pull of a group it stops inside
         lag = overlap and self.lif._pull_active() and self.lif.n_delay >= 2
+        L = self.lif.pull_group if lag else 1
         pulling = False
         for k in range(int(n)):
             if before is not None:
@@ -159,13 +165,10 @@ class WholeFly:
                 main.wait_stream(hi)
                 main.wait_stream(side)
                 if lag:
-                    if pulling:
-                        main.wait_stream(self._pull_stream)
                     self.lif.advance(1, pull=False)
-                    self._pull_stream.wait_stream(main)
-                    with torch.cuda.stream(self._pull_stream):
-                        self.lif.pull_previous()
-                    pulling = True
+                    if self.lif.step_count % L == 0:          # a group is complete
+                        self._pull_beside(main, pulling)
+                        pulling = True
                 else:
                     self.lif.advance(1)
             else:
@@ -173,11 +176,23 @@ class WholeFly:
                 self.lif.step(1)
             if after is not None:
                 after(k)
+        if lag and self.lif._pull_pending:
+            self._pull_beside(main, pulling)
+            pulling = True
         if pulling:
             main.wait_stream(self._pull_stream)
         if torch.cuda.is_current_stream_capturing():
             self.optic.pin_dr(cur0)
         self.steps_taken += int(n)
+
+    def _pull_beside(self, main, pulling: bool) -> None:
+        """Deliver the pending steps on the pull stream, after the previous pull and after the
+        main stream's work so far."""
+        if pulling:
+            main.wait_stream(self._pull_stream)
+        self._pull_stream.wait_stream(main)
+        with torch.cuda.stream(self._pull_stream):
+            self.lif.deliver()
 
     def _optic_and_drive(self, drive: torch.Tensor) -> None:
         o = self.cfg.optic
@@ -194,8 +209,11 @@ class WholeFly:
         per = 4 * (5 * 2 + 4 + 1)
         total = self.cfg.n_spiking * (self.B * per + 4)
         if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
+            # the input tables once per group of L steps, the write slot read + written every step
             ptr, pre, planes, meta = self.lif._pull_t
-            total += pre.numel() * 4 + planes.numel() * 4 + meta.numel() * 4 + self.cfg.n_spiking * self.B * 4 * 2
+            L = self.lif.pull_group if self.overlapping else 1
+            total += (pre.numel() * 4 + planes.numel() * 4 + meta.numel() * 4) // L
+            total += self.cfg.n_spiking * self.B * 4 * 2
         return total
 
     def optic_bytes_per_step(self) -> int:

@@ -200,15 +200,26 @@ typedef struct flyb_lif_args {
    * pull_pre [chunks][32] presynaptic neuron, pull_meta [chunks] = (base << 5) | planes: entry l
    * of the chunk carries count base + d_l, 0 <= d_l < 2^planes, planes <= pull_nplanes;
    * pull_planes [chunks][pull_nplanes] the d_l as bit planes (bit l of plane p = bit p of d_l);
-   * pull_nplanes (the plane stride) 8 or 16. */
+   * pull_nplanes (the plane stride) 8 or 16.
+   * The update kernels record each step's spike words in pull_bits as well, and pulls deliver
+   * groups of pull_group consecutive steps at once: one gather per input then fetches the input's
+   * words of every step of the group (one 32-byte sector when pull_group = 8 / (batch / 32)). */
   const int* pull_ptr;
   const int* pull_pre;
   const unsigned* pull_planes;
   int pull_nplanes;
   const int* pull_meta;
-  int pull_lag;          /* flyb_lif_pull: 0 delivers the step the device clock is at (before
-                            flyb_lif_advance), 1 the step before it (after the advance; needs
-                            raster_slots > 0 and n_delay >= 2) */
+  int pull_group;        /* L: 1, or 8 / (batch / 32) when 2 L <= n_delay                       */
+  int pull_steps;        /* flyb_lif_pull: undelivered steps to deliver now, 1..L               */
+  int pull_phase;        /* runs over all neurons: (index of the first step) mod L; they pull
+                            at every group end and after their last step                       */
+  unsigned* pull_bits;   /* [2][ceil(n * batch / 32)][L] words (device, 32-byte aligned): the
+                            spike words of the last two groups, word w of step t at
+                            (((t / L) & 1) * words + w) * L + t % L                            */
+  long long* pull_state; /* [3] device: {first undelivered step, the ring position of that step,
+                            0}; moved on by each pull. It must equal {step, ring position} of the
+                            next step to run (step0 / ring_pos, or clock[0] / clock[1]) whenever
+                            nothing is pending                                                  */
 } flyb_lif_args;
 
 /* flyb_lif_args.slow_mode */
@@ -223,12 +234,14 @@ enum {
 
 int flyb_lif_run(const flyb_lif_args* a, void* stream);
 
-/* FLYB_LIF_PULL_DELIVERY over neuron ranges: after every range of a step ran (each with
- * FLYB_LIF_NO_ADVANCE and nsteps 1), delivers that step's spikes from the raster into the write
- * slot; then flyb_lif_advance. With pull_lag 1 it delivers the step before the clock instead, so
- * it may run after the advance, beside the next step's updates (which touch neither that step's
- * raster slot nor its write slot), as long as it completes before the next advance. The
- * arguments are those of the launches (any range). */
+/* FLYB_LIF_PULL_DELIVERY over neuron ranges: delivers the next a->pull_steps undelivered steps
+ * (from pull_state, at most pull_group, after every range of those steps ran with
+ * FLYB_LIF_NO_ADVANCE) from pull_bits into their write slots, and moves pull_state on. A pull may
+ * run on another stream beside the updates of the steps that follow, as long as the update of a
+ * step whose words go to the same half of pull_bits (a step of the group after next) and the next
+ * pull start only after it; the steps' write slots are read n_delay >= 2 L steps after them.
+ * The arguments are those of the launches (any range). No counterpart in the reference (its
+ * delivery is a scatter inside the step). */
 int flyb_lif_pull(const flyb_lif_args* a, void* stream);
 
 /* Entries a FLYB_LIF_DEFER_DELIVERY step of these arguments can write when every item of the
