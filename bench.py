@@ -9,21 +9,29 @@ Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthet
 5,895 photoreceptors. One step advances all 167,106 neurons of every fly once (flyb200.whole).
 
   value          neuron-steps/s of B=64 flies per GPU (whole job over N GPUs, weak scaling),
-                 steps replayed from a CUDA graph; state > L2, so no flush is needed
-  batch1         the plain single-instance kernels (B=1, one launch per kernel per step), L2 flushed
-                 between timed steps, for the "vs plain" ratio
+                 steps replayed from a CUDA graph at steady firing; state > L2, so no flush is needed
+  e2e            the same B=64 step through the public API with, every step, the radiance copied in
+                 from pinned host memory and the motor readout copied out, 20 steps per CUDA graph
+                 and the host synchronising on each graph's readouts (the eager launch-by-launch
+                 figure is reported beside it)
+  roofline       the dominant kernel (LIF step or optic substep): algorithmic bytes / CUDA-event time
+                 against the measured HBM copy rate, with ncu's DRAM bytes per launch
+  cpu_baseline   the C oracle port (oracle/) on this host's cores from this run's settled state
+  batch1         the plain single-instance kernels (B=1) at the same steady firing, graph-replayed
+                 (the "vs plain" ratio uses it) and eager with L2 flushed between steps
   adjoint        optic-lobe adjoint over 200 substeps (89,390 units, 6 M nnz, checkpoint 20) over
                  the forward pass time
-  e2e            the same B=64 step through the public API with, every step, the radiance copied in
-                 from pinned host memory and the motor readout copied out, the calls captured once
-                 as a CUDA graph and the host synchronising on every step's readout (the eager
-                 launch-by-launch figure is reported beside it)
-  roofline       the LIF step kernel: algorithmic bytes / CUDA-event time against measured HBM copy
-  tracer         the eye's ray tracer at 64 flies x 1,634 columns x 7 rays: device time, the frame
-                 path beside the reference's own torch tracer on the same GPU (baseline/_ref), and
-                 the C oracle on host cores
-  cpu_baseline   the C oracle port (oracle/) on this host's cores, a bounded sample of the workload
-`--impl reference` times that CPU port alone on the same config and prints the same line.
+  fp64_max_err   max |FP32 - FP64| of the optic state after 200 substeps (config 3, whole-fly lobe)
+  batch256       the whole fly at 256 flies (config 5's width)
+  uneven_*       uneven rollouts: config 5 at 256 flies (episodes of 200-2,000 steps) and config 4
+                 (config 2's graph + config 3's lobe) at 64 flies (500-4,000 steps, 20-200 Hz)
+  reference_gpu  the reference's own CUDA path (baseline/_ref, its neural.cu kernels) beside ours on
+                 config 2's LIF and config 3's optic substep at 1 and 64 flies, on this GPU
+  reference_own_cpu  the reference's own CPU code (Brain.step, OpticLobe._substep) on host cores
+  tracer         the eye's ray tracer at 64 flies x 1,634 columns x 7 rays, beside the reference's
+                 torch tracer on this GPU and the C oracle on host cores
+`--impl reference` times the CPU port alone, from a state settled the same number of steps, and
+prints the same line.
 """
 from __future__ import annotations
 
@@ -186,11 +194,22 @@ def photoreceptor_contrast(cfg, rad: torch.Tensor, tables=None) -> torch.Tensor:
 
 
 def graph_chunk(steps: int, most: int = 26) -> int:
-    """Steps per captured graph: a divisor of `steps` (so exactly `steps` are timed), even when
-    possible (an odd count ends each replay with a copy of the optic dr back to its start buffer)."""
+    """Steps per captured graph: a divisor of `steps` (so exactly `steps` are timed), a multiple of
+    4 when possible (whole groups of the pull delivery at 64 flies, so every replay pulls at group
+    ends), else even (an odd count ends each replay with a copy of the optic dr back to its start)."""
     divs = [d for d in range(min(most, steps), 0, -1) if steps % d == 0]
+    by4 = [d for d in divs if d % 4 == 0]
     even = [d for d in divs if d % 2 == 0]
-    return (even or divs)[0]
+    return (by4 or even or divs)[0]
+
+
+def to_group_end(eng, at_least: int = 2) -> int:
+    """Steps (at least `at_least`) that bring the engine's step count to a multiple of 4, so that a
+    graph of a multiple of 4 steps captured next pulls at the ends of whole delivery groups."""
+    k = at_least
+    while (eng.lif.step_count + k) % 4:
+        k += 1
+    return k
 
 
 def capture(eng, steps: int):
@@ -220,7 +239,7 @@ def measure_batched(cfg, device, steps, warmup, fly0, batch=BATCH, settle=SETTLE
     eng = build_engine(cfg, batch, device, "step", fly0)
     eng.step(max(3, warmup))
     eng.tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
-    eng.step(2)                    # the tuners restored the state: one step re-derives the carried dr
+    eng.step(to_group_end(eng))    # the tuners restored the state: a step re-derives the carried dr
     chunk = graph_chunk(steps)
     g = capture(eng, chunk)
     reps = steps // chunk
@@ -236,7 +255,7 @@ def measure_batched(cfg, device, steps, warmup, fly0, batch=BATCH, settle=SETTLE
     torch.cuda.synchronize()
     del g
     eng.tuned["lif"] = autotune.tune_lif(eng.lif, steps=10)
-    eng.step(2)
+    eng.step(to_group_end(eng))
     g = capture(eng, chunk)
     g.replay()
     torch.cuda.synchronize()
@@ -257,14 +276,17 @@ def time_graph(g, reps) -> float:
 
 def kernel_roofline(eng, reps=20) -> dict:
     """The LIF step and the optic substep timed alone with CUDA events (B=64), after one untimed
-    call of each (the first whole-range LIF step sizes its spike list)."""
-    eng.lif.step(1)
+    call of each (the first whole-range LIF step sizes its spike list). The LIF is timed over calls
+    of one delivery group (Brain.pull_group steps: the updates and one pull) started at a group
+    boundary, per step."""
+    L = eng.lif.pull_group if eng.lif._pull_active() else 1
+    eng.lif.step(to_group_end(eng, 1))
     eng.optic.substeps(1, carry=True)
     torch.cuda.synchronize()
-    lif_ms = events_time(lambda: eng.lif.step(1), reps)
+    lif_ms = events_time(lambda: eng.lif.step(L), reps) / L
     opt_ms = events_time(lambda: eng.optic.substeps(1, carry=True), reps)
-    lif_b, opt_b = eng.lif_bytes_per_step(), eng.optic_bytes_per_step()
-    return {"lif_ms": lif_ms, "optic_ms": opt_ms, "lif_bytes": lif_b, "optic_bytes": opt_b}
+    lif_b, opt_b = eng.lif_bytes_per_step(group=L), eng.optic_bytes_per_step()
+    return {"lif_ms": lif_ms, "optic_ms": opt_ms, "lif_bytes": lif_b, "optic_bytes": opt_b, "lif_group": L}
 
 
 def measure_l2_gather(device, rows: int = 89_390, n_idx: int = 6_000_000) -> dict:
@@ -308,20 +330,29 @@ def read_traffic() -> dict:
     return out
 
 
-def measure_plain(cfg, device, steps, warmup, settle=SETTLE_STEPS):
+def measure_plain(cfg, device, steps, warmup, settle=SETTLE_STEPS) -> dict:
+    """The plain single-instance kernels (one fly), settled to the same steady firing as the batched
+    engine, timed two ways: replayed from a CUDA graph of 20 steps with the L2 left warm (like the
+    batched figure), and launched eagerly step by step with the L2 flushed between timed steps."""
     eng = build_engine(cfg, 1, device, "step")
     eng.step(max(3, warmup))
-    g = capture(eng, 10)              # settle to the steady firing the batched figures are timed at
-    for _ in range(max(0, settle) // 10):
+    g = capture(eng, 20)              # settle to the steady firing the batched figures are timed at
+    for _ in range(max(0, settle) // 20):
         g.replay()
     torch.cuda.synchronize()
+    graph_ms = time_graph(g, 10) / 200
     del g
     eng.step(1)
     buf = torch.zeros(int(2 * L2_BYTES // 4), device=device)
     n = min(steps, 50)
-    ms = events_time(lambda: eng.step(1), n, flush=lambda: flush_l2(buf))
-    del buf
-    return eng, ms
+    eager_ms = events_time(lambda: eng.step(1), n, flush=lambda: flush_l2(buf))
+    del buf, eng
+    torch.cuda.empty_cache()
+    N = cfg.n_rate + cfg.n_spiking
+    return {"graph": {"value": N / (graph_ms / 1000.0), "ms_per_step": graph_ms,
+                      "how": "CUDA graph of 20 steps replayed back to back, L2 warm"},
+            "eager_flushed": {"value": N / (eager_ms / 1000.0), "ms_per_step": eager_ms,
+                              "how": "one call per step, L2 flushed between timed steps"}}
 
 
 def measure_adjoint(device) -> dict:
@@ -348,7 +379,7 @@ def measure_adjoint(device) -> dict:
             "checkpoint": 20}
 
 
-def measure_e2e(cfg, eng, device, steps, chunk: int = 10) -> dict:
+def measure_e2e(cfg, eng, device, steps, chunk: int = 20) -> dict:
     """Public-API loop: every step copies its own radiance frame in from pinned host memory, forms
     the photoreceptor activity, steps the whole fly and copies its motor readout out to pinned host
     memory. The copies run on two copy streams, so a step's input arrives while the previous step
@@ -416,6 +447,7 @@ def measure_e2e(cfg, eng, device, steps, chunk: int = 10) -> dict:
         one(k % chunk)
         torch.cuda.current_stream().synchronize()           # the host reads this step's readout
     dt_eager = time.perf_counter() - t0
+    eng.step(to_group_end(eng, 0))                          # the graph below starts at a group boundary
     s = torch.cuda.Stream()
     s.wait_stream(torch.cuda.current_stream())
     g = torch.cuda.CUDAGraph()
@@ -446,49 +478,102 @@ def measure_e2e(cfg, eng, device, steps, chunk: int = 10) -> dict:
                       "note": "the same calls launched one by one, the host synchronising every step"}}
 
 
-def cpu_port_rate(cfg, batch: int, steps: int, threads: int) -> dict:
-    """The oracle whole-fly step on host cores: neuron-steps/s over a bounded sample."""
-    import oracle
-    from flyb200 import _abi
-    from flyb200.brain import LIFParams, lif_coefficients, out_edges
-    from flyb200.weights import lif_weights
-    p = LIFParams(**cfg.lif.params)
-    W, _ = lif_weights(cfg.lif.c, p)
-    ptr, edges, mode = out_edges(W, p.w_syn)
-    n = cfg.n_spiking
-    st = oracle.LifState(n, batch, 19, mode, p.v_rest)
-    st.poisson_p[cfg.sensory_idx, :] = np.float32(cfg.lif.poisson_hz) * np.float32(p.dt / 1000.0)
-    o = cfg.optic
-    Wr = o.W_rr()
-    tau = o.tau_of_type[o.type_of].astype(np.float32)
-    a = np.exp(-0.1 / tau).astype(np.float32)
-    aad = float(np.exp(-0.1 / o.adapt_tau_ms))
-    m = o.m
-    v = np.zeros((m, batch), np.float32)
-    ad = np.zeros((m, batch), np.float32)
-    rng = np.random.default_rng(0)
-    pr = (rng.standard_normal((m, batch)) * 0.1).astype(np.float32)
-    Wrs, Wsr = o.W_rs.tocsr(), o.W_sr.tocsr()
-    P = lif_coefficients(p, False)
-    flags = _abi.LIF_POISSON | _abi.LIF_COUNTS
+class OraclePort:
+    """The whole-fly step restated in C (oracle/), run on host cores in the engine's order: spike
+    input, optic substep, VPN drive, LIF step. The LIF population is in the engine's stored order
+    (WholeFly.lif_order), so a settled engine's state can be copied in as it is."""
 
-    def step():
-        spk = oracle.spmm(Wrs.indptr, Wrs.indices, Wrs.data, st.rate, batch, rows=m, x_div=100.0, x_lo=0.0, x_hi=3.0,
-                          alpha=o.gain_fb)
-        oracle.optic_run(v, ad, Wr.indptr, Wr.indices, Wr.data, pr, spk, a, o.b, o.gain_rr, o.adapt_gain, aad, 1,
-                         threads=threads)
-        dr = (np.clip(v + o.b[:, None], 0, 1) - o.b[:, None]).astype(np.float32)
-        oracle.spmm(Wsr.indptr, Wsr.indices, Wsr.data, dr, batch, rows=n, y=st.drive, alpha=o.gain_out_mv,
-                    y_lo=-o.drive_clip_mv, y_hi=o.drive_clip_mv)
-        oracle.lif_run(st, ptr, edges, P, n_delay=18, flags=flags, nsteps=1, seed=1, threads=threads)
+    def __init__(self, cfg, batch: int, threads: int):
+        import oracle
+        from flyb200 import _abi
+        from flyb200.brain import LIFParams, lif_coefficients, out_edges
+        from flyb200.weights import lif_weights
+        self.oracle, self.cfg, self.B, self.threads = oracle, cfg, batch, threads
+        o = cfg.optic
+        n = cfg.n_spiking
+        driven = np.unique(o.W_sr.tocoo().row)
+        order = np.concatenate([np.setdiff1d(np.arange(n), driven), driven])      # WholeFly.lif_order
+        pos = np.empty(n, np.int64)
+        pos[order] = np.arange(n)
+        self.p = LIFParams(**{**cfg.lif.params, "dt": 0.1})
+        W, _ = lif_weights(cfg.lif.c.subset(order), self.p)
+        self.ptr, self.edges, mode = out_edges(W, self.p.w_syn)
+        self.st = oracle.LifState(n, batch, 19, mode, self.p.v_rest)
+        self.st.poisson_p[pos[np.asarray(cfg.sensory_idx)], :] = np.float32(cfg.lif.poisson_hz) * np.float32(self.p.dt / 1000.0)
+        self.Wr = o.W_rr()
+        self.a = np.exp(-0.1 / o.tau_of_type[o.type_of].astype(np.float32)).astype(np.float32)
+        self.aad = float(np.exp(-0.1 / o.adapt_tau_ms))
+        self.v = np.zeros((o.m, batch), np.float32)
+        self.ad = np.zeros((o.m, batch), np.float32)
+        rad = o.grating(0.0, batch, seed=0)
+        ip = (rad[:, o.pr_column, :] * o.sens[None]).sum(-1)
+        mean = ip.mean(1, keepdims=True)
+        a_pr = np.clip((ip - mean) / (mean + 0.02), -1.0, 2.0).T.astype(np.float32)
+        M = o.W_rp.tocsr()
+        self.pr = oracle.spmm(M.indptr, M.indices, M.data, a_pr, batch, rows=o.m, alpha=o.gain_in)
+        self.Wrs = o.W_rs.tocsc()[:, order].tocsr()
+        self.Wsr = o.W_sr.tocsr()[order]
+        self.P = lif_coefficients(self.p, False)
+        self.flags = _abi.LIF_POISSON | _abi.LIF_COUNTS
+        self.events = 0
 
-    step()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        step()
-    dt = time.perf_counter() - t0
-    return {"value": (m + n) * batch * steps / dt, "unit": "neuron-steps/s", "cores": threads,
-            "kind": "port", "sample": f"{steps} whole-fly steps x {batch} flies ({m + n:,} neurons) on the C oracle"}
+    @classmethod
+    def from_engine(cls, eng, threads: int, flies: int | None = None):
+        """The engine's state (its first `flies` flies) copied into a port."""
+        B = eng.B if flies is None else flies
+        port = cls(eng.cfg, B, threads)
+        lif = eng.lif
+        for name, oname in (("v", "v"), ("g", "g"), ("refrac", "refrac"), ("rate", "rate"), ("spike_counts", "counts"),
+                            ("spikes", "spikes"), ("adapt", "adapt"), ("res", "res"), ("drive", "drive"),
+                            ("poisson_p", "poisson_p")):
+            getattr(port.st, oname)[...] = lif._st[name][:, :B].cpu().numpy()
+        port.st.ring[...] = lif.ring[:, :, :B].cpu().numpy()
+        clock = lif._clock.cpu().numpy()
+        port.st.step, port.st.ring_pos = int(clock[0]), int(clock[1]) % lif.R
+        port.v[...] = eng.optic.v_s[:, :B].cpu().numpy()
+        port.ad[...] = eng.optic.adapt_s[:, :B].cpu().numpy()
+        port.pr[...] = eng.optic.pr_in[:, :B].cpu().numpy()
+        return port
+
+    def widen(self, batch: int):
+        """A port of `batch` flies, each starting from fly 0's state (their Poisson streams differ)."""
+        wide = OraclePort.__new__(OraclePort)
+        wide.__dict__ = dict(self.__dict__)
+        st = self.st.copy()
+        for name in self.oracle.LifState.NAMES:
+            setattr(st, name, np.ascontiguousarray(np.repeat(getattr(self.st, name)[:, :1], batch, axis=1)))
+        st.ring = np.ascontiguousarray(np.repeat(self.st.ring[:, :, :1], batch, axis=2))
+        st.batch = batch
+        wide.st, wide.B = st, batch
+        wide.v = np.ascontiguousarray(np.repeat(self.v[:, :1], batch, axis=1))
+        wide.ad = np.ascontiguousarray(np.repeat(self.ad[:, :1], batch, axis=1))
+        wide.pr = np.ascontiguousarray(np.repeat(self.pr[:, :1], batch, axis=1))
+        return wide
+
+    def step(self) -> None:
+        o, st, ora, B = self.cfg.optic, self.st, self.oracle, self.B
+        spk = ora.spmm(self.Wrs.indptr, self.Wrs.indices, self.Wrs.data, st.rate, B, rows=o.m, x_div=100.0, x_lo=0.0,
+                       x_hi=3.0, alpha=o.gain_fb)
+        ora.optic_run(self.v, self.ad, self.Wr.indptr, self.Wr.indices, self.Wr.data, self.pr, spk, self.a, o.b,
+                      o.gain_rr, o.adapt_gain, self.aad, 1, threads=self.threads)
+        dr = (np.clip(self.v + o.b[:, None], 0, 1) - o.b[:, None]).astype(np.float32)
+        ora.spmm(self.Wsr.indptr, self.Wsr.indices, self.Wsr.data, dr, B, rows=self.cfg.n_spiking, y=st.drive,
+                 alpha=o.gain_out_mv, y_lo=-o.drive_clip_mv, y_hi=o.drive_clip_mv)
+        self.events += ora.lif_run(st, self.ptr, self.edges, self.P, n_delay=18, flags=self.flags, nsteps=1, seed=1,
+                                   threads=self.threads)[1]
+
+    def rate(self, steps: int) -> dict:
+        """neuron-steps/s over `steps` timed steps (after one untimed step)."""
+        self.step()
+        ev0 = self.events
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            self.step()
+        dt = time.perf_counter() - t0
+        n = self.cfg.n_rate + self.cfg.n_spiking
+        return {"value": n * self.B * steps / dt, "unit": "neuron-steps/s", "cores": self.threads, "kind": "port",
+                "ms_per_step": dt / steps * 1000.0, "synaptic_events_per_step": (self.events - ev0) / steps,
+                "mean_rate_hz": float(self.st.rate.mean())}
 
 
 def measure_tracer(device, batch: int = BATCH, reps: int = 50, cpu: bool = True) -> dict:
@@ -603,6 +688,301 @@ def reference_tracer(device, scenes, dirs, w, pose, ours, reps: int):
     return res
 
 
+# ------------------------------------------------------------------ the reference's own code
+REF_DIR = ROOT / "baseline" / "_ref"
+
+
+def reference_modules():
+    """flyverse (the unmodified reference, installed under baseline/_ref): {name: module}, or
+    {"unavailable": why}."""
+    if not (REF_DIR / "flyverse" / "brain.py").exists():
+        return {"unavailable": "the reference is not installed under baseline/_ref"}
+    import importlib
+    os.environ.setdefault("FLYVERSE_CUDA_CACHE", tempfile.mkdtemp(prefix="flyverse_cuda_"))
+    sys.path.insert(0, str(REF_DIR))
+    try:
+        return {k: importlib.import_module(f"flyverse.{k}") for k in ("brain", "connectome", "cuda", "optic")}
+    except Exception as e:                # noqa: BLE001 - report, do not fail the bench
+        return {"unavailable": f"import failed: {e}"}
+    finally:
+        sys.path.remove(str(REF_DIR))
+
+
+def reference_brain(ref, cfg2, device, batch):
+    """The reference's Brain on config 2's graph, event-driven, with the benchmark's model constants."""
+    import pandas as pd
+    c = cfg2.c
+    rc = ref["connectome"].Connectome(c.neurons[["bodyId", "type", "superclass", "nt"]].copy(), c.W.copy(),
+                                      pd.Series(np.arange(c.n), index=c.neurons.bodyId.to_numpy()))
+    cuda = torch.device(device).type == "cuda"
+    b = ref["brain"].Brain(rc, ref["brain"].LIFParams(**cfg2.params, event_driven=True), device=device, seed=0,
+                           batch=batch, cuda_kernels=True if cuda else None)
+    b.set_poisson(cfg2.poisson_idx, cfg2.poisson_hz)
+    b.record_activity = True
+    return b
+
+
+def graph_ms_per_step(step, steps: int, reps: int, generator=None) -> float:
+    """Device ms per step of `step(steps)` captured once as a CUDA graph and replayed `reps` times."""
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    if generator is not None:
+        g.register_generator_state(generator)
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            step(steps)
+    torch.cuda.current_stream().wait_stream(s)
+    g.replay()
+    ms = time_graph(g, reps) / (steps * reps)
+    del g
+    return ms
+
+
+def reference_lif_gpu(ref, cfg2, device, batch) -> dict:
+    """The reference's CUDA LIF step (flyverse/cuda.py + kernels/neural.cu, compiled by its own nvcc
+    call for this GPU: g decay, event scatter, torch.rand, fused update) on config 2's graph, eager
+    and captured in a CUDA graph of n_delay steps (its FlyBrain replays such graphs), after 500
+    steps from rest."""
+    b = reference_brain(ref, cfg2, device, batch)
+    b.step(500)
+    torch.cuda.synchronize()
+    eager = events_time(lambda: b.step(1), 50)
+    graph = graph_ms_per_step(b.step, b.n_delay, 10, b.gen)
+    return {"eager_ms": eager, "graph_ms": graph, "path": "native neural.cu (launch_events, launch_lif), cuda_sparse=torch"}
+
+
+def ours_lif(cfg2, device, batch) -> float:
+    """This library's Brain on the same graph and constants: device ms per step, graph-replayed
+    chunks of 20 steps after 500 steps from rest, the launch shape autotuned."""
+    from flyb200 import autotune
+    from flyb200.brain import Brain, LIFParams
+    b = Brain(cfg2.c, LIFParams(**cfg2.params), device=device, seed=0, batch=batch, launch="step")
+    b.set_poisson(cfg2.poisson_idx, cfg2.poisson_hz)
+    b.record_activity = True
+    b.step(500)
+    autotune.tune_lif(b, steps=10)
+    b.step(4 - b.step_count % 4)
+    return graph_ms_per_step(b.step, 20, 10)
+
+
+def reference_optic_gpu(ref, cfg3, device, batch) -> dict:
+    """The reference's CUDA optic substep on config 3's lobe (optic.py:585-589: the recurrent
+    product through its `_mv` with torch's sparse CSR (cuSPARSE, its default cuda_sparse) or its
+    warp CSR kernel, then launch_optic), under a held random input."""
+    from types import SimpleNamespace
+    optic, cuda = ref["optic"], ref["cuda"]
+    W = cfg3.W_rr()
+    rng = np.random.default_rng(0)
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a, np.float32), device=device)  # noqa: E731
+    out = {}
+    for sparse in ("torch", "warp"):
+        M = optic._csr(W, device, cuda_sparse=sparse)
+        lobe = SimpleNamespace(v=t(np.zeros((batch, cfg3.m))), adapt=t(np.zeros((batch, cfg3.m))), B=batch,
+                               n_rate=cfg3.m, p=optic.OpticParams(adapt_tau_ms=cfg3.adapt_tau_ms, dt_ms=cfg3.dt_ms),
+                               _a=t(cfg3.a), b_vec=t(cfg3.b), _a_ad=cfg3.aad, _cuda_dr=t(np.zeros((batch, cfg3.m))))
+        pr, spk = t(rng.standard_normal((batch, cfg3.m)) * 0.2), t(np.zeros((batch, cfg3.m)))
+        cuda.optic_dr(lobe.v, lobe.b_vec, lobe._cuda_dr)
+
+        def substeps(n):
+            for _ in range(n):
+                cuda.optic_update(lobe, optic._mv(M, lobe._cuda_dr), pr, spk)
+
+        substeps(5)
+        torch.cuda.synchronize()
+        out[sparse] = {"eager_ms": events_time(lambda: substeps(1), 20), "graph_ms": graph_ms_per_step(substeps, 10, 5)}
+    return out
+
+
+def ours_optic(cfg3, device, batch) -> float:
+    """This library's fused substep on the same lobe: device ms per substep (autotuned shape)."""
+    from flyb200 import autotune
+    from flyb200.optic import OpticCore
+    core = OpticCore(cfg3.W_rr(), cfg3.a, cfg3.b, batch=batch, device=device, gain_rr=cfg3.gain_rr,
+                     adapt_gain=cfg3.adapt_gain, aad=cfg3.aad, launch="step")
+    rng = np.random.default_rng(0)
+    core.pr_in.copy_(torch.from_numpy((rng.standard_normal((cfg3.m, batch)) * 0.2).astype(np.float32)))
+    autotune.tune_optic(core, steps=10)
+    core.substeps(2)
+    return graph_ms_per_step(lambda n: core.substeps(n, carry=True), 10, 5)
+
+
+def measure_reference_gpu(device, cfg2, cfg3) -> dict:
+    """The reference's own GPU kernels (its stock cuda_kernels=True path from baseline/_ref) beside
+    this library's kernels on the same configurations and this GPU: config 2's LIF at 1 and 64
+    flies, config 3's optic substep at 1 and 64 flies."""
+    ref = reference_modules()
+    if "unavailable" in ref:
+        return ref
+    res = {"lif_c2": {}, "optic_c3": {}}
+    for B in (1, 64):
+        try:
+            r = reference_lif_gpu(ref, cfg2, device, B)
+            r["ours_ms"] = ours_lif(cfg2, device, B)
+            r["speedup_vs_graph"] = r["graph_ms"] / r["ours_ms"]
+        except Exception as e:            # noqa: BLE001 - report, do not fail the bench
+            r = {"unavailable": f"{type(e).__name__}: {e}"}
+        res["lif_c2"][f"B{B}"] = r
+        torch.cuda.empty_cache()
+        try:
+            r = reference_optic_gpu(ref, cfg3, device, B)
+            r["ours_ms"] = ours_optic(cfg3, device, B)
+            r["speedup_vs_best_graph"] = min(v["graph_ms"] for v in r.values() if isinstance(v, dict)) / r["ours_ms"]
+        except Exception as e:            # noqa: BLE001
+            r = {"unavailable": f"{type(e).__name__}: {e}"}
+        res["optic_c3"][f"B{B}"] = r
+        torch.cuda.empty_cache()
+    return res
+
+
+def reference_own_cpu(cfg2, cfg3, threads: int) -> dict:
+    """The reference's own CPU code on this host (torch CPU, `threads` threads): Brain.step of
+    config 2 at one fly (event-driven, after 100 steps from rest; median of 5 runs of 20 steps) and
+    OpticLobe._substep of config 3 at one fly (median of 5 runs of 5 substeps)."""
+    ref = reference_modules()
+    if "unavailable" in ref:
+        return ref
+    torch.set_num_threads(threads)
+    b = reference_brain(ref, cfg2, "cpu", 1)
+    b.step(100)
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        b.step(20)
+        runs.append((time.perf_counter() - t0) / 20)
+    lif_s = float(np.median(runs))
+    optic = ref["optic"]
+    W = cfg3.W_rr()
+    lobe = object.__new__(optic.OpticLobe)
+    lobe.p = optic.OpticParams(adapt_tau_ms=cfg3.adapt_tau_ms, dt_ms=cfg3.dt_ms)
+    lobe.slow, lobe._hooks = None, False
+    lobe.W_rr = torch.sparse_csr_tensor(torch.from_numpy(W.indptr.astype(np.int64)),
+                                        torch.from_numpy(W.indices.astype(np.int64)), torch.from_numpy(W.data),
+                                        size=W.shape)
+    lobe._a, lobe.b_vec, lobe._a_ad = torch.from_numpy(cfg3.a), torch.from_numpy(cfg3.b), cfg3.aad
+    lobe.v, lobe.adapt = torch.zeros(1, cfg3.m), torch.zeros(1, cfg3.m)
+    rng = np.random.default_rng(0)
+    pr = torch.from_numpy((rng.standard_normal((1, cfg3.m)) * 0.2).astype(np.float32))
+    spk = torch.zeros(1, cfg3.m)
+    optic.OpticLobe._substep(lobe, pr, spk)
+    runs = []
+    for _ in range(5):
+        t0 = time.perf_counter()
+        for _ in range(5):
+            optic.OpticLobe._substep(lobe, pr, spk)
+        runs.append((time.perf_counter() - t0) / 5)
+    opt_s = float(np.median(runs))
+    return {"lif_c2_b1": {"ms_per_step": lif_s * 1000, "neuron_steps_per_s": cfg2.c.n / lif_s},
+            "optic_c3_b1": {"ms_per_substep": opt_s * 1000, "unit_steps_per_s": cfg3.m / opt_s},
+            "cores": threads, "code": "flyverse.brain.Brain.step (event_driven) / flyverse.optic.OpticLobe._substep, "
+                                      "torch CPU, from baseline/_ref"}
+
+
+# ------------------------------------------------------------------ uneven rollouts
+def measure_uneven(cfg, device, batch: int, lengths: tuple, steps: int, warm: int, chunk: int = 20,
+                   seed: int = 0) -> dict:
+    """Uneven rollouts: every fly runs episodes back to back, lengths uniform on `lengths` steps,
+    each with its own Poisson rate (uniform 20-200 Hz on the sensory cells); a fly whose episode
+    ends inside a replay of `chunk` steps is reset after that replay (WholeFly.reset: state, pending
+    input and spike history to rest; BatchSim's per-row resets, batch_sim.py:282-304) and starts
+    the next episode with a new rate while the others run on. `steps` steps are timed on the device
+    (replays and resets) after `warm` steps; the autotuners pick the launch shapes after the warm-up."""
+    from flyb200 import autotune
+    from flyb200.whole import WholeFly
+    rng = np.random.default_rng(seed)
+    eng = WholeFly(cfg, batch, device=device, seed=seed + 1, launch="step")
+    eng.set_poisson_rates(rng.uniform(20.0, 200.0, batch))
+    eng.set_radiance(torch.from_numpy(cfg.optic.grating(0.0, batch, seed=seed)).to(device), 0.1)
+    left = rng.integers(lengths[0], lengths[1] + 1, batch)
+    eng.step(chunk)
+    left -= chunk
+    g = capture(eng, chunk)
+
+    def run(n_replays: int) -> int:
+        nonlocal left
+        resets = 0
+        for _ in range(n_replays):
+            g.replay()
+            left -= chunk
+            done = np.flatnonzero(left <= 0)
+            if done.size:
+                eng.reset(done, rng.uniform(20.0, 200.0, done.size))
+                left[done] = rng.integers(lengths[0], lengths[1] + 1, done.size)
+                resets += int(done.size)
+        return resets
+
+    run(warm // chunk)
+    torch.cuda.synchronize()
+    del g
+    eng.tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
+    eng.step(chunk)                              # keeps the step count a multiple of the chunk
+    left -= chunk
+    g = capture(eng, chunk)
+    torch.cuda.synchronize()
+    ev0 = eng.lif.synaptic_events
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    resets = run(steps // chunk)
+    t1.record()
+    t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    n_steps = steps // chunk * chunk
+    eng.lif.check()
+    out = {"value": eng.n_neurons * batch * n_steps / (ms / 1000.0), "unit": "neuron-steps/s",
+           "ms_per_step": ms / n_steps, "flies": batch, "episode_steps": list(lengths), "timed_steps": n_steps,
+           "episodes_ended": resets, "synaptic_events_per_step": (eng.lif.synaptic_events - ev0) / n_steps,
+           "lif": {k: v for k, v in eng.tuned["lif"].items() if k != "all"},
+           "note": f"episode ends take effect at the end of the {chunk}-step replay they fall in"}
+    del g, eng
+    torch.cuda.empty_cache()
+    return out
+
+
+# ------------------------------------------------------------------ FP32 against FP64
+def fp64_error(device, cfg3, eng) -> dict:
+    """max |FP32 - FP64| of the optic state after 200 substeps: config 3's lobe at one fly from rest
+    under a held random input, and the whole fly's lobe continued from the settled engine (its first
+    8 flies, their held inputs), each against the FP64 oracle from the same start."""
+    import oracle
+    from flyb200.optic import OpticCore
+    out = {}
+    W = cfg3.W_rr()
+    rng = np.random.default_rng(0)
+    pr = (rng.standard_normal((cfg3.m, 1)) * 0.2).astype(np.float32)
+    core = OpticCore(W, cfg3.a, cfg3.b, batch=1, device=device, gain_rr=cfg3.gain_rr, adapt_gain=cfg3.adapt_gain,
+                     aad=cfg3.aad, launch="step")
+    core.pr_in.copy_(torch.from_numpy(pr))
+    core.substeps(200)
+    v64, a64 = np.zeros((cfg3.m, 1)), np.zeros((cfg3.m, 1))
+    oracle.optic_run_f64(v64, a64, W.indptr, W.indices, W.data, pr, np.zeros_like(pr), cfg3.a, cfg3.b, cfg3.gain_rr,
+                         cfg3.adapt_gain, cfg3.aad, 200)
+    out["C3_b1_200_substeps"] = _err(core.v_s.cpu().numpy(), v64, cfg3.b)
+    o, B = eng.cfg.optic, 8
+    W = o.W_rr()
+    a = np.exp(-0.1 / o.tau_of_type[o.type_of].astype(np.float32)).astype(np.float32)
+    aad = float(np.exp(-0.1 / o.adapt_tau_ms))
+    v0 = eng.optic.v_s[:, :B].cpu().numpy()
+    ad0 = eng.optic.adapt_s[:, :B].cpu().numpy()
+    pr = eng.optic.pr_in[:, :B].cpu().numpy()
+    spk = eng.optic.spk_in[:, :B].cpu().numpy()
+    core = OpticCore(W, a, o.b, batch=B, device=device, gain_rr=o.gain_rr, adapt_gain=o.adapt_gain, aad=aad,
+                     launch="step")
+    for dst, src in ((core.v_s, v0), (core.adapt_s, ad0), (core.pr_in, pr), (core.spk_in, spk)):
+        dst.copy_(torch.from_numpy(src))
+    core.substeps(200)
+    v64, a64 = v0.astype(np.float64), ad0.astype(np.float64)
+    oracle.optic_run_f64(v64, a64, W.indptr, W.indices, W.data, pr, spk, a, o.b, o.gain_rr, o.adapt_gain, aad, 200)
+    out["C5_lobe_8_flies_200_substeps"] = _err(core.v_s.cpu().numpy(), v64, o.b)
+    return out
+
+
+def _err(v32: np.ndarray, v64: np.ndarray, b: np.ndarray) -> dict:
+    r32 = np.clip(v32 + b[:, None], 0, 1)
+    r64 = np.clip(v64 + b[:, None], 0, 1)
+    return {"v_abs": float(np.abs(v32 - v64).max()), "rate_abs": float(np.abs(r32 - r64).max()),
+            "v_scale": float(np.abs(v64).max())}
+
+
 # ------------------------------------------------------------------ arms
 def arm_config(world: int) -> dict:
     """The workload both arms report (the reference arm times a bounded sample of it)."""
@@ -610,28 +990,35 @@ def arm_config(world: int) -> dict:
                         "dt 0.1 ms, optic<->LIF coupling every step", "batch_per_gpu": BATCH,
             "flies_total": BATCH * world, "l2": "state of 64 flies > 126 MB L2; no flush needed",
             "parallelism": f"fly shards x{world}, no per-step collective",
-            "state": f"our arm: steady firing after {SETTLE_STEPS} settling steps (onset from rest reported "
-                     f"under 'onset'); reference arm: a sample of the first steps from rest"}
+            "state": f"steady firing after {SETTLE_STEPS} settling steps"}
 
 
 def reference_arm(args) -> None:
-    """The CPU port of the path (the C oracle; the reference itself is Python/torch and is not
-    installed on the GPU machines), timed on every host thread, same metric and config."""
+    """The CPU port of the path (the C oracle; the reference itself is Python/torch and has no C
+    implementation of the step to build) on every host thread, same metric, config and state: one
+    fly settled for the same number of steps from rest, its state given to all 64 flies (their
+    Poisson streams differ), then whole 64-fly steps timed."""
     from flyb200 import synthetic
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cfg = synthetic.whole_fly_config5(seed=0)
     threads = os.cpu_count() or 1
-    batch = 8
-    r = cpu_port_rate(cfg, batch, max(1, min(args.steps, 6)), threads)
-    n = cfg.n_rate + cfg.n_spiking
-    line = {"metric": METRIC, "value": r["value"], "unit": "neuron-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": n * BATCH / r["value"] * 1000.0, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded whole_fly_config5)",
-            "config": {**arm_config(args.gpus), "sample": f"{batch} flies per timed step; ms_per_step is a "
-                                                         f"{BATCH}-fly step at the sampled rate"},
-            "impl": "reference", "cpu_baseline": r,
+    one = OraclePort(cfg, 1, threads)
+    t0 = time.perf_counter()
+    for _ in range(SETTLE_STEPS):
+        one.step()
+    settle_s = time.perf_counter() - t0
+    port = one.widen(BATCH)
+    steps = max(2, min(args.steps, 6))
+    r = port.rate(steps)
+    r["sample"] = (f"{steps} whole-fly steps x {BATCH} flies ({cfg.n_rate + cfg.n_spiking:,} neurons) on the C oracle, "
+                   f"from a fly settled {SETTLE_STEPS} steps ({settle_s:.0f} s, untimed; {r.pop('mean_rate_hz'):.0f} Hz "
+                   f"mean)")
+    line = {"metric": METRIC, "value": r["value"], "unit": "neuron-steps/s", "n_gpus": args.gpus, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded whole_fly_config5)",
+            "config": arm_config(args.gpus), "impl": "reference", "cpu_baseline": r,
             "e2e": {"value": r["value"], "unit": "neuron-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -643,6 +1030,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="flyb200", choices=["flyb200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="the headline, roofline and e2e only")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -678,6 +1066,7 @@ def main() -> None:
         del g                      # no collective is captured; release the graph before the group
         dist.destroy_process_group()
     value = N * BATCH * world * timed_steps / (ms / 1000.0)
+    launches = eng.launches(chunk) * reps
     eng.lif.check()
     if rank != 0:
         return
@@ -687,49 +1076,63 @@ def main() -> None:
     opt_gbs = roof["optic_bytes"] / (roof["optic_ms"] / 1000.0) / 1e9
     dom = "lif" if roof["lif_ms"] >= roof["optic_ms"] else "optic"
     achieved = lif_gbs if dom == "lif" else opt_gbs
-    # the whole-fly configuration at 256 flies (its uneven-rollout variant runs through BatchSim)
-    n256 = min(args.steps, 40)
-    eng256, g256, c256, r256, onset256 = measure_batched(cfg, device, n256, args.warmup, fly0=0, batch=256)
-    ev256 = eng256.lif.synaptic_events
-    ms256 = time_graph(g256, r256) / (c256 * r256)
-    batch256 = {"value": N * 256 / (ms256 / 1000.0), "ms_per_step": ms256, "steps": c256 * r256,
-                "synaptic_events_per_step": (eng256.lif.synaptic_events - ev256) / (c256 * r256),
-                "onset": {k: onset256[k] for k in ("value", "ms_per_step", "synaptic_events_per_step")},
-                "autotune": {k: {kk: vv for kk, vv in v.items() if kk != "all"} for k, v in eng256.tuned.items()}}
-    del g256, eng256
-    torch.cuda.empty_cache()
-    plain_eng, plain_ms = measure_plain(cfg, device, args.steps, args.warmup)
-    batch1 = N / (plain_ms / 1000.0)
-    adj = measure_adjoint(device)
-    tracer = measure_tracer(device, cpu=not args.no_cpu_baseline)
+    threads = os.cpu_count() or 1
+    cpu = None
+    if not args.no_cpu_baseline:             # the same settled state, copied into the C oracle
+        cpu = OraclePort.from_engine(eng, threads).rate(3)
+        cpu["sample"] = (f"3 whole-fly steps x {BATCH} flies ({N:,} neurons) on the C oracle, from this run's settled "
+                         f"state ({cpu.pop('mean_rate_hz'):.0f} Hz mean)")
     e2e = measure_e2e(cfg, eng, device, args.steps)
     traffic = read_traffic().get(dom)
     l2 = measure_l2_gather(device)
-    o = cfg.optic
-    optic_l2_bytes = int(o.W0.nnz) * BATCH * 4 + roof["optic_bytes"]     # dr gathers + the streamed bytes
-    cpu = None
-    if not args.no_cpu_baseline:
-        cpu = cpu_port_rate(cfg, 8, 3, os.cpu_count() or 1)
+    optic_l2_bytes = int(cfg.optic.W0.nnz) * BATCH * 4 + roof["optic_bytes"]     # dr gathers + the streamed bytes
+    extras = {}
+    if not args.no_extras:
+        cfg3 = synthetic.optic_config3(seed=3)
+        extras["fp64_max_err"] = fp64_error(device, cfg3, eng)
+        del g
+        autotune_summary = {k: {kk: vv for kk, vv in v.items() if kk != "all"} for k, v in eng.tuned.items()}
+        state = f"steady firing after {SETTLE_STEPS} settling steps (mean rate {float(eng.lif.rate.mean()):.0f} Hz)"
+        del eng
+        torch.cuda.empty_cache()
+        # the whole fly at 256 flies (config 5's width), even lengths from the steady state
+        n256 = min(args.steps, 40)
+        eng256, g256, c256, r256, onset256 = measure_batched(cfg, device, n256, args.warmup, fly0=0, batch=256)
+        ev256 = eng256.lif.synaptic_events
+        ms256 = time_graph(g256, r256) / (c256 * r256)
+        extras["batch256"] = {"value": N * 256 / (ms256 / 1000.0), "ms_per_step": ms256, "steps": c256 * r256,
+                              "synaptic_events_per_step": (eng256.lif.synaptic_events - ev256) / (c256 * r256),
+                              "onset": {k: onset256[k] for k in ("value", "ms_per_step", "synaptic_events_per_step")},
+                              "autotune": {k: {kk: vv for kk, vv in v.items() if kk != "all"}
+                                           for k, v in eng256.tuned.items()}}
+        del g256, eng256
+        torch.cuda.empty_cache()
+        extras["uneven_c5_b256"] = measure_uneven(cfg, device, 256, (200, 2000), 2000, 600)
+        cfg4 = synthetic.batched_config4(seed=0)
+        extras["uneven_c4_b64"] = measure_uneven(cfg4, device, BATCH, (500, 4000), 2000, 1000)
+        plain = measure_plain(cfg, device, args.steps, args.warmup)
+        extras["reference_gpu"] = measure_reference_gpu(device, cfg4.lif, cfg3)
+        if not args.no_cpu_baseline:
+            extras["reference_own_cpu"] = reference_own_cpu(cfg4.lif, cfg3, threads)
+        del cfg4
+        adj = measure_adjoint(device)
+        extras["tracer"] = measure_tracer(device, cpu=not args.no_cpu_baseline)
+        extras["onset"] = onset
+        extras["autotune"] = autotune_summary
+        extras["state"] = state
     line = {
         "metric": METRIC, "value": value, "unit": "neuron-steps/s", "n_gpus": world, "steps": timed_steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms / timed_steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded whole_fly_config5)",
         "config": arm_config(world),
-        "batch1": {"value": batch1, "ms_per_step": plain_ms, "l2": "flushed between timed steps",
-                   "launches": "one launch per kernel per step"},
-        "batched_over_plain": value / world / batch1,
-        "batch256": batch256,
-        "adjoint": adj,
-        "tracer": tracer,
+        **{k: v for k, v in extras.items() if k != "fp64_max_err"},
         "synaptic_events_per_s": events_per_step * world * timed_steps / (ms / 1000.0),
         "synaptic_events_per_step": events_per_step,
-        "state": f"steady firing after {SETTLE_STEPS} settling steps (mean rate {float(eng.lif.rate.mean()):.0f} Hz)",
-        "onset": onset,
         "roofline": {"bound": "hbm", "kernel": f"{dom} step (B=64)", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                      "peak_source": peaks["source"], "lif_gbs": lif_gbs, "optic_gbs": opt_gbs,
                      "lif_ms": roof["lif_ms"], "optic_ms": roof["optic_ms"], "lif_bytes": roof["lif_bytes"],
-                     "optic_bytes": roof["optic_bytes"],
+                     "optic_bytes": roof["optic_bytes"], "lif_group": roof["lif_group"],
                      "l2_gather": {"kernel": "optic step (B=64)", "bytes": optic_l2_bytes,
                                    "achieved_tbs": optic_l2_bytes / (roof["optic_ms"] / 1000.0) / 1e12,
                                    "peak_tbs": l2["tbs"],
@@ -738,10 +1141,14 @@ def main() -> None:
                                    "note": "the optic substep gathers nnz x 64 x 4 B of L2-resident dr"}},
         "cpu_baseline": cpu,
         "e2e": e2e,
-        "autotune": {k: {kk: vv for kk, vv in v.items()} for k, v in eng.tuned.items()},
-        "gpu_launches": eng.launches(chunk) * reps,
-        "clocks": clocks,
     }
+    if not args.no_extras:
+        line["batch1"] = plain
+        line["batched_over_plain"] = value / world / plain["graph"]["value"]
+        line["adjoint"] = adj
+        line["fp64_max_err"] = extras["fp64_max_err"]
+    line["gpu_launches"] = launches
+    line["clocks"] = clocks
     print(json.dumps(line))
 
 

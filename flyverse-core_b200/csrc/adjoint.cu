@@ -222,9 +222,47 @@ int adjoint_blocks_per_sm() {
   return b;
 }
 
+// Segmented gather-sum for the gradient reductions: out[s] = alpha * sum over positions e of
+// segment s (seg_ptr[s] <= e < seg_ptr[s + 1]) of x[idx[e]] * (w ? w[idx[e]] : 1). One warp per
+// segment: lane l sums positions l, l + 32, ... in order, then a fixed butterfly; the result is
+// deterministic and FP32 throughout. The pair gains' gradient is the per-edge accumulator summed
+// over the edges of each pair (idx: edges grouped by pair) times gr * W0; the time constants'
+// is g_a * a summed over the units of each type.
+__global__ void __launch_bounds__(256) segment_sum_kernel(const int* __restrict__ seg_ptr, const int* __restrict__ idx,
+                                                           const float* __restrict__ x, const float* __restrict__ w,
+                                                           float alpha, float* __restrict__ out, int segments) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long s = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); s < segments; s += warps) {
+    const int e0 = __ldg(&seg_ptr[s]), e1 = __ldg(&seg_ptr[s + 1]);
+    float sum = 0.0f;
+    for (int e = e0 + lane; e < e1; e += 32) {
+      const int i = __ldg(&idx[e]);
+      const float term = w ? __ldg(&x[i]) * __ldg(&w[i]) : __ldg(&x[i]);
+      sum = sum + term;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) sum = sum + __shfl_xor_sync(0xffffffffu, sum, o);
+    if (lane == 0) out[s] = alpha * sum;
+  }
+}
+
 }  // namespace flyb
 
 using namespace flyb;
+
+FLYB_API int flyb_segment_sum(const int* seg_ptr, const int* idx, const float* x, const float* w, float alpha,
+                              float* out, int segments, void* stream) {
+  if (!seg_ptr || !idx || !x || !out || segments < 0) return FLYB_EINVAL;
+  if (segments == 0) return 0;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long blocks = ((long long)segments + 7) / 8;
+  if (blocks > (long long)sms * 8) blocks = (long long)sms * 8;
+  segment_sum_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(seg_ptr, idx, x, w, alpha, out, segments);
+  return (int)cudaGetLastError();
+}
 
 FLYB_API int flyb_optic_adjoint(const flyb_adjoint_args* a, void* stream) {
   if (!a || a->m <= 0 || a->batch <= 0 || a->nsteps < 0 || !a->t_ptr || !a->t_col || !a->t_w || !a->v_hist ||

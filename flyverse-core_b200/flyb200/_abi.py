@@ -134,6 +134,7 @@ SIGNATURES = {
     "flyb_optic_run_noalloc": [ct.POINTER(OpticArgs), _VP],
     "flyb_spmm": [ct.POINTER(SpmmArgs), _VP],
     "flyb_optic_adjoint": [ct.POINTER(AdjointArgs), _VP],
+    "flyb_segment_sum": [_VP, _VP, _VP, _VP, ct.c_float, _VP, _I, _VP],
     "flyb_photoreceptor": [ct.POINTER(PhotoArgs), _VP],
     "flyb_group_means": [_VP, _VP, _VP, _VP, _I, _I, _VP],
     "flyb_trace_scene_floats": [_I, _I, _I],

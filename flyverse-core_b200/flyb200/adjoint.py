@@ -10,7 +10,9 @@ FP64 is used only by the check (oracle/optic64.py).
 
 Parameters: per-type-pair gains g (W_ij = g[pair(j -> i)] * W0_ij) and per-type time constants tau
 (a_i = exp(-dt / tau[type(i)])). `OpticRollout.apply` wraps one checkpointed rollout as a
-torch.autograd.Function from (gains, tau, v0, adapt0) to (v_T, adapt_T).
+torch.autograd.Function from (gains, tau, v0, adapt0) to (v_T, adapt_T). The parameter gradients
+are segmented FP32 sums on the device (flyb_segment_sum). Under torch.distributed each rank
+rolls out its own flies and the parameter gradients are summed over ranks.
 """
 from __future__ import annotations
 
@@ -22,6 +24,7 @@ import torch
 
 from . import _abi
 from .optic import DeviceCSR, OpticCore
+from .parallel import allreduce_gradients
 
 
 class OpticAdjoint:
@@ -52,7 +55,16 @@ class OpticAdjoint:
         # single writer); the pair reduction reads W0 and the pair ids in that order too
         perm = self.perm.long()
         self.W0_t, self.pair_t = self.W0[perm].contiguous(), self.pair_id[perm].contiguous()
+        # the parameter gradients are segmented sums (flyb_segment_sum): the accumulator's edges
+        # grouped by pair, the units grouped by type
+        self._pair_seg = self._segments(self.pair_t.cpu().numpy(), self.n_pairs)
+        self._type_seg = self._segments(np.asarray(type_of, np.int64), self.n_types)
+        self._d_gains = torch.zeros(self.n_pairs, device=dev)
+        self._d_tau = torch.zeros(self.n_types, device=dev)
         self.launch = launch
+        # with a process group, each rank holds its own shard of flies and the parameters are shared:
+        # their gradients are summed over ranks (NCCL over NVLink between GPUs)
+        self.reduce_over_ranks = True
         M, B = self.m, self.B
         self.lam_v = torch.zeros(M, B, device=dev)
         self.lam_a = torch.zeros(M, B, device=dev)
@@ -65,6 +77,21 @@ class OpticAdjoint:
         self._status = torch.zeros(4, dtype=torch.int32, device=dev)
         self._sync = torch.zeros(64, dtype=torch.int32, device=dev)
         self.ckpt = []
+
+    def _segments(self, key: np.ndarray, count: int):
+        """(ptr [count + 1], positions grouped by key) as int32 device tensors."""
+        order = np.argsort(key, kind="stable").astype(np.int32)
+        ptr = np.concatenate([[0], np.cumsum(np.bincount(key, minlength=count))]).astype(np.int32)
+        return torch.from_numpy(ptr).to(self.device), torch.from_numpy(order).to(self.device)
+
+    def _segment_sum(self, seg, x: torch.Tensor, w: torch.Tensor | None, alpha: float, out: torch.Tensor) -> None:
+        ptr, idx = seg
+        with torch.cuda.device(self.device):
+            rc = _abi.lib().flyb_segment_sum(ptr.data_ptr(), idx.data_ptr(), x.data_ptr(),
+                                             None if w is None else w.data_ptr(), alpha, out.data_ptr(),
+                                             out.numel(), torch.cuda.current_stream(self.device).cuda_stream)
+        if rc:
+            raise RuntimeError(f"flyb_segment_sum: error {rc}")
 
     # ------------------------------------------------------------------ parameters
     def set_params(self, gains: torch.Tensor, tau: torch.Tensor) -> None:
@@ -115,18 +142,28 @@ class OpticAdjoint:
                 rc = _abi.lib().flyb_optic_adjoint(ct.byref(args), stream)
             if rc:
                 raise RuntimeError(f"flyb_optic_adjoint: error {rc}")
-        contrib = (self.gr * self.W0_t.double()) * self.g_edge.double()
-        d_gains = torch.zeros(self.n_pairs, dtype=torch.float64, device=self.device).index_add_(0, self.pair_t, contrib)
-        a = self.core.a.double()
-        tau_i = self.tau.double()[self.type_of]
-        d_tau = torch.zeros(self.n_types, dtype=torch.float64, device=self.device).index_add_(
-            0, self.type_of, self.g_a.double() * a * self.dt / tau_i**2)
-        return d_gains.float(), d_tau.float(), self.lam_v.clone(), self.lam_a.clone()
+        # dL/dgain_p = gr * sum over the pair's edges of W0_e * g_edge[e];
+        # dL/dtau_k = dt / tau_k^2 * sum over the type's units of g_a[i] * a_i   (all FP32)
+        self._segment_sum(self._pair_seg, self.g_edge, self.W0_t, self.gr, self._d_gains)
+        self._segment_sum(self._type_seg, self.g_a, self.core.a, 1.0, self._d_tau)
+        d_tau = self._d_tau * (self.dt / (self.tau * self.tau))
+        d_gains = self._d_gains.clone()
+        if self.reduce_over_ranks:
+            parameter_grads_over_ranks([d_gains, d_tau])
+        return d_gains, d_tau, self.lam_v.clone(), self.lam_a.clone()
 
     def check(self) -> None:
         s = self._status.cpu().tolist()
         if s[0]:
             raise RuntimeError(f"flyb200 adjoint kernel status {s[0]} (where {s[1]}, step {s[2]})")
+
+
+def parameter_grads_over_ranks(grads) -> None:
+    """Sum the shared parameters' gradients over the ranks of the default process group, in place
+    (each rank's loss covers its own flies); nothing without a group of more than one rank."""
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        allreduce_gradients(grads)
 
 
 class OpticRollout(torch.autograd.Function):

@@ -17,6 +17,7 @@ reference's headline numbers are quoted on:
                 (operating point 0) whose inhibitory inputs from 35 "delayed inhibition" types
                 (tau 10 ms) carry a x5 pair gain; 5,895 photoreceptors on a hex eye driven by a
                 drifting sinusoidal grating in 4 spectral channels.
+  batched_config4  config 2's spiking graph coupled to config 3's lobe (the 64-fly uneven-rollout tier).
   eye_grid      the eye the ray tracer casts: two hexagonal column patches of radius 16 (817
                 columns each, 1,634 in all, about the ommatidia of a fly's pair of eyes) through
                 the retina's own geometry, 7 sample rays per column.
@@ -307,6 +308,19 @@ def whole_fly_config5(seed: int = 0, n_rate: int = 89_390, n_lif: int = 71_618, 
     vpn = np.unique(optic.W_sr.tocoo().row)
     return WholeFlyConfig(lif=lif, optic=optic, sensory_idx=sensory, vpn_idx=vpn, n_rate=n_rate, n_spiking=n_spk,
                           edges=int(W.nnz + optic.W0.nnz + coupling))
+
+
+def batched_config4(seed: int = 0) -> WholeFlyConfig:
+    """The batched-rollout tier: config 2's spiking graph (71,618 LIF neurons, 15 M edges, Poisson
+    drive on its 2,000 designated cells) coupled to config 3's optic lobe (89,390 units, 6 M nnz)
+    through the lobe's feedback (W_rs) and visual projection (W_sr) blocks. Per-fly Poisson rates
+    and episode lengths are the caller's (the benchmark draws 20-200 Hz and 500-4,000 steps)."""
+    lif = lif_config2(seed=seed)
+    optic = optic_config3(seed=seed + 1, n_spk=lif.c.n)
+    vpn = np.unique(optic.W_sr.tocoo().row)
+    coupling = optic.W_rp.nnz + optic.W_rs.nnz + optic.W_sr.nnz
+    return WholeFlyConfig(lif=lif, optic=optic, sensory_idx=np.asarray(lif.poisson_idx), vpn_idx=vpn,
+                          n_rate=optic.m, n_spiking=lif.c.n, edges=int(lif.c.W.nnz + optic.W0.nnz + coupling))
 
 
 def eye_grid(radius: int = 16):

@@ -112,6 +112,35 @@ class WholeFly:
     def n_neurons(self) -> int:
         return self.cfg.n_rate + self.cfg.n_spiking
 
+    def set_poisson_rates(self, hz) -> None:
+        """Poisson drive of the sensory cells: a rate for all, or per fly (B,) or (B, cells)."""
+        r = torch.as_tensor(hz, dtype=torch.float32)
+        if r.ndim == 1:
+            r = r[:, None].expand(self.B, len(self.sensory_idx))
+        self.lif.set_poisson(self.sensory_idx, r)
+
+    def reset(self, rows, poisson_hz=None) -> None:
+        """Start new episodes in fly rows `rows`: their LIF state, pending input and spike history
+        back to rest (Brain.reset), their optic state to the operating point (v = adapt = 0, and
+        the carried dr to match), then their Poisson drive set to `poisson_hz` (per row, or one
+        rate). The other flies and the held photoreceptor input are untouched. Between calls
+        only (nothing is pending then)."""
+        rows = np.asarray(rows, dtype=np.int64)
+        if not rows.size:
+            return
+        sel = torch.as_tensor(rows, device=self.device)
+        self.lif.reset(rows)
+        o = self.optic
+        o.v_s[:, sel] = 0.0
+        o.adapt_s[:, sel] = 0.0
+        o.dr_out[:, sel] = o.b.clamp(0.0, 1.0)[:, None] - o.b[:, None]     # clip(0 + b, 0, 1) - b
+        o._dr_key = o._state_key()
+        if poisson_hz is not None:
+            hz = torch.as_tensor(poisson_hz, dtype=torch.float32).reshape(-1, 1).expand(len(rows), len(self.sensory_idx))
+            cols = torch.as_tensor(self.sensory_idx, device=self.device)
+            self.lif.poisson_p[sel[:, None], cols[None, :]] = hz.to(self.device) * (self.lif.p.dt / 1000.0)
+            self.lif._poisson_on = True
+
     def set_photoreceptors(self, a_pr: torch.Tensor) -> None:
         """Photoreceptor activity [n_pr][B] (contiguous, on the device) -> held pr_in =
         gain_in * W_rp a_pr (a frame's input), read from `a_pr` where it lies."""
@@ -201,19 +230,20 @@ class WholeFly:
              y_hi=o.drive_clip_mv)
 
     # ------------------------------------------------------------------ algorithmic bytes (roofline)
-    def lif_bytes_per_step(self) -> int:
+    def lif_bytes_per_step(self, group: int | None = None) -> int:
         """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate, counts
         read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active.
-        Under pull delivery also its input tables once (presynaptic index per input slot, the
-        count bit planes per 32 slots) and the write slot read + written."""
+        Under pull delivery also its input tables once per delivery group of `group` steps
+        (presynaptic index per input slot, the count bit planes and base per chunk of 32 slots), the
+        spike words written to and read back from the pull buffer, and the write slot read + written."""
         per = 4 * (5 * 2 + 4 + 1)
         total = self.cfg.n_spiking * (self.B * per + 4)
         if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
             # the input tables once per group of L steps, the write slot read + written every step
             ptr, pre, planes, meta = self.lif._pull_t
-            L = self.lif.pull_group if self.overlapping else 1
+            L = self.lif.pull_group if group is None else group
             total += (pre.numel() * 4 + planes.numel() * 4 + meta.numel() * 4) // L
-            total += self.cfg.n_spiking * self.B * 4 * 2
+            total += self.cfg.n_spiking * self.B * 4 * 2 + self.cfg.n_spiking * self.B // 8 * 2
         return total
 
     def optic_bytes_per_step(self) -> int:

@@ -391,6 +391,14 @@ typedef struct flyb_adjoint_args {
 
 int flyb_optic_adjoint(const flyb_adjoint_args* a, void* stream);
 
+/* Segmented gather-sum in FP32 (device arrays): out[s] = alpha * sum_{seg_ptr[s] <= e < seg_ptr[s+1]}
+ * x[idx[e]] * w[idx[e]] (w null: 1), summed in a fixed order (deterministic). The adjoint's
+ * parameter gradients: per pair gain, the per-edge accumulator over the pair's edges times
+ * gr * W0; per time constant, g_a * a over the type's units. No counterpart in the reference
+ * (its gradients come from torch autograd). */
+int flyb_segment_sum(const int* seg_ptr, const int* idx, const float* x, const float* w, float alpha, float* out,
+                     int segments, void* stream);
+
 /* Photoreceptor stage (flyverse/optic.py:496-517), fly-minor:
  * rad [batch][n_col][4] -> I_pr -> column x family mean -> low-pass / adaptation -> contrast,
  * writes a_pr [n_pr][batch]. `fresh` [batch] bytes are consumed (cleared). */

@@ -91,3 +91,54 @@ def test_checkpoint_interval_does_not_change_gradients():
     g7, t7, _ = gpu_grads(*prob, checkpoint=7)
     np.testing.assert_allclose(g7, g20, rtol=1e-6, atol=1e-9)
     np.testing.assert_allclose(t7, t20, rtol=1e-6, atol=1e-9)
+
+
+def test_c3_full_lobe_gradients_match_fp64_central_differences():
+    """Config 3 at its stated size (89,390 units, 6 M nnz, 200 substeps, checkpoint 20), one fly,
+    the readout L = sum of the rates of one fixed 50-unit group minus another's: the 20 largest
+    pair-gain and the 10 largest time-constant gradients of the FP32 adjoint against FP64 central
+    differences (h = 1e-4) of the C FP64 oracle, within 1e-4 relative. Components whose +-h and
+    +-h/2 differences disagree (a clip kink inside the interval) are left out; most are smooth."""
+    import oracle
+    cfg = synthetic.optic_config3(seed=3)
+    assert cfg.m == 89_390 and cfg.W0.nnz == 6_000_000
+    B, steps = 1, 200
+    rng = np.random.default_rng(3)
+    v0 = (rng.standard_normal((cfg.m, B)) * 0.2).astype(np.float32)
+    ad0 = np.zeros((cfg.m, B), np.float32)
+    pr = (rng.standard_normal((cfg.m, B)) * 0.2).astype(np.float32)
+    spk = np.zeros((cfg.m, B), np.float32)
+    w = np.zeros(cfg.m)
+    groups = rng.permutation(cfg.m)[:100]
+    w[groups[:50]], w[groups[50:]] = 1 / 50, -1 / 50
+    gains, tau = cfg.gain0.astype(np.float64), cfg.tau_of_type.astype(np.float64)
+    g32, t32, L32 = gpu_grads(cfg, v0, ad0, pr, spk, w, gains, tau, steps)
+    W = cfg.W0.tocsr()
+    aad = float(np.exp(-cfg.dt_ms / cfg.adapt_tau_ms))
+
+    def loss(g, t):
+        v, ad = v0.astype(np.float64), ad0.astype(np.float64)
+        a = np.exp(-cfg.dt_ms / t[cfg.type_of])
+        oracle.optic_run_f64(v, ad, W.indptr, W.indices, W.data.astype(np.float64) * g[cfg.pair_id], pr, spk, a, cfg.b,
+                             cfg.gain_rr, cfg.adapt_gain, aad, steps)
+        return optic64.readout(v, cfg.b, w)
+
+    L64 = loss(gains, tau)
+    assert abs(L32 - L64) <= 1e-5 * max(1.0, abs(L64))
+
+    def fd(which, k, h):
+        xp, xm = (gains.copy(), tau.copy()), (gains.copy(), tau.copy())
+        xp[which][k] += h
+        xm[which][k] -= h
+        return (loss(*xp) - loss(*xm)) / (2 * h)
+
+    for which, grad, count in ((0, g32, 20), (1, t32, 10)):
+        top = np.argsort(-np.abs(grad))[:count]
+        h1 = np.array([fd(which, k, 1e-4) for k in top])
+        h2 = np.array([fd(which, k, 5e-5) for k in top])
+        smooth = np.abs(h1 - h2) <= 1e-6 * np.abs(h1).max() + 1e-5 * np.abs(h1)
+        assert smooth.sum() >= 0.75 * count, (which, smooth)
+        err = np.abs(grad[top] - h1) / np.abs(h1)
+        print(f"C3 adjoint {'gains' if which == 0 else 'tau'}: {int(smooth.sum())}/{count} smooth components, "
+              f"max relative error {err[smooth].max():.2e} against FP64 central differences")
+        np.testing.assert_allclose(grad[top][smooth], h1[smooth], rtol=1e-4, atol=1e-6 * np.abs(h1).max())

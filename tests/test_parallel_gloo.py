@@ -11,6 +11,7 @@ import torch.multiprocessing as mp
 
 import oracle
 from flyb200 import _abi
+from flyb200.adjoint import parameter_grads_over_ranks
 from flyb200.parallel import allreduce_gradients, gather_rows, shard
 from gpu_helpers import LIF_ARRAYS
 from test_gpu_lif import case_random
@@ -49,6 +50,10 @@ def _worker(rank, world, port, out_dir):
         v = gather_rows(torch.from_numpy(st.v.T.copy()), TOTAL)            # (flies, n) on every rank
         g = torch.full((5,), float(rank + 1), dtype=torch.float64)
         allreduce_gradients([g])
+        # the adjoint's reduction of the shared parameters' gradients (OpticAdjoint.backward)
+        d_gains, d_tau = torch.full((3,), float(rank + 1)), torch.full((2,), 10.0 * (rank + 1))
+        parameter_grads_over_ranks([d_gains, d_tau])
+        np.save(os.path.join(out_dir, f"p{rank}.npy"), torch.cat([d_gains, d_tau]).numpy())
         np.save(os.path.join(out_dir, f"v{rank}.npy"), v.numpy())
         np.save(os.path.join(out_dir, f"g{rank}.npy"), g.numpy())
     finally:
@@ -65,4 +70,5 @@ def test_two_rank_shards_equal_single_batch(tmp_path):
     for r in range(world):
         np.testing.assert_array_equal(np.load(tmp_path / f"v{r}.npy"), st.v.T)
         np.testing.assert_array_equal(np.load(tmp_path / f"g{r}.npy"), np.full(5, 3.0))
+        np.testing.assert_array_equal(np.load(tmp_path / f"p{r}.npy"), np.array([3, 3, 3, 30, 30], np.float32))
     assert _abi.LIF_POISSON & case["flags"]
