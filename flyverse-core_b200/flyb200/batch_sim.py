@@ -12,7 +12,7 @@ The body and behaviour programs of the reference are not part of the brain step.
 """
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -27,13 +27,40 @@ class EpisodeStats:
     frames: int = 0
 
 
+# Keyword arguments of the reference's BatchSim (batch_sim.py:89-94) that configure the room, the
+# body, the senses or the behaviour programs rather than the brain step: accepted at their
+# reference defaults, refused by name otherwise (this package steps the brain only).
+OUTSIDE_THE_BRAIN = {"seeds": None, "start": None, "sensory_cuda_graphs": None, "modules": None, "wind_speed": 0.3,
+                     "wind_dir": 180.0, "fruit_set": "all", "fence": False, "program": "none", "escape_gating": False,
+                     "proprioception": None, "preset": "raw", "instruments": None}
+
+
 class BatchSim:
     FRAME_MS = 10.0
 
-    def __init__(self, batch: int = 1, *, c, seed: int = 0, device=None, brain_dt: float = 0.5, optic_dt: float = 1.0,
-                 cuda_graphs: bool = False, lif_params: LIFParams | None = None, optic_params: OpticParams | None = None,
-                 episode_frames=(50, 400), groups: dict | None = None, stimulus=None, retina=None, world=None,
-                 pose=None):
+    def __init__(self, batch: int = 1, *, c=None, seed: int = 0, device=None, brain_dt: float = 0.5,
+                 optic_dt: float = 1.0, cuda_graphs: bool = False, cuda_kernels=None, event_driven=None,
+                 cuda_sparse: str = "torch", cuda_compact: bool = True, weight_dtype: str = "float32",
+                 dt_by_module=None, prune_frozen: bool = True, lif_params: LIFParams | None = None,
+                 optic_params: OpticParams | None = None, episode_frames=(50, 400), groups: dict | None = None,
+                 stimulus=None, retina=None, world=None, pose=None, **outside):
+        """The reference's brain-step arguments keep their names and meaning: `cuda_kernels`
+        (only True/None: the native step is the only path), `event_driven`, `cuda_sparse`,
+        `cuda_compact`, `weight_dtype`, `dt_by_module`, `prune_frozen` go into the LIF parameters
+        and the Brain. Room, body, sense and program arguments are accepted at their defaults
+        only (OUTSIDE_THE_BRAIN)."""
+        for name, value in outside.items():
+            if name not in OUTSIDE_THE_BRAIN:
+                raise TypeError(f"BatchSim got an unexpected keyword argument {name!r}")
+            if value != OUTSIDE_THE_BRAIN[name]:
+                raise ValueError(f"BatchSim argument {name}={value!r} configures the room, body, senses or programs, "
+                                 f"which flyb200 does not simulate (only its default {OUTSIDE_THE_BRAIN[name]!r} is "
+                                 f"accepted)")
+        if c is None:
+            raise ValueError("BatchSim needs the connectome `c` (connectome.load(cache_dir)); the dataset is not "
+                             "bundled")
+        if cuda_kernels is False:
+            raise ValueError("cuda_kernels=False asks for the torch path, which flyb200 does not have")
         if not isinstance(batch, (int, np.integer)) or batch < 1:
             raise ValueError("batch must be a positive integer")
         if not np.isfinite(brain_dt) or brain_dt <= 0 or not np.isclose(self.FRAME_MS / brain_dt,
@@ -43,9 +70,12 @@ class BatchSim:
         lp = lif_params or LIFParams(dt=brain_dt)
         if lp.dt != brain_dt:
             raise ValueError("lif_params.dt must equal brain_dt")
+        lp = replace(lp, event_driven=event_driven if event_driven is not None else lp.event_driven,
+                     weight_dtype=weight_dtype, prune_frozen=prune_frozen,
+                     dt_by_module=dt_by_module if dt_by_module is not None else lp.dt_by_module)
         op = optic_params or OpticParams(dt_ms=optic_dt)
         self.fb = FlyBrain(c, batch=self.B, device=device, seed=seed, lif_params=lp, optic_params=op,
-                           cuda_graphs=cuda_graphs, retina=retina)
+                           cuda_graphs=cuda_graphs, retina=retina, cuda_sparse=cuda_sparse, cuda_compact=cuda_compact)
         self.rng = np.random.default_rng(seed)
         self.episode_frames = episode_frames
         self.frames_left = self._draw(self.B)

@@ -96,14 +96,31 @@ class FlyBrain:
     OPTIC_TENSORS = ("v", "adapt", "I_lp", "I_mean", "contrast", "delta_rate", "g_slow", "g_slow_cls", "_slow_in_s",
                      "stream_adapt_state")
 
+    # reference constructor arguments for parts outside the brain step: accepted at these defaults
+    OUTSIDE_THE_BRAIN = {"modules": None, "eye_geometry": None, "nt_source": None, "dataset": None, "optic": "auto",
+                         "preset": "raw", "instruments": None}
+
     def __init__(self, c, *, batch: int = 1, device=None, seed: int = 0, lif_params: LIFParams | None = None,
                  optic_params: OpticParams | None = None, cuda_graphs: bool = False, retina=None,
-                 launch: str = "persistent", receptor=None):
+                 launch: str = "persistent", receptor=None, cuda_kernels=None, cuda_sparse: str = "torch",
+                 cuda_compact: bool = True, **outside):
+        """The reference's constructor (fly.py:41-44): `cuda_kernels`, `cuda_sparse` and
+        `cuda_compact` reach the Brain with the reference's meaning; modules, instruments, presets,
+        NT sources and eye geometry are parts outside the brain step, accepted at their defaults."""
+        for name, value in outside.items():
+            if name not in self.OUTSIDE_THE_BRAIN:
+                raise TypeError(f"FlyBrain got an unexpected keyword argument {name!r}")
+            if value is not self.OUTSIDE_THE_BRAIN[name] and value != self.OUTSIDE_THE_BRAIN[name]:
+                raise ValueError(f"FlyBrain argument {name}={value!r} is outside the brain step flyb200 provides "
+                                 f"(only {self.OUTSIDE_THE_BRAIN[name]!r} is accepted)")
+        if c is None:
+            raise ValueError("FlyBrain needs the connectome `c` (connectome.load(cache_dir)); the dataset is not bundled")
         if c.n == 0:
             raise ValueError("FlyBrain needs at least one neuron")
         self.c = c
         lp = lif_params or LIFParams()
-        self.brain = Brain(c, lp, device=device, seed=seed, batch=batch, launch=launch, receptor=receptor)
+        self.brain = Brain(c, lp, device=device, seed=seed, batch=batch, launch=launch, receptor=receptor,
+                           cuda_kernels=cuda_kernels, cuda_sparse=cuda_sparse, cuda_compact=cuda_compact)
         self.B, self.device = self.brain.B, self.brain.device
         self.brain.record_activity = True
         self.cuda_graphs = bool(cuda_graphs)
@@ -130,6 +147,9 @@ class FlyBrain:
         self._activity_ms = np.zeros(self.B)
         self._motor = None                # (names, ptr, idx, device means, pinned means, event)
         self._motor_fresh = False
+        # parity runs: uniform_source(n) -> (n, B, N) Poisson uniforms for the next n LIF steps (the
+        # reference generator's draws, in the order it made them); frames then run eagerly
+        self.uniform_source = None
 
     @property
     def t(self) -> float:
@@ -199,7 +219,7 @@ class FlyBrain:
         self._pending_ms = max(0.0, total - elapsed)
         if not steps:
             return 0.0
-        if self.cuda_graphs and not self.poisson.ends_before(self.t + elapsed):
+        if self.cuda_graphs and self.uniform_source is None and not self.poisson.ends_before(self.t + elapsed):
             self._graph_frame(steps)
             self._mark_readout()
             if self.poisson.pulses:
@@ -213,7 +233,7 @@ class FlyBrain:
             end = self.poisson.next_end()
             if end is not None:            # stop at the next pulse end (a LIF step boundary)
                 count = min(count, max(1, int(round((end - self.t) / self.brain.p.dt))))
-            self.brain.step(count)
+            self.brain.step(count, uniforms=self._uniforms(count))
             remaining -= count
             if self.poisson.pulses:
                 self.poisson.apply()
@@ -221,6 +241,11 @@ class FlyBrain:
         self._mark_readout()
         self._activity_ms += elapsed
         return elapsed
+
+    def _uniforms(self, n: int):
+        if self.uniform_source is None:
+            return None
+        return self.uniform_source(n)
 
     def _vision_frame(self, elapsed: float) -> None:
         if self.optic is not None and self._radiance is not None:

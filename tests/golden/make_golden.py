@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures of tests/golden/ from the reference's own CPU implementation.
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <flyverse checkout>   (or FLYVERSE_REFERENCE=<checkout>)
 
 Runs in the build container only (the reference is not on the GPU machines): it imports
 flyverse from the reference checkout and records what its CPU path produces on inputs both sides
@@ -453,11 +453,141 @@ def tracer(ref) -> dict:
     return out
 
 
+def _full_table(n: pd.DataFrame) -> dict:
+    """Every column of a neuron table: strings as unicode arrays, numbers as they are."""
+    out = {}
+    for col in n.columns:
+        v = n[col]
+        if v.dtype == object or pd.api.types.is_string_dtype(v):
+            out[f"tbl_{col}"] = v.fillna("").astype(str).to_numpy().astype("U")
+        else:
+            out[f"tbl_{col}"] = v.to_numpy()
+    return out
+
+
+FLY_RADIANCE = np.array([[.10, .20, .30, .40], [.90, .10, .55, .05], [.33, .66, .11, .77], [.50, .50, .50, .50]],
+                        np.float32)
+
+
+def fly_frames(ref) -> dict:
+    """The reference's FlyBrain (CPU) on the 19-cell graph of tests/test_bit_identity.py, batch 2,
+    seed 7, frame by frame, in the manner of that file's scenario: two held Poisson inputs and a
+    radiance frame for three 10 ms frames; then a 300 Hz pulse on LC4 for 7 ms (it ends inside the
+    next frame), a 12 mV drive on DNp01 and the mirrored radiance for two 13.3 ms frames (the
+    fractional milliseconds carry over); a reset of fly 0 and a frame; a full reset, one input and
+    a 20 ms frame. Recorded: every LIF step's spikes and the uniforms the brain drew for it (zeros
+    when it drew none), and the state at each frame end."""
+    fly, brain, tb = ref["fly"], ref["brain"], ref["test_bit_identity"]
+    c = tb.graph()
+    fb = fly.FlyBrain(c, batch=2, device="cpu", seed=7, lif_params=brain.LIFParams(receptor_model=None))
+    b = fb.brain
+    B, N = b.B, b.n
+    U, R = [], []
+    plain_step = b.step
+
+    def recording_step(n=1):
+        for _ in range(int(n)):
+            if b._poisson_on:
+                state = b.gen.get_state()
+                U.append(torch.rand((B, N), generator=b.gen).numpy().copy())
+                b.gen.set_state(state)
+            else:
+                U.append(np.zeros((B, N), np.float32))
+            plain_step(1)
+            R.append(b.spikes.numpy() > 0)
+
+    b.step = recording_step
+    orn, jo = c.select(type="ORN_DM1"), c.select(type="~^JO-")
+    out = _full_table(c.neurons) | {"W_data": c.W.data, "W_indices": c.W.indices, "W_indptr": c.W.indptr,
+                                    "orn": orn, "jo": jo, "radiance": FLY_RADIANCE}
+    frames = []
+
+    def frame(ms):
+        fb.step(ms)
+        k = len(frames)
+        for key in ("v", "g", "refrac", "rate", "spike_counts", "adapt", "res", "drive", "poisson_p"):
+            out[f"f{k}_brain_{key}"] = getattr(b, key).numpy().copy()
+        for key in ("v", "adapt", "delta_rate"):
+            out[f"f{k}_optic_{key}"] = getattr(fb.optic, key).numpy().copy()
+        out[f"f{k}_steps"] = np.int64(len(R))
+        out[f"f{k}_pending_ms"] = np.float64(fb._pending_ms)
+        frames.append(ms)
+
+    fb._input("smell", orn, np.array([[120.0], [40.0]], np.float32))
+    fb._input("wind", jo, np.array([[90.0, 10.0], [0.0, 150.0]], np.float32))
+    fb.vision(FLY_RADIANCE)
+    for _ in range(3):
+        frame(10.0)
+    fb.stimulate([9], 300.0, 7.0)
+    fb.brain.set_drive([15], np.float32(12.0))
+    fb.vision(FLY_RADIANCE[::-1].copy())
+    for _ in range(2):
+        frame(13.3)
+    fb.reset([0])
+    frame(10.0)
+    fb.reset()
+    fb._input("smell", orn, np.float32(75.0))
+    fb.vision(FLY_RADIANCE)
+    frame(20.0)
+    assert len(R) == sum(int(np.floor(x / b.p.dt + 1e-9)) for x in (10, 10, 10, 26.6, 10, 20)), len(R)
+    out["frames_ms"] = np.array(frames)
+    out["raster"] = np.stack(R)
+    out["uniforms"] = np.stack(U)
+    print(f"fly_frames: {len(frames)} frames, {len(R)} LIF steps, {int(np.stack(R).sum())} spikes")
+    return out
+
+
+def ref_cache(ref) -> dict:
+    """A graph cache written by the reference's own `connectome.save` (a subset of the 19-cell graph,
+    so the reference_* files are written too) into tests/golden/ref_cache/, and what the
+    reference's `connectome.load` reads back from it; plus the digest of what the reference reads
+    from a cache that flyb200.connectome.save wrote for the same graph."""
+    import hashlib
+    import json
+    import shutil
+    cn, tb = ref["connectome"], ref["test_bit_identity"]
+    full = tb.graph()
+    sub = full.subset(np.arange(4, 19))
+    folder = HERE / "ref_cache"
+    shutil.rmtree(folder, ignore_errors=True)
+    cn.save(sub, folder)
+    back = cn.load(folder, verbose=False)
+
+    def digest(c) -> str:
+        h = hashlib.sha256()
+        for part in (c.W.data, c.W.indices, c.W.indptr, c.reference.W.data, c.reference.W.indices,
+                     c.reference.W.indptr, c.neurons.bodyId.to_numpy(), c.neurons["in_syn"].to_numpy(),
+                     c.neurons["in_syn_l2"].to_numpy(), c.reference.neurons.bodyId.to_numpy()):
+            h.update(np.ascontiguousarray(part).tobytes())
+        h.update(json.dumps([list(c.neurons.columns), c.neurons.type.tolist()]).encode())
+        return h.hexdigest()
+
+    from flyb200 import connectome as ours
+    mine = ours.Connectome(sub.neurons.copy(), sub.W.copy(), sub.body_to_index,
+                           ours.Connectome(full.neurons.copy(), full.W.copy(), full.body_to_index))
+    tmp = HERE / "_ours_cache_tmp"
+    shutil.rmtree(tmp, ignore_errors=True)
+    ours.save(mine, tmp)
+    back_ours = cn.load(tmp, verbose=False)
+    shutil.rmtree(tmp)
+    print(f"ref_cache: {sub.n} neurons, {sub.W.nnz} entries; reference reads its own cache and ours alike:",
+          digest(back) == digest(back_ours))
+    return {"n": np.int64(back.n), "nnz": np.int64(back.W.nnz), "ref_n": np.int64(back.reference.n),
+            "W_data": back.W.data, "W_indices": back.W.indices, "W_indptr": back.W.indptr,
+            "in_syn": back.neurons["in_syn"].to_numpy(), "in_syn_l2": back.neurons["in_syn_l2"].to_numpy(),
+            "body": back.neurons.bodyId.to_numpy(), "ref_body": back.reference.neurons.bodyId.to_numpy(),
+            "columns": np.array(list(back.neurons.columns), dtype="U"),
+            "digest_reference_cache": np.array(digest(back)), "digest_flyb200_cache": np.array(digest(back_ours))}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("FLYVERSE_REFERENCE"),
+                    help="the flyverse checkout whose CPU path records the fixtures (or FLYVERSE_REFERENCE)")
     ap.add_argument("--only", default=None, help="regenerate one fixture (its file stem)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give the reference checkout with --reference or FLYVERSE_REFERENCE")
     sys.path.insert(1, args.reference)
     sys.path.insert(2, str(Path(args.reference) / "tests"))
     import importlib
@@ -465,7 +595,8 @@ def main() -> None:
                                                       ("optic", "flyverse.optic"), ("retina", "flyverse.retina"),
                                                       ("test_bit_identity", "test_bit_identity"),
                                                       ("test_optic_hooks", "test_optic_hooks"),
-                                                      ("world", "flyverse.world"), ("batch_world", "flyverse.batch_world"))}
+                                                      ("world", "flyverse.world"), ("batch_world", "flyverse.batch_world"),
+                                                      ("fly", "flyverse.fly"))}
     torch.set_num_threads(1)
     fixtures = {"lif_c1": lambda: lif_c1(ref), "lif_19cell": lambda: lif_19cell(ref),
                 "lif_19cell_adapt_by_type": lambda: lif_19cell(ref, ADAPT_BY_TYPE),
@@ -475,7 +606,8 @@ def main() -> None:
                 **{f"lif_19cell_clocks_slow_{m}": (lambda m=m: lif_19cell_slow(ref, m, clocks=True))
                    for m in ("additive", "gain", "threshold")},
                 "optic_hex": lambda: optic_hex(ref), "optic_synth": lambda: optic_synth(ref),
-                "tracer": lambda: tracer(ref),
+                "tracer": lambda: tracer(ref), "fly_frames": lambda: fly_frames(ref),
+                "ref_cache": lambda: ref_cache(ref),
                 **{f"optic_hex_slow_{m}": (lambda m=m: optic_hex_slow(ref, m)) for m in ("additive", "gain", "threshold")},
                 **{f"optic_hex_hooks_{k}": (lambda k=k: optic_hex_hooks(ref, k)) for k in HOOK_CASES}}
     for name, make in fixtures.items():

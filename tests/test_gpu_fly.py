@@ -130,3 +130,97 @@ def test_motor_readout_inside_captured_frames():
         np.testing.assert_array_equal(after["spk"][0], 0.0)
         if graphs:
             assert len(fb._graphs) >= 1
+
+
+def fly_frames_connectome(z):
+    import pandas as pd
+    import scipy.sparse as sp
+    from flyb200.connectome import Connectome
+    n = pd.DataFrame({k[4:]: z[k] for k in z if k.startswith("tbl_")})
+    W = sp.csr_matrix((z["W_data"], z["W_indices"], z["W_indptr"]), shape=(len(n), len(n)))
+    return Connectome(n, W, pd.Series(np.arange(len(n)), index=n.bodyId.to_numpy()))
+
+
+@pytest.mark.parametrize("launch", ["step", "persistent"])
+def test_flybrain_frames_equal_reference_golden(launch):
+    """The FlyBrain drop-in against the reference's FlyBrain frame by frame (tests/golden
+    fly_frames: the 19-cell graph at 2 flies, held inputs and vision, a pulse ending inside a frame,
+    an injected drive, 13.3 ms frames carrying fractional milliseconds, a row reset, a full reset),
+    fed the uniforms the reference's generator drew: every LIF step's spikes bit-exact; at every
+    frame end the LIF state within 1e-4 (the reference sums float weights in event order, the
+    native ring sums exact integers), the optic state within 1e-5, the Poisson forcing exact."""
+    from helpers import golden
+    z = golden("fly_frames")
+    c = fly_frames_connectome(z)
+    fb = FlyBrain(c, batch=2, device="cuda", seed=7, lif_params=LIFParams(receptor_model=None), launch=launch)
+    assert fb.optic is not None
+    U = torch.from_numpy(z["uniforms"])
+    cursor = [0]
+
+    def uniforms(n):
+        out = U[cursor[0]:cursor[0] + n]
+        cursor[0] += n
+        return out
+
+    fb.uniform_source = uniforms
+    raster = []
+    plain_step = fb.brain.step
+
+    def recording_step(n=1, uniforms=None):
+        for k in range(int(n)):
+            plain_step(1, uniforms=None if uniforms is None else uniforms[k:k + 1])
+            raster.append(fb.brain.spikes.cpu().numpy() > 0)
+
+    fb.brain.step = recording_step
+    frames = iter(range(100))
+
+    def frame(ms):
+        fb.step(ms)
+        k = next(frames)
+        assert len(raster) == int(z[f"f{k}_steps"])
+        np.testing.assert_array_equal(np.stack(raster), z["raster"][:len(raster)], err_msg=f"raster by frame {k}")
+        for key in ("v", "g", "refrac", "rate", "spike_counts", "adapt", "res", "drive"):
+            np.testing.assert_allclose(getattr(fb.brain, key).cpu().numpy(), z[f"f{k}_brain_{key}"], rtol=0, atol=1e-4,
+                                       err_msg=f"brain {key} frame {k}")
+        np.testing.assert_array_equal(fb.brain.poisson_p.cpu().numpy(), z[f"f{k}_brain_poisson_p"])
+        for key in ("v", "adapt", "delta_rate"):
+            np.testing.assert_allclose(getattr(fb.optic, key).cpu().numpy(), z[f"f{k}_optic_{key}"], rtol=1e-5,
+                                       atol=1e-6, err_msg=f"optic {key} frame {k}")
+        assert abs(fb._pending_ms - float(z[f"f{k}_pending_ms"])) < 1e-9
+
+    rad = z["radiance"]
+    fb.set_input("smell", z["orn"], np.array([[120.0], [40.0]], np.float32))
+    fb.set_input("wind", z["jo"], np.array([[90.0, 10.0], [0.0, 150.0]], np.float32))
+    fb.vision(rad)
+    for _ in range(3):
+        frame(10.0)
+    fb.stimulate([9], 300.0, 7.0)
+    fb.brain.set_drive([15], np.float32(12.0))
+    fb.vision(rad[::-1].copy())
+    for _ in range(2):
+        frame(13.3)
+    fb.reset([0])
+    frame(10.0)
+    fb.reset()
+    fb.set_input("smell", z["orn"], np.float32(75.0))
+    fb.vision(rad)
+    frame(20.0)
+    assert cursor[0] == len(U) and z["raster"].sum() > 0
+
+
+def test_batch_sim_takes_the_reference_brain_arguments():
+    """BatchSim accepts the reference's brain-step keywords (batch_sim.py:89-94) and refuses room,
+    body and program settings by name."""
+    z, c, r = hex_lobe()
+    lp = LIFParams(receptor_model=None, dt=0.5)
+    sim = BatchSim(2, c=c, seed=1, device="cuda", brain_dt=0.5, cuda_kernels=True, event_driven=True,
+                   cuda_sparse="warp", cuda_compact=False, weight_dtype="float32", prune_frozen=True, lif_params=lp,
+                   wind_speed=0.3, program="none", preset="raw")
+    assert sim.fb.brain.cuda_sparse == "warp" and not sim.fb.brain.cuda_compact
+    sim.step()
+    with pytest.raises(ValueError, match="program"):
+        BatchSim(2, c=c, device="cuda", lif_params=lp, program="walk")
+    with pytest.raises(TypeError, match="bogus"):
+        BatchSim(2, c=c, device="cuda", lif_params=lp, bogus=1)
+    with pytest.raises(ValueError, match="cuda_kernels"):
+        BatchSim(2, c=c, device="cuda", lif_params=lp, cuda_kernels=False)
