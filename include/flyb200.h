@@ -297,8 +297,7 @@ int flyb_optic_run(const flyb_optic_args* a, void* stream);
 
 /* Allocation-free variant of flyb_optic_run; no counterpart in the reference. For callers that
  * cannot allocate device memory: a host that owns every device buffer and forbids allocation in its
- * step callback, code running under a fixed memory budget, or a CUDA-graph recorder that must not
- * see allocations. The dr ping-pong buffers and the barrier words (`dr`, `dr_tmp`, `sync` of the
+ * step callback, or code running under a fixed memory budget. The dr ping-pong buffers and the barrier words (`dr`, `dr_tmp`, `sync` of the
  * argument struct, which are ignored here) live in a file-scope device array of the library, sized
  * for m * batch <= FLYB_OPTIC_NOALLOC_MAX unit-flies (2 x 4 MiB + 256 B, held by every GPU that loads
  * the library until the process exits); larger requests return FLYB_ETOOBIG. The caller still passes
@@ -306,7 +305,12 @@ int flyb_optic_run(const flyb_optic_args* a, void* stream);
  * The first call on a device looks up the array's device address (cudaGetSymbolAddress, with that
  * device current) and should come before any stream capture. Every call shares the array: calls
  * that overlap on the GPU (other streams, other threads) race on it and must be serialised; each
- * call recomputes dr from v and clears the barrier words, so no state carries over between calls. */
+ * call recomputes dr from v and clears the barrier words, so no state carries over between calls.
+ * The dr of the final state stays in the library's array and is not returned: a caller that needs
+ * it (the whole-fly step feeds it to the W_sr drive product) computes clip(v + b, 0, 1) - b from v.
+ * The looked-up address is kept per device ordinal for the life of the process; after a
+ * cudaDeviceReset the library's module is loaded anew, so do not call this entry point after a
+ * device reset in the same process. */
 #define FLYB_OPTIC_NOALLOC_MAX (1 << 20)
 int flyb_optic_run_noalloc(const flyb_optic_args* a, void* stream);
 

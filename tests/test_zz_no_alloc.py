@@ -3,11 +3,17 @@
 Some hosts cannot allocate device memory while they step the brain (they own every buffer, or
 forbid allocation inside their step callback). For them the library keeps the optic substep's
 scratch in its own file-scope device array. This checks, on two calls in a row, that the
-allocation-free entry point gives what flyb_optic_run gives with caller-provided scratch, and that
-requests beyond the array's stated size are refused. Collected last so that a stop at the first
-failure has already run every other test; it also passes alone in a fresh process.
+allocation-free entry point gives what flyb_optic_run gives with caller-provided scratch (the
+same kernels on the same inputs: bit for bit), at a small size, at a wide batch (several flies
+per lane) and at exactly the array's stated limit, and that larger requests are refused. Collected
+last so that a stop at the first failure has already run every other test; it also passes alone
+in a fresh process.
 """
 import ctypes as ct
+import os
+import subprocess
+import sys
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -17,7 +23,7 @@ from flyb200 import _abi, synthetic
 
 pytestmark = pytest.mark.gpu
 
-RTOL, ATOL = 1e-5, 1e-6
+NOALLOC_MAX = 1 << 20            # FLYB_OPTIC_NOALLOC_MAX
 
 
 def _args(cfg, W, state, launch, status, with_scratch):
@@ -34,15 +40,16 @@ def _args(cfg, W, state, launch, status, with_scratch):
     return args, (dr, dr_tmp, sync)
 
 
-@pytest.mark.parametrize("launch", [_abi.LAUNCH_PERSISTENT, _abi.LAUNCH_STEP])
-def test_noalloc_matches_the_allocating_entry_point_twice(launch):
+@pytest.mark.parametrize("m,B,launch", [(5000, 3, _abi.LAUNCH_PERSISTENT), (5000, 3, _abi.LAUNCH_STEP),
+                                        (4096, 64, _abi.LAUNCH_PERSISTENT), (16384, 64, _abi.LAUNCH_STEP)])
+def test_noalloc_matches_the_allocating_entry_point_twice(m, B, launch):
     lib = _abi.lib()
-    cfg = synthetic.optic_config3(seed=9, m=5000, nnz=250_000, n_pr=300, n_types=40, n_spk=400)
+    assert m * B <= NOALLOC_MAX
+    cfg = synthetic.optic_config3(seed=9, m=m, nnz=50 * m, n_pr=300, n_types=40, n_spk=400)
     Wr = cfg.W_rr()
     cw = np.stack([Wr.indices.astype(np.int32), Wr.data.astype(np.float32).view(np.int32)], axis=1)
     W = [torch.from_numpy(Wr.indptr.astype(np.int32)).cuda(), torch.from_numpy(np.ascontiguousarray(cw)).cuda()]
     rng = np.random.default_rng(4)
-    B = 3
     init = [torch.from_numpy((rng.standard_normal((cfg.m, B)) * s).astype(np.float32)).cuda() for s in (0.3, 0.05, 0.3, 0.1)]
     consts = [torch.from_numpy(cfg.a).cuda(), torch.from_numpy(cfg.b).cuda()]
     ref_state = [t.clone() for t in init] + consts
@@ -58,13 +65,32 @@ def test_noalloc_matches_the_allocating_entry_point_twice(launch):
         torch.cuda.synchronize()
         assert status_ref[0].item() == 0 and status_new[0].item() == 0
         for k, name in ((0, "v"), (1, "adapt")):
-            np.testing.assert_allclose(new_state[k].cpu().numpy(), ref_state[k].cpu().numpy(), rtol=RTOL, atol=ATOL,
-                                       err_msg=f"{name}, call {call}")
+            np.testing.assert_array_equal(new_state[k].cpu().numpy(), ref_state[k].cpu().numpy(),
+                                          err_msg=f"{name}, call {call}")
         del keep
 
 
+REFUSAL = r"""
+import ctypes as ct, sys
+sys.path.insert(0, sys.argv[1])
+from flyb200 import _abi
+lib = _abi.lib()
+MAX = 1 << 20
+for m, batch in ((MAX + 1, 1), (16385, 64), (1 << 20, 2)):
+    big = _abi.OpticArgs(m=m, batch=batch, nsteps=1, launch=_abi.LAUNCH_STEP, ptr=4096, cw=4096, v=4096, adapt=4096,
+                         pr=4096, spk=4096, a=4096, b=4096)
+    rc = lib.flyb_optic_run_noalloc(ct.byref(big), None)
+    assert rc == _abi.ETOOBIG, (m, batch, rc)
+print("refused 3")
+"""
+
+
 def test_noalloc_refuses_sizes_beyond_its_array():
-    lib = _abi.lib()
-    m = 1 << 20
-    big = _abi.OpticArgs(m=m, batch=2, nsteps=1, launch=_abi.LAUNCH_STEP, ptr=1, v=1, adapt=1, pr=1, spk=1, a=1, b=1)
-    assert lib.flyb_optic_run_noalloc(ct.byref(big), None) == _abi.ETOOBIG
+    """m * batch above the limit returns FLYB_ETOOBIG before any device work. Run in a child process
+    that sees no GPU, with placeholder addresses, so a weakened check fails there instead of
+    launching a kernel."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    pkg = str(Path(__file__).resolve().parents[1] / "flyverse-core_b200")
+    r = subprocess.run([sys.executable, "-c", REFUSAL, pkg], env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "refused 3" in r.stdout
