@@ -51,7 +51,7 @@ def test_pulses_split_frames_and_expire():
     fb = make(True)
     fb.stimulate([int(fb.optic.spk_idx[0])], 500.0, 7.0)
     fb.step(10.0)
-    assert not fb._pulses
+    assert not fb.poisson.pulses
     assert float(fb.brain.spike_counts.sum()) > 0
 
 
