@@ -469,13 +469,9 @@ def measure_e2e(cfg, eng, device, steps, chunk: int = 20) -> dict:
     return {"value": eng.n_neurons * B * n / dt, "unit": "neuron-steps/s",
             "h2d_bytes_per_step": int(rad_host[0].numel() * 4), "d2h_bytes_per_step": int(out_host[0].numel() * 8),
             "steps": n, "synaptic_events_per_step": events,
-            "path": f"per step: its radiance frame H2D from pinned memory and the photoreceptor stage "
-                    f"(flyb_photoreceptor, input stream), the photoreceptor input installed and the whole fly "
-                    f"stepped, motor readout D2H to pinned memory (output stream); {chunk} steps per CUDA graph "
-                    f"(WholeFly.step with per-step before/after calls), the host synchronising on each graph's "
-                    f"readouts",
-            "eager": {"value": eng.n_neurons * B * n / dt_eager,
-                      "note": "the same calls launched one by one, the host synchronising every step"}}
+            "path": f"per step: radiance H2D (pinned) + photoreceptor stage on an input stream, whole-fly step, "
+                    f"motor readout D2H on an output stream; {chunk} steps per CUDA graph, host sync per graph",
+            "eager": {"value": eng.n_neurons * B * n / dt_eager, "note": "launched one by one, host sync every step"}}
 
 
 class OraclePort:

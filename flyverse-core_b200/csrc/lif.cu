@@ -67,6 +67,7 @@ struct LifK {
   int pull_phase;                              // runs that pull themselves: first step's index mod L
   unsigned* pull_bits;                         // [2][words][L] spike words of the last two groups
   long long* pull_state;                       // {first undelivered step, its ring position, counter}
+  int pull_grid;                               // blocks of a pull launch (0: one wave)
   LifP P;
 };
 
@@ -519,6 +520,118 @@ __device__ __forceinline__ int pos_mod(long long a, int m) {
   return (int)(r < 0 ? r + m : r);
 }
 
+// One chunk of a warp's input stream: every lane's G * L spike words of its input, the chunk's
+// count planes and its base << 5 | plane count.
+template <int NW, int P>
+struct PullChunk {
+  unsigned w[NW];
+  unsigned pl[P];
+  int meta;
+};
+
+template <int NW, int P>
+__device__ __forceinline__ void pull_fetch(const LifK& k, const unsigned* __restrict__ bits, int pre, long long c,
+                                           PullChunk<NW, P>& x) {
+  pull_words<NW>(bits, pre, x.w);
+  pull_planes<P>(k.pull_planes, c, x.pl);
+  x.meta = __ldcs(&k.pull_meta[c]);
+}
+
+// The chunk's contribution for every step of the group: per step and fly group, the transposed
+// mask m of the inputs that spiked and base x popc(m) + sum_{q < Q} 2^q popc(m & plane_q), Q the
+// chunk's plane count as a template argument (chunk_sums dispatches on it once per chunk). Steps
+// of the group outside the pull's range are summed too (one code path, no per-step tests) and
+// never written.
+template <int G, int L, int P, int Q>
+__device__ __forceinline__ void chunk_sums_q(const Transpose32& transpose, const PullChunk<G * L, P>& x,
+                                             int (&acc)[G * L]) {
+  const int base = x.meta >> 5;
+#pragma unroll
+  for (int u = 0; u < L; ++u) {
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const unsigned m = transpose(x.w[g * L + u]);
+      int sum = base * __popc(m);
+#pragma unroll
+      for (int q = 0; q < Q; ++q) sum += __popc(m & x.pl[q]) << q;
+      acc[g * L + u] += sum;
+    }
+  }
+}
+
+template <int G, int L, int P>
+__device__ __forceinline__ void chunk_sums(const Transpose32& transpose, const PullChunk<G * L, P>& x,
+                                           int (&acc)[G * L]) {
+#define FLYB_CHUNK(q) case q: chunk_sums_q<G, L, P, (q <= P ? q : P)>(transpose, x, acc); break;
+  switch (x.meta & 31) {              // warp-uniform: one dispatch per chunk
+    FLYB_CHUNK(0) FLYB_CHUNK(1) FLYB_CHUNK(2) FLYB_CHUNK(3) FLYB_CHUNK(4) FLYB_CHUNK(5) FLYB_CHUNK(6)
+    FLYB_CHUNK(7) FLYB_CHUNK(8)
+    default:
+      if constexpr (P > 8) {
+        switch (x.meta & 31) {
+          FLYB_CHUNK(9) FLYB_CHUNK(10) FLYB_CHUNK(11) FLYB_CHUNK(12) FLYB_CHUNK(13) FLYB_CHUNK(14)
+          FLYB_CHUNK(15) FLYB_CHUNK(16)
+          default: break;
+        }
+      }
+      break;
+  }
+#undef FLYB_CHUNK
+}
+
+// One warp's pass over postsynaptic rows [r0, r1) for the steps [lo, hi) of one group. The chunk stream is software-pipelined (the next chunk's words
+// and planes and the inputs of the one after are in flight while a chunk is summed); per chunk
+// every step's words are transposed first and the plane sums of all of them are dispatched once
+// on the chunk's plane count.
+template <int G, int L, int P>
+__device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restrict__ bits, int r0, int r1, int lo,
+                                          int hi, int ws0, int lane) {
+  constexpr int NW = G * L;
+  const Transpose32 transpose(lane);
+  const size_t slot = (size_t)k.n * k.batch;
+  const int ce = __ldg(&k.pull_ptr[r1]);
+  int c = __ldg(&k.pull_ptr[r0]);
+  int row = r0, bound = __ldg(&k.pull_ptr[r0 + 1]);
+  int acc[NW];                               // [g * L + u], like the words
+#pragma unroll
+  for (int i = 0; i < NW; ++i) acc[i] = 0;
+  const auto flush_row = [&]() {             // add the finished row into the write slots of steps [lo, hi)
+#pragma unroll
+    for (int u = 0; u < L; ++u) {
+      if (u < lo || u >= hi) continue;
+      int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        if (acc[g * L + u]) dst[g * 32] += acc[g * L + u];
+        acc[g * L + u] = 0;
+      }
+    }
+  };
+  PullChunk<NW, P> cur;
+  int pre_next = -1;
+  if (c < ce) {
+    pull_fetch<NW, P>(k, bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), c, cur);
+    if (c + 1 < ce) pre_next = __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
+  }
+  for (; c < ce; ++c) {
+    PullChunk<NW, P> nxt;
+    int pre_after = -1;
+    if (c + 1 < ce) {
+      pull_fetch<NW, P>(k, bits, pre_next, c + 1, nxt);
+      if (c + 2 < ce) pre_after = __ldcs(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
+    }
+    while (c >= bound) {                     // chunk c starts a later row: the current one is done
+      flush_row();
+      ++row;
+      bound = __ldg(&k.pull_ptr[row + 1]);
+    }
+    chunk_sums<G, L, P>(transpose, cur, acc);
+    cur = nxt;
+    pre_next = pre_after;
+  }
+  flush_row();                               // the last row with inputs
+}
+
 // Pull delivery of `nsteps` (1..L) undelivered steps, starting at pull_state[0] (its ring position
 // pull_state[1]). Each warp owns a contiguous block of postsynaptic rows and walks their 32-input
 // chunks as one stream, once per group of L steps the range touches (one group when the pulls
@@ -529,24 +642,21 @@ __device__ __forceinline__ int pos_mod(long long a, int m) {
 // inputs are sorted by count; a chunk stores its smallest count as the base and the excess of each
 // entry in as few bit planes as its range needs). Integer and exact: each step's write slot ends
 // with the sums the scatter's atomics give. The chunk tables (inputs, planes, base) are read once
-// per group instead of once per step. The stream is software-pipelined (the next chunk's words and
-// planes and the inputs of the one after are in flight while a chunk is summed); a finished row is
-// added into each step's write slot with coalesced 128-byte accesses per group of 32 flies. The
-// synaptic events of presynaptic neurons in the warp's row block are counted from the same words.
-// The last block to finish moves pull_state on by nsteps (every block has read it by then).
+// per group instead of once per step. A finished row is added into each step's write slot with
+// coalesced 128-byte accesses per group of 32 flies. The synaptic events of presynaptic neurons in
+// the warp's row block are counted from the same words. The last block to finish moves pull_state
+// on by nsteps (every block has read it by then).
 template <int G, int L, int P>
-__global__ void __launch_bounds__(256, 3) lif_pull_kernel(LifK k, int nsteps) {
+__global__ void __launch_bounds__(256, G == 8 ? 2 : 3) lif_pull_kernel(LifK k, int nsteps) {
   constexpr int NW = G * L;
   const long long done = k.pull_state[0];
   const int rp_done = (int)k.pull_state[1];
   const int lane = threadIdx.x & 31;
-  const Transpose32 transpose(lane);
   const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
   const long long wid = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int per = (int)((k.n + warps - 1) / warps);
   const int r0 = (int)(wid * per < k.n ? wid * per : k.n);
   const int r1 = r0 + per < k.n ? r0 + per : k.n;
-  const size_t slot = (size_t)k.n * k.batch;
   unsigned long long ev = 0;
   const long long end = done + nsteps;
   for (long long grp = done / L; grp * L < end; ++grp) {
@@ -556,75 +666,7 @@ __global__ void __launch_bounds__(256, 3) lif_pull_kernel(LifK k, int nsteps) {
     // write slot of step grp * L + u: D slots after its read slot (consecutive steps, consecutive slots)
     const int ws0 = pos_mod(rp_done + (grp * L - done) + k.n_delay, k.R);
     if (r0 >= r1) continue;
-    const int ce = __ldg(&k.pull_ptr[r1]);
-    int c = __ldg(&k.pull_ptr[r0]);
-    int row = r0, bound = __ldg(&k.pull_ptr[r0 + 1]);
-    int acc[L][G];
-#pragma unroll
-    for (int u = 0; u < L; ++u)
-#pragma unroll
-      for (int g = 0; g < G; ++g) acc[u][g] = 0;
-    unsigned w[NW], pl[P];
-    int meta = 0, pre_next = -1;
-    if (c < ce) {
-      pull_words<NW>(bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), w);
-      pull_planes<P>(k.pull_planes, c, pl);
-      meta = __ldcs(&k.pull_meta[c]);
-      if (c + 1 < ce) pre_next = __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
-    }
-    for (; c < ce; ++c) {
-      unsigned wn[NW], pn[P];
-      int meta_next = 0, pre_after = -1;
-      if (c + 1 < ce) {
-        pull_words<NW>(bits, pre_next, wn);
-        pull_planes<P>(k.pull_planes, c + 1, pn);
-        meta_next = __ldcs(&k.pull_meta[c + 1]);
-        if (c + 2 < ce) pre_after = __ldcs(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
-      }
-      while (c >= bound) {                 // chunk c starts a later row: the current one is done
-#pragma unroll
-        for (int u = 0; u < L; ++u) {
-          if (u < lo || u >= hi) continue;
-          int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
-#pragma unroll
-          for (int g = 0; g < G; ++g) {
-            if (acc[u][g]) dst[g * 32] += acc[u][g];
-            acc[u][g] = 0;
-          }
-        }
-        ++row;
-        bound = __ldg(&k.pull_ptr[row + 1]);
-      }
-      const int base = meta >> 5, planes = meta & 31;
-#pragma unroll
-      for (int u = 0; u < L; ++u) {
-        if (u < lo || u >= hi) continue;   // kernel-uniform: no divergence
-        unsigned m[G];
-        int add[G];
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-          m[g] = transpose(w[g * L + u]);
-          add[g] = base * __popc(m[g]);
-        }
-        plane_sums<G, P>(m, pl, planes, add);
-#pragma unroll
-        for (int g = 0; g < G; ++g) acc[u][g] += add[g];
-      }
-#pragma unroll
-      for (int i = 0; i < NW; ++i) w[i] = wn[i];
-#pragma unroll
-      for (int q = 0; q < P; ++q) pl[q] = pn[q];
-      meta = meta_next;
-      pre_next = pre_after;
-    }
-#pragma unroll
-    for (int u = 0; u < L; ++u) {            // the last row with inputs
-      if (u < lo || u >= hi) continue;
-      int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
-#pragma unroll
-      for (int g = 0; g < G; ++g)
-        if (acc[u][g]) dst[g * 32] += acc[u][g];
-    }
+    pull_pass<G, L, P>(k, bits, r0, r1, lo, hi, ws0, lane);
     if (k.events) {                          // events of presynaptic neurons r0 .. r1 in these steps
       for (int j = r0 + lane; j < r1; j += 32) {
         unsigned wj[NW];
@@ -667,7 +709,8 @@ static void launch_pull_glp(const LifK& k, int nsteps, int sms, cudaStream_t st)
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, L, P>, 256, 0);
     if (per_sm < 1) per_sm = 1;
   }
-  lif_pull_kernel<G, L, P><<<sms * per_sm, 256, 0, st>>>(k, nsteps);
+  const int grid = k.pull_grid > 0 && k.pull_grid < sms * per_sm ? k.pull_grid : sms * per_sm;
+  lif_pull_kernel<G, L, P><<<grid, 256, 0, st>>>(k, nsteps);
 }
 
 template <int G, int L>
@@ -1615,6 +1658,8 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.pull_ptr = a->pull_ptr; k.pull_pre = a->pull_pre; k.pull_planes = a->pull_planes;
   k.pull_nplanes = a->pull_nplanes; k.pull_meta = a->pull_meta;
   k.pull_group = a->pull_group; k.pull_phase = a->pull_phase; k.pull_bits = nullptr; k.pull_state = nullptr;
+  k.pull_grid = a->pull_grid;
+  if (a->pull_grid < 0) return FLYB_EINVAL;
   if (a->flags & FLYB_LIF_PULL_DELIVERY) {
     const int g = a->batch / 32;
     // a group's pull may run beside the next group's updates and must end before the steps after

@@ -57,7 +57,7 @@ class LifArgs(ct.Structure):
                 ("slow_out_ptr", _VP * 2), ("slow_out_edge", _VP * 2), ("slow_ring", _VP * 2), ("slow_g", _VP * 2),
                 ("g_slow", _VP), ("pull_ptr", _VP), ("pull_pre", _VP), ("pull_planes", _VP), ("pull_nplanes", _I),
                 ("pull_meta", _VP), ("pull_group", _I), ("pull_steps", _I), ("pull_phase", _I),
-                ("pull_bits", _VP), ("pull_state", _VP)]
+                ("pull_bits", _VP), ("pull_state", _VP), ("pull_grid", _I)]
 
 
 class OpticArgs(ct.Structure):

@@ -440,6 +440,7 @@ class Brain:
         if self._pull_bits is None or self._pull_bits.numel() != 2 * L * self.words:
             self._pull_bits = torch.zeros(2 * L * self.words, dtype=torch.int32, device=self.device)
         a.pull_group, a.pull_bits, a.pull_state = L, self._pull_bits.data_ptr(), self._pull_state.data_ptr()
+        a.pull_grid = int(getattr(self, "pull_grid", 0))      # pull launch block cap (0: one wave)
         a.pull_phase = self.step_count % L
 
     @property

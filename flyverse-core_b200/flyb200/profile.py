@@ -6,6 +6,7 @@
                               [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
                               [--no-overlap]
     python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
+    (--per-call K: K whole-fly steps per call, `--steps` calls)
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
 `--steps` steps of the chosen part. Used for the launch list and the per-kernel captures whose
@@ -141,6 +142,8 @@ def main() -> None:
     ap.add_argument("--lif-pull", action="store_true", help="LIF spikes delivered by the pull kernel")
     ap.add_argument("--density", type=float, default=0.024, help="spike density for --part pull")
     ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--per-call", type=int, default=1, help="whole-fly steps per WholeFly.step call (the pull "
+                                                             "delivers whole groups of steps within a call)")
     ap.add_argument("--lif-block", type=int, default=256)
     ap.add_argument("--lif-ipt", type=int, default=0, help="LIF items per thread (0: automatic)")
     ap.add_argument("--lif-staged", action="store_true", help="LIF step through the bulk-copy kernel")
@@ -174,7 +177,7 @@ def main() -> None:
         return
     for _ in range(args.steps):
         if args.part == "whole":
-            eng.step(1)
+            eng.step(args.per_call)
         elif args.part == "lif":
             eng.lif.step(1)
         else:

@@ -220,6 +220,8 @@ typedef struct flyb_lif_args {
                             0}; moved on by each pull. It must equal {step, ring position} of the
                             next step to run (step0 / ring_pos, or clock[0] / clock[1]) whenever
                             nothing is pending                                                  */
+  int pull_grid;         /* blocks of a pull launch (0: one wave of resident blocks); fewer leave
+                            SM room to kernels running beside it on other streams               */
 } flyb_lif_args;
 
 /* flyb_lif_args.slow_mode */

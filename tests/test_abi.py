@@ -64,7 +64,7 @@ bad = [dict(batch=48), dict(batch=512), dict(ring_mode=_abi.RING_FIXED),
        dict(pull_ptr=None), dict(pull_meta=None), dict(pull_nplanes=12), dict(pull_bits=None),
        dict(pull_state=None), dict(pull_bits=fake + 16), dict(pull_group=2), dict(pull_group=8),
        dict(pull_group=4, n_delay=7, ring_slots=8), dict(pull_steps=0), dict(pull_steps=5),
-       dict(pull_phase=4), dict(pull_phase=-1), dict(flags=0)]
+       dict(pull_phase=4), dict(pull_phase=-1), dict(pull_grid=-1), dict(flags=0)]
 for kw in bad:
     rc = lib.flyb_lif_pull(ct.byref(args(**kw)), None)
     assert rc == _abi.EINVAL, (kw, rc)
@@ -87,4 +87,4 @@ def test_pull_delivery_arguments_are_validated_before_any_launch():
     r = subprocess.run([sys.executable, "-c", PULL_VALIDATION, pkg], env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "rejected 20" in r.stdout
+    assert "rejected 21" in r.stdout
