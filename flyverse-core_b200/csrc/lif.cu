@@ -68,6 +68,7 @@ struct LifK {
   unsigned* pull_bits;                         // [2][words][L] spike words of the last two groups
   long long* pull_state;                       // {first undelivered step, its ring position, counter}
   int pull_grid;                               // blocks of a pull launch (0: one wave)
+  int pull_group_log2;                         // log2(pull_group)
   LifP P;
 };
 
@@ -445,11 +446,11 @@ struct Transpose32 {
 // input then fetches every step of the group at once, where a per-step pull fetched a whole
 // sector for G words of one step.
 __device__ __forceinline__ size_t pull_word_index(const LifK& k, long long step, long long word) {
-  const long long L = k.pull_group;
-  return (size_t)(((step / L) & 1) * k.words + word) * (size_t)L + (size_t)(step % L);
+  const int sh = k.pull_group_log2;            // L is a power of two: shifts, no 64-bit division
+  return (size_t)(((step >> sh) & 1) * k.words + word) * ((size_t)1 << sh) + (size_t)(step & ((1ll << sh) - 1));
 }
 
-// One input's words of a group: NW = G * L adjacent words (16-byte aligned for NW >= 4).
+// One input's words of a group: NW = G * L adjacent words (NW x 4-byte aligned).
 template <int NW>
 __device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, int pre, unsigned (&w)[NW]) {
   if (pre < 0) {
@@ -463,6 +464,11 @@ __device__ __forceinline__ void pull_words(const unsigned* __restrict__ bits, in
   } else if constexpr (NW == 2) {
     const uint2 v = __ldg(reinterpret_cast<const uint2*>(src));
     w[0] = v.x; w[1] = v.y;
+  } else if constexpr (NW == 8) {
+    // the group's 32-byte sector in one 256-bit load (sm_100; `src` is 32-byte aligned)
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(w[0]), "=r"(w[1]), "=r"(w[2]), "=r"(w[3]), "=r"(w[4]), "=r"(w[5]), "=r"(w[6]), "=r"(w[7])
+                 : "l"(src));
   } else {
 #pragma unroll
     for (int i = 0; i < NW; i += 4) {
@@ -647,7 +653,7 @@ __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restr
 // the warp's row block are counted from the same words. The last block to finish moves pull_state
 // on by nsteps (every block has read it by then).
 template <int G, int L, int P>
-__global__ void __launch_bounds__(256, G == 8 ? 2 : 3) lif_pull_kernel(LifK k, int nsteps) {
+__global__ void __launch_bounds__(256, 3) lif_pull_kernel(LifK k, int nsteps) {
   constexpr int NW = G * L;
   const long long done = k.pull_state[0];
   const int rp_done = (int)k.pull_state[1];
@@ -1660,6 +1666,8 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
   k.pull_group = a->pull_group; k.pull_phase = a->pull_phase; k.pull_bits = nullptr; k.pull_state = nullptr;
   k.pull_grid = a->pull_grid;
   if (a->pull_grid < 0) return FLYB_EINVAL;
+  k.pull_group_log2 = 0;
+  while ((1 << k.pull_group_log2) < a->pull_group && k.pull_group_log2 < 4) ++k.pull_group_log2;
   if (a->flags & FLYB_LIF_PULL_DELIVERY) {
     const int g = a->batch / 32;
     // a group's pull may run beside the next group's updates and must end before the steps after

@@ -6,7 +6,7 @@
                               [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
                               [--no-overlap]
     python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
-    (--per-call K: K whole-fly steps per call, `--steps` calls)
+    (--per-call K: K whole-fly steps per call, `--steps` calls; --settle S: S steps first, from CUDA graphs)
 
 Builds flyb200.synthetic.whole_fly_config5 (167,106 neurons, 25.6 M edges), warms up, then runs
 `--steps` steps of the chosen part. Used for the launch list and the per-kernel captures whose
@@ -142,6 +142,8 @@ def main() -> None:
     ap.add_argument("--lif-pull", action="store_true", help="LIF spikes delivered by the pull kernel")
     ap.add_argument("--density", type=float, default=0.024, help="spike density for --part pull")
     ap.add_argument("--breakdown", action="store_true")
+    ap.add_argument("--settle", type=int, default=0, help="steps replayed from CUDA graphs of 20 before the "
+                                                           "profiled ones (3,000: the steady firing the bench times)")
     ap.add_argument("--per-call", type=int, default=1, help="whole-fly steps per WholeFly.step call (the pull "
                                                              "delivers whole groups of steps within a call)")
     ap.add_argument("--lif-block", type=int, default=256)
@@ -166,6 +168,17 @@ def main() -> None:
     eng.lif._make_args()
     eng.optic.pr_in.normal_(0.0, 0.2)
     eng.step(args.warmup)
+    if args.settle > 0:
+        stream = torch.cuda.Stream()
+        stream.wait_stream(torch.cuda.current_stream())
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(stream):
+            with torch.cuda.graph(graph, stream=stream):
+                eng.step(20)
+        torch.cuda.current_stream().wait_stream(stream)
+        for _ in range(args.settle // 20):
+            graph.replay()
+        del graph
     torch.cuda.synchronize()
     if args.breakdown:
         res = breakdown(eng, max(10, args.steps))
