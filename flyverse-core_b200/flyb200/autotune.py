@@ -99,29 +99,39 @@ def _apply(brain, choice: dict) -> None:
     brain._make_args()
 
 
+# Row lengths above which a row is shared by a whole block (OpticCore.set_long_rows): the split
+# pays at many flies per row gather; at one fly a row of a few hundred entries is better left to
+# its warp slot.
+OPTIC_LONG_ROWS = (192, 512, 2048)
+
+
 def tune_optic(core, steps: int = 10) -> dict:
-    """Pick the optic substep's launch mode and kernel shape (fly lanes x flies per lane x lanes
-    per row, flyb_optic_args.variant) by timing each on a copy of the state."""
+    """Pick the optic substep's launch mode, kernel shape (fly lanes x flies per lane x lanes per
+    row, flyb_optic_args.variant) and long-row threshold by timing each on a copy of the state."""
     key = ("optic", core.m, core.W.nnz, core.B)
     if key in CACHE:
         core.launch, core.variant = CACHE[key]["launch"], CACHE[key]["variant"]
+        core.set_long_rows(CACHE[key]["long_row"])
         return CACHE[key]
     v, a = core.v_s.clone(), core.adapt_s.clone()
     results = {}
-    for launch in ("step", "persistent"):
-        for variant in range(OPTIC_VARIANTS):
-            core.launch, core.variant = launch, variant
-            try:
-                core.substeps(2)
-            except RuntimeError:                 # no such shape for this batch width
-                continue
-            results[(launch, variant)] = _time(lambda: core.substeps(steps, carry=True), 1) / steps
-            core.v_s.copy_(v)
-            core.adapt_s.copy_(a)
+    for long_row in OPTIC_LONG_ROWS:
+        core.set_long_rows(long_row)
+        for launch in ("step", "persistent"):
+            for variant in range(OPTIC_VARIANTS):
+                core.launch, core.variant = launch, variant
+                try:
+                    core.substeps(2)
+                except RuntimeError:                 # no such shape for this batch width
+                    continue
+                results[(launch, variant, long_row)] = _time(lambda: core.substeps(steps, carry=True), 1) / steps
+                core.v_s.copy_(v)
+                core.adapt_s.copy_(a)
     best = min(results, key=results.get)
-    CACHE[key] = {"launch": best[0], "variant": best[1], "ms_per_step": results[best],
-                  "all": {f"{k[0]}/{k[1]}": t for k, t in results.items()}}
-    core.launch, core.variant = best
+    CACHE[key] = {"launch": best[0], "variant": best[1], "long_row": best[2], "ms_per_step": results[best],
+                  "all": {f"{k[0]}/{k[1]}/{k[2]}": t for k, t in results.items()}}
+    core.launch, core.variant = best[0], best[1]
+    core.set_long_rows(best[2])
     return CACHE[key]
 
 

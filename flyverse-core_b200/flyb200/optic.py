@@ -174,10 +174,14 @@ class OpticCore:
     `long_row` entries are each shared by all warps of a block (flyb_optic_args.rows / n_long)."""
 
     def set_long_rows(self, long_row: int) -> None:
-        deg = np.diff(self.W.ptr.cpu().numpy())
-        order = np.argsort(-deg, kind="stable").astype(np.int32)
-        self.rows = torch.from_numpy(order).to(self.device)
-        self.n_long = int((deg > long_row).sum())
+        """Rows with more than `long_row` entries are split across a block. The row order (longest
+        first) is built once and kept in the same device buffer, so captured graphs stay valid;
+        only the count of long rows (a launch argument) changes."""
+        if getattr(self, "_deg", None) is None:
+            self._deg = np.diff(self.W.ptr.cpu().numpy())
+            order = np.argsort(-self._deg, kind="stable").astype(np.int32)
+            self.rows = torch.from_numpy(order).to(self.device)
+        self.n_long = int((self._deg > long_row).sum())
         self.long_row = int(long_row)
 
     def __init__(self, W_rr: sp.spmatrix, a: np.ndarray, b: np.ndarray, *, batch: int, device, gain_rr: float,
