@@ -82,6 +82,40 @@ def test_kernel_shape_variants_match_oracle(batch, variant, launch):
     np.testing.assert_allclose(core.adapt_s.cpu().numpy(), ad, rtol=RTOL, atol=ATOL)
 
 
+@pytest.mark.parametrize("batch", [1, 64])
+@pytest.mark.parametrize("launch", ["step", "persistent"])
+def test_every_long_row_threshold_matches_oracle(batch, launch):
+    """The autotuner's long-row thresholds (and the extremes: every non-empty row split across a
+    block, none split) against the FP32 oracle; changing the threshold keeps the row-order buffer."""
+    from flyb200.autotune import OPTIC_LONG_ROWS
+    cfg = small_optic(seed=12)
+    W = cfg.W_rr()
+    rng = np.random.default_rng(batch)
+    v = (rng.standard_normal((cfg.m, batch)) * 0.3).astype(np.float32)
+    ad = (rng.standard_normal((cfg.m, batch)) * 0.05).astype(np.float32)
+    pr = (rng.standard_normal((cfg.m, batch)) * 0.3).astype(np.float32)
+    spk = (rng.standard_normal((cfg.m, batch)) * 0.1).astype(np.float32)
+    ov, oad = v.copy(), ad.copy()
+    oracle.optic_run(ov, oad, W.indptr, W.indices, W.data, pr, spk, cfg.a, cfg.b, cfg.gain_rr, cfg.adapt_gain,
+                     cfg.aad, 20)
+    core = OpticCore(W, cfg.a, cfg.b, batch=batch, device="cuda", gain_rr=cfg.gain_rr, adapt_gain=cfg.adapt_gain,
+                     aad=cfg.aad, launch=launch)
+    rows = core.rows
+    deg = np.diff(W.indptr)
+    for long_row in (0, 16) + tuple(OPTIC_LONG_ROWS) + (1 << 30,):
+        core.set_long_rows(long_row)
+        assert core.rows is rows and core.n_long == int((deg > long_row).sum())
+        core.v_s.copy_(torch.from_numpy(v))
+        core.adapt_s.copy_(torch.from_numpy(ad))
+        core.pr_in.copy_(torch.from_numpy(pr))
+        core.spk_in.copy_(torch.from_numpy(spk))
+        core.substeps(20)
+        torch.cuda.synchronize()
+        core.check()
+        np.testing.assert_allclose(core.v_s.cpu().numpy(), ov, rtol=RTOL, atol=ATOL, err_msg=f"long_row {long_row}")
+        np.testing.assert_allclose(core.adapt_s.cpu().numpy(), oad, rtol=RTOL, atol=ATOL)
+
+
 def test_single_carried_persistent_substeps_with_a_block_cap_equal_step_launches():
     """One substep on a carried dr is an ordinary launch of a capped grid looping over the rows:
     bit-identical to one launch per substep."""
