@@ -790,17 +790,19 @@ def reference_optic_gpu(ref, cfg3, device, batch) -> dict:
     return out
 
 
-def ours_optic(cfg3, device, batch) -> float:
-    """This library's fused substep on the same lobe: device ms per substep (autotuned shape)."""
+def ours_optic(cfg3, device, batch) -> tuple:
+    """This library's fused substep on the same lobe: device ms per substep (autotuned shape) and
+    the tuner's choice (launch, kernel shape, long-row threshold)."""
     from flyb200 import autotune
     from flyb200.optic import OpticCore
     core = OpticCore(cfg3.W_rr(), cfg3.a, cfg3.b, batch=batch, device=device, gain_rr=cfg3.gain_rr,
                      adapt_gain=cfg3.adapt_gain, aad=cfg3.aad, launch="step")
     rng = np.random.default_rng(0)
     core.pr_in.copy_(torch.from_numpy((rng.standard_normal((cfg3.m, batch)) * 0.2).astype(np.float32)))
-    autotune.tune_optic(core, steps=10)
+    pick = autotune.tune_optic(core, steps=10)
     core.substeps(2)
-    return graph_ms_per_step(lambda n: core.substeps(n, carry=True), 10, 5)
+    tuned = {k: pick[k] for k in ("launch", "variant", "long_row")}
+    return graph_ms_per_step(lambda n: core.substeps(n, carry=True), 10, 5), tuned
 
 
 def measure_reference_gpu(device, cfg2, cfg3) -> dict:
@@ -822,8 +824,9 @@ def measure_reference_gpu(device, cfg2, cfg3) -> dict:
         torch.cuda.empty_cache()
         try:
             r = reference_optic_gpu(ref, cfg3, device, B)
-            r["ours_ms"] = ours_optic(cfg3, device, B)
-            r["speedup_vs_best_graph"] = min(v["graph_ms"] for v in r.values() if isinstance(v, dict)) / r["ours_ms"]
+            r["ours_ms"], r["ours_tuned"] = ours_optic(cfg3, device, B)
+            r["speedup_vs_best_graph"] = min(v["graph_ms"] for v in r.values()
+                                             if isinstance(v, dict) and "graph_ms" in v) / r["ours_ms"]
         except Exception as e:            # noqa: BLE001
             r = {"unavailable": f"{type(e).__name__}: {e}"}
         res["optic_c3"][f"B{B}"] = r

@@ -59,9 +59,10 @@ struct LifK {
   float* slow_g[FLYB_SLOW_MAX_CLASSES];
   float* g_slow;
   const int* __restrict__ pull_ptr;            // pull delivery: first 32-entry input chunk per row
-  const int* __restrict__ pull_pre;            // [chunks][32] presynaptic neuron (-1: padding)
+  const int* __restrict__ pull_pre;            // [chunks][32] presynaptic neuron (-1: padding), or
+                                               // packed: neuron | excess << 24 (0xFFFFFF: padding)
   const unsigned* __restrict__ pull_planes;    // [chunks][pull_nplanes] count bit planes
-  int pull_nplanes;                            // plane stride per chunk (8 or 16)
+  int pull_nplanes;                            // plane stride per chunk (16), or 0: packed entries
   const int* __restrict__ pull_meta;           // per chunk: base count << 5 | planes used
   int pull_group;                              // L: steps a pull delivers together
   int pull_phase;                              // runs that pull themselves: first step's index mod L
@@ -527,19 +528,29 @@ __device__ __forceinline__ int pos_mod(long long a, int m) {
 }
 
 // One chunk of a warp's input stream: every lane's G * L spike words of its input, the chunk's
-// count planes and its base << 5 | plane count.
+// count planes (P of them from the plane table; P = 0: packed entries, the lane's own excess
+// instead, from which the planes are rebuilt by ballots) and its base << 5 | plane count.
 template <int NW, int P>
 struct PullChunk {
   unsigned w[NW];
-  unsigned pl[P];
+  unsigned pl[P > 0 ? P : 1];
+  unsigned ex;
   int meta;
 };
 
+constexpr unsigned kPullPad = 0xFFFFFFu;        // packed entry: no input (a row's last chunk)
+
 template <int NW, int P>
-__device__ __forceinline__ void pull_fetch(const LifK& k, const unsigned* __restrict__ bits, int pre, long long c,
+__device__ __forceinline__ void pull_fetch(const LifK& k, const unsigned* __restrict__ bits, int entry, long long c,
                                            PullChunk<NW, P>& x) {
-  pull_words<NW>(bits, pre, x.w);
-  pull_planes<P>(k.pull_planes, c, x.pl);
+  if constexpr (P == 0) {
+    const unsigned pre = (unsigned)entry & kPullPad;
+    pull_words<NW>(bits, pre == kPullPad ? -1 : (int)pre, x.w);
+    x.ex = (unsigned)entry >> 24;
+  } else {
+    pull_words<NW>(bits, entry, x.w);
+    pull_planes<P>(k.pull_planes, c, x.pl);
+  }
   x.meta = __ldcs(&k.pull_meta[c]);
 }
 
@@ -552,6 +563,9 @@ template <int G, int L, int P, int Q>
 __device__ __forceinline__ void chunk_sums_q(const Transpose32& transpose, const PullChunk<G * L, P>& x,
                                              int (&acc)[G * L]) {
   const int base = x.meta >> 5;
+  unsigned pl[Q > 0 ? Q : 1];
+#pragma unroll
+  for (int q = 0; q < Q; ++q) pl[q] = P == 0 ? __ballot_sync(0xffffffffu, (x.ex >> q) & 1u) : x.pl[q];
 #pragma unroll
   for (int u = 0; u < L; ++u) {
 #pragma unroll
@@ -559,7 +573,7 @@ __device__ __forceinline__ void chunk_sums_q(const Transpose32& transpose, const
       const unsigned m = transpose(x.w[g * L + u]);
       int sum = base * __popc(m);
 #pragma unroll
-      for (int q = 0; q < Q; ++q) sum += __popc(m & x.pl[q]) << q;
+      for (int q = 0; q < Q; ++q) sum += __popc(m & pl[q]) << q;
       acc[g * L + u] += sum;
     }
   }
@@ -568,7 +582,8 @@ __device__ __forceinline__ void chunk_sums_q(const Transpose32& transpose, const
 template <int G, int L, int P>
 __device__ __forceinline__ void chunk_sums(const Transpose32& transpose, const PullChunk<G * L, P>& x,
                                            int (&acc)[G * L]) {
-#define FLYB_CHUNK(q) case q: chunk_sums_q<G, L, P, (q <= P ? q : P)>(transpose, x, acc); break;
+  constexpr int QMAX = P == 0 ? 8 : P;   // packed entries carry 8-bit excesses
+#define FLYB_CHUNK(q) case q: chunk_sums_q<G, L, P, (q <= QMAX ? q : QMAX)>(transpose, x, acc); break;
   switch (x.meta & 31) {              // warp-uniform: one dispatch per chunk
     FLYB_CHUNK(0) FLYB_CHUNK(1) FLYB_CHUNK(2) FLYB_CHUNK(3) FLYB_CHUNK(4) FLYB_CHUNK(5) FLYB_CHUNK(6)
     FLYB_CHUNK(7) FLYB_CHUNK(8)
@@ -652,8 +667,9 @@ __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restr
 // coalesced 128-byte accesses per group of 32 flies. The synaptic events of presynaptic neurons in
 // the warp's row block are counted from the same words. The last block to finish moves pull_state
 // on by nsteps (every block has read it by then).
+constexpr int kPullBlock = 256, kPullBlocksPerSm = 3;   // launch shape of the pull kernel
 template <int G, int L, int P>
-__global__ void __launch_bounds__(256, 3) lif_pull_kernel(LifK k, int nsteps) {
+__global__ void __launch_bounds__(kPullBlock, kPullBlocksPerSm) lif_pull_kernel(LifK k, int nsteps) {
   constexpr int NW = G * L;
   const long long done = k.pull_state[0];
   const int rp_done = (int)k.pull_state[1];
@@ -712,16 +728,16 @@ static void launch_pull_glp(const LifK& k, int nsteps, int sms, cudaStream_t st)
   static int per_sm = 0;                 // resident blocks: one wave, each warp a longer row stream
   if (!per_sm) {
     cudaFuncSetAttribute(lif_pull_kernel<G, L, P>, cudaFuncAttributePreferredSharedMemoryCarveout, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, L, P>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lif_pull_kernel<G, L, P>, kPullBlock, 0);
     if (per_sm < 1) per_sm = 1;
   }
   const int grid = k.pull_grid > 0 && k.pull_grid < sms * per_sm ? k.pull_grid : sms * per_sm;
-  lif_pull_kernel<G, L, P><<<grid, 256, 0, st>>>(k, nsteps);
+  lif_pull_kernel<G, L, P><<<grid, kPullBlock, 0, st>>>(k, nsteps);
 }
 
 template <int G, int L>
 static void launch_pull_gl(const LifK& k, int nsteps, int sms, cudaStream_t st) {
-  if (k.pull_nplanes == 8) launch_pull_glp<G, L, 8>(k, nsteps, sms, st);
+  if (k.pull_nplanes == 0) launch_pull_glp<G, L, 0>(k, nsteps, sms, st);
   else launch_pull_glp<G, L, 16>(k, nsteps, sms, st);
 }
 
@@ -1674,8 +1690,10 @@ static int make_lif_k(const flyb_lif_args* a, LifK& k) {
     // them: its earliest write slot is read n_delay steps after its first step, so 2 L <= n_delay
     if (a->batch % 32 || (g != 1 && g != 2 && g != 4 && g != 8) || a->ring_mode != FLYB_RING_COUNT ||
         a->launch != FLYB_LAUNCH_STEP || (a->flags & (FLYB_LIF_DEFER_DELIVERY | FLYB_LIF_STD)) || a->clock_k ||
-        a->slow_classes || !a->pull_ptr || !a->pull_pre || !a->pull_planes || !a->pull_meta ||
-        (a->pull_nplanes != 8 && a->pull_nplanes != 16) || (reinterpret_cast<uintptr_t>(a->pull_planes) & 15) ||
+        a->slow_classes || !a->pull_ptr || !a->pull_pre || !a->pull_meta ||
+        (a->pull_nplanes != 0 && a->pull_nplanes != 16) ||
+        (a->pull_nplanes && (!a->pull_planes || (reinterpret_cast<uintptr_t>(a->pull_planes) & 15))) ||
+        (a->pull_nplanes == 0 && a->n > (int)kPullPad) ||
         !a->pull_bits || !a->pull_state || (reinterpret_cast<uintptr_t>(a->pull_bits) & 31) ||
         !pull_group_ok(a->batch, a->pull_group) || (a->pull_group > 1 && 2 * a->pull_group > a->n_delay) ||
         a->pull_phase < 0 || a->pull_phase >= a->pull_group)

@@ -127,14 +127,21 @@ def clock_coefficients(p: LIFParams, std_on: bool, max_period: int, slow_tau=())
     return out.numpy()
 
 
+PULL_PAD = 0xFFFFFF           # packed pull entry without an input
+
+
 def pull_inputs(W, w_syn: float):
     """The inputs of every neuron for FLYB_LIF_PULL_DELIVERY, from W[post, pre] = w_syn x signed
-    integer counts: (pull_ptr int32 [N+1] in 32-entry chunks, pull_pre int32 [chunks * 32] with -1
-    padding the last chunk of a row, pull_planes uint32 [chunks * S], pull_meta int32 [chunks], S).
-    A row's inputs are sorted by count, so a chunk's counts lie close together: it stores its
-    smallest count as the base and each entry's excess over it in as few bit planes as that range
-    needs (meta = base << 5 | planes; bit l of plane p = bit p of entry l's excess); S, the plane
-    stride, is 8 or 16. None when the weights are not such counts or a chunk's range needs more
+    integer counts: (pull_ptr int32 [N+1] in 32-entry chunks, pull_pre int32 [chunks * 32],
+    pull_planes uint32 [chunks * S], pull_meta int32 [chunks], S). A row's inputs are sorted by
+    count, so a chunk's counts lie close together: it stores its smallest count as the base and
+    each entry's excess over it (meta = base << 5 | planes, the bits that range needs).
+
+    When every excess fits 8 bits (and N < 2^24 - 1) the tables are packed, S = 0: an entry is
+    pre | excess << 24, 0xFFFFFF padding the last chunk of a row, and pull_planes is empty (the
+    kernel rebuilds the planes with warp ballots). Otherwise S = 16: entries are pre with -1
+    padding, and pull_planes holds each chunk's excesses as 16 bit planes (bit l of plane p = bit p
+    of entry l's excess). None when the weights are not such counts or a chunk's range needs more
     than 16 bits."""
     Wr = sp.csr_matrix(W, dtype=np.float32)
     Wr.sum_duplicates()
@@ -167,13 +174,16 @@ def pull_inputs(W, w_syn: float):
         return None
     if base.size and (base.min() < -(1 << 26) or base.max() >= (1 << 26)):
         return None
-    S = 8 if not planes_needed.size or planes_needed.max() <= 8 else 16
+    meta = ((base << 5) | planes_needed).astype(np.int32)
+    if (not planes_needed.size or planes_needed.max() <= 8) and max(Wr.shape) < PULL_PAD:
+        packed = np.where(pre >= 0, pre.astype(np.int64) | (excess << 24), PULL_PAD).astype(np.uint32)
+        return ptr.astype(np.int32), packed.view(np.int32), np.zeros(0, np.uint32), meta, 0
+    S = 16
     u = excess.astype(np.uint64).reshape(chunks, 32)
     lanes = np.arange(32, dtype=np.uint64)
     planes = np.zeros((chunks, S), np.uint64)
     for q in range(S):
         planes[:, q] = (((u >> np.uint64(q)) & np.uint64(1)) << lanes).sum(axis=1)
-    meta = ((base << 5) | planes_needed).astype(np.int32)
     return ptr.astype(np.int32), pre, planes.astype(np.uint32).ravel(), meta, S
 
 
@@ -432,9 +442,11 @@ class Brain:
             if t is None:
                 raise ValueError("pull delivery needs weights of w_syn x counts within 16 bits")
             ptr, pre, planes, meta, S = t
-            self._pull_t = tuple(torch.from_numpy(x).to(self.device) for x in (ptr, pre, planes.view(np.int32), meta))
+            self._pull_t = tuple(torch.from_numpy(x).to(self.device) if x.size else None
+                                 for x in (ptr, pre, planes.view(np.int32), meta))
             self._pull_planes_n, self._pull_key = S, key
-        a.pull_ptr, a.pull_pre, a.pull_planes, a.pull_meta = (x.data_ptr() for x in self._pull_t)
+        a.pull_ptr, a.pull_pre, a.pull_planes, a.pull_meta = (None if x is None else x.data_ptr()
+                                                              for x in self._pull_t)
         a.pull_nplanes = self._pull_planes_n
         L = self.pull_group
         if self._pull_bits is None or self._pull_bits.numel() != 2 * L * self.words:

@@ -82,7 +82,7 @@ int launch_means(void** p, int n, int groups, int batch, int stride, void* strea
                                       batch a multiple of 32 (at most 256), raster on: the
                                       update kernels only record the step's spikes in the raster,
                                       then each postsynaptic row sums count x spike over its
-                                      inputs (pull_ptr / pull_pre / pull_planes) into the write
+                                      inputs (pull_ptr / pull_pre / pull_meta) into the write
                                       slot, the same exact integers the scatter adds. A launch
                                       over all neurons pulls after every step; launches over
                                       neuron ranges leave it to flyb_lif_pull                    */
@@ -196,11 +196,12 @@ typedef struct flyb_lif_args {
   float* slow_g[FLYB_SLOW_MAX_CLASSES];             /* [n][batch] tone per class (mV)    */
   float* g_slow;                                    /* [n][batch] summed tone (mV)       */
   /* FLYB_LIF_PULL_DELIVERY: the inputs of each neuron (rows of W[post, pre]) in chunks of 32
-   * entries, a row's last chunk padded with pre = -1: pull_ptr [n+1] first chunk of each row,
-   * pull_pre [chunks][32] presynaptic neuron, pull_meta [chunks] = (base << 5) | planes: entry l
-   * of the chunk carries count base + d_l, 0 <= d_l < 2^planes, planes <= pull_nplanes;
-   * pull_planes [chunks][pull_nplanes] the d_l as bit planes (bit l of plane p = bit p of d_l);
-   * pull_nplanes (the plane stride) 8 or 16.
+   * entries: pull_ptr [n+1] first chunk of each row, pull_meta [chunks] = (base << 5) | planes:
+   * entry l of the chunk carries count base + d_l, 0 <= d_l < 2^planes. Two table formats:
+   * pull_nplanes = 0 (packed, planes <= 8, n < 2^24): pull_pre [chunks][32] = pre | d_l << 24,
+   * 0xFFFFFF padding a row's last chunk, pull_planes unused (may be null);
+   * pull_nplanes = 16: pull_pre [chunks][32] presynaptic neuron (-1 padding) and pull_planes
+   * [chunks][16] the d_l as bit planes (bit l of plane p = bit p of d_l), 16-byte aligned.
    * The update kernels record each step's spike words in pull_bits as well, and pulls deliver
    * groups of pull_group consecutive steps at once: one gather per input then fetches the input's
    * words of every step of the group (one 32-byte sector when pull_group = 8 / (batch / 32)). */

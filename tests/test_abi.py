@@ -52,7 +52,7 @@ def args(**kw):
               "pull_state"):
         setattr(a, f, fake)
     a.params = params.ctypes.data
-    a.pull_nplanes = 8
+    a.pull_nplanes = 0
     for k, v in kw.items():
         setattr(a, k, v)
     return a
@@ -61,7 +61,9 @@ def args(**kw):
 bad = [dict(batch=48), dict(batch=512), dict(ring_mode=_abi.RING_FIXED),
        dict(flags=_abi.LIF_PULL_DELIVERY | _abi.LIF_STD, std_u=fake),
        dict(flags=_abi.LIF_PULL_DELIVERY | _abi.LIF_DEFER_DELIVERY), dict(launch=_abi.LAUNCH_PERSISTENT),
-       dict(pull_ptr=None), dict(pull_meta=None), dict(pull_nplanes=12), dict(pull_bits=None),
+       dict(pull_ptr=None), dict(pull_meta=None), dict(pull_nplanes=12), dict(pull_nplanes=8),
+       dict(pull_nplanes=16, pull_planes=None), dict(pull_nplanes=16, pull_planes=fake + 4),
+       dict(n=1 << 24), dict(pull_bits=None),
        dict(pull_state=None), dict(pull_bits=fake + 16), dict(pull_group=2), dict(pull_group=8),
        dict(pull_group=4, n_delay=7, ring_slots=8), dict(pull_steps=0), dict(pull_steps=5),
        dict(pull_phase=4), dict(pull_phase=-1), dict(pull_grid=-1), dict(flags=0)]
@@ -75,7 +77,8 @@ print("rejected", len(bad))
 def test_pull_delivery_arguments_are_validated_before_any_launch():
     """flyb_lif_pull / FLYB_LIF_PULL_DELIVERY reject what the pull cannot do (a batch that is not
     32, 64, 128 or 256 flies, the fixed-point ring, depression, persistent launches, missing tables
-    or buffers, a misaligned pull buffer, a group size the batch or the delay does not allow, a
+    or buffers, an unknown table format, a plane table that is missing or misaligned, packed entries
+    for more neurons than their 24-bit field holds, a misaligned pull buffer, a group size the batch or the delay does not allow, a
     step count outside 1..group, a bad phase) with FLYB_EINVAL before touching the device. The
     cases run in a child process that sees no GPU, so that a check that ever weakens fails there
     instead of launching a kernel on the fake addresses."""
@@ -87,4 +90,4 @@ def test_pull_delivery_arguments_are_validated_before_any_launch():
     r = subprocess.run([sys.executable, "-c", PULL_VALIDATION, pkg], env=env, capture_output=True, text=True,
                        timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "rejected 21" in r.stdout
+    assert "rejected 25" in r.stdout
