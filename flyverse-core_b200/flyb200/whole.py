@@ -234,15 +234,16 @@ class WholeFly:
         """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate, counts
         read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active.
         Under pull delivery also its input tables once per delivery group of `group` steps
-        (presynaptic index per input slot, the count bit planes and base per chunk of 32 slots), the
-        spike words written to and read back from the pull buffer, and the write slot read + written."""
+        (per input slot its packed entry, per chunk of 32 slots its base and, for wide count ranges,
+        its 16 bit planes), the spike words written to and read back from the pull buffer, and the
+        write slot read + written."""
         per = 4 * (5 * 2 + 4 + 1)
         total = self.cfg.n_spiking * (self.B * per + 4)
         if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
             # the input tables once per group of L steps, the write slot read + written every step
             ptr, pre, planes, meta = self.lif._pull_t
             L = self.lif.pull_group if group is None else group
-            total += (pre.numel() * 4 + planes.numel() * 4 + meta.numel() * 4) // L
+            total += (pre.numel() * 4 + (0 if planes is None else planes.numel() * 4) + meta.numel() * 4) // L
             total += self.cfg.n_spiking * self.B * 4 * 2 + self.cfg.n_spiking * self.B // 8 * 2
         return total
 
