@@ -421,14 +421,24 @@ __global__ void __launch_bounds__(256) lif_scatter_kernel(LifK k, int s) {
 // column r (bit c = row c) on return. Five exchanges: at distance j a lane keeps the half of each
 // 2j-bit group on its own side and takes the partner's other half, rotated into place. The
 // rotation and the kept bits depend only on the lane's side of each exchange, so they are
-// computed once per thread.
+// computed once per thread. At distances 16 and 8 the halves are whole bytes, and one byte
+// permute of (own word, partner's word) does the rotation and the merge: the lower side takes
+// bytes {x0, x1, y0, y1} / {x0, y0, x2, y2}, the upper side {y2, y3, x2, x3} / {y1, x1, y3, x3}.
 struct Transpose32 {
   int lane;
   __device__ __forceinline__ explicit Transpose32(int l) : lane(l) {}
   __device__ __forceinline__ unsigned operator()(unsigned x) const {
     constexpr unsigned M[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
+    {
+      const unsigned y = __shfl_xor_sync(0xffffffffu, x, 16);
+      x = __byte_perm(x, y, (lane & 16) ? 0x3276u : 0x5410u);
+    }
+    {
+      const unsigned y = __shfl_xor_sync(0xffffffffu, x, 8);
+      x = __byte_perm(x, y, (lane & 8) ? 0x3715u : 0x6240u);
+    }
 #pragma unroll
-    for (int q = 0; q < 5; ++q) {
+    for (int q = 2; q < 5; ++q) {
       const int j = 16 >> q;
       const bool hi = lane & j;
       const unsigned y = __shfl_xor_sync(0xffffffffu, x, j);
@@ -600,10 +610,14 @@ __device__ __forceinline__ void chunk_sums(const Transpose32& transpose, const P
 #undef FLYB_CHUNK
 }
 
-// One warp's pass over postsynaptic rows [r0, r1) for the steps [lo, hi) of one group. The chunk stream is software-pipelined (the next chunk's words
-// and planes and the inputs of the one after are in flight while a chunk is summed); per chunk
-// every step's words are transposed first and the plane sums of all of them are dispatched once
-// on the chunk's plane count.
+// One warp's pass over postsynaptic rows [r0, r1) for the steps [lo, hi) of one group. The chunk
+// stream is software-pipelined (the next chunk's words and the inputs of the one after are in
+// flight while a chunk is summed); per chunk every step's words are transposed first and the plane
+// sums of all of them are dispatched once on the chunk's plane count. A row's sums start from the
+// values its write slots already hold, loaded when the row starts (their latency hides behind the
+// row's first chunk), and are stored when it ends: the slots end with the same integers an add
+// into them would leave, without a load waiting at the end of each row. Rows without inputs are
+// not touched.
 template <int G, int L, int P>
 __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restrict__ bits, int r0, int r1, int lo,
                                           int hi, int ws0, int lane) {
@@ -612,28 +626,35 @@ __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restr
   const size_t slot = (size_t)k.n * k.batch;
   const int ce = __ldg(&k.pull_ptr[r1]);
   int c = __ldg(&k.pull_ptr[r0]);
+  if (c >= ce) return;                       // no row of the block has inputs
   int row = r0, bound = __ldg(&k.pull_ptr[r0 + 1]);
   int acc[NW];                               // [g * L + u], like the words
+  const auto row_slot = [&](int u) {         // this lane's entry of `row` in the write slot of step u
+    return (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
+  };
+  const auto start_row = [&]() {             // the first row at or after `row` that owns chunk c
+    while (c >= bound) bound = __ldg(&k.pull_ptr[++row + 1]);
 #pragma unroll
-  for (int i = 0; i < NW; ++i) acc[i] = 0;
-  const auto flush_row = [&]() {             // add the finished row into the write slots of steps [lo, hi)
+    for (int u = 0; u < L; ++u) {
+      const bool on = u >= lo && u < hi;
+      const int* src = on ? row_slot(u) : nullptr;
+#pragma unroll
+      for (int g = 0; g < G; ++g) acc[g * L + u] = on ? src[g * 32] : 0;
+    }
+  };
+  const auto end_row = [&]() {               // the row's slots of steps [lo, hi) take the sums
 #pragma unroll
     for (int u = 0; u < L; ++u) {
       if (u < lo || u >= hi) continue;
-      int* dst = (int*)k.ring + (size_t)slot_after(ws0, u, k.R) * slot + (size_t)row * k.batch + lane;
+      int* dst = row_slot(u);
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
-        if (acc[g * L + u]) dst[g * 32] += acc[g * L + u];
-        acc[g * L + u] = 0;
-      }
+      for (int g = 0; g < G; ++g) dst[g * 32] = acc[g * L + u];
     }
   };
   PullChunk<NW, P> cur;
-  int pre_next = -1;
-  if (c < ce) {
-    pull_fetch<NW, P>(k, bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), c, cur);
-    if (c + 1 < ce) pre_next = __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]);
-  }
+  pull_fetch<NW, P>(k, bits, __ldcs(&k.pull_pre[(size_t)c * 32 + lane]), c, cur);
+  int pre_next = c + 1 < ce ? __ldcs(&k.pull_pre[(size_t)(c + 1) * 32 + lane]) : -1;
+  start_row();
   for (; c < ce; ++c) {
     PullChunk<NW, P> nxt;
     int pre_after = -1;
@@ -641,16 +662,15 @@ __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restr
       pull_fetch<NW, P>(k, bits, pre_next, c + 1, nxt);
       if (c + 2 < ce) pre_after = __ldcs(&k.pull_pre[(size_t)(c + 2) * 32 + lane]);
     }
-    while (c >= bound) {                     // chunk c starts a later row: the current one is done
-      flush_row();
-      ++row;
-      bound = __ldg(&k.pull_ptr[row + 1]);
+    if (c >= bound) {                        // chunk c starts a later row: the current one is done
+      end_row();
+      start_row();
     }
     chunk_sums<G, L, P>(transpose, cur, acc);
     cur = nxt;
     pre_next = pre_after;
   }
-  flush_row();                               // the last row with inputs
+  end_row();                                 // the last row with inputs
 }
 
 // Pull delivery of `nsteps` (1..L) undelivered steps, starting at pull_state[0] (its ring position
