@@ -332,13 +332,21 @@ def read_traffic() -> dict:
 
 def measure_plain(cfg, device, steps, warmup, settle=SETTLE_STEPS) -> dict:
     """The plain single-instance kernels (one fly), settled to the same steady firing as the batched
-    engine, timed two ways: replayed from a CUDA graph of 20 steps with the L2 left warm (like the
-    batched figure), and launched eagerly step by step with the L2 flushed between timed steps."""
+    engine and tuned there as it is (LIF launch and delivery, optic shape and long-row threshold),
+    timed two ways: replayed from a CUDA graph of 20 steps with the L2 left warm (like the batched
+    figure), and launched eagerly step by step with the L2 flushed between timed steps."""
+    from flyb200 import autotune
     eng = build_engine(cfg, 1, device, "step")
     eng.step(max(3, warmup))
     g = capture(eng, 20)              # settle to the steady firing the batched figures are timed at
     for _ in range(max(0, settle) // 20):
         g.replay()
+    torch.cuda.synchronize()
+    del g
+    tuned = {"lif": autotune.tune_lif(eng.lif, steps=10), "optic": autotune.tune_optic(eng.optic, steps=10)}
+    eng.step(to_group_end(eng))       # the tuners restored the state: a step re-derives the carried dr
+    g = capture(eng, 20)
+    g.replay()
     torch.cuda.synchronize()
     graph_ms = time_graph(g, 10) / 200
     del g
@@ -352,7 +360,9 @@ def measure_plain(cfg, device, steps, warmup, settle=SETTLE_STEPS) -> dict:
     return {"graph": {"value": N / (graph_ms / 1000.0), "ms_per_step": graph_ms,
                       "how": "CUDA graph of 20 steps replayed back to back, L2 warm"},
             "eager_flushed": {"value": N / (eager_ms / 1000.0), "ms_per_step": eager_ms,
-                              "how": "one call per step, L2 flushed between timed steps"}}
+                              "how": "one call per step, L2 flushed between timed steps"},
+            "tuned": {part: {k: v for k, v in t.items() if k in ("launch", "delivery", "variant", "long_row")}
+                      for part, t in tuned.items()}}
 
 
 def measure_adjoint(device) -> dict:
