@@ -231,14 +231,18 @@ class WholeFly:
 
     # ------------------------------------------------------------------ algorithmic bytes (roofline)
     def lif_bytes_per_step(self, group: int | None = None) -> int:
-        """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate, counts
-        read + written, adapt / drive / poisson_p / ring read, spikes written; per neuron active.
+        """Bytes the LIF step must move per step for B flies: per neuron-fly v, g, refrac, rate read +
+        written, adapt read (and written when adaptation is on), spike counts read + written when
+        activity is recorded, drive / poisson_p (when the Poisson drive is on) / ring read, spikes
+        written; per neuron active.
         Under pull delivery also its input tables once per delivery group of `group` steps
         (per input slot its packed entry, per chunk of 32 slots its base and, for wide count ranges,
         its 16 bit planes), the spike words written to and read back from the pull buffer, and the
         write slot read + written."""
-        per = 4 * (5 * 2 + 4 + 1)
-        total = self.cfg.n_spiking * (self.B * per + 4)
+        b = self.lif
+        words = 4 * 2 + 1 + 1 + 1 + 1                       # v g refrac rate r+w, adapt / drive / ring r, spikes w
+        words += (1 if b._adapt_on else 0) + (2 if b.record_activity else 0) + (1 if b._poisson_on else 0)
+        total = self.cfg.n_spiking * (self.B * 4 * words + 4)
         if self.lif._pull_active() and getattr(self.lif, "_pull_t", None) is not None:
             # the input tables once per group of L steps, the write slot read + written every step
             ptr, pre, planes, meta = self.lif._pull_t

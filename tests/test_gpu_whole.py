@@ -255,6 +255,44 @@ def test_pull_delivery_equals_scatter_at_high_activity(B, staged):
     assert float(pull.spike_counts.sum()) / (48 * B * cfg.c.n) > 0.005     # dense firing
 
 
+@pytest.mark.parametrize("B", [32, 64])
+def test_pull_delivery_with_wide_count_ranges_equals_scatter(B):
+    """Counts whose range inside a chunk needs more than 8 bits (up to +-3,000 synapses per edge)
+    take the 16-plane input table instead of the packed entries: pull delivery against the
+    scatter, bit for bit (state, ring, synaptic event count)."""
+    import scipy.sparse as sp
+    from flyb200.brain import Brain, pull_inputs
+    cfg = synthetic.lif_config2(seed=5, n=3000, edges=200_000, n_poisson=600, poisson_hz=300.0)
+    p = LIFParams(**cfg.params)
+    n, w = cfg.c.n, np.float32(p.w_syn)
+    rng = np.random.default_rng(7)
+    W = sp.random(n, n, density=0.02, random_state=11, format="csr")
+    W.data = (rng.integers(-3000, 3001, W.nnz) * w).astype(np.float32)
+    W.eliminate_zeros()
+    assert pull_inputs(W, w)[4] == 16
+    brains = []
+    for pull in (False, True):
+        b = Brain(cfg.c, p, device="cuda", seed=3, batch=B, launch="step")
+        b.set_weights(W)
+        b.set_poisson(cfg.poisson_idx, 300.0)
+        b.set_drive(np.arange(n), 3.0)
+        b.pull, b.staged = pull, True
+        b._make_args()
+        assert b._pull_active() == pull
+        brains.append(b)
+    push, pull = brains
+    assert pull._pull_planes_n == 16
+    for chunk in (1, 7, 24):
+        push.step(chunk)
+        pull.step(chunk)
+        torch.cuda.synchronize()
+        for k in ("v", "g", "refrac", "rate", "spikes"):
+            assert torch.equal(getattr(push, k), getattr(pull, k)), k
+        assert torch.equal(push.ring, pull.ring)
+        assert push.synaptic_events == pull.synaptic_events
+    assert push.synaptic_events > 0
+
+
 def test_lagged_pull_beside_the_next_step_equals_one_step_per_call():
     """Under pull delivery the whole-fly step delivers each step's spikes on a side stream beside
     the next step (joined before that step's clock advance): ten steps per call, eager or from a
