@@ -27,7 +27,8 @@ LIF_CANDIDATES = (("step", 256, 4, "fused"), ("step", 256, 2, "fused"), ("step",
                   ("step", 256, 4, "defer"), ("step", 256, 2, "staged-defer"), ("step", 512, 2, "staged-defer"),
                   ("step", 256, 4, "staged-defer"), ("persistent", 256, 4, "fused"), ("persistent", 512, 2, "fused"),
                   ("step", 256, 2, "pull"), ("step", 256, 1, "pull"), ("step", 256, 2, "staged-pull"),
-                  ("step", 512, 2, "staged-pull"))
+                  ("step", 512, 2, "staged-pull"), ("step", 128, 2, "staged"), ("step", 128, 2, "staged-defer"),
+                  ("step", 128, 2, "staged-pull"))
 
 
 def graph_key(brain) -> str:

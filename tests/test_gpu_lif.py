@@ -153,7 +153,7 @@ def test_deferred_delivery_equals_oracle(block, ipt, kind):
     _compare(case, STEP, block, ipt=ipt, defer=True)
 
 
-@pytest.mark.parametrize("block,ipt", [(256, 2), (512, 2), (256, 4)])
+@pytest.mark.parametrize("block,ipt", [(256, 2), (512, 2), (256, 4), (128, 2)])
 @pytest.mark.parametrize("kind", ["count", "fixed", "episodes"])
 def test_staged_deferred_delivery_equals_oracle(block, ipt, kind):
     """The staged (bulk-copy) update listing its spikers for the scatter kernel: every state bit,

@@ -226,10 +226,11 @@ def test_set_radiance_equals_oracle_photoreceptor_stage():
 
 
 @pytest.mark.parametrize("B", [32, 64, 128, 256])
-@pytest.mark.parametrize("staged", [False, True])
+@pytest.mark.parametrize("staged", [False, True, "128x2"])
 def test_pull_delivery_equals_scatter_at_high_activity(B, staged):
     """Pull delivery against the scatter, bit for bit (state, ring, rasters, synaptic event count),
-    on a graph driven into dense firing, at every supported batch width."""
+    on a graph driven into dense firing, at every supported batch width, after the register update,
+    the staged update, and the staged update in blocks of 128 threads with 2 items each."""
     from flyb200.brain import Brain
     cfg = synthetic.lif_config2(seed=4, n=4000, edges=600_000, n_poisson=800, poisson_hz=400.0)
     p = LIFParams(**cfg.params)
@@ -239,7 +240,9 @@ def test_pull_delivery_equals_scatter_at_high_activity(B, staged):
         b.set_poisson(cfg.poisson_idx, 400.0)
         b.set_drive(np.arange(cfg.c.n), 5.0)
         b.record_activity = True
-        b.pull, b.staged = pull, staged
+        b.pull, b.staged = pull, bool(staged)
+        if staged == "128x2":
+            b.block, b.items_per_thread = 128, 2
         b._make_args()
         assert b._pull_active() == pull
         brains.append(b)
@@ -281,11 +284,11 @@ def test_pull_delivery_with_wide_count_ranges_equals_scatter(B):
         assert b._pull_active() == pull
         brains.append(b)
     push, pull = brains
-    assert pull._pull_planes_n == 16
     for chunk in (1, 7, 24):
         push.step(chunk)
         pull.step(chunk)
         torch.cuda.synchronize()
+        assert pull._pull_planes_n == 16                # the tables are built at the first step
         for k in ("v", "g", "refrac", "rate", "spikes"):
             assert torch.equal(getattr(push, k), getattr(pull, k)), k
         assert torch.equal(push.ring, pull.ring)
