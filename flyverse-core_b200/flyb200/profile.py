@@ -3,7 +3,7 @@
     python -m flyb200.profile [--batch 64] [--steps 5] [--warmup 2] [--part whole|lif|optic|tracer|pull]
                               [--lif-block 256] [--lif-ipt 0|1|2|4] [--lif-staged] [--lif-defer] [--lif-grid 0]
                               [--lif-pull] [--density 0.024]
-                              [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0]
+                              [--optic-launch step|persistent] [--optic-variant 0] [--optic-grid 0] [--optic-long-row 0]
                               [--no-overlap]
     python -m flyb200.profile --breakdown [--batch 64] [--steps 50]
     (--per-call K: K whole-fly steps per call, `--steps` calls; --settle S: S steps first, from CUDA graphs)
@@ -154,6 +154,8 @@ def main() -> None:
     ap.add_argument("--lif-defer", action="store_true", help="LIF spikes delivered by a second kernel")
     ap.add_argument("--optic-launch", default="step", choices=["step", "persistent"])
     ap.add_argument("--optic-variant", type=int, default=0)
+    ap.add_argument("--optic-long-row", type=int, default=0, help="rows longer than this are split across a "
+                    "block (0: the library default)")
     ap.add_argument("--optic-grid", type=int, default=0, help="persistent optic block cap")
     args = ap.parse_args()
     if args.part == "tracer":
@@ -165,6 +167,8 @@ def main() -> None:
     eng.lif.grid, eng.lif.defer = args.lif_grid, args.lif_defer
     eng.lif.pull = args.lif_pull or args.part == "pull"
     eng.optic.launch, eng.optic.variant, eng.optic.grid = args.optic_launch, args.optic_variant, args.optic_grid
+    if args.optic_long_row:
+        eng.optic.set_long_rows(args.optic_long_row)
     eng.lif._make_args()
     eng.optic.pr_in.normal_(0.0, 0.2)
     eng.step(args.warmup)
