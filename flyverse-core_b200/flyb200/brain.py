@@ -679,6 +679,16 @@ class Brain:
         self._rate_np_key = None
 
     def _clear_hist_rows(self, rows: np.ndarray) -> None:
+        """Clear the spike-history bits of flies `rows`. Item (neuron i, fly b) is bit i * B + b; with
+        B a multiple of 32 a word holds one neuron's flies 32 g .. 32 g + 31, so the bits to keep
+        depend only on the word's fly group g: one word per group, applied on the device."""
+        rows = np.asarray(rows, dtype=np.int64)
+        if self.B % 32 == 0:
+            keep = np.full(self.B // 32, 0xFFFFFFFF, np.uint32)
+            np.bitwise_and.at(keep, rows // 32, ~(np.uint32(1) << (rows % 32).astype(np.uint32)))
+            k = torch.from_numpy(keep.view(np.int32)).to(self.device)
+            self._hist.view(self.n_delay, self.n, self.B // 32).bitwise_and_(k)
+            return
         flat = (np.arange(self.n)[:, None] * self.B + rows[None, :]).ravel()
         mask = np.zeros(self.words * 32, bool)
         mask[flat] = True
