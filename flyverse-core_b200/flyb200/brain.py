@@ -76,6 +76,17 @@ class LIFParams:
 
 
 _STATE = ("v", "g", "refrac", "drive", "poisson_p", "rate", "spikes", "spike_counts", "adapt", "res")
+
+
+def upload(x, device, dtype=None) -> torch.Tensor:
+    """A small host array on `device` without waiting for the device: staged through pinned memory
+    and copied asynchronously on the current stream, so a caller between two launches (a reset
+    between graph replays) does not wait for the work already queued. Plain copy off CUDA."""
+    t = torch.as_tensor(x, dtype=dtype)
+    device = torch.device(device)
+    if device.type != "cuda":
+        return t.to(device)
+    return t.pin_memory().to(device, non_blocking=True)
 LAUNCHES = {"step": _abi.LAUNCH_STEP, "persistent": _abi.LAUNCH_PERSISTENT}
 
 
@@ -658,7 +669,7 @@ class Brain:
 
     def reset(self, rows=None) -> None:
         """Reset brains `rows` (all if None) to rest, their pending input included."""
-        sel = slice(None) if rows is None else torch.as_tensor(np.asarray(rows), device=self.device, dtype=torch.long)
+        sel = slice(None) if rows is None else upload(np.asarray(rows, dtype=np.int64), self.device)
         st = self._st
         st["v"][:, sel] = self.p.v_rest
         for k in ("g", "refrac", "drive", "poisson_p", "rate", "spikes", "adapt", "spike_counts"):
@@ -686,7 +697,7 @@ class Brain:
         if self.B % 32 == 0:
             keep = np.full(self.B // 32, 0xFFFFFFFF, np.uint32)
             np.bitwise_and.at(keep, rows // 32, ~(np.uint32(1) << (rows % 32).astype(np.uint32)))
-            k = torch.from_numpy(keep.view(np.int32)).to(self.device)
+            k = upload(keep.view(np.int32), self.device)
             self._hist.view(self.n_delay, self.n, self.B // 32).bitwise_and_(k)
             return
         flat = (np.arange(self.n)[:, None] * self.B + rows[None, :]).ravel()

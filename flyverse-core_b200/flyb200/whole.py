@@ -26,7 +26,7 @@ import numpy as np
 import torch
 
 from . import _abi
-from .brain import Brain, LIFParams
+from .brain import Brain, LIFParams, upload
 from .optic import DeviceCSR, OpticCore, PhotoreceptorStage, spmm
 from .synthetic import WholeFlyConfig
 
@@ -128,7 +128,7 @@ class WholeFly:
         rows = np.asarray(rows, dtype=np.int64)
         if not rows.size:
             return
-        sel = torch.as_tensor(rows, device=self.device)
+        sel = upload(rows, self.device)
         self.lif.reset(rows)
         o = self.optic
         o.v_s[:, sel] = 0.0
@@ -136,9 +136,12 @@ class WholeFly:
         o.dr_out[:, sel] = o.b.clamp(0.0, 1.0)[:, None] - o.b[:, None]     # clip(0 + b, 0, 1) - b
         o._dr_key = o._state_key()
         if poisson_hz is not None:
-            hz = torch.as_tensor(poisson_hz, dtype=torch.float32).reshape(-1, 1).expand(len(rows), len(self.sensory_idx))
-            cols = torch.as_tensor(self.sensory_idx, device=self.device)
-            self.lif.poisson_p[sel[:, None], cols[None, :]] = hz.to(self.device) * (self.lif.p.dt / 1000.0)
+            hz = np.broadcast_to(np.asarray(poisson_hz, np.float32).reshape(-1, 1), (len(rows), 1))
+            if getattr(self, "_sensory_dev", None) is None:
+                self._sensory_dev = torch.as_tensor(self.sensory_idx, device=self.device)
+            cols = self._sensory_dev
+            p = upload(np.ascontiguousarray(hz * np.float32(self.lif.p.dt / 1000.0)), self.device)
+            self.lif.poisson_p[sel[:, None], cols[None, :]] = p.expand(len(rows), len(self.sensory_idx))
             self.lif._poisson_on = True
 
     def set_photoreceptors(self, a_pr: torch.Tensor) -> None:
