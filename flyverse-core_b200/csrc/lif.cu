@@ -501,36 +501,6 @@ __device__ __forceinline__ void pull_planes(const unsigned* __restrict__ planes,
   }
 }
 
-// sum[g] += 2^Q popc(m[g] & pl[Q]) for every fly group.
-template <int G, int P, int Q>
-__device__ __forceinline__ void add_plane(const unsigned (&m)[G], const unsigned (&pl)[P], int (&sum)[G]) {
-#pragma unroll
-  for (int g = 0; g < G; ++g) sum[g] += __popc(m[g] & pl[Q]) << Q;
-}
-
-// sum[g] += sum_{p < planes} 2^p popc(m[g] & pl[p]) for every group, dispatched once on the
-// warp-uniform plane count (a uniform branch, no predicated-off work).
-template <int G, int P>
-__device__ __forceinline__ void plane_sums(const unsigned (&m)[G], const unsigned (&pl)[P], int planes, int (&sum)[G]) {
-#define FLYB_PLANE(q) case q + 1: add_plane<G, P, q>(m, pl, sum); [[fallthrough]];
-  if constexpr (P > 8) {
-    if (planes > 8) {
-      switch (planes) {
-        FLYB_PLANE(15) FLYB_PLANE(14) FLYB_PLANE(13) FLYB_PLANE(12)
-        FLYB_PLANE(11) FLYB_PLANE(10) FLYB_PLANE(9) FLYB_PLANE(8)
-        default: break;
-      }
-      planes = 8;
-    }
-  }
-  switch (planes) {
-    FLYB_PLANE(7) FLYB_PLANE(6) FLYB_PLANE(5) FLYB_PLANE(4) FLYB_PLANE(3) FLYB_PLANE(2) FLYB_PLANE(1)
-    FLYB_PLANE(0)
-    default: break;
-  }
-#undef FLYB_PLANE
-}
-
 // a mod m in [0, m) for any sign of a (m > 0).
 __device__ __forceinline__ int pos_mod(long long a, int m) {
   const long long r = a % m;
