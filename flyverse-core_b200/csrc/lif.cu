@@ -647,14 +647,14 @@ __device__ __forceinline__ void pull_pass(const LifK& k, const unsigned* __restr
 // pull_state[1]). Each warp owns a contiguous block of postsynaptic rows and walks their 32-input
 // chunks as one stream, once per group of L steps the range touches (one group when the pulls
 // follow the group ends, two when a range straddles a group end). Per chunk a lane gathers its
-// input's G * L spike words of the group (one 32-byte sector); for each step of the range the warp
-// transposes the step's G words so that lane f holds, for fly f of a group of 32, the mask of the
-// chunk's inputs that spiked, and adds base x popc(mask) + sum_p 2^p popc(mask & plane_p) (a row's
-// inputs are sorted by count; a chunk stores its smallest count as the base and the excess of each
-// entry in as few bit planes as its range needs). Integer and exact: each step's write slot ends
-// with the sums the scatter's atomics give. The chunk tables (inputs, planes, base) are read once
-// per group instead of once per step. A finished row is added into each step's write slot with
-// coalesced 128-byte accesses per group of 32 flies. The synaptic events of presynaptic neurons in
+// input's G * L spike words of the group (one 32-byte sector); the warp transposes every word so
+// that lane f holds, for fly f of a group of 32, the mask of the chunk's inputs that spiked, and
+// adds base x popc(mask) + sum_p 2^p popc(mask & plane_p) (a row's inputs are sorted by count; a
+// chunk stores its smallest count as the base and each entry's excess, packed into the entry's top
+// byte or, for wide ranges, as up to 16 bit planes). Integer and exact: each step's write slot ends
+// with the sums the scatter's atomics give. The chunk tables are read once per group instead of
+// once per step. A row's sums start from its write slots' values and are stored back when the row
+// ends, with coalesced 128-byte accesses per group of 32 flies. The synaptic events of presynaptic neurons in
 // the warp's row block are counted from the same words. The last block to finish moves pull_state
 // on by nsteps (every block has read it by then).
 constexpr int kPullBlock = 256, kPullBlocksPerSm = 3;   // launch shape of the pull kernel
