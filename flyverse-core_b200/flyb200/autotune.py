@@ -103,7 +103,7 @@ def _apply(brain, choice: dict) -> None:
 # Row lengths above which a row is shared by a whole block (OpticCore.set_long_rows): the split
 # pays at many flies per row gather; at one fly a row of a few hundred entries is better left to
 # its warp slot.
-OPTIC_LONG_ROWS = (192, 512, 2048)
+OPTIC_LONG_ROWS = (192, 384, 512, 768, 1024, 2048)
 
 
 def tune_optic(core, steps: int = 10) -> dict:
