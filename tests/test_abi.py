@@ -78,8 +78,9 @@ def test_pull_delivery_arguments_are_validated_before_any_launch():
     """flyb_lif_pull / FLYB_LIF_PULL_DELIVERY reject what the pull cannot do (a batch that is not
     32, 64, 128 or 256 flies, the fixed-point ring, depression, persistent launches, missing tables
     or buffers, an unknown table format, a plane table that is missing or misaligned, packed entries
-    for more neurons than their 24-bit field holds, a misaligned pull buffer, a group size the batch or the delay does not allow, a
-    step count outside 1..group, a bad phase) with FLYB_EINVAL before touching the device. The
+    for more neurons than their 24-bit field holds, a misaligned pull buffer, a group size the batch
+    or the delay does not allow, a step count outside 1..group, a bad phase, a negative block cap)
+    with FLYB_EINVAL before touching the device. The
     cases run in a child process that sees no GPU, so that a check that ever weakens fails there
     instead of launching a kernel on the fake addresses."""
     import os
