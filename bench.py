@@ -17,8 +17,9 @@ Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthet
   roofline       the dominant kernel (LIF step or optic substep): algorithmic bytes / CUDA-event time
                  against the measured HBM copy rate, with ncu's DRAM bytes per launch
   cpu_baseline   the C oracle port (oracle/) on this host's cores from this run's settled state
-  batch1         the plain single-instance kernels (B=1) at the same steady firing, graph-replayed
-                 (the "vs plain" ratio uses it) and eager with L2 flushed between steps
+  batch1         the plain single-instance kernels (B=1) at the same steady firing, tuned there
+                 like the batched engine, graph-replayed (the "vs plain" ratio uses it) and eager
+                 with L2 flushed between steps
   adjoint        optic-lobe adjoint over 200 substeps (89,390 units, 6 M nnz, checkpoint 20) over
                  the forward pass time
   fp64_max_err   max |FP32 - FP64| of the optic state after 200 substeps (config 3, whole-fly lobe)
@@ -30,8 +31,9 @@ Workload (synthetic, seeded; the MaleCNS data is not available): flyb200.synthet
   reference_own_cpu  the reference's own CPU code (Brain.step, OpticLobe._substep) on host cores
   tracer         the eye's ray tracer at 64 flies x 1,634 columns x 7 rays, beside the reference's
                  torch tracer on this GPU and the C oracle on host cores
-`--impl reference` times the CPU port alone, from a state settled the same number of steps, and
-prints the same line.
+`--impl reference` times the CPU port alone on this host's cores (the reference's own CPU
+implementation of the path, restated in oracle/), from one fly settled the same number of steps
+and widened to the same 64 flies, and prints the same line with impl "reference".
 """
 from __future__ import annotations
 
